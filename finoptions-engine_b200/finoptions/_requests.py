@@ -1,0 +1,330 @@
+"""Marshalling between Python values and the C ABI's request/result structs."""
+
+from __future__ import annotations
+
+import ctypes
+from collections.abc import Sequence
+from dataclasses import dataclass
+from typing import Any
+
+import numpy as np
+
+from . import _abi
+
+
+def _f64(values: Sequence[float] | np.ndarray) -> np.ndarray:
+    return np.ascontiguousarray(np.asarray(values, dtype=np.float64))
+
+
+def _u32(values: Sequence[int] | np.ndarray) -> np.ndarray:
+    return np.ascontiguousarray(np.asarray(values, dtype=np.uint32))
+
+
+def _ptr(array: np.ndarray | None, ctype: type) -> Any:
+    if array is None:
+        return ctypes.POINTER(ctype)()
+    return array.ctypes.data_as(ctypes.POINTER(ctype))
+
+
+@dataclass
+class CallRequest:
+    """A filled FoLsmCallRequest and the arrays its pointers borrow."""
+
+    struct: _abi.FoLsmCallRequest
+    keepalive: tuple[np.ndarray, ...]
+    exercise_rows: int
+
+
+def lsm_call_request(
+    *,
+    initial_spot: float,
+    strike: float,
+    schedule_times: Sequence[float],
+    curve_times: Sequence[float],
+    log_discounts: Sequence[float],
+    dividend_yield_times: Sequence[float],
+    cumulative_dividend_yields: Sequence[float],
+    dividend_nodes: Sequence[int],
+    dividend_amounts: Sequence[float],
+    exercise_nodes: Sequence[int],
+    expiry_node: int,
+    annualized_volatility: float,
+    dividend_policy: int,
+    training_paths: int,
+    evaluation_paths: int,
+    training_seed: int,
+    training_domain: int,
+    evaluation_seed: int,
+    evaluation_domain: int,
+    polynomial_degree: int,
+    rank_tolerance: float,
+    condition_limit: float,
+    tie_rule: int,
+    insufficient_exercise_support: int,
+) -> CallRequest:
+    arrays = (
+        _f64(schedule_times),
+        _f64(curve_times),
+        _f64(log_discounts),
+        _f64(dividend_yield_times),
+        _f64(cumulative_dividend_yields),
+        _u32(dividend_nodes),
+        _f64(dividend_amounts),
+        _u32(exercise_nodes),
+    )
+    st, ct, ld, yt, cy, dn, da, en = arrays
+    q = _abi.FoLsmCallRequest()
+    q.initial_spot = initial_spot
+    q.strike = strike
+    q.schedule_times, q.n_schedule_times = _ptr(st, ctypes.c_double), st.size
+    q.curve_times, q.n_curve_times = _ptr(ct, ctypes.c_double), ct.size
+    q.log_discounts, q.n_log_discounts = _ptr(ld, ctypes.c_double), ld.size
+    q.dividend_yield_times, q.n_dividend_yield_times = _ptr(yt, ctypes.c_double), yt.size
+    q.cumulative_dividend_yields, q.n_cumulative_dividend_yields = _ptr(cy, ctypes.c_double), cy.size
+    q.dividend_nodes, q.n_dividend_nodes = _ptr(dn, ctypes.c_uint32), dn.size
+    q.dividend_amounts, q.n_dividend_amounts = _ptr(da, ctypes.c_double), da.size
+    q.exercise_nodes, q.n_exercise_nodes = _ptr(en, ctypes.c_uint32), en.size
+    q.expiry_node = expiry_node
+    q.annualized_volatility = annualized_volatility
+    q.dividend_policy = dividend_policy
+    q.training_paths = training_paths
+    q.evaluation_paths = evaluation_paths
+    q.training_seed = training_seed
+    q.training_domain = training_domain
+    q.evaluation_seed = evaluation_seed
+    q.evaluation_domain = evaluation_domain
+    q.polynomial_degree = polynomial_degree
+    q.rank_tolerance = rank_tolerance
+    q.condition_limit = condition_limit
+    q.tie_rule = tie_rule
+    q.insufficient_exercise_support = insufficient_exercise_support
+    return CallRequest(q, arrays, int(en.size))
+
+
+@dataclass
+class CallResult:
+    """Caller-owned result buffers for one single-contract call."""
+
+    struct: _abi.FoLsmCallResult
+    observation_nodes: np.ndarray
+    exercise_counts: np.ndarray
+    diagnostics: ctypes.Array
+
+    def as_tuple(self) -> tuple:
+        """NativeLsmResult-shaped tuple (crates/finoptions-python/src/lib.rs:1074-1082)."""
+        r = self.struct
+        rows = int(r.n_observations)
+        diags = []
+        for i in range(int(r.n_diagnostics)):
+            d = self.diagnostics[i]
+            if d.kind == _abi.FO_DIAG_ORIGIN_DECISION:
+                diags.append((d.node, "origin_decision", bool(d.exercise), d.estimated_continuation,
+                              None, None, None, None, None, None, None))
+            elif d.kind == _abi.FO_DIAG_NO_IN_THE_MONEY_PATHS:
+                diags.append((d.node, "no_in_the_money_paths", None, None, None, None, None, None,
+                              None, None, None))
+            elif d.kind == _abi.FO_DIAG_INSUFFICIENT_SUPPORT:
+                diags.append((d.node, "insufficient_exercise_support", None, None,
+                              d.in_the_money_paths, None, int(d.columns), None, None, None, None))
+            else:
+                diags.append((d.node, "regression", None, None, d.in_the_money_paths,
+                              int(d.observations), int(d.columns), int(d.rank), d.condition_number,
+                              d.predictor_mean, d.predictor_scale))
+        return (
+            r.price,
+            int(r.paths),
+            r.sample_standard_deviation if r.has_sample_standard_deviation else None,
+            r.standard_error if r.has_standard_error else None,
+            [int(v) for v in self.observation_nodes[:rows]],
+            [int(v) for v in self.exercise_counts[:rows]],
+            diags,
+        )
+
+
+def lsm_call_result(exercise_rows: int) -> CallResult:
+    rows = exercise_rows + 1
+    nodes = np.zeros(rows, dtype=np.uint32)
+    counts = np.zeros(rows, dtype=np.uint32)
+    diags = (_abi.FoLsmNodeDiagnostic * max(exercise_rows, 1))()
+    r = _abi.FoLsmCallResult()
+    r.observation_nodes = _ptr(nodes, ctypes.c_uint32)
+    r.observation_capacity = rows
+    r.exercise_counts = _ptr(counts, ctypes.c_uint32)
+    r.diagnostics = ctypes.cast(diags, ctypes.POINTER(_abi.FoLsmNodeDiagnostic))
+    r.diagnostics_capacity = exercise_rows
+    return CallResult(r, nodes, counts, diags)
+
+
+@dataclass
+class GroupedRequest:
+    struct: _abi.FoLsmGroupedRequest
+    keepalive: tuple[Any, ...]
+    rows: int
+
+
+def lsm_grouped_request(
+    *,
+    group_offsets: np.ndarray | None,
+    initial_spots: np.ndarray,
+    strikes: np.ndarray,
+    maturities: np.ndarray,
+    rates: np.ndarray,
+    volatilities: np.ndarray,
+    dividend_model: int,
+    dividend_yields: np.ndarray | None = None,
+    dividend_offsets: np.ndarray | None = None,
+    dividend_times: np.ndarray | None = None,
+    dividend_amounts: np.ndarray | None = None,
+    dividend_policy: int = 0,
+    maturity_boundary: int = 0,
+    volatility_convention: int = 0,
+    exercise_mesh: int,
+    base_intervals: int | None,
+    origin_exercise: int | None,
+    explicit_exercise_offsets: np.ndarray | None,
+    explicit_exercise_times: np.ndarray | None,
+    training_paths: int,
+    evaluation_paths: int,
+    training_seed: int,
+    training_domain_start: int,
+    evaluation_seed: int,
+    evaluation_domain_start: int,
+    polynomial_degree: int,
+    rank_tolerance: float,
+    condition_limit: float,
+    tie_rule: int,
+    insufficient_exercise_support: int,
+) -> GroupedRequest:
+    q = _abi.FoLsmGroupedRequest()
+    keep: list[Any] = []
+
+    def put(name: str, array: np.ndarray | None, ctype: type) -> None:
+        keep.append(array)
+        setattr(q, name, _ptr(array, ctype))
+        setattr(q, "n_" + name, 0 if array is None else int(array.size))
+
+    put("group_offsets", group_offsets, ctypes.c_uint32)
+    put("initial_spots", initial_spots, ctypes.c_double)
+    put("strikes", strikes, ctypes.c_double)
+    put("maturities", maturities, ctypes.c_double)
+    put("rates", rates, ctypes.c_double)
+    put("volatilities", volatilities, ctypes.c_double)
+    q.dividend_model = dividend_model
+    put("dividend_yields", dividend_yields, ctypes.c_double)
+    put("dividend_offsets", dividend_offsets, ctypes.c_int64)
+    put("dividend_times", dividend_times, ctypes.c_double)
+    put("dividend_amounts", dividend_amounts, ctypes.c_double)
+    q.dividend_policy = dividend_policy
+    q.maturity_boundary = maturity_boundary
+    q.volatility_convention = volatility_convention
+    q.exercise_mesh = exercise_mesh
+    q.has_base_intervals = 0 if base_intervals is None else 1
+    q.base_intervals = 0 if base_intervals is None else base_intervals
+    q.has_origin_exercise = 0 if origin_exercise is None else 1
+    q.origin_exercise = 0 if origin_exercise is None else origin_exercise
+    put("explicit_exercise_offsets", explicit_exercise_offsets, ctypes.c_int64)
+    put("explicit_exercise_times", explicit_exercise_times, ctypes.c_double)
+    q.training_paths = training_paths
+    q.evaluation_paths = evaluation_paths
+    q.training_seed = training_seed
+    q.training_domain_start = training_domain_start
+    q.evaluation_seed = evaluation_seed
+    q.evaluation_domain_start = evaluation_domain_start
+    q.polynomial_degree = polynomial_degree
+    q.rank_tolerance = rank_tolerance
+    q.condition_limit = condition_limit
+    q.tie_rule = tie_rule
+    q.insufficient_exercise_support = insufficient_exercise_support
+    return GroupedRequest(q, tuple(keep), int(strikes.size))
+
+
+@dataclass
+class BatchColumns:
+    struct: _abi.FoBatchResultColumns
+    arrays: dict[str, np.ndarray]
+
+    def as_tuple(self) -> tuple[np.ndarray, ...]:
+        a = self.arrays
+        return (
+            a["prices"], a["sample_standard_deviations"], a["standard_errors"],
+            a["origin_decisions_fitted"].astype(np.bool_), a["origin_exercised"].astype(np.bool_),
+            a["regression_nodes"], a["no_training_support_nodes"],
+            a["insufficient_exercise_support_nodes"], a["minimum_in_the_money_training_paths"],
+            a["maximum_regression_condition_numbers"], a["early_exercise_paths"], a["expiry_paths"],
+        )
+
+
+_COLUMN_TYPES = (
+    ("prices", np.float64, ctypes.c_double),
+    ("sample_standard_deviations", np.float64, ctypes.c_double),
+    ("standard_errors", np.float64, ctypes.c_double),
+    ("origin_decisions_fitted", np.uint8, ctypes.c_uint8),
+    ("origin_exercised", np.uint8, ctypes.c_uint8),
+    ("regression_nodes", np.uint32, ctypes.c_uint32),
+    ("no_training_support_nodes", np.uint32, ctypes.c_uint32),
+    ("insufficient_exercise_support_nodes", np.uint32, ctypes.c_uint32),
+    ("minimum_in_the_money_training_paths", np.uint32, ctypes.c_uint32),
+    ("maximum_regression_condition_numbers", np.float64, ctypes.c_double),
+    ("early_exercise_paths", np.uint32, ctypes.c_uint32),
+    ("expiry_paths", np.uint32, ctypes.c_uint32),
+)
+
+
+def batch_columns(rows: int) -> BatchColumns:
+    s = _abi.FoBatchResultColumns()
+    s.rows = rows
+    arrays: dict[str, np.ndarray] = {}
+    for name, dtype, ctype in _COLUMN_TYPES:
+        array = np.zeros(rows, dtype=dtype)
+        arrays[name] = array
+        setattr(s, name, _ptr(array, ctype))
+    return BatchColumns(s, arrays)
+
+
+@dataclass
+class GbmRequest:
+    struct: _abi.FoGbmSeededRequest
+    keepalive: tuple[np.ndarray, ...]
+    rows: int
+
+
+def gbm_seeded_request(
+    *,
+    initial_spot: float,
+    schedule_times: Sequence[float],
+    curve_times: Sequence[float],
+    log_discounts: Sequence[float],
+    dividend_yield_times: Sequence[float],
+    cumulative_dividend_yields: Sequence[float],
+    dividend_nodes: Sequence[int],
+    dividend_amounts: Sequence[float],
+    exercise_nodes: Sequence[int],
+    expiry_node: int,
+    annualized_volatility: float,
+    dividend_policy: int,
+    paths: int,
+    seed: int,
+    domain: int,
+) -> GbmRequest:
+    arrays = (
+        _f64(schedule_times), _f64(curve_times), _f64(log_discounts), _f64(dividend_yield_times),
+        _f64(cumulative_dividend_yields), _u32(dividend_nodes), _f64(dividend_amounts), _u32(exercise_nodes),
+    )
+    st, ct, ld, yt, cy, dn, da, en = arrays
+    q = _abi.FoGbmSeededRequest()
+    q.initial_spot = initial_spot
+    q.schedule_times, q.n_schedule_times = _ptr(st, ctypes.c_double), st.size
+    q.curve_times, q.n_curve_times = _ptr(ct, ctypes.c_double), ct.size
+    q.log_discounts, q.n_log_discounts = _ptr(ld, ctypes.c_double), ld.size
+    q.dividend_yield_times, q.n_dividend_yield_times = _ptr(yt, ctypes.c_double), yt.size
+    q.cumulative_dividend_yields, q.n_cumulative_dividend_yields = _ptr(cy, ctypes.c_double), cy.size
+    q.dividend_nodes, q.n_dividend_nodes = _ptr(dn, ctypes.c_uint32), dn.size
+    q.dividend_amounts, q.n_dividend_amounts = _ptr(da, ctypes.c_double), da.size
+    q.exercise_nodes, q.n_exercise_nodes = _ptr(en, ctypes.c_uint32), en.size
+    q.expiry_node = expiry_node
+    q.annualized_volatility = annualized_volatility
+    q.dividend_policy = dividend_policy
+    q.paths = paths
+    q.seed = seed
+    q.domain = domain
+    return GbmRequest(q, arrays, int(en.size) + 1)

@@ -1,0 +1,305 @@
+/*
+ * finoptions_cuda.h - C ABI of the B200 Longstaff-Schwartz engine.
+ *
+ * Plain C types only: pointers, sizes, enums and caller-owned buffers. Every entry point returns
+ * an fo_status and, on failure, fills the caller's fo_error with the failure category, the
+ * row/group/node/path it concerns and a message worded like the reference's typed errors.
+ * No partial result is ever written on failure.
+ *
+ * Reference interfaces each entry replaces (paths inside jorgensandhaug/finoptions-engine):
+ *   fo_cuda_executor_create      - CpuExecutor construction, crates/finoptions-python/src/lib.rs:167-186
+ *                                   and crates/finoptions-runtime/src/lib.rs:341-443 (the new
+ *                                   CudaExecutor sits beside CpuExecutor; explicit, fail-fast,
+ *                                   no CPU fallback)
+ *   fo_price_lsm_call_f64        - price_lsm_call_seeded_f64, crates/finoptions-python/src/lib.rs:1169-1241
+ *   fo_price_lsm_grouped_f64     - price_lsm_call_grouped_batch_{continuous_yield,cash_dividends,
+ *                                   escrowed_cash_dividends}_f64, crates/finoptions-python/src/lib.rs:1884-2100
+ *   fo_price_lsm_batch_f64       - price_lsm_call_batch_*_f64 (row-addressed batch; one contract per
+ *                                   group), crates/finoptions-lsm/src/batch/pricing.rs:191-300
+ *   fo_simulate_gbm_seeded_f64   - simulate_gbm_seeded_f64, crates/finoptions-python/src/lib.rs:1019-1058
+ *   fo_sample_standard_normals_f64 - PhiloxPathStream + sample_standard_normal,
+ *                                   crates/finoptions-sim/src/random/{philox,normal}.rs
+ *   fo_build_info                - build_info, crates/finoptions-python/src/lib.rs:400-404
+ */
+#ifndef FINOPTIONS_CUDA_H
+#define FINOPTIONS_CUDA_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define FO_ABI_VERSION 1
+
+/* ---- status / error ------------------------------------------------------------------------ */
+
+typedef enum fo_status {
+    FO_OK = 0,
+    FO_ERR_INPUT = 1,      /* InputError(ValueError): request/validation failures            */
+    FO_ERR_LSM = 2,        /* LsmError(RuntimeError): simulation/regression/support/evaluation */
+    FO_ERR_SIMULATION = 3, /* SimulationError(RuntimeError)                                  */
+    FO_ERR_EXECUTION = 4,  /* ExecutionError(RuntimeError): device/executor failures         */
+    FO_ERR_BATCH = 5       /* BatchError(ValueError): ragged-view structure failures         */
+} fo_status;
+
+#define FO_ERROR_MESSAGE_CAPACITY 1024
+
+typedef struct fo_error {
+    int32_t kind;  /* fo_status of the failure                                    */
+    int32_t code;  /* fo_error_code: the typed reference error it corresponds to   */
+    int64_t row;   /* contract row, -1 when not applicable                         */
+    int64_t group; /* strike group, -1 when not applicable                         */
+    int64_t node;  /* grid node, -1 when not applicable                            */
+    int64_t path;  /* path index, -1 when not applicable                           */
+    char message[FO_ERROR_MESSAGE_CAPACITY];
+} fo_error;
+
+/* ---- enums mirroring the reference's string enums (lib.rs:514-556) ------------------------ */
+
+typedef enum fo_dividend_policy {
+    FO_DIVIDEND_LIQUIDATOR = 0, /* "liquidator": max(S - D, 0)      (dividend.rs:69-70) */
+    FO_DIVIDEND_SURVIVOR = 1    /* "survivor": S > D ? S - D : S    (dividend.rs:71-77) */
+} fo_dividend_policy;
+
+typedef enum fo_tie_rule {
+    FO_TIE_STRICTLY_GREATER = 0, /* exercise iff intrinsic >  continuation (policy.rs:21-26) */
+    FO_TIE_GREATER_OR_EQUAL = 1  /* exercise iff intrinsic >= continuation                   */
+} fo_tie_rule;
+
+typedef enum fo_insufficient_support {
+    FO_SUPPORT_FAIL = 0,    /* "fail"     (policy.rs:31-37) */
+    FO_SUPPORT_CONTINUE = 1 /* "continue"                   */
+} fo_insufficient_support;
+
+typedef enum fo_dividend_model {
+    FO_MODEL_CONTINUOUS_YIELD = 0,
+    FO_MODEL_CASH_DIVIDENDS = 1,
+    FO_MODEL_ESCROWED_CASH_DIVIDENDS = 2
+} fo_dividend_model;
+
+typedef enum fo_maturity_boundary {
+    FO_MATURITY_STRICTLY_BEFORE = 0,
+    FO_MATURITY_AT_OR_BEFORE = 1
+} fo_maturity_boundary;
+
+typedef enum fo_escrowed_volatility {
+    FO_ESCROWED_PREPAID_FORWARD = 0,
+    FO_ESCROWED_SPOT_MATCHED_AT_ORIGIN = 1
+} fo_escrowed_volatility;
+
+typedef enum fo_exercise_mesh {
+    FO_MESH_UNIFORM = 0,
+    FO_MESH_CASH_DIVIDEND_DATES = 1,
+    FO_MESH_EXPLICIT_TIMES = 2
+} fo_exercise_mesh;
+
+typedef enum fo_origin_exercise {
+    FO_ORIGIN_EXCLUDED = 0,
+    FO_ORIGIN_INCLUDED = 1
+} fo_origin_exercise;
+
+typedef enum fo_diag_kind {
+    FO_DIAG_ORIGIN_DECISION = 0,        /* ExerciseFitDiagnostics::OriginDecision        */
+    FO_DIAG_NO_IN_THE_MONEY_PATHS = 1,  /* ExerciseFitDiagnostics::NoInTheMoneyPaths     */
+    FO_DIAG_INSUFFICIENT_SUPPORT = 2,   /* ExerciseFitDiagnostics::InsufficientExerciseSupport */
+    FO_DIAG_REGRESSION = 3              /* ExerciseFitDiagnostics::Regression            */
+} fo_diag_kind;
+
+/* ---- executor ----------------------------------------------------------------------------- */
+
+typedef struct fo_executor fo_executor;
+
+/* Opens an sm_100 device. Fails with FO_ERR_EXECUTION when the device is absent or is not a
+ * compute-capability-10.x part; there is no CPU fallback. The executor owns one CUDA stream and a
+ * growable device arena; calls on one executor are serialised. */
+int fo_cuda_executor_create(int32_t device, fo_executor** out, fo_error* err);
+void fo_executor_destroy(fo_executor* executor);
+int fo_executor_device(const fo_executor* executor, int32_t* device);
+
+/* ---- single contract: price_lsm_call ------------------------------------------------------ */
+
+/* Field-for-field image of price_lsm_call_seeded_f64's arguments (lib.rs:1170-1197). */
+typedef struct fo_lsm_call_request {
+    double initial_spot;
+    double strike;
+    const double* schedule_times;             uint64_t n_schedule_times;
+    const double* curve_times;                uint64_t n_curve_times;
+    const double* log_discounts;              uint64_t n_log_discounts;
+    const double* dividend_yield_times;       uint64_t n_dividend_yield_times;
+    const double* cumulative_dividend_yields; uint64_t n_cumulative_dividend_yields;
+    const uint32_t* dividend_nodes;           uint64_t n_dividend_nodes;
+    const double* dividend_amounts;           uint64_t n_dividend_amounts;
+    const uint32_t* exercise_nodes;           uint64_t n_exercise_nodes;
+    uint32_t expiry_node;
+    double annualized_volatility;
+    int32_t dividend_policy;                  /* fo_dividend_policy */
+    uint64_t training_paths;
+    uint64_t evaluation_paths;
+    uint64_t training_seed;
+    uint32_t training_domain;
+    uint64_t evaluation_seed;
+    uint32_t evaluation_domain;
+    uint32_t polynomial_degree;
+    double rank_tolerance;
+    double condition_limit;
+    int32_t tie_rule;                         /* fo_tie_rule */
+    int32_t insufficient_exercise_support;    /* fo_insufficient_support */
+} fo_lsm_call_request;
+
+/* One ExerciseNodeDiagnostics (policy.rs:39-87), flattened like NativeExerciseDiagnostic
+ * (lib.rs:1060-1072). For FO_DIAG_INSUFFICIENT_SUPPORT, `columns` carries required_paths. */
+typedef struct fo_lsm_node_diagnostic {
+    uint32_t node;
+    int32_t kind;                  /* fo_diag_kind */
+    int32_t exercise;              /* origin decision only */
+    double estimated_continuation; /* origin decision only */
+    uint32_t in_the_money_paths;
+    uint64_t observations;
+    uint64_t columns;
+    uint64_t rank;
+    double condition_number;
+    double predictor_mean;
+    double predictor_scale;
+} fo_lsm_node_diagnostic;
+
+/* NativeLsmResult (lib.rs:1074-1082). The caller owns every array: observation_nodes and
+ * exercise_counts need n_exercise_nodes + 1 entries, diagnostics n_exercise_nodes entries. */
+typedef struct fo_lsm_call_result {
+    double price;
+    uint32_t paths;
+    int32_t has_sample_standard_deviation;
+    double sample_standard_deviation;
+    int32_t has_standard_error;
+    double standard_error;
+    uint32_t* observation_nodes;         uint64_t observation_capacity;
+    uint32_t* exercise_counts;           /* same capacity as observation_nodes */
+    uint64_t n_observations;             /* written */
+    fo_lsm_node_diagnostic* diagnostics; uint64_t diagnostics_capacity;
+    uint64_t n_diagnostics;              /* written */
+} fo_lsm_call_result;
+
+int fo_price_lsm_call_f64(fo_executor* executor, const fo_lsm_call_request* request,
+                          fo_lsm_call_result* result, fo_error* err);
+
+/* Split form of fo_price_lsm_call_f64 for callers that keep a contract resident on the device:
+ * create validates the request and uploads the plan once; launch enqueues the whole pricing pass
+ * (simulation, backward fit, evaluation) on the executor's stream without synchronising and
+ * without host transfers; collect waits, downloads and assembles the result or the typed error. */
+typedef struct fo_lsm_call_plan fo_lsm_call_plan;
+int fo_lsm_call_plan_create(fo_executor* executor, const fo_lsm_call_request* request,
+                            fo_lsm_call_plan** out, fo_error* err);
+int fo_lsm_call_plan_launch(fo_lsm_call_plan* plan, fo_error* err);
+int fo_lsm_call_plan_collect(fo_lsm_call_plan* plan, fo_lsm_call_result* result, fo_error* err);
+/* Number of kernels one launch enqueues (for launch accounting). */
+int fo_lsm_call_plan_kernel_count(const fo_lsm_call_plan* plan, uint64_t* kernels);
+/* The cudaStream_t (as void*) the plan's kernels run on. */
+int fo_lsm_call_plan_stream(const fo_lsm_call_plan* plan, void** stream);
+void fo_lsm_call_plan_destroy(fo_lsm_call_plan* plan);
+
+/* ---- grouped / row batches ------------------------------------------------------------------ */
+
+/* Arguments of price_lsm_call_grouped_batch_*_f64 (lib.rs:1884-2100) with the dividend model and
+ * the mesh as tags. Optional buffers are NULL when absent. */
+typedef struct fo_lsm_grouped_request {
+    const uint32_t* group_offsets;    uint64_t n_group_offsets;
+    const double* initial_spots;      uint64_t n_initial_spots;  /* one per group */
+    const double* strikes;            uint64_t n_strikes;        /* one per contract row */
+    const double* maturities;         uint64_t n_maturities;
+    const double* rates;              uint64_t n_rates;
+    const double* volatilities;       uint64_t n_volatilities;
+    int32_t dividend_model;           /* fo_dividend_model */
+    const double* dividend_yields;    uint64_t n_dividend_yields;   /* continuous yield */
+    const int64_t* dividend_offsets;  uint64_t n_dividend_offsets;  /* cash / escrowed */
+    const double* dividend_times;     uint64_t n_dividend_times;
+    const double* dividend_amounts;   uint64_t n_dividend_amounts;
+    int32_t dividend_policy;          /* cash dividends */
+    int32_t maturity_boundary;        /* cash / escrowed */
+    int32_t volatility_convention;    /* escrowed */
+    int32_t exercise_mesh;            /* fo_exercise_mesh */
+    int32_t has_base_intervals;       uint32_t base_intervals;
+    int32_t has_origin_exercise;      int32_t origin_exercise;
+    const int64_t* explicit_exercise_offsets; uint64_t n_explicit_exercise_offsets;
+    const double* explicit_exercise_times;    uint64_t n_explicit_exercise_times;
+    uint64_t training_paths;
+    uint64_t evaluation_paths;
+    uint64_t training_seed;
+    uint32_t training_domain_start;
+    uint64_t evaluation_seed;
+    uint32_t evaluation_domain_start;
+    uint32_t polynomial_degree;
+    double rank_tolerance;
+    double condition_limit;
+    int32_t tie_rule;
+    int32_t insufficient_exercise_support;
+} fo_lsm_grouped_request;
+
+/* NativeBatchLsmResult (lib.rs:1417-1430): twelve caller-owned row-aligned columns. */
+typedef struct fo_batch_result_columns {
+    uint64_t rows;
+    double* prices;
+    double* sample_standard_deviations;
+    double* standard_errors;
+    uint8_t* origin_decisions_fitted;
+    uint8_t* origin_exercised;
+    uint32_t* regression_nodes;
+    uint32_t* no_training_support_nodes;
+    uint32_t* insufficient_exercise_support_nodes;
+    uint32_t* minimum_in_the_money_training_paths;
+    double* maximum_regression_condition_numbers;
+    uint32_t* early_exercise_paths;
+    uint32_t* expiry_paths;
+} fo_batch_result_columns;
+
+int fo_price_lsm_grouped_f64(fo_executor* executor, const fo_lsm_grouped_request* request,
+                             fo_batch_result_columns* out, fo_error* err);
+
+/* Row-addressed batch (price_lsm_call_batch): every column (spots, strikes, maturities, rates,
+ * volatilities, dividend rows, explicit schedules) has one entry per contract and group_offsets
+ * must be NULL; row r uses domains training_domain_start + r and evaluation_domain_start + r. */
+int fo_price_lsm_batch_f64(fo_executor* executor, const fo_lsm_grouped_request* request,
+                           fo_batch_result_columns* out, fo_error* err);
+
+/* ---- simulation exports --------------------------------------------------------------------- */
+
+typedef struct fo_gbm_seeded_request {
+    double initial_spot;
+    const double* schedule_times;             uint64_t n_schedule_times;
+    const double* curve_times;                uint64_t n_curve_times;
+    const double* log_discounts;              uint64_t n_log_discounts;
+    const double* dividend_yield_times;       uint64_t n_dividend_yield_times;
+    const double* cumulative_dividend_yields; uint64_t n_cumulative_dividend_yields;
+    const uint32_t* dividend_nodes;           uint64_t n_dividend_nodes;
+    const double* dividend_amounts;           uint64_t n_dividend_amounts;
+    const uint32_t* exercise_nodes;           uint64_t n_exercise_nodes;
+    uint32_t expiry_node;
+    double annualized_volatility;
+    int32_t dividend_policy;
+    uint64_t paths;
+    uint64_t seed;
+    uint32_t domain;
+} fo_gbm_seeded_request;
+
+/* Time-major [n_exercise_nodes + 1, paths] pre-event states at every exercise node followed by
+ * the post-event expiry state (path.rs:948-1024). `states` holds out_len doubles, exactly
+ * (n_exercise_nodes + 1) * paths. */
+int fo_simulate_gbm_seeded_f64(fo_executor* executor, const fo_gbm_seeded_request* request,
+                               double* states, uint64_t out_len, fo_error* err);
+
+/* Path-local standard normals: out[p * normals_per_path + k] is the k-th ZIGNOR normal of path
+ * path_start + p in namespace (seed, domain), with a normal budget of normals_per_path. */
+int fo_sample_standard_normals_f64(fo_executor* executor, uint64_t seed, uint32_t domain,
+                                   uint32_t path_start, uint64_t paths, uint32_t normals_per_path,
+                                   double* out, uint64_t out_len, fo_error* err);
+
+/* ---- build identity ------------------------------------------------------------------------- */
+
+/* Writes "package_version;nvcc_version;arch" into buf (NUL-terminated, truncated to capacity). */
+int fo_build_info(char* buf, uint64_t capacity);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* FINOPTIONS_CUDA_H */
