@@ -1,0 +1,898 @@
+// capi.cu - the C ABI (include/finoptions_cuda.h): executor, device arena, single-contract plans
+// and the simulation exports. Host orchestration of LsmCallEstimator::price_seeded
+// (crates/finoptions-lsm/src/policy.rs:306-336) over the kernels in lsm_kernels.cu.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/finoptions_cuda.h"
+#include "host.h"
+#include "lsm_kernels.h"
+
+#ifndef FO_PACKAGE_VERSION
+#define FO_PACKAGE_VERSION "0.1.0"
+#endif
+
+using namespace fo;
+
+namespace {
+
+constexpr unsigned long long kNone = ~0ull;
+
+Error cuda_error(cudaError_t e, const char* what) {
+    return make_error(FO_ERR_EXECUTION, FO_CODE_CUDA_FAILURE,
+                      std::string("CUDA failure in ") + what + ": " + cudaGetErrorName(e) + " (" + cudaGetErrorString(e) + ")");
+}
+
+#define FO_CUDA_TRY(expr, what)                        \
+    do {                                               \
+        cudaError_t _e = (expr);                       \
+        if (_e != cudaSuccess) return cuda_error(_e, what); \
+    } while (0)
+
+// Grow-only device buffer.
+struct DeviceBuffer {
+    void* ptr = nullptr;
+    size_t bytes = 0;
+    Error reserve(size_t need) {
+        if (need <= bytes) return Error{};
+        if (ptr) cudaFree(ptr);
+        ptr = nullptr;
+        bytes = 0;
+        const size_t grow = std::max(need, size_t(1) << 20);
+        cudaError_t e = cudaMalloc(&ptr, grow);
+        if (e != cudaSuccess) return cuda_error(e, "cudaMalloc");
+        bytes = grow;
+        return Error{};
+    }
+    ~DeviceBuffer() {
+        if (ptr) cudaFree(ptr);
+    }
+};
+
+// Grow-only pinned host buffer.
+struct PinnedBuffer {
+    void* ptr = nullptr;
+    size_t bytes = 0;
+    Error reserve(size_t need) {
+        if (need <= bytes) return Error{};
+        if (ptr) cudaFreeHost(ptr);
+        ptr = nullptr;
+        bytes = 0;
+        const size_t grow = std::max(need, size_t(1) << 16);
+        cudaError_t e = cudaMallocHost(&ptr, grow);
+        if (e != cudaSuccess) return cuda_error(e, "cudaMallocHost");
+        bytes = grow;
+        return Error{};
+    }
+    ~PinnedBuffer() {
+        if (ptr) cudaFreeHost(ptr);
+    }
+};
+
+size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
+
+}  // namespace
+
+struct fo_executor {
+    int device = 0;
+    int sms = 0;
+    int backward_blocks_max = 0;
+    int eval_blocks_per_sm = 0;
+    cudaStream_t stream = nullptr;
+    std::mutex mu;
+    DeviceBuffer slab;        // training path storage shared by this executor's plans (stream-ordered)
+    DeviceBuffer scratch;     // per-call block for one-shot calls
+    PinnedBuffer staging;     // one-shot upload / download staging
+};
+
+// Layout of a plan's device block. Everything the host reads back is contiguous at `out`.
+struct PlanLayout {
+    size_t steps, events, row_node, disc_from_later, disc_to_origin, escrow_cash;  // inputs
+    size_t partials;          // backward partials: 2 * blocks * 16 double2
+    size_t eval_partials;     // eval partials: eval_blocks * 2 double2
+    size_t out;               // start of the read-back region
+    size_t status, result, records, counts, itm_counts, replay;
+    size_t out_bytes;
+    size_t total;
+    size_t inputs_bytes;
+};
+
+struct fo_lsm_call_plan {
+    fo_executor* ex = nullptr;
+    HostPlan hp;
+    Error eval_error;          // deferred evaluation-population validation failure
+    bool run_eval = true;
+    int backward_blocks = 0;
+    int ppt = 0;
+    int eval_blocks = 0;
+    uint32_t first_stored_row = 0;
+    PlanLayout lay{};
+    DeviceBuffer own_block;    // used when the plan was created through the public API
+    void* d_block = nullptr;
+    double* d_slab = nullptr;
+    PinnedBuffer own_staging;
+    void* h_out = nullptr;
+    DevicePlan dp{};
+    bool launched = false;
+};
+
+namespace {
+
+Error open_device(int device, fo_executor* ex) {
+    int count = 0;
+    cudaError_t e = cudaGetDeviceCount(&count);
+    if (e != cudaSuccess || count <= 0)
+        return make_error(FO_ERR_EXECUTION, FO_CODE_NO_DEVICE,
+                          "no CUDA device is available for CudaExecutor; there is no CPU fallback");
+    if (device < 0 || device >= count)
+        return make_error(FO_ERR_EXECUTION, FO_CODE_NO_DEVICE,
+                          "CUDA device " + std::to_string(device) + " does not exist; " + std::to_string(count) +
+                              " device(s) are visible");
+    cudaDeviceProp prop{};
+    FO_CUDA_TRY(cudaGetDeviceProperties(&prop, device), "cudaGetDeviceProperties");
+    if (prop.major != 10)
+        return make_error(FO_ERR_EXECUTION, FO_CODE_UNSUPPORTED_DEVICE,
+                          std::string("CudaExecutor requires an sm_100 (Blackwell B200) device; device ") +
+                              std::to_string(device) + " is " + prop.name + " (sm_" + std::to_string(prop.major) +
+                              std::to_string(prop.minor) + ")");
+    FO_CUDA_TRY(cudaSetDevice(device), "cudaSetDevice");
+    if (!prop.cooperativeLaunch)
+        return make_error(FO_ERR_EXECUTION, FO_CODE_UNSUPPORTED_DEVICE, "device does not support cooperative launches");
+    ex->device = device;
+    ex->sms = prop.multiProcessorCount;
+    FO_CUDA_TRY(cudaStreamCreateWithFlags(&ex->stream, cudaStreamNonBlocking), "cudaStreamCreate");
+    ex->backward_blocks_max = backward_max_blocks(device);
+    ex->eval_blocks_per_sm = 8;
+    return Error{};
+}
+
+// Chooses the persistent grid and paths-per-thread for the backward kernel.
+Error choose_backward_shape(const fo_executor* ex, uint64_t paths, int* blocks, int* ppt) {
+    const uint64_t threads = kBackwardThreads;
+    const uint64_t max_blocks = uint64_t(ex->backward_blocks_max);
+    static const int choices[] = {1, 2, 4, 8, 16, 32};
+    for (int c : choices) {
+        const uint64_t need = (paths + threads * c - 1) / (threads * c);
+        if (need <= max_blocks) {
+            *blocks = int(std::max<uint64_t>(need, 1));
+            *ppt = c;
+            return Error{};
+        }
+    }
+    return make_error(FO_ERR_EXECUTION, FO_CODE_CAPACITY_EXCEEDED,
+                      "training population of " + std::to_string(paths) +
+                          " paths exceeds the register-resident backward pass capacity of " +
+                          std::to_string(max_blocks * threads * 32) + " paths on this device");
+}
+
+PlanLayout layout_for(const HostPlan& hp, int backward_blocks, int eval_blocks) {
+    PlanLayout L{};
+    size_t off = 0;
+    auto take = [&](size_t bytes) {
+        off = align_up(off, 256);
+        const size_t at = off;
+        off += bytes;
+        return at;
+    };
+    const size_t rows = hp.rows();
+    L.steps = take(sizeof(StepCoef) * std::max<size_t>(hp.intervals(), 1));
+    L.events = take(sizeof(NodeEvent) * (hp.intervals() + 1));
+    L.row_node = take(sizeof(uint32_t) * rows);
+    L.disc_from_later = take(sizeof(double) * rows);
+    L.disc_to_origin = take(sizeof(double) * rows);
+    L.escrow_cash = take(sizeof(double) * rows);
+    L.inputs_bytes = off;
+    L.partials = take(sizeof(double2) * 2 * size_t(backward_blocks) * 16);
+    L.eval_partials = take(sizeof(double2) * size_t(eval_blocks) * 2);
+    off = align_up(off, 256);
+    L.out = off;
+    L.status = take(sizeof(DeviceStatus));
+    L.result = take(sizeof(double) * 4);
+    L.records = take(sizeof(FitRecord) * rows);
+    L.counts = take(sizeof(unsigned) * rows);
+    L.itm_counts = take(sizeof(unsigned) * rows);
+    L.replay = take(sizeof(SimFailure));
+    L.out_bytes = align_up(off, 256) - L.out;
+    L.total = align_up(off, 256);
+    return L;
+}
+
+// Packs the plan arrays in the same layout as the device block's input region.
+void pack_inputs(const HostPlan& hp, const PlanLayout& L, unsigned char* host) {
+    std::memset(host, 0, L.inputs_bytes);
+    std::memcpy(host + L.steps, hp.steps.data(), sizeof(StepCoef) * hp.steps.size());
+    std::memcpy(host + L.events, hp.events.data(), sizeof(NodeEvent) * hp.events.size());
+    std::memcpy(host + L.row_node, hp.row_node.data(), sizeof(uint32_t) * hp.row_node.size());
+    std::memcpy(host + L.disc_from_later, hp.disc_from_later.data(), sizeof(double) * hp.rows());
+    std::memcpy(host + L.disc_to_origin, hp.disc_to_origin.data(), sizeof(double) * hp.rows());
+    std::memcpy(host + L.escrow_cash, hp.escrow_cash.data(), sizeof(double) * hp.rows());
+}
+
+DevicePlan device_plan(const HostPlan& hp, const PlanLayout& L, unsigned char* dev, uint32_t first_stored_row) {
+    DevicePlan p{};
+    p.intervals = hp.intervals();
+    p.rows = hp.rows();
+    p.first_stored_row = first_stored_row;
+    p.strike = hp.strike;
+    p.sim_start = hp.sim_start;
+    p.initial_spot = hp.initial_spot;
+    p.policy = hp.policy;
+    p.escrowed = hp.escrowed ? 1 : 0;
+    p.degree = hp.degree;
+    p.tie_rule = hp.tie_rule;
+    p.support = hp.support;
+    p.origin_row = hp.origin_row ? 1 : 0;
+    p.rank_tolerance = hp.rank_tolerance;
+    p.condition_limit = hp.condition_limit;
+    p.train_paths = hp.train_paths;
+    p.eval_paths = hp.eval_paths;
+    p.train_seed = hp.train_seed;
+    p.eval_seed = hp.eval_seed;
+    p.train_domain = hp.train_domain;
+    p.eval_domain = hp.eval_domain;
+    p.steps = reinterpret_cast<const StepCoef*>(dev + L.steps);
+    p.events = reinterpret_cast<const NodeEvent*>(dev + L.events);
+    p.row_node = reinterpret_cast<const uint32_t*>(dev + L.row_node);
+    p.disc_from_later = reinterpret_cast<const double*>(dev + L.disc_from_later);
+    p.disc_to_origin = reinterpret_cast<const double*>(dev + L.disc_to_origin);
+    p.escrow_cash = reinterpret_cast<const double*>(dev + L.escrow_cash);
+    p.origin_discount = hp.origin_discount;
+    return p;
+}
+
+Error plan_create(fo_executor* ex, const fo_lsm_call_request& q, bool own_memory, fo_lsm_call_plan** out) {
+    auto plan = std::make_unique<fo_lsm_call_plan>();
+    plan->ex = ex;
+    Error e = build_call_plan(q, &plan->hp);
+    if (!e.ok()) return e;
+    HostPlan& hp = plan->hp;
+    // Evaluation population checks run after the fit in the reference (policy.rs:330-333).
+    if (q.evaluation_paths == 0) {
+        plan->eval_error = make_error(FO_ERR_LSM, FO_CODE_EMPTY_PATH_SET,
+                                      "LSM evaluation simulation failed: simulation path count must be positive");
+    } else if (q.evaluation_paths > 0xffffffffull) {
+        plan->eval_error = make_error(FO_ERR_LSM, FO_CODE_RANDOM_PATH_NAMESPACE_OVERFLOW,
+                                      "LSM evaluation simulation failed: seeded simulation supports at most 4294967295 "
+                                      "paths in one random domain; observed " + std::to_string(q.evaluation_paths));
+    }
+    plan->run_eval = plan->eval_error.ok();
+    e = choose_backward_shape(ex, hp.train_paths, &plan->backward_blocks, &plan->ppt);
+    if (!e.ok()) return e;
+    const uint64_t eval_threads = kEvalThreads;
+    const uint64_t eval_needed = plan->run_eval ? (hp.eval_paths + eval_threads - 1) / eval_threads : 1;
+    plan->eval_blocks = int(std::max<uint64_t>(1, std::min<uint64_t>(eval_needed, uint64_t(ex->sms) * ex->eval_blocks_per_sm)));
+    plan->first_stored_row = hp.origin_row ? 1u : 0u;
+    plan->lay = layout_for(hp, plan->backward_blocks, plan->eval_blocks);
+    const PlanLayout& L = plan->lay;
+    // device memory: plan block + slab
+    if (own_memory) {
+        e = plan->own_block.reserve(L.total);
+        if (!e.ok()) return e;
+        plan->d_block = plan->own_block.ptr;
+        e = plan->own_staging.reserve(std::max(L.inputs_bytes, L.out_bytes));
+        if (!e.ok()) return e;
+        plan->h_out = plan->own_staging.ptr;
+    } else {
+        e = ex->scratch.reserve(L.total);
+        if (!e.ok()) return e;
+        plan->d_block = ex->scratch.ptr;
+        e = ex->staging.reserve(std::max(L.inputs_bytes, L.out_bytes));
+        if (!e.ok()) return e;
+        plan->h_out = ex->staging.ptr;
+    }
+    const uint64_t stored_rows = hp.rows() - plan->first_stored_row;
+    const size_t slab_bytes = sizeof(double) * stored_rows * hp.train_paths;
+    e = ex->slab.reserve(std::max<size_t>(slab_bytes, 8));
+    if (!e.ok()) return e;
+    plan->d_slab = static_cast<double*>(ex->slab.ptr);
+    unsigned char* dev = static_cast<unsigned char*>(plan->d_block);
+    plan->dp = device_plan(hp, L, dev, plan->first_stored_row);
+    // upload inputs once
+    pack_inputs(hp, L, static_cast<unsigned char*>(plan->h_out));
+    FO_CUDA_TRY(cudaMemcpyAsync(dev, plan->h_out, L.inputs_bytes, cudaMemcpyHostToDevice, ex->stream), "plan upload");
+    FO_CUDA_TRY(cudaStreamSynchronize(ex->stream), "plan upload");
+    *out = plan.release();
+    return Error{};
+}
+
+Error plan_launch(fo_lsm_call_plan* plan) {
+    fo_executor* ex = plan->ex;
+    const PlanLayout& L = plan->lay;
+    unsigned char* dev = static_cast<unsigned char*>(plan->d_block);
+    cudaStream_t s = ex->stream;
+    auto* status = reinterpret_cast<DeviceStatus*>(dev + L.status);
+    auto* records = reinterpret_cast<FitRecord*>(dev + L.records);
+    FO_CUDA_TRY(cudaMemsetAsync(dev + L.out, 0, L.out_bytes, s), "reset");
+    FO_CUDA_TRY(cudaMemsetAsync(status, 0xff, kStatusNoneBytes, s), "reset");
+    // K1 training simulation
+    FO_CUDA_TRY(launch_simulate(plan->dp, plan->hp.train_paths, plan->hp.train_seed, plan->hp.train_domain, plan->d_slab,
+                                plan->first_stored_row, plan->hp.escrowed ? 1 : 0, &status->train_sim_fail, s),
+                "training simulation launch");
+    // K2 backward induction
+    BackwardArgs b{};
+    b.plan = plan->dp;
+    b.slab = plan->d_slab;
+    b.partials = reinterpret_cast<double2*>(dev + L.partials);
+    b.partial_stride = size_t(plan->backward_blocks) * 16;
+    b.records = records;
+    b.status = status;
+    FO_CUDA_TRY(launch_backward(b, plan->backward_blocks, plan->ppt, s), "backward launch");
+    // K3 diagnostics
+    FO_CUDA_TRY(launch_diagnose(plan->dp, records, s), "diagnose launch");
+    if (plan->run_eval) {
+        EvalArgs a{};
+        a.plan = plan->dp;
+        a.records = records;
+        a.partials = reinterpret_cast<double2*>(dev + L.eval_partials);
+        a.counts = reinterpret_cast<unsigned*>(dev + L.counts);
+        a.itm_counts = reinterpret_cast<unsigned*>(dev + L.itm_counts);
+        a.status = status;
+        FO_CUDA_TRY(launch_evaluate(a, plan->eval_blocks, s), "evaluation launch");
+        FO_CUDA_TRY(launch_finalize(a.partials, plan->eval_blocks, plan->hp.eval_paths,
+                                    reinterpret_cast<double*>(dev + L.result), s),
+                    "finalize launch");
+    }
+    plan->launched = true;
+    return Error{};
+}
+
+uint64_t kernels_per_launch(const fo_lsm_call_plan* plan) { return plan->run_eval ? 5 : 3; }
+
+std::string node_str(uint32_t node) { return std::to_string(node); }
+
+// Message of a failed fit row (RegressionError Display wrapped in LsmError::RegressionAtNode).
+Error fit_failure(const HostPlan& hp, const FitRecord& rec, uint32_t node) {
+    const int d = hp.degree;
+    const std::string prefix = "continuation regression failed at exercise node " + node_str(node) + ": ";
+    if (rec.itm < uint64_t(d + 1)) {
+        Error e = make_error(FO_ERR_LSM, FO_CODE_INSUFFICIENT_OBSERVATIONS,
+                             prefix + "regression has " + std::to_string(rec.itm) + " observations but degree " +
+                                 std::to_string(d) + " requires at least " + std::to_string(d + 1));
+        e.node = node;
+        return e;
+    }
+    Error e;
+    switch (rec.model.status) {
+        case kFitDegeneratePredictor:
+            e = make_error(FO_ERR_LSM, FO_CODE_DEGENERATE_PREDICTOR,
+                           prefix + "degree " + std::to_string(d) + " regression predictor scale is degenerate; observed " +
+                               fmt_f64(rec.model.aux_value));
+            break;
+        case kFitRankDeficient:
+            e = make_error(FO_ERR_LSM, FO_CODE_RANK_DEFICIENT,
+                           prefix + "degree " + std::to_string(d) + " polynomial design has numerical rank " +
+                               std::to_string(rec.model.aux) + " of " + std::to_string(d + 1) + " at rank tolerance " +
+                               fmt_f64(hp.rank_tolerance));
+            break;
+        case kFitNonFinite:
+            e = make_error(FO_ERR_LSM, FO_CODE_NON_FINITE_FIT,
+                           prefix + "polynomial regression produced non-finite arithmetic at basis degree " +
+                               std::to_string(rec.model.aux));
+            break;
+        default:
+            e = make_error(FO_ERR_LSM, FO_CODE_NON_FINITE_PREDICTOR,
+                           prefix + "regression population contains a non-finite predictor or response");
+            break;
+    }
+    e.node = node;
+    return e;
+}
+
+Error diag_failure(const HostPlan& hp, const FitRecord& rec, uint32_t node) {
+    const int d = hp.degree;
+    const std::string prefix = "continuation regression failed at exercise node " + node_str(node) + ": ";
+    Error e;
+    switch (rec.diag_status) {
+        case kDiagRankDeficient:
+            e = make_error(FO_ERR_LSM, FO_CODE_RANK_DEFICIENT,
+                           prefix + "degree " + std::to_string(d) + " polynomial design has numerical rank " +
+                               std::to_string(rec.diag_rank) + " of " + std::to_string(d + 1) + " at rank tolerance " +
+                               fmt_f64(hp.rank_tolerance));
+            break;
+        case kDiagConditionExceeded:
+            e = make_error(FO_ERR_LSM, FO_CODE_CONDITION_LIMIT_EXCEEDED,
+                           prefix + "degree " + std::to_string(d) + " polynomial design condition number " +
+                               fmt_f64(rec.diag_condition) + " exceeds configured limit " + fmt_f64(hp.condition_limit));
+            break;
+        case kDiagNotConverged:
+            e = make_error(FO_ERR_LSM, FO_CODE_CONDITION_DIAGNOSTIC_DID_NOT_CONVERGE,
+                           prefix + "polynomial condition diagnostic did not converge for " + std::to_string(d + 1) +
+                               " columns after 32 sweeps");
+            break;
+        default:
+            e = make_error(FO_ERR_LSM, FO_CODE_NON_FINITE_FIT,
+                           prefix + "polynomial regression produced non-finite arithmetic at basis degree " +
+                               std::to_string(rec.diag_aux));
+            break;
+    }
+    e.node = node;
+    return e;
+}
+
+Error replay(fo_lsm_call_plan* plan, bool training, uint64_t path, int want_row, SimFailure* out) {
+    fo_executor* ex = plan->ex;
+    unsigned char* dev = static_cast<unsigned char*>(plan->d_block);
+    auto* d_replay = reinterpret_cast<SimFailure*>(dev + plan->lay.replay);
+    const HostPlan& hp = plan->hp;
+    FO_CUDA_TRY(launch_replay(plan->dp, training ? hp.train_seed : hp.eval_seed, training ? hp.train_domain : hp.eval_domain,
+                              uint32_t(path), want_row, d_replay, ex->stream),
+                "replay launch");
+    FO_CUDA_TRY(cudaMemcpyAsync(out, d_replay, sizeof(SimFailure), cudaMemcpyDeviceToHost, ex->stream), "replay copy");
+    FO_CUDA_TRY(cudaStreamSynchronize(ex->stream), "replay");
+    return Error{};
+}
+
+Error simulation_error(fo_lsm_call_plan* plan, bool training, uint64_t path) {
+    SimFailure f{};
+    Error e = replay(plan, training, path, -1, &f);
+    if (!e.ok()) return e;
+    const std::string role = training ? "training" : "evaluation";
+    Error out = make_error(FO_ERR_LSM, simulation_failure_code(f.code),
+                           "LSM " + role + " simulation failed: " +
+                               simulation_failure_message(f.code, uint32_t(f.interval), path, f.spot, f.normal));
+    out.path = int64_t(path);
+    return out;
+}
+
+Error plan_collect(fo_lsm_call_plan* plan, fo_lsm_call_result* result) {
+    if (!plan->launched)
+        return make_error(FO_ERR_EXECUTION, FO_CODE_INVALID_ARGUMENT, "plan was collected before it was launched");
+    fo_executor* ex = plan->ex;
+    const PlanLayout& L = plan->lay;
+    const HostPlan& hp = plan->hp;
+    unsigned char* dev = static_cast<unsigned char*>(plan->d_block);
+    unsigned char* host = static_cast<unsigned char*>(plan->h_out);
+    FO_CUDA_TRY(cudaMemcpyAsync(host, dev + L.out, L.out_bytes, cudaMemcpyDeviceToHost, ex->stream), "result copy");
+    FO_CUDA_TRY(cudaStreamSynchronize(ex->stream), "pricing");
+    plan->launched = false;
+    const auto* status = reinterpret_cast<const DeviceStatus*>(host + (L.status - L.out));
+    const auto* res = reinterpret_cast<const double*>(host + (L.result - L.out));
+    const auto* records = reinterpret_cast<const FitRecord*>(host + (L.records - L.out));
+    const auto* counts = reinterpret_cast<const unsigned*>(host + (L.counts - L.out));
+    const auto* itm_counts = reinterpret_cast<const unsigned*>(host + (L.itm_counts - L.out));
+    const uint32_t rows = hp.rows();
+    const uint32_t E = rows - 1;
+    if (status->barrier_timeout)
+        return make_error(FO_ERR_EXECUTION, FO_CODE_BARRIER_TIMEOUT,
+                          "backward-induction grid barrier timed out; the device result was discarded");
+    if (status->train_sim_fail != kNone) return simulation_error(plan, true, status->train_sim_fail);
+    // Fit failures in backward order: discount, population, regression, diagnostic, update.
+    const uint32_t lowest = hp.origin_row ? 1u : 0u;
+    const uint32_t fitted_rows = E > lowest ? E - lowest : 0;
+    for (uint32_t order = 0; order <= fitted_rows; ++order) {
+        const unsigned long long lo = (unsigned long long)order << 32, hi = lo | 0xffffffffull;
+        if (status->fit_payoff_fail >= lo && status->fit_payoff_fail <= hi) {
+            Error e = make_error(FO_ERR_LSM, FO_CODE_NON_FINITE_DISCOUNTED_PAYOFF,
+                                 "LSM evaluation produced non-finite discounted payoff at path " +
+                                     std::to_string(status->fit_payoff_fail & 0xffffffffull));
+            e.path = int64_t(status->fit_payoff_fail & 0xffffffffull);
+            return e;
+        }
+        if (order == fitted_rows) break;
+        const uint32_t row = E - 1 - order;
+        const uint32_t node = hp.row_node[row];
+        const FitRecord& rec = records[row];
+        if (status->fit_nonfinite >= lo && status->fit_nonfinite <= hi) {
+            Error e = make_error(FO_ERR_LSM, FO_CODE_NON_FINITE_PREDICTOR,
+                                 "continuation regression failed at exercise node " + node_str(node) +
+                                     ": regression predictor or response at path " +
+                                     std::to_string(status->fit_nonfinite & 0xffffffffull) + " must be finite");
+            e.node = node;
+            e.path = int64_t(status->fit_nonfinite & 0xffffffffull);
+            return e;
+        }
+        if (rec.kind == kRuleFitFailed) return fit_failure(hp, rec, node);
+        if (rec.kind == kRuleRegression && rec.diag_status != kDiagOk) return diag_failure(hp, rec, node);
+        if (status->fit_predict_fail >= lo && status->fit_predict_fail <= hi) {
+            const uint64_t path = status->fit_predict_fail & 0xffffffffull;
+            double spot = 0.0;
+            cudaMemcpy(&spot, plan->d_slab + uint64_t(row - plan->first_stored_row) * hp.train_paths + path,
+                       sizeof(double), cudaMemcpyDeviceToHost);
+            Error e = make_error(FO_ERR_LSM, FO_CODE_NON_FINITE_PREDICTION,
+                                 "continuation prediction failed at exercise node " + node_str(node) + ", path " +
+                                     std::to_string(path) + ": polynomial regression produced non-finite prediction for predictor " +
+                                     fmt_f64(spot / hp.strike));
+            e.node = node;
+            e.path = int64_t(path);
+            return e;
+        }
+    }
+    if (!plan->run_eval) return plan->eval_error;
+    if (status->eval_sim_fail != kNone) return simulation_error(plan, false, status->eval_sim_fail);
+    // Assemble diagnostics (policy.rs:39-65) in row order.
+    result->paths = uint32_t(hp.eval_paths);
+    result->n_observations = rows;
+    result->n_diagnostics = 0;
+    const bool origin = hp.origin_row;
+    const bool origin_exercise = origin && records[0].kind == kRuleOrigin && records[0].origin_exercise;
+    for (uint32_t r = 0; r < E; ++r) {
+        const FitRecord& rec = records[r];
+        fo_lsm_node_diagnostic d{};
+        d.node = hp.row_node[r];
+        switch (rec.kind) {
+            case kRuleOrigin:
+                d.kind = FO_DIAG_ORIGIN_DECISION;
+                d.exercise = rec.origin_exercise;
+                d.estimated_continuation = rec.origin_continuation;
+                break;
+            case kRuleNoSupport: d.kind = FO_DIAG_NO_IN_THE_MONEY_PATHS; break;
+            case kRuleContinue:
+                d.kind = FO_DIAG_INSUFFICIENT_SUPPORT;
+                d.in_the_money_paths = uint32_t(rec.itm);
+                d.columns = uint64_t(hp.degree + 1);
+                break;
+            case kRuleRegression:
+                d.kind = FO_DIAG_REGRESSION;
+                d.in_the_money_paths = uint32_t(rec.itm);
+                d.observations = rec.itm;
+                d.columns = uint64_t(hp.degree + 1);
+                d.rank = uint64_t(rec.diag_rank);
+                d.condition_number = rec.diag_condition;
+                d.predictor_mean = rec.model.mean;
+                d.predictor_scale = rec.model.scale;
+                break;
+            default:
+                return make_error(FO_ERR_EXECUTION, FO_CODE_CUDA_FAILURE,
+                                  "backward pass left exercise row " + std::to_string(r) + " unfitted");
+        }
+        if (result->diagnostics && result->n_diagnostics < result->diagnostics_capacity)
+            result->diagnostics[result->n_diagnostics] = d;
+        result->n_diagnostics += 1;
+    }
+    for (uint32_t r = 0; r < rows && result->observation_nodes && r < result->observation_capacity; ++r)
+        result->observation_nodes[r] = hp.row_node[r];
+    if (origin_exercise) {
+        // LsmEvaluation::deterministic (policy.rs:657-669)
+        for (uint32_t r = 0; r < rows && result->exercise_counts && r < result->observation_capacity; ++r)
+            result->exercise_counts[r] = r == 0 ? uint32_t(hp.eval_paths) : 0u;
+        const double d = hp.initial_spot - hp.strike;
+        result->price = d > 0.0 ? d : 0.0;
+        result->has_sample_standard_deviation = 1;
+        result->sample_standard_deviation = 0.0;
+        result->has_standard_error = 1;
+        result->standard_error = 0.0;
+        return Error{};
+    }
+    // Evaluation failures in row order: prediction/payoff (key) or unsupported in-the-money paths.
+    const uint64_t eval_row = status->eval_fail != kNone ? (status->eval_fail >> 33) : ~0ull;
+    for (uint32_t r = 0; r < E; ++r) {
+        if (records[r].kind == kRuleNoSupport && itm_counts[r] > 0) {
+            if (eval_row < r) break;
+            Error e = make_error(FO_ERR_LSM, FO_CODE_EVALUATION_OUTSIDE_TRAINING_SUPPORT,
+                                 std::to_string(itm_counts[r]) + " active evaluation paths are in the money at node " +
+                                     node_str(hp.row_node[r]) + ", but training had no in-the-money support");
+            e.node = hp.row_node[r];
+            return e;
+        }
+    }
+    if (status->eval_fail != kNone) {
+        const uint32_t r = uint32_t(status->eval_fail >> 33);
+        const uint64_t path = (status->eval_fail >> 1) & 0xffffffffull;
+        if (status->eval_fail & 1ull) {
+            Error e = make_error(FO_ERR_LSM, FO_CODE_NON_FINITE_DISCOUNTED_PAYOFF,
+                                 "LSM evaluation produced non-finite discounted payoff at path " + std::to_string(path));
+            e.path = int64_t(path);
+            return e;
+        }
+        SimFailure f{};
+        Error re = replay(plan, false, path, int(r), &f);
+        if (!re.ok()) return re;
+        Error e = make_error(FO_ERR_LSM, FO_CODE_NON_FINITE_PREDICTION,
+                             "continuation prediction failed at exercise node " + node_str(hp.row_node[r]) + ", path " +
+                                 std::to_string(path) + ": polynomial regression produced non-finite prediction for predictor " +
+                                 fmt_f64(f.observed / hp.strike));
+        e.node = hp.row_node[r];
+        e.path = int64_t(path);
+        return e;
+    }
+    if (status->eval_terminal_fail != kNone) {
+        Error e = make_error(FO_ERR_LSM, FO_CODE_NON_FINITE_DISCOUNTED_PAYOFF,
+                             "LSM evaluation produced non-finite discounted payoff at path " +
+                                 std::to_string(status->eval_terminal_fail));
+        e.path = int64_t(status->eval_terminal_fail);
+        return e;
+    }
+    for (uint32_t r = 0; r < rows && result->exercise_counts && r < result->observation_capacity; ++r)
+        result->exercise_counts[r] = counts[r];
+    result->price = res[0];
+    if (hp.eval_paths > 1) {
+        if (!std::isfinite(res[2]) || !std::isfinite(res[3])) {
+            Error e = make_error(FO_ERR_LSM, FO_CODE_NON_FINITE_DISCOUNTED_PAYOFF,
+                                 "LSM evaluation produced non-finite discounted payoff at path 0");
+            e.path = 0;
+            return e;
+        }
+        result->has_sample_standard_deviation = 1;
+        result->sample_standard_deviation = res[2];
+        result->has_standard_error = 1;
+        result->standard_error = res[3];
+    } else {
+        result->has_sample_standard_deviation = 0;
+        result->has_standard_error = 0;
+        result->sample_standard_deviation = 0.0;
+        result->standard_error = 0.0;
+    }
+    return Error{};
+}
+
+int finish(fo_error* err, const Error& e) {
+    if (!e.ok()) write_error(err, e);
+    return e.kind;
+}
+
+Error require(const void* p, const char* what) {
+    if (!p) return make_error(FO_ERR_EXECUTION, FO_CODE_INVALID_ARGUMENT, std::string(what) + " must not be NULL");
+    return Error{};
+}
+
+}  // namespace
+
+// =============================================================================================
+// extern "C"
+// =============================================================================================
+
+extern "C" {
+
+int fo_cuda_executor_create(int32_t device, fo_executor** out, fo_error* err) {
+    Error e = require(out, "executor output");
+    if (!e.ok()) return finish(err, e);
+    auto ex = std::make_unique<fo_executor>();
+    e = open_device(device, ex.get());
+    if (!e.ok()) return finish(err, e);
+    *out = ex.release();
+    return FO_OK;
+}
+
+void fo_executor_destroy(fo_executor* executor) {
+    if (!executor) return;
+    cudaSetDevice(executor->device);
+    if (executor->stream) {
+        cudaStreamSynchronize(executor->stream);
+        cudaStreamDestroy(executor->stream);
+    }
+    delete executor;
+}
+
+int fo_executor_device(const fo_executor* executor, int32_t* device) {
+    if (!executor || !device) return FO_ERR_EXECUTION;
+    *device = executor->device;
+    return FO_OK;
+}
+
+int fo_lsm_call_plan_create(fo_executor* executor, const fo_lsm_call_request* request, fo_lsm_call_plan** out,
+                            fo_error* err) {
+    Error e = require(executor, "executor");
+    if (e.ok()) e = require(request, "request");
+    if (e.ok()) e = require(out, "plan output");
+    if (!e.ok()) return finish(err, e);
+    std::lock_guard<std::mutex> lock(executor->mu);
+    cudaSetDevice(executor->device);
+    return finish(err, plan_create(executor, *request, true, out));
+}
+
+int fo_lsm_call_plan_launch(fo_lsm_call_plan* plan, fo_error* err) {
+    Error e = require(plan, "plan");
+    if (!e.ok()) return finish(err, e);
+    std::lock_guard<std::mutex> lock(plan->ex->mu);
+    cudaSetDevice(plan->ex->device);
+    return finish(err, plan_launch(plan));
+}
+
+int fo_lsm_call_plan_collect(fo_lsm_call_plan* plan, fo_lsm_call_result* result, fo_error* err) {
+    Error e = require(plan, "plan");
+    if (e.ok()) e = require(result, "result");
+    if (!e.ok()) return finish(err, e);
+    std::lock_guard<std::mutex> lock(plan->ex->mu);
+    cudaSetDevice(plan->ex->device);
+    return finish(err, plan_collect(plan, result));
+}
+
+int fo_lsm_call_plan_kernel_count(const fo_lsm_call_plan* plan, uint64_t* kernels) {
+    if (!plan || !kernels) return FO_ERR_EXECUTION;
+    *kernels = kernels_per_launch(plan);
+    return FO_OK;
+}
+
+int fo_lsm_call_plan_stream(const fo_lsm_call_plan* plan, void** stream) {
+    if (!plan || !stream) return FO_ERR_EXECUTION;
+    *stream = plan->ex->stream;
+    return FO_OK;
+}
+
+void fo_lsm_call_plan_destroy(fo_lsm_call_plan* plan) {
+    if (!plan) return;
+    {
+        std::lock_guard<std::mutex> lock(plan->ex->mu);
+        cudaSetDevice(plan->ex->device);
+        cudaStreamSynchronize(plan->ex->stream);
+    }
+    delete plan;
+}
+
+int fo_price_lsm_call_f64(fo_executor* executor, const fo_lsm_call_request* request, fo_lsm_call_result* result,
+                          fo_error* err) {
+    Error e = require(executor, "executor");
+    if (e.ok()) e = require(request, "request");
+    if (e.ok()) e = require(result, "result");
+    if (!e.ok()) return finish(err, e);
+    std::lock_guard<std::mutex> lock(executor->mu);
+    cudaSetDevice(executor->device);
+    fo_lsm_call_plan* raw = nullptr;
+    e = plan_create(executor, *request, false, &raw);
+    if (!e.ok()) return finish(err, e);
+    std::unique_ptr<fo_lsm_call_plan> plan(raw);
+    e = plan_launch(plan.get());
+    if (e.ok()) e = plan_collect(plan.get(), result);
+    return finish(err, e);
+}
+
+int fo_simulate_gbm_seeded_f64(fo_executor* executor, const fo_gbm_seeded_request* q, double* states, uint64_t out_len,
+                               fo_error* err) {
+    Error e = require(executor, "executor");
+    if (e.ok()) e = require(q, "request");
+    if (!e.ok()) return finish(err, e);
+    std::lock_guard<std::mutex> lock(executor->mu);
+    cudaSetDevice(executor->device);
+    HostPlan hp;
+    e = build_gbm_plan(q->schedule_times, q->n_schedule_times, q->curve_times, q->n_curve_times, q->log_discounts,
+                       q->n_log_discounts, q->dividend_yield_times, q->n_dividend_yield_times, q->cumulative_dividend_yields,
+                       q->n_cumulative_dividend_yields, q->dividend_nodes, q->n_dividend_nodes, q->dividend_amounts,
+                       q->n_dividend_amounts, q->exercise_nodes, q->n_exercise_nodes, q->expiry_node,
+                       q->annualized_volatility, q->dividend_policy, &hp);
+    if (!e.ok()) return finish(err, e);
+    // validate_seeded (seeded.rs:384-397)
+    const double s0 = q->initial_spot;
+    if (!std::isfinite(s0) || s0 < 0.0 || (s0 == 0.0 && std::signbit(s0)))
+        return finish(err, make_error(FO_ERR_SIMULATION, FO_CODE_INVALID_INITIAL_SPOT,
+                                      "initial spot must be finite, nonnegative, and canonical; observed " + fmt_f64(s0)));
+    if (q->paths == 0)
+        return finish(err, make_error(FO_ERR_SIMULATION, FO_CODE_EMPTY_PATH_SET, "simulation path count must be positive"));
+    if (q->paths > 0xffffffffull)
+        return finish(err, make_error(FO_ERR_SIMULATION, FO_CODE_RANDOM_PATH_NAMESPACE_OVERFLOW,
+                                      "seeded simulation supports at most 4294967295 paths in one random domain; observed " +
+                                          std::to_string(q->paths)));
+    const uint64_t rows = hp.rows();
+    if (!states || out_len != rows * q->paths)
+        return finish(err, make_error(FO_ERR_EXECUTION, FO_CODE_INVALID_ARGUMENT,
+                                      "states buffer must hold exactly " + std::to_string(rows * q->paths) + " values"));
+    hp.sim_start = s0;
+    hp.initial_spot = s0;
+    hp.disc_from_later.assign(rows, 1.0);
+    hp.disc_to_origin.assign(rows, 1.0);
+    PlanLayout L = layout_for(hp, 1, 1);
+    e = executor->scratch.reserve(L.total);
+    if (e.ok()) e = executor->staging.reserve(std::max(L.inputs_bytes, L.out_bytes));
+    if (e.ok()) e = executor->slab.reserve(sizeof(double) * rows * q->paths);
+    if (!e.ok()) return finish(err, e);
+    unsigned char* dev = static_cast<unsigned char*>(executor->scratch.ptr);
+    pack_inputs(hp, L, static_cast<unsigned char*>(executor->staging.ptr));
+    cudaStream_t s = executor->stream;
+    DevicePlan dp = device_plan(hp, L, dev, 0);
+    auto* status = reinterpret_cast<DeviceStatus*>(dev + L.status);
+    auto run = [&]() -> Error {
+        FO_CUDA_TRY(cudaMemcpyAsync(dev, executor->staging.ptr, L.inputs_bytes, cudaMemcpyHostToDevice, s), "upload");
+        FO_CUDA_TRY(cudaMemsetAsync(status, 0xff, kStatusNoneBytes, s), "reset");
+        FO_CUDA_TRY(launch_simulate(dp, q->paths, q->seed, q->domain, static_cast<double*>(executor->slab.ptr), 0, 0,
+                                    &status->train_sim_fail, s),
+                    "simulation launch");
+        unsigned long long fail = 0;
+        FO_CUDA_TRY(cudaMemcpyAsync(&fail, &status->train_sim_fail, sizeof(fail), cudaMemcpyDeviceToHost, s), "status");
+        FO_CUDA_TRY(cudaStreamSynchronize(s), "simulation");
+        if (fail != kNone) {
+            auto* d_replay = reinterpret_cast<SimFailure*>(dev + L.replay);
+            SimFailure f{};
+            FO_CUDA_TRY(launch_replay(dp, q->seed, q->domain, uint32_t(fail), -1, d_replay, s), "replay");
+            FO_CUDA_TRY(cudaMemcpyAsync(&f, d_replay, sizeof(f), cudaMemcpyDeviceToHost, s), "replay copy");
+            FO_CUDA_TRY(cudaStreamSynchronize(s), "replay");
+            Error se = make_error(FO_ERR_SIMULATION, simulation_failure_code(f.code),
+                                  simulation_failure_message(f.code, uint32_t(f.interval), fail, f.spot, f.normal));
+            se.path = int64_t(fail);
+            return se;
+        }
+        FO_CUDA_TRY(cudaMemcpy(states, executor->slab.ptr, sizeof(double) * rows * q->paths, cudaMemcpyDeviceToHost),
+                    "states copy");
+        return Error{};
+    };
+    return finish(err, run());
+}
+
+int fo_sample_standard_normals_f64(fo_executor* executor, uint64_t seed, uint32_t domain, uint32_t path_start,
+                                   uint64_t paths, uint32_t normals_per_path, double* out, uint64_t out_len,
+                                   fo_error* err) {
+    Error e = require(executor, "executor");
+    if (e.ok()) e = require(out, "output");
+    if (!e.ok()) return finish(err, e);
+    if (out_len != paths * uint64_t(normals_per_path) || uint64_t(path_start) + paths > (1ull << 32))
+        return finish(err, make_error(FO_ERR_EXECUTION, FO_CODE_INVALID_ARGUMENT,
+                                      "normal buffer must hold paths * normals_per_path values within the u32 path domain"));
+    std::lock_guard<std::mutex> lock(executor->mu);
+    cudaSetDevice(executor->device);
+    const size_t bytes = sizeof(double) * out_len + 256;
+    e = executor->slab.reserve(bytes);
+    if (!e.ok()) return finish(err, e);
+    cudaStream_t s = executor->stream;
+    auto run = [&]() -> Error {
+        auto* fail = reinterpret_cast<unsigned long long*>(static_cast<unsigned char*>(executor->slab.ptr) + sizeof(double) * out_len);
+        FO_CUDA_TRY(cudaMemsetAsync(fail, 0xff, sizeof(unsigned long long), s), "reset");
+        FO_CUDA_TRY(launch_normals(seed, domain, path_start, paths, normals_per_path, static_cast<double*>(executor->slab.ptr),
+                                   fail, s),
+                    "normals launch");
+        unsigned long long f = 0;
+        FO_CUDA_TRY(cudaMemcpyAsync(&f, fail, sizeof(f), cudaMemcpyDeviceToHost, s), "status");
+        FO_CUDA_TRY(cudaStreamSynchronize(s), "normals");
+        if (f != kNone) {
+            Error se = make_error(FO_ERR_SIMULATION, FO_CODE_RANDOM_NORMAL_REJECTION_LIMIT,
+                                  "standard-normal generation failed at path " + std::to_string(uint64_t(path_start) + f));
+            se.path = int64_t(path_start + f);
+            return se;
+        }
+        FO_CUDA_TRY(cudaMemcpy(out, executor->slab.ptr, sizeof(double) * out_len, cudaMemcpyDeviceToHost), "copy");
+        return Error{};
+    };
+    return finish(err, run());
+}
+
+int fo_build_info(char* buf, uint64_t capacity) {
+    if (!buf || capacity == 0) return FO_ERR_EXECUTION;
+    int runtime = 0;
+    cudaRuntimeGetVersion(&runtime);
+    std::snprintf(buf, capacity, "%s;nvcc %d.%d;sm_100a;cudart %d", FO_PACKAGE_VERSION, __CUDACC_VER_MAJOR__,
+                  __CUDACC_VER_MINOR__, runtime);
+    return FO_OK;
+}
+
+// ---- host-only validation -----------------------------------------------------------------------
+
+int fo_validate_cash_dividend_amount(double amount, fo_error* err) { return finish(err, validate_cash_dividend(1, amount)); }
+
+int fo_validate_constant_volatility(double sigma, fo_error* err) { return finish(err, validate_constant_volatility(sigma)); }
+
+int fo_validate_event_schedule(const double* times, uint64_t n_times, const uint32_t* dividend_nodes,
+                               uint64_t n_dividend_nodes, const double* dividend_amounts, uint64_t n_dividend_amounts,
+                               const uint32_t* exercise_nodes, uint64_t n_exercise_nodes, uint32_t expiry_node,
+                               fo_error* err) {
+    std::vector<double> t(times, times + n_times);
+    std::vector<uint32_t> dn(dividend_nodes, dividend_nodes + n_dividend_nodes);
+    std::vector<double> da(dividend_amounts, dividend_amounts + n_dividend_amounts);
+    std::vector<uint32_t> ex(exercise_nodes, exercise_nodes + n_exercise_nodes);
+    return finish(err, validate_event_schedule(t, dn, da, ex, expiry_node));
+}
+
+int fo_validate_log_discount_curve(const double* times, uint64_t n_times, const double* log_discounts, uint64_t n,
+                                   fo_error* err) {
+    std::vector<double> t(times, times + n_times), v(log_discounts, log_discounts + n);
+    return finish(err, validate_log_discount_curve(t, v));
+}
+
+int fo_validate_cumulative_dividend_yield_curve(const double* times, uint64_t n_times, const double* yields, uint64_t n,
+                                                fo_error* err) {
+    std::vector<double> t(times, times + n_times), v(yields, yields + n);
+    return finish(err, validate_cumulative_yield_curve(t, v));
+}
+
+int fo_validate_ragged_cash_dividends(const int64_t* offsets, uint64_t n_offsets, const double* times, uint64_t n_times,
+                                      const double* amounts, uint64_t n_amounts, fo_error* err) {
+    return finish(err, validate_ragged_cash(offsets, n_offsets, times, n_times, amounts, n_amounts));
+}
+
+int fo_validate_ragged_exercise_times(const int64_t* offsets, uint64_t n_offsets, const double* times, uint64_t n_times,
+                                      fo_error* err) {
+    return finish(err, validate_ragged_exercise(offsets, n_offsets, times, n_times));
+}
+
+int fo_validate_lsm_call_request(const fo_lsm_call_request* request, fo_error* err) {
+    Error e = require(request, "request");
+    if (!e.ok()) return finish(err, e);
+    HostPlan hp;
+    return finish(err, build_call_plan(*request, &hp));
+}
+
+}  // extern "C"

@@ -1,0 +1,684 @@
+// lsm_kernels.cu - sm_100a kernels of the single-contract LSM path.
+//
+//   K1 simulate_kernel     Philox -> ZIGNOR -> GBM -> event phases, one thread per path; stores the
+//                          observed rows time-major [rows, paths] with coalesced row stores
+//                          (path/seeded.rs:399-474 fused with the transpose).
+//   K2 backward_kernel     persistent cooperative kernel: backward induction over exercise rows
+//                          with every thread's discounted values held in registers; one grid-wide
+//                          reduction of in-the-money power sums per row, then each CTA solves the
+//                          continuation regression redundantly and applies the exercise rule
+//                          (policy.rs:215-296, 471-601).
+//   K3 diagnose_kernel     rank / condition diagnostic per fitted row, off the critical path
+//                          (regression.rs:540-577).
+//   K4 evaluate_kernel     re-simulates the evaluation population and applies the fixed policy on
+//                          the fly: no path storage (policy.rs:642-834).
+//   K5 finalize_kernel     price / standard error from the CTA partials (policy.rs:891-926).
+//   replay_kernel          re-runs one failing path to recover the typed failure details.
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "lsm_device.cuh"
+#include "lsm_kernels.h"
+
+namespace fo {
+
+__constant__ uint64_t c_zig_x[257] = FO_ZIG_NORM_X_BITS;
+__constant__ uint64_t c_zig_f[257] = FO_ZIG_NORM_F_BITS;
+
+constexpr unsigned long long kNone = ~0ull;
+
+__device__ __forceinline__ void load_zig_tables(double* sx, double* sf) {
+    for (int i = threadIdx.x; i < 257; i += blockDim.x) {
+        sx[i] = bits_to_double(c_zig_x[i]);
+        sf[i] = bits_to_double(c_zig_f[i]);
+    }
+    __syncthreads();
+}
+
+__device__ __forceinline__ SmemZig make_zig(const double* sx, const double* sf) {
+    SmemZig z;
+    z.xs = sx;
+    z.fs = sf;
+    z.rr = bits_to_double(FO_ZIG_NORM_R_BITS);
+    return z;
+}
+
+__device__ __forceinline__ unsigned ld_acquire_gpu(const unsigned* p) {
+    unsigned v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+__device__ __forceinline__ unsigned ld_volatile_u32(const unsigned* p) {
+    return *(const volatile unsigned*)p;
+}
+
+// Bounded grid-wide barrier for a cooperatively launched grid (all CTAs co-resident). Gives up
+// after kBarrierSpinLimit polls, raising status->barrier_timeout; every CTA then leaves.
+constexpr unsigned long long kBarrierSpinLimit = 1ull << 25;
+
+__device__ bool grid_barrier(unsigned* local_gen, DeviceStatus* st) {
+    unsigned* arrive = &st->arrive;
+    unsigned* generation = &st->generation;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const unsigned gen = *local_gen;
+        __threadfence();
+        const unsigned prev = atomicAdd(arrive, 1u);
+        if (prev == gridDim.x - 1) {
+            atomicExch(arrive, 0u);
+            __threadfence();
+            atomicExch(generation, gen + 1);
+        } else {
+            unsigned long long spins = 0;
+            while (ld_acquire_gpu(generation) == gen) {
+                if (ld_volatile_u32(&st->barrier_timeout) != 0) break;
+                if (++spins > kBarrierSpinLimit) {
+                    atomicExch(&st->barrier_timeout, 1u);
+                    break;
+                }
+                __nanosleep(64);
+            }
+        }
+        __threadfence();
+        *local_gen = gen + 1;
+    }
+    __syncthreads();
+    return ld_volatile_u32(&st->barrier_timeout) == 0;
+}
+
+// ---------------------------------------------------------------------------------------------
+// Normals export
+// ---------------------------------------------------------------------------------------------
+
+__global__ void __launch_bounds__(256) normals_kernel(uint64_t seed, uint32_t domain, uint32_t path_start,
+                                                      uint64_t paths, uint32_t count, double* out,
+                                                      unsigned long long* fail) {
+    __shared__ double sx[257], sf[257];
+    load_zig_tables(sx, sf);
+    const SmemZig zig = make_zig(sx, sf);
+    for (uint64_t p = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; p < paths;
+         p += uint64_t(gridDim.x) * blockDim.x) {
+        PathStream s;
+        s.init(seed, domain, uint32_t(path_start + p), count);
+        for (uint32_t k = 0; k < count; ++k) {
+            double z = 0.0;
+            const int status = zig_sample(s, zig, &z);
+            if (status != kNormalOk) {
+                atomicMin(fail, (unsigned long long)p);
+                break;
+            }
+            out[p * count + k] = z;
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------------------------
+// K1: seeded simulation with time-major row stores.
+// ---------------------------------------------------------------------------------------------
+
+struct SimResult {
+    int code;  // 0 ok, kNormalBudget, kNormalRejection, 3 non-finite transition
+    int interval;
+    double spot;
+    double normal;
+};
+
+// Simulates one path; calls store(row, value) at every observation. Mirrors simulate_one_seeded
+// (seeded.rs:399-459) including the terminal-dividend phase order.
+template <typename Store>
+__device__ __forceinline__ SimResult simulate_path(const DevicePlan& plan, const SmemZig& zig, uint64_t seed,
+                                                   uint32_t domain, uint32_t path, Store&& store) {
+    PathStream s;
+    s.init(seed, domain, path, plan.intervals);
+    double spot = plan.sim_start;
+    SimResult r{0, 0, 0.0, 0.0};
+    if (plan.row_node[0] == 0) store(0, spot);
+    for (uint32_t i = 0; i < plan.intervals; ++i) {
+        double z = 0.0;
+        const int status = zig_sample(s, zig, &z);
+        if (status != kNormalOk) {
+            r.code = status;
+            r.interval = int(i);
+            return r;
+        }
+        const StepCoef c = plan.steps[i];
+        const double next = gbm_advance(spot, c.diffusion, c.log_drift, z);
+        if (!fo_isfinite(next)) {
+            r.code = 3;
+            r.interval = int(i);
+            r.spot = spot;
+            r.normal = z;
+            return r;
+        }
+        spot = next;
+        const NodeEvent ev = plan.events[i + 1];
+        const bool dividend = (ev.flags & kEventDividend) != 0;
+        const bool terminal = (ev.flags & kEventTerminal) != 0;
+        if (dividend && terminal) spot = apply_cash_dividend(plan.policy, ev.dividend_amount, spot);
+        if (ev.row >= 0) store(ev.row, spot);
+        if (dividend && !terminal) spot = apply_cash_dividend(plan.policy, ev.dividend_amount, spot);
+    }
+    return r;
+}
+
+__global__ void __launch_bounds__(256) simulate_kernel(DevicePlan plan, uint64_t paths, uint64_t seed,
+                                                       uint32_t domain, double* out, uint32_t store_first_row,
+                                                       int reconstruct_escrowed, unsigned long long* fail) {
+    __shared__ double sx[257], sf[257];
+    load_zig_tables(sx, sf);
+    const SmemZig zig = make_zig(sx, sf);
+    for (uint64_t p = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; p < paths;
+         p += uint64_t(gridDim.x) * blockDim.x) {
+        auto store = [&](int row, double value) {
+            if (uint32_t(row) < store_first_row) return;
+            if (reconstruct_escrowed) {
+                // Escrowed observations: origin -> S0; otherwise prepaid forward + prepaid cash.
+                value = plan.row_node[row] == 0 ? plan.initial_spot : value + plan.escrow_cash[row];
+            }
+            out[uint64_t(row - store_first_row) * paths + p] = value;
+        };
+        const SimResult r = simulate_path(plan, zig, seed, domain, uint32_t(p), store);
+        if (r.code != 0) atomicMin(fail, (unsigned long long)p);
+    }
+}
+
+// Re-runs one path serially to recover the typed failure details and the state at `want_row`.
+__global__ void replay_kernel(DevicePlan plan, uint64_t seed, uint32_t domain, uint32_t path, int want_row,
+                              SimFailure* out) {
+    __shared__ double sx[257], sf[257];
+    load_zig_tables(sx, sf);
+    if (threadIdx.x != 0) return;
+    const SmemZig zig = make_zig(sx, sf);
+    double observed = 0.0;
+    const SimResult r = simulate_path(plan, zig, seed, domain, path, [&](int row, double v) {
+        if (row == want_row) observed = v;
+    });
+    out->code = r.code;
+    out->interval = r.interval;
+    out->spot = r.spot;
+    out->normal = r.normal;
+    out->observed = observed;
+}
+
+// ---------------------------------------------------------------------------------------------
+// Reductions
+// ---------------------------------------------------------------------------------------------
+
+constexpr int kSlots = 16;  // T_0..T_8, U_0..U_4, non-finite count, spare
+
+// Warp sums in double, CTA combination in double-double; lane k of warp 0 writes slot k.
+template <int S>
+__device__ __forceinline__ void cta_reduce_to(double (&acc)[S], double* smem /* [32 * S] */, double2* dst) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, warps = blockDim.x >> 5;
+#pragma unroll
+    for (int k = 0; k < S; ++k) {
+        double v = acc[k];
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
+        acc[k] = v;
+    }
+    if (lane == 0) {
+#pragma unroll
+        for (int k = 0; k < S; ++k) smem[warp * S + k] = acc[k];
+    }
+    __syncthreads();
+    if (threadIdx.x < S) {
+        dd sum = dd_make(0.0);
+        for (int w = 0; w < warps; ++w) sum = dd_add(sum, dd_make(smem[w * S + threadIdx.x]));
+        dst[threadIdx.x] = make_double2(sum.hi, sum.lo);
+    }
+    __syncthreads();
+}
+
+__device__ __forceinline__ dd shfl_dd_down(dd v, int off) {
+    dd o;
+    o.hi = __shfl_down_sync(0xffffffffu, v.hi, off);
+    o.lo = __shfl_down_sync(0xffffffffu, v.lo, off);
+    return o;
+}
+
+// Sums partials[b * S + k] over b in a fixed order; warp k handles slot k. Identical in every CTA.
+template <int S>
+__device__ __forceinline__ void grid_combine(const double2* partials, int blocks, dd* out /* smem [S] */) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (warp < S) {
+        dd acc = dd_make(0.0);
+        for (int b = lane; b < blocks; b += 32) {
+            const double2 v = __ldcg(&partials[b * S + warp]);
+            acc = dd_add(acc, dd{v.x, v.y});
+        }
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) acc = dd_add(acc, shfl_dd_down(acc, off));
+        if (lane == 0) out[warp] = acc;
+    }
+    __syncthreads();
+}
+
+// ---------------------------------------------------------------------------------------------
+// K2: persistent backward induction.
+// ---------------------------------------------------------------------------------------------
+
+struct BackwardSmem {
+    double red[32 * kSlots];
+    dd total[kSlots];
+    FitModel model;
+    int kind;
+    int stop;
+    unsigned local_gen;
+};
+
+__device__ __forceinline__ bool exercise_rule(int tie_rule, double intrinsic, double continuation) {
+    return tie_rule == 0 ? intrinsic > continuation : intrinsic >= continuation;
+}
+
+template <int PPT>
+__global__ void __launch_bounds__(kBackwardThreads, 1) backward_kernel(BackwardArgs a) {
+    __shared__ BackwardSmem sm;
+    const DevicePlan& plan = a.plan;
+    if (threadIdx.x == 0) {
+        sm.local_gen = 0;
+        sm.stop = 0;
+    }
+    if (*(const volatile unsigned long long*)&a.status->train_sim_fail != kNone)
+        return;  // training simulation failed: every CTA reads the same word and leaves
+    __syncthreads();
+    const uint64_t P = plan.train_paths;
+    const uint64_t nthreads = uint64_t(gridDim.x) * blockDim.x;
+    const uint64_t gtid = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    const double K = plan.strike;
+    const int degree = plan.degree;
+    const uint32_t rows = plan.rows;
+    const uint32_t E = rows - 1;
+    const uint32_t fsr = plan.first_stored_row;
+    auto row_ptr = [&](uint32_t row) { return a.slab + uint64_t(row - fsr) * P; };
+
+    double v[PPT];
+    {
+        const double* terminal = row_ptr(E);
+#pragma unroll
+        for (int j = 0; j < PPT; ++j) {
+            const uint64_t p = gtid + uint64_t(j) * nthreads;
+            const double s = p < P ? __ldcs(&terminal[p]) : 0.0;
+            const double d = s - K;
+            v[j] = d > 0.0 ? d : 0.0;
+        }
+    }
+    double pivot = 0.0;
+    bool have_pivot = false;
+    uint32_t order = 0;
+    const uint32_t lowest = plan.origin_row ? 1u : 0u;
+    double2* parts = a.partials;
+    int parity = 0;
+    for (int row = int(E) - 1; row >= int(lowest); --row, ++order) {
+        const double disc = plan.disc_from_later[row];
+        const double* srow = row_ptr(uint32_t(row));
+        // discount (policy.rs:1049-1063)
+#pragma unroll
+        for (int j = 0; j < PPT; ++j) {
+            const uint64_t p = gtid + uint64_t(j) * nthreads;
+            if (p < P) {
+                v[j] *= disc;
+                if (!fo_isfinite(v[j]))
+                    atomicMin(&a.status->fit_payoff_fail, ((unsigned long long)order << 32) | p);
+            }
+        }
+        if (!have_pivot) {
+            // One-off location pass for the first fitted row: pivot = in-the-money mean moneyness.
+            double acc[2] = {0.0, 0.0};
+#pragma unroll
+            for (int j = 0; j < PPT; ++j) {
+                const uint64_t p = gtid + uint64_t(j) * nthreads;
+                if (p < P) {
+                    const double s = srow[p];
+                    if (s > K) {
+                        const double x = s / K;
+                        if (fo_isfinite(x)) {
+                            acc[0] += 1.0;
+                            acc[1] += x;
+                        }
+                    }
+                }
+            }
+            cta_reduce_to<2>(acc, sm.red, parts + size_t(parity) * a.partial_stride + size_t(blockIdx.x) * 2);
+            if (!grid_barrier(&sm.local_gen, a.status)) return;
+            grid_combine<2>(parts + size_t(parity) * a.partial_stride, gridDim.x, sm.total);
+            parity ^= 1;
+            pivot = sm.total[0].hi > 0.0 ? dd_round(dd_div(sm.total[1], sm.total[0])) : 1.0;
+            have_pivot = true;
+        }
+        // In-the-money power sums about the pivot.
+        double acc[kSlots];
+#pragma unroll
+        for (int k = 0; k < kSlots; ++k) acc[k] = 0.0;
+#pragma unroll
+        for (int j = 0; j < PPT; ++j) {
+            const uint64_t p = gtid + uint64_t(j) * nthreads;
+            if (p < P) {
+                const double s = srow[p];
+                if (s > K) {
+                    const double x = s / K;
+                    const double y = v[j];
+                    if (!fo_isfinite(x) || !fo_isfinite(y)) {
+                        acc[14] += 1.0;
+                        atomicMin(&a.status->fit_nonfinite, ((unsigned long long)order << 32) | p);
+                    } else {
+                        const double t = x - pivot;
+                        acc[0] += 1.0;
+                        double pw = t;
+                        acc[kPowerSums] += y;
+#pragma unroll
+                        for (int k = 1; k < kPowerSums; ++k) {
+                            acc[k] += pw;
+                            if (k < kResponseSums) acc[kPowerSums + k] += y * pw;
+                            pw *= t;
+                        }
+                    }
+                }
+            }
+        }
+        cta_reduce_to<kSlots>(acc, sm.red, parts + size_t(parity) * a.partial_stride + size_t(blockIdx.x) * kSlots);
+        if (!grid_barrier(&sm.local_gen, a.status)) return;
+        grid_combine<kSlots>(parts + size_t(parity) * a.partial_stride, gridDim.x, sm.total);
+        parity ^= 1;
+        if (threadIdx.x == 0) {
+            const uint64_t itm = uint64_t(sm.total[0].hi);
+            const uint64_t bad = uint64_t(sm.total[14].hi);
+            const uint64_t population = itm + bad;
+            const uint32_t required = uint32_t(degree + 1);
+            int kind;
+            if (population == 0) {
+                kind = plan.support == 1 ? kRuleContinue : kRuleNoSupport;
+            } else if (population < required && plan.support == 1) {
+                kind = kRuleContinue;
+            } else if (population < required || bad > 0) {
+                kind = kRuleFitFailed;  // InsufficientObservations / non-finite population
+            } else {
+                fit_from_moments(sm.total, pivot, itm, degree, plan.rank_tolerance, &sm.model);
+                kind = sm.model.status == kFitOk ? kRuleRegression : kRuleFitFailed;
+            }
+            sm.kind = kind;
+            if (blockIdx.x == 0) {
+                FitRecord& rec = a.records[row];
+                rec.kind = kind;
+                rec.itm = population;
+                rec.pivot = pivot;
+                rec.model = sm.model;
+                rec.origin_exercise = 0;
+                rec.origin_continuation = 0.0;
+                rec.diag_status = -1;
+                if (kind == kRuleFitFailed) atomicMin(&a.status->fit_failed_order, order);
+            }
+        }
+        __syncthreads();
+        const int kind = sm.kind;
+        if (kind == kRuleFitFailed) return;  // identical decision in every CTA
+        if (kind == kRuleRegression) {
+            const FitModel& model = sm.model;  // read from shared memory
+#pragma unroll
+            for (int j = 0; j < PPT; ++j) {
+                const uint64_t p = gtid + uint64_t(j) * nthreads;
+                if (p < P) {
+                    const double s = srow[p];
+                    if (s > K) {
+                        const double intrinsic = s - K;
+                        double continuation;
+                        if (!predict_continuation(model, degree, s / K, &continuation)) {
+                            atomicMin(&a.status->fit_predict_fail, ((unsigned long long)order << 32) | p);
+                        } else if (exercise_rule(plan.tie_rule, intrinsic, continuation)) {
+                            v[j] = intrinsic;
+                        }
+                    }
+                }
+            }
+            pivot = model.mean;
+        }
+        __syncthreads();
+    }
+    // Common origin decision (policy.rs:265-281): mean of values discounted to the origin.
+    if (plan.origin_row) {
+        double acc[2] = {0.0, 0.0};
+#pragma unroll
+        for (int j = 0; j < PPT; ++j) {
+            const uint64_t p = gtid + uint64_t(j) * nthreads;
+            if (p < P) {
+                const double w = v[j] * plan.origin_discount;
+                if (!fo_isfinite(w))
+                    atomicMin(&a.status->fit_payoff_fail, ((unsigned long long)order << 32) | p);
+                acc[0] += 1.0;
+                acc[1] += w;
+            }
+        }
+        cta_reduce_to<2>(acc, sm.red, parts + size_t(parity) * a.partial_stride + size_t(blockIdx.x) * 2);
+        if (!grid_barrier(&sm.local_gen, a.status)) return;
+        grid_combine<2>(parts + size_t(parity) * a.partial_stride, gridDim.x, sm.total);
+        if (blockIdx.x == 0 && threadIdx.x == 0) {
+            const double mean = dd_round(dd_div(sm.total[1], sm.total[0]));
+            const double intrinsic = plan.initial_spot - K > 0.0 ? plan.initial_spot - K : 0.0;
+            FitRecord& rec = a.records[0];
+            rec.kind = kRuleOrigin;
+            rec.origin_exercise = exercise_rule(plan.tie_rule, intrinsic, mean) ? 1 : 0;
+            rec.origin_continuation = mean;
+            rec.itm = 0;
+            rec.diag_status = -1;
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------------------------
+// K3: diagnostics for regression rows.
+// ---------------------------------------------------------------------------------------------
+
+__global__ void diagnose_kernel(DevicePlan plan, FitRecord* records) {
+    const uint32_t row = blockIdx.x * blockDim.x + threadIdx.x;
+    if (row + 1 >= plan.rows) return;
+    FitRecord& rec = records[row];
+    if (rec.kind != kRuleRegression) return;
+    int rank = 0, aux = 0;
+    double condition = 0.0;
+    rec.diag_status = diagnose_design(rec.model, plan.degree, plan.rank_tolerance, plan.condition_limit, &rank,
+                                      &condition, &aux);
+    rec.diag_rank = rank;
+    rec.diag_condition = condition;
+    rec.diag_aux = aux;
+}
+
+// ---------------------------------------------------------------------------------------------
+// K4: fused re-simulation + fixed-policy evaluation.
+// ---------------------------------------------------------------------------------------------
+
+struct EvalRow {
+    FitModel model;
+    int32_t kind;
+    int32_t pad;
+    double discount;
+};
+
+__global__ void __launch_bounds__(kEvalThreads) evaluate_kernel(EvalArgs a) {
+    extern __shared__ unsigned char eval_smem_raw[];
+    const DevicePlan& plan = a.plan;
+    const uint32_t rows = plan.rows;
+    double* sx = reinterpret_cast<double*>(eval_smem_raw);
+    double* sf = sx + 257;
+    double* red = sf + 257;                                      // [32 * 2]
+    EvalRow* rules = reinterpret_cast<EvalRow*>(red + 64);       // [rows]
+    unsigned* counts = reinterpret_cast<unsigned*>(rules + rows);    // [rows]
+    unsigned* itm_counts = counts + rows;                            // [rows]
+    for (uint32_t r = threadIdx.x; r < rows; r += blockDim.x) {
+        EvalRow er;
+        if (r + 1 < rows) {
+            er.model = a.records[r].model;
+            er.kind = a.records[r].kind;
+        } else {
+            er.kind = kRuleNone;
+        }
+        er.discount = plan.disc_to_origin[r];
+        rules[r] = er;
+        counts[r] = 0;
+        itm_counts[r] = 0;
+    }
+    load_zig_tables(sx, sf);
+    const SmemZig zig = make_zig(sx, sf);
+    const double K = plan.strike;
+    const uint64_t P = plan.eval_paths;
+    const int degree = plan.degree;
+    double sum = 0.0, sumsq = 0.0;
+    for (uint64_t p = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; p < P; p += uint64_t(gridDim.x) * blockDim.x) {
+        bool active = true;
+        double payoff = 0.0;
+        auto observe = [&](int row, double spot) {
+            if (!active) return;
+            const EvalRow& er = rules[row];
+            if (uint32_t(row) + 1 == rows) {
+                const double d = spot - K;
+                payoff = (d > 0.0 ? d : 0.0) * er.discount;
+                if (!fo_isfinite(payoff)) atomicMin(&a.status->eval_terminal_fail, (unsigned long long)p);
+                active = false;
+                atomicAdd(&counts[row], 1u);
+                return;
+            }
+            if (er.kind == kRuleNoSupport) {
+                if (spot > K) atomicAdd(&itm_counts[row], 1u);
+                return;
+            }
+            if (er.kind != kRuleRegression || !(spot > K)) return;
+            const double intrinsic = spot - K;
+            double continuation;
+            if (!predict_continuation(er.model, degree, spot / K, &continuation)) {
+                atomicMin(&a.status->eval_fail, ((unsigned long long)row << 33) | (p << 1));
+                return;
+            }
+            if (exercise_rule(plan.tie_rule, intrinsic, continuation)) {
+                payoff = intrinsic * er.discount;
+                if (!fo_isfinite(payoff))
+                    atomicMin(&a.status->eval_fail, ((unsigned long long)row << 33) | (p << 1) | 1ull);
+                active = false;
+                atomicAdd(&counts[row], 1u);
+            }
+        };
+        const SimResult r = simulate_path(plan, zig, plan.eval_seed, plan.eval_domain, uint32_t(p), observe);
+        if (r.code != 0) atomicMin(&a.status->eval_sim_fail, (unsigned long long)p);
+        sum += payoff;
+        sumsq += payoff * payoff;
+    }
+    double acc[2] = {sum, sumsq};
+    cta_reduce_to<2>(acc, red, a.partials + size_t(blockIdx.x) * 2);
+    for (uint32_t r = threadIdx.x; r < rows; r += blockDim.x) {
+        if (counts[r]) atomicAdd(&a.counts[r], counts[r]);
+        if (itm_counts[r]) atomicAdd(&a.itm_counts[r], itm_counts[r]);
+    }
+}
+
+// ---------------------------------------------------------------------------------------------
+// K5: price and standard error.
+// ---------------------------------------------------------------------------------------------
+
+__global__ void finalize_kernel(const double2* partials, int blocks, uint64_t paths, double* out) {
+    __shared__ dd total[2];
+    grid_combine<2>(partials, blocks, total);
+    if (threadIdx.x == 0) {
+        const dd n = dd_make(double(paths));
+        const dd mean = dd_div(total[0], n);
+        // M2 = sum x^2 - (sum x)^2 / n
+        dd m2 = dd_sub(total[1], dd_mul(total[0], mean));
+        if (m2.hi < 0.0) m2 = dd_make(0.0);
+        out[0] = dd_round(mean);
+        out[1] = dd_round(m2);
+        if (paths > 1) {
+            const dd var = dd_div(m2, dd_make(double(paths - 1)));
+            const double sd = dd_round(dd_sqrt(var));
+            out[2] = sd;
+            out[3] = sd / sqrt(double(paths));
+        } else {
+            out[2] = 0.0;
+            out[3] = 0.0;
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------------------------
+// Host-callable launchers
+// ---------------------------------------------------------------------------------------------
+
+cudaError_t launch_normals(uint64_t seed, uint32_t domain, uint32_t path_start, uint64_t paths, uint32_t count,
+                           double* out, unsigned long long* fail, cudaStream_t stream) {
+    const int threads = 256;
+    const uint64_t blocks = (paths + threads - 1) / threads;
+    normals_kernel<<<unsigned(blocks < 65535 * 16 ? blocks : 65535 * 16), threads, 0, stream>>>(
+        seed, domain, path_start, paths, count, out, fail);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_simulate(const DevicePlan& plan, uint64_t paths, uint64_t seed, uint32_t domain, double* out,
+                            uint32_t store_first_row, int reconstruct_escrowed, unsigned long long* fail,
+                            cudaStream_t stream) {
+    const int threads = 256;
+    uint64_t blocks = (paths + threads - 1) / threads;
+    if (blocks > (1u << 20)) blocks = 1u << 20;
+    simulate_kernel<<<unsigned(blocks), threads, 0, stream>>>(plan, paths, seed, domain, out, store_first_row,
+                                                               reconstruct_escrowed, fail);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_replay(const DevicePlan& plan, uint64_t seed, uint32_t domain, uint32_t path, int want_row,
+                          SimFailure* out, cudaStream_t stream) {
+    replay_kernel<<<1, 32, 0, stream>>>(plan, seed, domain, path, want_row, out);
+    return cudaGetLastError();
+}
+
+template <int PPT>
+static cudaError_t launch_backward_ppt(const BackwardArgs& args, int blocks, cudaStream_t stream) {
+    void* params[] = {const_cast<BackwardArgs*>(&args)};
+    return cudaLaunchCooperativeKernel((const void*)backward_kernel<PPT>, dim3(blocks), dim3(kBackwardThreads),
+                                       params, 0, stream);
+}
+
+int backward_max_blocks(int device) {
+    int per_sm = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, backward_kernel<32>, kBackwardThreads, 0);
+    int sms = 0;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+    int per_sm1 = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm1, backward_kernel<1>, kBackwardThreads, 0);
+    const int m = per_sm < per_sm1 ? per_sm : per_sm1;
+    return (m > 0 ? m : 1) * sms;
+}
+
+cudaError_t launch_backward(const BackwardArgs& args, int blocks, int ppt, cudaStream_t stream) {
+    switch (ppt) {
+        case 1: return launch_backward_ppt<1>(args, blocks, stream);
+        case 2: return launch_backward_ppt<2>(args, blocks, stream);
+        case 4: return launch_backward_ppt<4>(args, blocks, stream);
+        case 8: return launch_backward_ppt<8>(args, blocks, stream);
+        case 16: return launch_backward_ppt<16>(args, blocks, stream);
+        case 32: return launch_backward_ppt<32>(args, blocks, stream);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
+cudaError_t launch_diagnose(const DevicePlan& plan, FitRecord* records, cudaStream_t stream) {
+    const unsigned rows = plan.rows;
+    diagnose_kernel<<<(rows + 63) / 64, 64, 0, stream>>>(plan, records);
+    return cudaGetLastError();
+}
+
+size_t evaluate_smem_bytes(uint32_t rows) {
+    return sizeof(double) * (257 * 2 + 64) + sizeof(EvalRow) * rows + sizeof(unsigned) * 2 * rows;
+}
+
+cudaError_t launch_evaluate(const EvalArgs& args, int blocks, cudaStream_t stream) {
+    const size_t smem = evaluate_smem_bytes(args.plan.rows);
+    if (smem > 48 * 1024) {
+        cudaError_t e = cudaFuncSetAttribute(evaluate_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+        if (e != cudaSuccess) return e;
+    }
+    evaluate_kernel<<<blocks, kEvalThreads, smem, stream>>>(args);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_finalize(const double2* partials, int blocks, uint64_t paths, double* out, cudaStream_t stream) {
+    finalize_kernel<<<1, 64, 0, stream>>>(partials, blocks, paths, out);
+    return cudaGetLastError();
+}
+
+}  // namespace fo

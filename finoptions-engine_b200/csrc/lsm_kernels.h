@@ -1,0 +1,47 @@
+// lsm_kernels.h - launch interface of the single-contract LSM kernels (host <-> device).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stddef.h>
+#include <stdint.h>
+
+#include "lsm_device.cuh"
+
+namespace fo {
+
+constexpr int kBackwardThreads = 512;
+constexpr int kEvalThreads = 256;
+
+struct BackwardArgs {
+    DevicePlan plan;
+    const double* slab;          // stored training rows [rows - first_stored_row, paths]
+    double2* partials;           // [2][blocks][16] double-double CTA partials (ping-pong)
+    size_t partial_stride;       // doubles2 per ping-pong half
+    FitRecord* records;          // [rows]
+    DeviceStatus* status;
+};
+
+struct EvalArgs {
+    DevicePlan plan;
+    const FitRecord* records;
+    double2* partials;           // [blocks][2]
+    unsigned* counts;            // [rows] stopping counts
+    unsigned* itm_counts;        // [rows] active in-the-money paths at unsupported rows
+    DeviceStatus* status;
+};
+
+cudaError_t launch_normals(uint64_t seed, uint32_t domain, uint32_t path_start, uint64_t paths, uint32_t count,
+                           double* out, unsigned long long* fail, cudaStream_t stream);
+cudaError_t launch_simulate(const DevicePlan& plan, uint64_t paths, uint64_t seed, uint32_t domain, double* out,
+                            uint32_t store_first_row, int reconstruct_escrowed, unsigned long long* fail,
+                            cudaStream_t stream);
+cudaError_t launch_replay(const DevicePlan& plan, uint64_t seed, uint32_t domain, uint32_t path, int want_row,
+                          SimFailure* out, cudaStream_t stream);
+int backward_max_blocks(int device);
+cudaError_t launch_backward(const BackwardArgs& args, int blocks, int ppt, cudaStream_t stream);
+cudaError_t launch_diagnose(const DevicePlan& plan, FitRecord* records, cudaStream_t stream);
+size_t evaluate_smem_bytes(uint32_t rows);
+cudaError_t launch_evaluate(const EvalArgs& args, int blocks, cudaStream_t stream);
+cudaError_t launch_finalize(const double2* partials, int blocks, uint64_t paths, double* out, cudaStream_t stream);
+
+}  // namespace fo

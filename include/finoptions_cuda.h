@@ -56,6 +56,121 @@ typedef struct fo_error {
     char message[FO_ERROR_MESSAGE_CAPACITY];
 } fo_error;
 
+/* fo_error.code: which typed reference error a failure corresponds to. */
+typedef enum fo_error_code {
+    FO_CODE_NONE = 0,
+    /* InputError (crates/finoptions-core/src/error.rs) */
+    FO_CODE_EMPTY_TIME_GRID = 100,
+    FO_CODE_INVALID_TIME_ORIGIN,
+    FO_CODE_NON_FINITE_TIME,
+    FO_CODE_NON_INCREASING_TIME,
+    FO_CODE_TOO_MANY_NODES,
+    FO_CODE_NODE_OUT_OF_BOUNDS,
+    FO_CODE_CURVE_LENGTH_MISMATCH,
+    FO_CODE_INVALID_DISCOUNT_ORIGIN,
+    FO_CODE_NON_FINITE_LOG_DISCOUNT,
+    FO_CODE_UNREPRESENTABLE_INTERVAL_DISCOUNT,
+    FO_CODE_DIVIDEND_YIELD_CURVE_LENGTH_MISMATCH,
+    FO_CODE_INVALID_CUMULATIVE_DIVIDEND_YIELD_ORIGIN,
+    FO_CODE_INVALID_CUMULATIVE_DIVIDEND_YIELD,
+    FO_CODE_DECREASING_CUMULATIVE_DIVIDEND_YIELD,
+    FO_CODE_UNREPRESENTABLE_INTERVAL_DIVIDEND_YIELD,
+    FO_CODE_INVALID_CASH_DIVIDEND,
+    FO_CODE_INVALID_EXPIRY_NODE,
+    FO_CODE_DUPLICATE_DIVIDEND_NODE,
+    FO_CODE_UNORDERED_DIVIDEND_NODE,
+    FO_CODE_INVALID_DIVIDEND_NODE,
+    FO_CODE_DUPLICATE_EXERCISE_NODE,
+    FO_CODE_UNORDERED_EXERCISE_NODE,
+    FO_CODE_INVALID_EXERCISE_NODE,
+    FO_CODE_DIVIDEND_COLUMN_LENGTH_MISMATCH,
+    FO_CODE_INVALID_CONSTANT_VOLATILITY,
+    FO_CODE_UNSUPPORTED_ENUM,
+    /* SimulationError (crates/finoptions-sim/src/error.rs) */
+    FO_CODE_TIME_GRID_MISMATCH = 200,
+    FO_CODE_DIVIDEND_YIELD_TIME_GRID_MISMATCH,
+    FO_CODE_EMPTY_PATH_SET,
+    FO_CODE_RANDOM_PATH_NAMESPACE_OVERFLOW,
+    FO_CODE_INVALID_INITIAL_SPOT,
+    FO_CODE_NON_POSITIVE_ESCROWED_PREPAID_FORWARD,
+    FO_CODE_NON_FINITE_ESCROWED_PREPAID_CASH,
+    FO_CODE_NON_FINITE_ESCROWED_OBSERVATION,
+    FO_CODE_RANDOM_NORMAL_BUDGET_EXHAUSTED,
+    FO_CODE_RANDOM_NORMAL_REJECTION_LIMIT,
+    FO_CODE_NON_FINITE_PATH_TRANSITION,
+    FO_CODE_SHAPE_OVERFLOW,
+    /* RegressionError (crates/finoptions-lsm/src/error.rs:1-160) */
+    FO_CODE_UNSUPPORTED_DEGREE = 300,
+    FO_CODE_INVALID_RANK_TOLERANCE,
+    FO_CODE_INVALID_CONDITION_LIMIT,
+    FO_CODE_INSUFFICIENT_OBSERVATIONS,
+    FO_CODE_NON_FINITE_PREDICTOR,
+    FO_CODE_NON_FINITE_RESPONSE,
+    FO_CODE_DEGENERATE_PREDICTOR,
+    FO_CODE_RANK_DEFICIENT,
+    FO_CODE_CONDITION_LIMIT_EXCEEDED,
+    FO_CODE_CONDITION_DIAGNOSTIC_DID_NOT_CONVERGE,
+    FO_CODE_NON_FINITE_FIT,
+    FO_CODE_NON_FINITE_PREDICTION,
+    /* LsmError (crates/finoptions-lsm/src/error.rs:160-319) */
+    FO_CODE_INVALID_STRIKE = 400,
+    FO_CODE_LSM_INVALID_INITIAL_SPOT,
+    FO_CODE_PATH_COUNT_OUTSIDE_DOMAIN,
+    FO_CODE_UNREPRESENTABLE_OBSERVATION_DISCOUNT,
+    FO_CODE_EVALUATION_OUTSIDE_TRAINING_SUPPORT,
+    FO_CODE_NON_FINITE_DISCOUNTED_PAYOFF,
+    FO_CODE_RANDOM_DOMAIN_COLLISION,
+    /* BatchLsmError (crates/finoptions-lsm/src/batch/error.rs) */
+    FO_CODE_EMPTY_BATCH = 500,
+    FO_CODE_ROW_COUNT_MISMATCH,
+    FO_CODE_GROUP_OFFSET_COUNT_MISMATCH,
+    FO_CODE_GROUP_OFFSETS_DO_NOT_START_AT_ZERO,
+    FO_CODE_INVALID_GROUP_RANGE,
+    FO_CODE_GROUP_OFFSET_END_MISMATCH,
+    FO_CODE_INVALID_ROW_VALUE,
+    FO_CODE_EMPTY_BASE_INTERVALS,
+    FO_CODE_CASH_MESH_REQUIRES_CASH_DIVIDENDS,
+    FO_CODE_NEGATIVE_RATE_FOR_CASH_MESH,
+    FO_CODE_TERMINAL_CASH_FOR_CASH_MESH,
+    FO_CODE_EXPLICIT_EXERCISE_AT_OR_AFTER_MATURITY,
+    FO_CODE_INSUFFICIENT_EVALUATION_PATHS,
+    FO_CODE_BATCH_PATH_COUNT_OUTSIDE_DOMAIN,
+    FO_CODE_RANDOM_DOMAIN_RANGE_OVERFLOW,
+    FO_CODE_RANDOM_DOMAIN_RANGE_COLLISION,
+    FO_CODE_CASH_DIVIDEND_AFTER_MATURITY,
+    FO_CODE_CASH_DIVIDEND_AT_EXCLUDED_MATURITY,
+    FO_CODE_UNSUPPORTED_CASH_MATURITY_BOUNDARY,
+    FO_CODE_DUPLICATE_CASH_DIVIDEND_TIME,
+    FO_CODE_ESCROWED_NON_FINITE_PREPAID_CASH,
+    FO_CODE_ESCROWED_NON_POSITIVE_PREPAID_FORWARD,
+    FO_CODE_ESCROWED_INVALID_VOLATILITY,
+    FO_CODE_CONTRACT_MESH_SHAPE_OVERFLOW,
+    FO_CODE_EXPLICIT_CONTRACT_MESH_SHAPE_OVERFLOW,
+    FO_CODE_CASH_DIVIDEND_NODE_MISSING,
+    FO_CODE_EXPLICIT_EXERCISE_NODE_MISSING,
+    FO_CODE_STOPPING_COUNT_MISMATCH,
+    FO_CODE_MISSING_SAMPLING_DIAGNOSTIC,
+    /* BatchError (crates/finoptions-batch/src/error.rs) */
+    FO_CODE_INSUFFICIENT_OFFSETS = 600,
+    FO_CODE_EVENT_COLUMN_LENGTH_MISMATCH,
+    FO_CODE_NEGATIVE_OFFSET,
+    FO_CODE_DECREASING_OFFSET,
+    FO_CODE_OFFSET_SPAN_MISMATCH,
+    FO_CODE_OFFSET_INDEX_OVERFLOW,
+    FO_CODE_INVALID_EVENT_TIME,
+    FO_CODE_DECREASING_EVENT_TIME,
+    FO_CODE_INVALID_CASH_AMOUNT,
+    FO_CODE_INVALID_EXERCISE_TIME,
+    FO_CODE_NON_INCREASING_EXERCISE_TIME,
+    /* ExecutionError (device / executor) */
+    FO_CODE_NO_DEVICE = 700,
+    FO_CODE_UNSUPPORTED_DEVICE,
+    FO_CODE_CUDA_FAILURE,
+    FO_CODE_BARRIER_TIMEOUT,
+    FO_CODE_CAPACITY_EXCEEDED,
+    FO_CODE_INVALID_ARGUMENT
+} fo_error_code;
+
 /* ---- enums mirroring the reference's string enums (lib.rs:514-556) ------------------------ */
 
 typedef enum fo_dividend_policy {
@@ -292,6 +407,30 @@ int fo_simulate_gbm_seeded_f64(fo_executor* executor, const fo_gbm_seeded_reques
 int fo_sample_standard_normals_f64(fo_executor* executor, uint64_t seed, uint32_t domain,
                                    uint32_t path_start, uint64_t paths, uint32_t normals_per_path,
                                    double* out, uint64_t out_len, fo_error* err);
+
+/* ---- host-only validation (no device needed) ------------------------------------------------ */
+
+/* The reference's validate_* functions (crates/finoptions-python/src/lib.rs:405-473) used by the
+ * Python model constructors. They return FO_ERR_INPUT (or FO_ERR_BATCH for ragged buffers) with
+ * the reference's message on failure. */
+int fo_validate_cash_dividend_amount(double amount, fo_error* err);
+int fo_validate_constant_volatility(double annualized_decimal, fo_error* err);
+int fo_validate_event_schedule(const double* times, uint64_t n_times, const uint32_t* dividend_nodes,
+                               uint64_t n_dividend_nodes, const double* dividend_amounts,
+                               uint64_t n_dividend_amounts, const uint32_t* exercise_nodes,
+                               uint64_t n_exercise_nodes, uint32_t expiry_node, fo_error* err);
+int fo_validate_log_discount_curve(const double* times, uint64_t n_times, const double* log_discounts,
+                                   uint64_t n_log_discounts, fo_error* err);
+int fo_validate_cumulative_dividend_yield_curve(const double* times, uint64_t n_times,
+                                                const double* cumulative_yields, uint64_t n_yields,
+                                                fo_error* err);
+int fo_validate_ragged_cash_dividends(const int64_t* offsets, uint64_t n_offsets, const double* times,
+                                      uint64_t n_times, const double* amounts, uint64_t n_amounts,
+                                      fo_error* err);
+int fo_validate_ragged_exercise_times(const int64_t* offsets, uint64_t n_offsets, const double* times,
+                                      uint64_t n_times, fo_error* err);
+/* Runs every host-side check fo_price_lsm_call_f64 performs before touching a device. */
+int fo_validate_lsm_call_request(const fo_lsm_call_request* request, fo_error* err);
 
 /* ---- build identity ------------------------------------------------------------------------- */
 
