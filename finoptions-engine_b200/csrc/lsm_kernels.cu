@@ -53,9 +53,15 @@ __device__ __forceinline__ unsigned ld_volatile_u32(const unsigned* p) {
     return *(const volatile unsigned*)p;
 }
 
-// Bounded grid-wide barrier for a cooperatively launched grid (all CTAs co-resident). Gives up
-// after kBarrierSpinLimit polls, raising status->barrier_timeout; every CTA then leaves.
-constexpr unsigned long long kBarrierSpinLimit = 1ull << 25;
+__device__ __forceinline__ unsigned long long global_timer_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t));
+    return t;
+}
+
+// Bounded grid-wide barrier for a cooperatively launched grid (all CTAs co-resident). A waiting
+// CTA gives up after kBarrierTimeoutNs, raising status->barrier_timeout; every CTA then leaves.
+constexpr unsigned long long kBarrierTimeoutNs = 2000000000ull;
 
 __device__ bool grid_barrier(unsigned* local_gen, DeviceStatus* st) {
     unsigned* arrive = &st->arrive;
@@ -71,13 +77,16 @@ __device__ bool grid_barrier(unsigned* local_gen, DeviceStatus* st) {
             atomicExch(generation, gen + 1);
         } else {
             unsigned long long spins = 0;
+            const unsigned long long start = global_timer_ns();
             while (ld_acquire_gpu(generation) == gen) {
-                if (ld_volatile_u32(&st->barrier_timeout) != 0) break;
-                if (++spins > kBarrierSpinLimit) {
-                    atomicExch(&st->barrier_timeout, 1u);
-                    break;
+                if ((++spins & 1023u) == 0) {
+                    if (ld_volatile_u32(&st->barrier_timeout) != 0) break;
+                    if (global_timer_ns() - start > kBarrierTimeoutNs) {
+                        atomicExch(&st->barrier_timeout, 1u);
+                        break;
+                    }
+                    __nanosleep(32);
                 }
-                __nanosleep(64);
             }
         }
         __threadfence();
@@ -207,26 +216,51 @@ __global__ void replay_kernel(DevicePlan plan, uint64_t seed, uint32_t domain, u
 
 constexpr int kSlots = 16;  // T_0..T_8, U_0..U_4, non-finite count, spare
 
-// Warp sums in double, CTA combination in double-double; lane k of warp 0 writes slot k.
+__device__ __forceinline__ dd shfl_dd_down(dd v, int off);
+
+// Butterfly "transpose" reduction of S values across a warp: at each stage a lane keeps half of
+// its remaining values and adds its partner's copy of that half, so S values need S - 1 + log2
+// shuffles instead of 5 S. Lane l ends holding the warp total of value (l % S) (S a power of two
+// no larger than 32).
+template <int S>
+__device__ __forceinline__ double warp_transpose_reduce(double (&v)[S]) {
+    const int lane = threadIdx.x & 31;
+    double buf[S];
+#pragma unroll
+    for (int k = 0; k < S; ++k) buf[k] = v[k];
+#pragma unroll
+    for (int half = S / 2; half >= 1; half >>= 1) {
+        // partner offset = half; lanes with (lane & half) keep the upper half.
+        const bool upper = (lane & half) != 0;
+#pragma unroll
+        for (int k = 0; k < half; ++k) {
+            const double send = upper ? buf[k] : buf[k + half];
+            const double keep = upper ? buf[k + half] : buf[k];
+            buf[k] = keep + __shfl_xor_sync(0xffffffffu, send, half);
+        }
+    }
+    double total = buf[0];
+#pragma unroll
+    for (int off = S; off < 32; off <<= 1) total += __shfl_xor_sync(0xffffffffu, total, off);
+    return total;
+}
+
+__device__ __forceinline__ dd shfl_dd_down(dd v, int off);
+
+// Warp sums in double, then warp k combines slot k across the CTA's warps with a double-double
+// shuffle tree; lane 0 of warp k writes slot k of the CTA partial. Requires S <= warps per CTA.
 template <int S>
 __device__ __forceinline__ void cta_reduce_to(double (&acc)[S], double* smem /* [32 * S] */, double2* dst) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, warps = blockDim.x >> 5;
-#pragma unroll
-    for (int k = 0; k < S; ++k) {
-        double v = acc[k];
-#pragma unroll
-        for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
-        acc[k] = v;
-    }
-    if (lane == 0) {
-#pragma unroll
-        for (int k = 0; k < S; ++k) smem[warp * S + k] = acc[k];
-    }
+    const double total = warp_transpose_reduce<S>(acc);
+    // lane l holds value l % S: lanes 0..S-1 publish
+    if (lane < S) smem[warp * S + lane] = total;
     __syncthreads();
-    if (threadIdx.x < S) {
-        dd sum = dd_make(0.0);
-        for (int w = 0; w < warps; ++w) sum = dd_add(sum, dd_make(smem[w * S + threadIdx.x]));
-        dst[threadIdx.x] = make_double2(sum.hi, sum.lo);
+    if (warp < S) {
+        dd v = dd_make(lane < warps ? smem[lane * S + warp] : 0.0);
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) v = dd_add(v, shfl_dd_down(v, off));
+        if (lane == 0) dst[warp] = make_double2(v.hi, v.lo);
     }
     __syncthreads();
 }
@@ -272,112 +306,120 @@ __device__ __forceinline__ bool exercise_rule(int tie_rule, double intrinsic, do
     return tie_rule == 0 ? intrinsic > continuation : intrinsic >= continuation;
 }
 
-template <int PPT>
+// Each thread owns paths gtid + j * nthreads (j < ppt). Their discounted values, the current
+// row's spots and moneyness x = S/K live in this CTA's shared memory ([j * blockDim + tid]) for the
+// whole backward pass, so the only HBM traffic is one read of each stored row. One pass over the
+// shared arrays per row applies row k's exercise rule and immediately stages row k-1: load its
+// spots, discount the values (policy.rs:1049-1063) and accumulate its in-the-money power sums.
+struct RowSums {
+    double acc[kSlots];
+};
+
+__device__ __forceinline__ void accumulate_itm(RowSums& r, double x, double y, double pivot) {
+    const double t = x - pivot;
+    r.acc[0] += 1.0;
+    double pw = t;
+    r.acc[kPowerSums] += y;
+#pragma unroll
+    for (int k = 1; k < kPowerSums; ++k) {
+        r.acc[k] += pw;
+        if (k < kResponseSums) r.acc[kPowerSums + k] += y * pw;
+        pw *= t;
+    }
+}
+
 __global__ void __launch_bounds__(kBackwardThreads, 1) backward_kernel(BackwardArgs a) {
     __shared__ BackwardSmem sm;
+    extern __shared__ double backward_dyn[];
     const DevicePlan& plan = a.plan;
+    if (*(const volatile unsigned long long*)&a.status->train_sim_fail != kNone)
+        return;  // training simulation failed: every CTA reads the same word and leaves
     if (threadIdx.x == 0) {
         sm.local_gen = 0;
         sm.stop = 0;
     }
-    if (*(const volatile unsigned long long*)&a.status->train_sim_fail != kNone)
-        return;  // training simulation failed: every CTA reads the same word and leaves
-    __syncthreads();
+    const int ppt = a.ppt;
+    const int T = blockDim.x;
+    double* values = backward_dyn;
+    double* spots = backward_dyn + size_t(ppt) * T;
+    double* xs = backward_dyn + 2 * size_t(ppt) * T;  // S / K when in the money
     const uint64_t P = plan.train_paths;
-    const uint64_t nthreads = uint64_t(gridDim.x) * blockDim.x;
-    const uint64_t gtid = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    const uint64_t nthreads = uint64_t(gridDim.x) * T;
+    const uint64_t gtid = uint64_t(blockIdx.x) * T + threadIdx.x;
     const double K = plan.strike;
     const int degree = plan.degree;
     const uint32_t rows = plan.rows;
     const uint32_t E = rows - 1;
     const uint32_t fsr = plan.first_stored_row;
+    const int lowest = plan.origin_row ? 1 : 0;
     auto row_ptr = [&](uint32_t row) { return a.slab + uint64_t(row - fsr) * P; };
-
-    double v[PPT];
     {
         const double* terminal = row_ptr(E);
-#pragma unroll
-        for (int j = 0; j < PPT; ++j) {
+#pragma unroll 4
+        for (int j = 0; j < ppt; ++j) {
             const uint64_t p = gtid + uint64_t(j) * nthreads;
-            const double s = p < P ? __ldcs(&terminal[p]) : 0.0;
-            const double d = s - K;
-            v[j] = d > 0.0 ? d : 0.0;
+            double v = 0.0;
+            if (p < P) {
+                const double d = __ldcs(&terminal[p]) - K;
+                v = d > 0.0 ? d : 0.0;
+            }
+            values[j * T + threadIdx.x] = v;
         }
     }
-    double pivot = 0.0;
-    bool have_pivot = false;
-    uint32_t order = 0;
-    const uint32_t lowest = plan.origin_row ? 1u : 0u;
     double2* parts = a.partials;
     int parity = 0;
-    for (int row = int(E) - 1; row >= int(lowest); --row, ++order) {
+    uint32_t order = 0;
+    int row = int(E) - 1;
+    double pivot = 1.0;
+    RowSums sums;
+#pragma unroll
+    for (int k = 0; k < kSlots; ++k) sums.acc[k] = 0.0;
+    if (row >= lowest) {
+        // Stage the first fitted row and locate its in-the-money mean (the moment pivot).
         const double disc = plan.disc_from_later[row];
         const double* srow = row_ptr(uint32_t(row));
-        // discount (policy.rs:1049-1063)
-#pragma unroll
-        for (int j = 0; j < PPT; ++j) {
+        double loc[2] = {0.0, 0.0};
+#pragma unroll 4
+        for (int j = 0; j < ppt; ++j) {
             const uint64_t p = gtid + uint64_t(j) * nthreads;
+            const int at = j * T + threadIdx.x;
+            double sp = 0.0, x = 0.0;
             if (p < P) {
-                v[j] *= disc;
-                if (!fo_isfinite(v[j]))
-                    atomicMin(&a.status->fit_payoff_fail, ((unsigned long long)order << 32) | p);
-            }
-        }
-        if (!have_pivot) {
-            // One-off location pass for the first fitted row: pivot = in-the-money mean moneyness.
-            double acc[2] = {0.0, 0.0};
-#pragma unroll
-            for (int j = 0; j < PPT; ++j) {
-                const uint64_t p = gtid + uint64_t(j) * nthreads;
-                if (p < P) {
-                    const double s = srow[p];
-                    if (s > K) {
-                        const double x = s / K;
-                        if (fo_isfinite(x)) {
-                            acc[0] += 1.0;
-                            acc[1] += x;
-                        }
+                sp = __ldcs(&srow[p]);
+                const double v = values[at] * disc;
+                values[at] = v;
+                if (!fo_isfinite(v)) atomicMin(&a.status->fit_payoff_fail, ((unsigned long long)order << 32) | p);
+                if (sp > K) {
+                    x = sp / K;
+                    if (fo_isfinite(x)) {
+                        loc[0] += 1.0;
+                        loc[1] += x;
                     }
                 }
             }
-            cta_reduce_to<2>(acc, sm.red, parts + size_t(parity) * a.partial_stride + size_t(blockIdx.x) * 2);
-            if (!grid_barrier(&sm.local_gen, a.status)) return;
-            grid_combine<2>(parts + size_t(parity) * a.partial_stride, gridDim.x, sm.total);
-            parity ^= 1;
-            pivot = sm.total[0].hi > 0.0 ? dd_round(dd_div(sm.total[1], sm.total[0])) : 1.0;
-            have_pivot = true;
+            spots[at] = sp;
+            xs[at] = x;
         }
-        // In-the-money power sums about the pivot.
-        double acc[kSlots];
-#pragma unroll
-        for (int k = 0; k < kSlots; ++k) acc[k] = 0.0;
-#pragma unroll
-        for (int j = 0; j < PPT; ++j) {
-            const uint64_t p = gtid + uint64_t(j) * nthreads;
-            if (p < P) {
-                const double s = srow[p];
-                if (s > K) {
-                    const double x = s / K;
-                    const double y = v[j];
-                    if (!fo_isfinite(x) || !fo_isfinite(y)) {
-                        acc[14] += 1.0;
-                        atomicMin(&a.status->fit_nonfinite, ((unsigned long long)order << 32) | p);
-                    } else {
-                        const double t = x - pivot;
-                        acc[0] += 1.0;
-                        double pw = t;
-                        acc[kPowerSums] += y;
-#pragma unroll
-                        for (int k = 1; k < kPowerSums; ++k) {
-                            acc[k] += pw;
-                            if (k < kResponseSums) acc[kPowerSums + k] += y * pw;
-                            pw *= t;
-                        }
-                    }
+        cta_reduce_to<2>(loc, sm.red, parts + size_t(parity) * a.partial_stride + size_t(blockIdx.x) * 2);
+        if (!grid_barrier(&sm.local_gen, a.status)) return;
+        grid_combine<2>(parts + size_t(parity) * a.partial_stride, gridDim.x, sm.total);
+        parity ^= 1;
+        if (sm.total[0].hi > 0.0) pivot = dd_round(dd_div(sm.total[1], sm.total[0]));
+        for (int j = 0; j < ppt; ++j) {
+            const int at = j * T + threadIdx.x;
+            if (spots[at] > K) {
+                const double x = xs[at], y = values[at];
+                if (!fo_isfinite(x) || !fo_isfinite(y)) {
+                    sums.acc[14] += 1.0;
+                    atomicMin(&a.status->fit_nonfinite, ((unsigned long long)order << 32) | (gtid + uint64_t(j) * nthreads));
+                } else {
+                    accumulate_itm(sums, x, y, pivot);
                 }
             }
         }
-        cta_reduce_to<kSlots>(acc, sm.red, parts + size_t(parity) * a.partial_stride + size_t(blockIdx.x) * kSlots);
+    }
+    for (; row >= lowest; --row, ++order) {
+        cta_reduce_to<kSlots>(sums.acc, sm.red, parts + size_t(parity) * a.partial_stride + size_t(blockIdx.x) * kSlots);
         if (!grid_barrier(&sm.local_gen, a.status)) return;
         grid_combine<kSlots>(parts + size_t(parity) * a.partial_stride, gridDim.x, sm.total);
         parity ^= 1;
@@ -394,7 +436,7 @@ __global__ void __launch_bounds__(kBackwardThreads, 1) backward_kernel(BackwardA
             } else if (population < required || bad > 0) {
                 kind = kRuleFitFailed;  // InsufficientObservations / non-finite population
             } else {
-                fit_from_moments(sm.total, pivot, itm, degree, plan.rank_tolerance, &sm.model);
+                fit_continuation(sm.total, pivot, itm, degree, plan.rank_tolerance, &sm.model);
                 kind = sm.model.status == kFitOk ? kRuleRegression : kRuleFitFailed;
             }
             sm.kind = kind;
@@ -413,36 +455,61 @@ __global__ void __launch_bounds__(kBackwardThreads, 1) backward_kernel(BackwardA
         __syncthreads();
         const int kind = sm.kind;
         if (kind == kRuleFitFailed) return;  // identical decision in every CTA
-        if (kind == kRuleRegression) {
-            const FitModel& model = sm.model;  // read from shared memory
+        const bool regression = kind == kRuleRegression;
+        const FitModel& model = sm.model;  // read from shared memory
+        if (regression) pivot = model.mean;
+        const bool stage_next = row - 1 >= lowest;
+        const double disc = stage_next ? plan.disc_from_later[row - 1] : 1.0;
+        const double* srow = stage_next ? row_ptr(uint32_t(row - 1)) : nullptr;
 #pragma unroll
-            for (int j = 0; j < PPT; ++j) {
-                const uint64_t p = gtid + uint64_t(j) * nthreads;
-                if (p < P) {
-                    const double s = srow[p];
-                    if (s > K) {
-                        const double intrinsic = s - K;
-                        double continuation;
-                        if (!predict_continuation(model, degree, s / K, &continuation)) {
-                            atomicMin(&a.status->fit_predict_fail, ((unsigned long long)order << 32) | p);
-                        } else if (exercise_rule(plan.tie_rule, intrinsic, continuation)) {
-                            v[j] = intrinsic;
-                        }
+        for (int k = 0; k < kSlots; ++k) sums.acc[k] = 0.0;
+#pragma unroll 2
+        for (int j = 0; j < ppt; ++j) {
+            const uint64_t p = gtid + uint64_t(j) * nthreads;
+            const int at = j * T + threadIdx.x;
+            double v = values[at];
+            if (regression) {
+                const double sp = spots[at];
+                if (sp > K) {
+                    const double intrinsic = sp - K;
+                    double continuation;
+                    if (!predict_continuation(model, degree, xs[at], &continuation)) {
+                        atomicMin(&a.status->fit_predict_fail, ((unsigned long long)order << 32) | p);
+                    } else if (exercise_rule(plan.tie_rule, intrinsic, continuation)) {
+                        v = intrinsic;
                     }
                 }
             }
-            pivot = model.mean;
+            if (stage_next) {
+                double sp = 0.0, x = 0.0;
+                if (p < P) {
+                    sp = __ldcs(&srow[p]);
+                    v *= disc;
+                    if (!fo_isfinite(v))
+                        atomicMin(&a.status->fit_payoff_fail, ((unsigned long long)(order + 1) << 32) | p);
+                    if (sp > K) {
+                        x = sp / K;
+                        if (!fo_isfinite(x) || !fo_isfinite(v)) {
+                            sums.acc[14] += 1.0;
+                            atomicMin(&a.status->fit_nonfinite, ((unsigned long long)(order + 1) << 32) | p);
+                        } else {
+                            accumulate_itm(sums, x, v, pivot);
+                        }
+                    }
+                }
+                spots[at] = sp;
+                xs[at] = x;
+            }
+            values[at] = v;
         }
-        __syncthreads();
     }
     // Common origin decision (policy.rs:265-281): mean of values discounted to the origin.
     if (plan.origin_row) {
         double acc[2] = {0.0, 0.0};
-#pragma unroll
-        for (int j = 0; j < PPT; ++j) {
+        for (int j = 0; j < ppt; ++j) {
             const uint64_t p = gtid + uint64_t(j) * nthreads;
             if (p < P) {
-                const double w = v[j] * plan.origin_discount;
+                const double w = values[j * T + threadIdx.x] * plan.origin_discount;
                 if (!fo_isfinite(w))
                     atomicMin(&a.status->fit_payoff_fail, ((unsigned long long)order << 32) | p);
                 acc[0] += 1.0;
@@ -494,7 +561,7 @@ struct EvalRow {
     double discount;
 };
 
-__global__ void __launch_bounds__(kEvalThreads) evaluate_kernel(EvalArgs a) {
+__global__ void __launch_bounds__(kEvalThreads, 3) evaluate_kernel(EvalArgs a) {
     extern __shared__ unsigned char eval_smem_raw[];
     const DevicePlan& plan = a.plan;
     const uint32_t rows = plan.rows;
@@ -626,34 +693,39 @@ cudaError_t launch_replay(const DevicePlan& plan, uint64_t seed, uint32_t domain
     return cudaGetLastError();
 }
 
-template <int PPT>
-static cudaError_t launch_backward_ppt(const BackwardArgs& args, int blocks, cudaStream_t stream) {
-    void* params[] = {const_cast<BackwardArgs*>(&args)};
-    return cudaLaunchCooperativeKernel((const void*)backward_kernel<PPT>, dim3(blocks), dim3(kBackwardThreads),
-                                       params, 0, stream);
+size_t backward_smem_bytes(int ppt) { return sizeof(double) * 3 * size_t(ppt) * kBackwardThreads; }
+
+int backward_max_ppt() {
+    // Dynamic shared memory available next to the kernel's static shared memory.
+    cudaFuncAttributes attr{};
+    cudaFuncGetAttributes(&attr, backward_kernel);
+    int optin = 0, device = 0;
+    cudaGetDevice(&device);
+    cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device);
+    const size_t avail = size_t(optin) > attr.sharedSizeBytes ? size_t(optin) - attr.sharedSizeBytes : 0;
+    return int(avail / (sizeof(double) * 3 * kBackwardThreads));
 }
 
 int backward_max_blocks(int device) {
-    int per_sm = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, backward_kernel<32>, kBackwardThreads, 0);
     int sms = 0;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
-    int per_sm1 = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm1, backward_kernel<1>, kBackwardThreads, 0);
-    const int m = per_sm < per_sm1 ? per_sm : per_sm1;
-    return (m > 0 ? m : 1) * sms;
+    return sms;  // one 1024-thread CTA per SM; the dynamic shared memory keeps it at one
 }
 
 cudaError_t launch_backward(const BackwardArgs& args, int blocks, int ppt, cudaStream_t stream) {
-    switch (ppt) {
-        case 1: return launch_backward_ppt<1>(args, blocks, stream);
-        case 2: return launch_backward_ppt<2>(args, blocks, stream);
-        case 4: return launch_backward_ppt<4>(args, blocks, stream);
-        case 8: return launch_backward_ppt<8>(args, blocks, stream);
-        case 16: return launch_backward_ppt<16>(args, blocks, stream);
-        case 32: return launch_backward_ppt<32>(args, blocks, stream);
-        default: return cudaErrorInvalidValue;
-    }
+    const size_t smem = backward_smem_bytes(ppt);
+    cudaError_t e = cudaFuncSetAttribute(backward_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+    if (e != cudaSuccess) return e;
+    int per_sm = 0;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, backward_kernel, kBackwardThreads, smem);
+    if (e != cudaSuccess) return e;
+    int device = 0, sms = 0;
+    cudaGetDevice(&device);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+    if (per_sm < 1 || blocks > per_sm * sms) return cudaErrorCooperativeLaunchTooLarge;
+    void* params[] = {const_cast<BackwardArgs*>(&args)};
+    return cudaLaunchCooperativeKernel((const void*)backward_kernel, dim3(blocks), dim3(kBackwardThreads), params, smem,
+                                       stream);
 }
 
 cudaError_t launch_diagnose(const DevicePlan& plan, FitRecord* records, cudaStream_t stream) {

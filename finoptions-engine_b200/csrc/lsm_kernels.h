@@ -19,6 +19,7 @@ struct BackwardArgs {
     size_t partial_stride;       // doubles2 per ping-pong half
     FitRecord* records;          // [rows]
     DeviceStatus* status;
+    int ppt;                     // paths per thread (values and spots staged in shared memory)
 };
 
 struct EvalArgs {
@@ -38,6 +39,8 @@ cudaError_t launch_simulate(const DevicePlan& plan, uint64_t paths, uint64_t see
 cudaError_t launch_replay(const DevicePlan& plan, uint64_t seed, uint32_t domain, uint32_t path, int want_row,
                           SimFailure* out, cudaStream_t stream);
 int backward_max_blocks(int device);
+int backward_max_ppt();
+size_t backward_smem_bytes(int ppt);
 cudaError_t launch_backward(const BackwardArgs& args, int blocks, int ppt, cudaStream_t stream);
 cudaError_t launch_diagnose(const DevicePlan& plan, FitRecord* records, cudaStream_t stream);
 size_t evaluate_smem_bytes(uint32_t rows);
