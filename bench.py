@@ -1,0 +1,392 @@
+#!/usr/bin/env python
+"""LSM path-steps/s on one B200: the 52-node weekly single-contract workload.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Workload (one "step" = pricing one contract end to end: training simulation, backward policy fit,
+independent evaluation): S0 = K = 100, T = 1, 53-node weekly grid t_i = i/52, exercise at nodes
+0..51 (the origin is a common decision) plus expiry 52, log-discounts -0.04 t, cumulative
+continuous yield 0.02 t, sigma = 0.25, 2^20 training + 2^20 evaluation paths (Philox seed 11,
+domains 1 / 2), degree-4 regression, rank tolerance 1e-12, condition limit 1e8, strictly-greater
+ties, insufficient support = fail. path-steps per step = (2^20 + 2^20) * 52 intervals.
+
+`value` is timed on the device (CUDA events around K launches of a resident plan); `e2e` is the
+same metric through the public API finoptions.price_lsm_call with host inputs and host results.
+Multi-GPU runs are independent replicas (a single contract does not shard): value = all ranks'
+path-steps / max-over-ranks time. `--impl reference` times the CPU restatement of the reference
+engine on the host cores on a bounded sample of the same workload.
+"""
+
+from __future__ import annotations
+
+import argparse
+import ctypes
+import json
+import os
+import statistics
+import sys
+import threading
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT / "finoptions-engine_b200"))
+sys.path.insert(0, str(ROOT / "tests"))
+
+STEPS_IN_GRID = 52
+PATHS = 1 << 20
+METRIC = "lsm_path_steps_per_s"
+UNIT = "path-steps/s"
+KERNEL_NAMES = ("simulate_kernel", "backward_kernel", "diagnose_kernel", "evaluate_kernel", "finalize_kernel")
+
+
+def workload_kwargs(paths: int = PATHS) -> dict:
+    t = [i / STEPS_IN_GRID for i in range(STEPS_IN_GRID + 1)]
+    return dict(
+        initial_spot=100.0, strike=100.0, schedule_times=t, curve_times=t,
+        log_discounts=[0.0 if i == 0 else -0.04 * t[i] for i in range(STEPS_IN_GRID + 1)],
+        dividend_yield_times=t,
+        cumulative_dividend_yields=[0.0 if i == 0 else 0.02 * t[i] for i in range(STEPS_IN_GRID + 1)],
+        dividend_nodes=[], dividend_amounts=[], exercise_nodes=list(range(STEPS_IN_GRID)),
+        expiry_node=STEPS_IN_GRID, annualized_volatility=0.25, dividend_policy=0, training_paths=paths,
+        evaluation_paths=paths, training_seed=11, training_domain=1, evaluation_seed=11, evaluation_domain=2,
+        polynomial_degree=4, rank_tolerance=1e-12, condition_limit=1e8, tie_rule=0, insufficient_exercise_support=0,
+    )
+
+
+def path_steps(paths: int = PATHS) -> int:
+    return 2 * paths * STEPS_IN_GRID
+
+
+CONFIG = {
+    "workload": "weekly single-contract LSM call: S0=K=100, T=1, 52 weekly intervals, exercise nodes 0..51 + expiry",
+    "contract": "r=0.04 (log-discount -r t), continuous yield q=0.02, sigma=0.25, degree 4",
+    "training_paths": PATHS,
+    "evaluation_paths": PATHS,
+    "streams": "Philox seed 11, domains 1 (training) / 2 (evaluation)",
+    "global_batch": 1,
+    "path_steps_per_step": path_steps(),
+    "parallelism": "replicas",
+    "l2": "working set > L2: 436 MB of stored training rows per step vs 126 MB L2",
+}
+
+
+# ---- helpers -----------------------------------------------------------------------------------
+
+
+def dist_info() -> tuple[int, int, int]:
+    return int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("LOCAL_RANK", "0"))
+
+
+class ClockSampler:
+    """Samples SM clocks and throttle reasons through NVML while the timed region runs."""
+
+    REASONS = {
+        "gpu_idle": 0x1, "applications_clocks_setting": 0x2, "sw_power_cap": 0x4, "hw_slowdown": 0x8,
+        "sync_boost": 0x10, "sw_thermal_slowdown": 0x20, "hw_thermal_slowdown": 0x40,
+        "hw_power_brake_slowdown": 0x80, "display_clock_setting": 0x100,
+    }
+
+    def __init__(self, device: int, period: float = 0.05) -> None:
+        self.device = device
+        self.period = period
+        self.samples: list[int] = []
+        self.reasons: set[str] = set()
+        self.max_mhz = None
+        self._stop = threading.Event()
+        self._thread = None
+        try:
+            import pynvml
+
+            pynvml.nvmlInit()
+            self._nvml = pynvml
+            self._handle = pynvml.nvmlDeviceGetHandleByIndex(device)
+            self.max_mhz = pynvml.nvmlDeviceGetMaxClockInfo(self._handle, pynvml.NVML_CLOCK_SM)
+        except Exception:  # noqa: BLE001 - clocks are reported as unavailable
+            self._nvml = None
+
+    def sample(self) -> None:
+        if self._nvml is None:
+            return
+        nv = self._nvml
+        self.samples.append(nv.nvmlDeviceGetClockInfo(self._handle, nv.NVML_CLOCK_SM))
+        mask = nv.nvmlDeviceGetCurrentClocksEventReasons(self._handle)
+        for name, bit in self.REASONS.items():
+            if mask & bit and name != "gpu_idle":
+                self.reasons.add(name)
+
+    def _run(self) -> None:
+        while not self._stop.is_set():
+            self.sample()
+            self._stop.wait(self.period)
+
+    def __enter__(self) -> ClockSampler:
+        self._thread = threading.Thread(target=self._run, daemon=True)
+        self._thread.start()
+        return self
+
+    def __exit__(self, *exc: object) -> None:
+        self._stop.set()
+        if self._thread:
+            self._thread.join()
+
+    def report(self) -> dict:
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": self.max_mhz, "reasons": ["unavailable"]}
+        return {"sm_mhz": statistics.median(self.samples), "sm_max_mhz": self.max_mhz, "reasons": sorted(self.reasons),
+                "samples": len(self.samples)}
+
+
+def measured_peaks() -> tuple[float, str]:
+    path = ROOT / "MEASURED_PEAKS.json"
+    if path.is_file():
+        return float(json.loads(path.read_text())["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def profiled_traffic(kernel: str) -> float | None:
+    """DRAM bytes per stored path-row for `kernel` from the committed ncu summary, if present."""
+    path = ROOT / "profiles" / "traffic.json"
+    if not path.is_file():
+        return None
+    data = json.loads(path.read_text())
+    entry = data.get(kernel)
+    return None if entry is None else float(entry["dram_bytes_per_path_row"])
+
+
+def cpu_threads() -> int:
+    return len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else (os.cpu_count() or 1)
+
+
+def oracle_price(kwargs: dict, threads: int) -> tuple:
+    import _oracle
+    from finoptions._requests import lsm_call_request
+
+    return _oracle.price_lsm_call(lsm_call_request(**kwargs), threads)
+
+
+# ---- our arm -----------------------------------------------------------------------------------
+
+
+def run_ours(args: argparse.Namespace) -> dict | None:
+    import torch
+
+    rank, world, local = dist_info()
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    from finoptions import _abi
+    from finoptions._native import CudaExecutor
+    from finoptions._requests import lsm_call_request, lsm_call_result
+
+    lib = _abi.load()
+    executor = CudaExecutor(local)
+    kwargs = workload_kwargs()
+    request = lsm_call_request(**kwargs)
+    err = _abi.FoError()
+    plan = ctypes.c_void_p()
+    status = lib.fo_lsm_call_plan_create(executor.raw, ctypes.byref(request.struct), ctypes.byref(plan), ctypes.byref(err))
+    if status:
+        raise RuntimeError(err.message.decode())
+    kernels = ctypes.c_uint64()
+    lib.fo_lsm_call_plan_kernel_count(plan, ctypes.byref(kernels))
+    h2d, d2h = ctypes.c_uint64(), ctypes.c_uint64()
+    lib.fo_lsm_call_plan_transfer_bytes(plan, ctypes.byref(h2d), ctypes.byref(d2h))
+    elapsed = ctypes.c_double()
+    kernel_ms = (ctypes.c_double * 8)()
+
+    def timed(iterations: int, per_kernel: bool) -> float:
+        st = lib.fo_lsm_call_plan_time_launches(plan, iterations, ctypes.byref(elapsed),
+                                                kernel_ms if per_kernel else None, 8, ctypes.byref(err))
+        if st:
+            raise RuntimeError(err.message.decode())
+        return elapsed.value
+
+    timed(args.warmup, False)
+    # Device-timed region: K launches between CUDA events on the plan's stream.
+    clocks = ClockSampler(local)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with clocks:
+        device_ms = timed(args.steps, False)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+        t = torch.tensor([device_ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        device_ms = float(t.item())
+    # Per-kernel device times (separate pass with events between kernels).
+    timed(max(1, min(args.steps, 20)), True)
+    per_kernel = {KERNEL_NAMES[k]: kernel_ms[k] for k in range(int(kernels.value))}
+    per_kernel_launches = max(1, min(args.steps, 20))
+    result = lsm_call_result(request.exercise_rows)
+    st = lib.fo_lsm_call_plan_collect(plan, ctypes.byref(result.struct), ctypes.byref(err))
+    if st:
+        raise RuntimeError(err.message.decode())
+    price, _, _, se, *_ = result.as_tuple()
+    lib.fo_lsm_call_plan_destroy(plan)
+
+    # End to end through the public API: host inputs in, host results out, every step.
+    import finoptions as fo
+
+    times = tuple(kwargs["schedule_times"])
+    schedule = fo.EventSchedule(times=times, dividends=(), exercise_nodes=tuple(kwargs["exercise_nodes"]),
+                                expiry_node=kwargs["expiry_node"])
+    api_args = dict(
+        initial_spot=kwargs["initial_spot"], strike=kwargs["strike"], schedule=schedule,
+        curve=fo.LogDiscountCurve(times=times, log_discounts=tuple(kwargs["log_discounts"])),
+        dividend_yield_curve=fo.CumulativeDividendYieldCurve(times=times,
+                                                             cumulative_yields=tuple(kwargs["cumulative_dividend_yields"])),
+        volatility=fo.ConstantVolatility(kwargs["annualized_volatility"]),
+        dividend_policy=fo.DividendPolicy.LIQUIDATOR, executor=fo.CudaExecutor(device=local),
+        method=fo.Lsm(training_paths=PATHS, evaluation_paths=PATHS, training_stream=fo.RandomStream(seed=11, domain=1),
+                      evaluation_stream=fo.RandomStream(seed=11, domain=2),
+                      insufficient_exercise_support=fo.InsufficientExerciseSupportPolicy.FAIL),
+    )
+    for _ in range(args.warmup):
+        fo.price_lsm_call(**api_args)
+    e2e_steps = max(1, min(args.steps, 100))
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        api_result = fo.price_lsm_call(**api_args)
+    torch.cuda.synchronize()
+    e2e_s = time.perf_counter() - t0
+    if dist:
+        t = torch.tensor([e2e_s], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+        dist.barrier()
+        dist.destroy_process_group()
+    if api_result.price != price:
+        raise RuntimeError("public API and resident plan disagree")
+    if rank != 0:
+        return None
+
+    ms_per_step = device_ms / args.steps
+    value = world * path_steps() * args.steps / (device_ms / 1e3)
+    # Roofline of the dominant path-data kernel: stored rows are written once (simulate) and read
+    # once (backward); algorithmic bytes = 8 B per stored path-row.
+    stored_rows = STEPS_IN_GRID  # rows 1..52 (the origin row is the constant S0, never stored)
+    algorithmic = 8 * stored_rows * PATHS
+    hbm_peak, peak_kind = measured_peaks()
+    roofline_all = {}
+    for name in KERNEL_NAMES[: int(kernels.value)]:
+        ms = per_kernel[name] / per_kernel_launches
+        bytes_per_launch = algorithmic if name in ("simulate_kernel", "backward_kernel") else 0
+        roofline_all[name] = {
+            "ms_per_launch": round(ms, 4),
+            "share": round(per_kernel[name] / sum(per_kernel.values()), 4),
+            "algorithmic_bytes": bytes_per_launch,
+            "achieved_gbs": round(bytes_per_launch / (ms / 1e3) / 1e9, 1) if bytes_per_launch else 0.0,
+        }
+    dominant = max(("simulate_kernel", "backward_kernel"), key=lambda k: per_kernel[k])
+    dom_ms = per_kernel[dominant] / per_kernel_launches
+    achieved = algorithmic / (dom_ms / 1e3) / 1e9
+    traffic_unit = profiled_traffic(dominant)
+    out = {
+        "metric": METRIC,
+        "value": value,
+        "unit": UNIT,
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": ms_per_step,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f64",
+        "data": "synthetic (seeded Philox paths of the configured contract)",
+        "config": dict(CONFIG, contracts_per_s=world * args.steps / (device_ms / 1e3)),
+        "e2e": {
+            "value": world * path_steps() * e2e_steps / e2e_s,
+            "unit": UNIT,
+            "h2d_bytes_per_step": int(h2d.value),
+            "d2h_bytes_per_step": int(d2h.value),
+            "api": "finoptions.price_lsm_call(executor=CudaExecutor)",
+        },
+        "gpu_launches": int(kernels.value) * args.steps,
+        "roofline": {
+            "kernel": dominant,
+            "bound": "hbm",
+            "achieved": round(achieved, 1),
+            "peak": hbm_peak,
+            "peak_source": peak_kind,
+            "unit": "GB/s",
+            "frac": round(achieved / hbm_peak, 4),
+            "traffic": None if traffic_unit is None else int(traffic_unit * stored_rows * PATHS),
+        },
+        "kernels": roofline_all,
+        "clocks": clocks.report(),
+        "result": {"price": price, "standard_error": se},
+    }
+    if world == 1:
+        out["cpu_baseline"] = cpu_baseline()
+    return out
+
+
+def cpu_baseline() -> dict:
+    """The CPU restatement of the reference engine (path-parallel simulation on every host thread,
+    serial fit and evaluation per contract) on one full contract of the workload."""
+    threads = cpu_threads()
+    kwargs = workload_kwargs()
+    oracle_price(workload_kwargs(1 << 14), threads)  # load + warm
+    t0 = time.perf_counter()
+    oracle_price(kwargs, threads)
+    seconds = time.perf_counter() - t0
+    return {"value": path_steps() / seconds, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"one full contract of the workload ({seconds:.2f} s on {threads} threads)"}
+
+
+# ---- reference arm -----------------------------------------------------------------------------
+
+
+def run_reference(args: argparse.Namespace) -> dict | None:
+    rank, world, _ = dist_info()
+    if rank != 0:
+        return None
+    threads = cpu_threads()
+    sample_paths = 1 << 18
+    kwargs = workload_kwargs(sample_paths)
+    for _ in range(args.warmup):
+        oracle_price(kwargs, threads)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        oracle_price(kwargs, threads)
+    seconds = time.perf_counter() - t0
+    value = path_steps(sample_paths) * args.steps / seconds
+    sample = (f"each step prices the workload contract at 2^18 + 2^18 paths (1/4 of a full step) on {threads} "
+              "host threads with the CPU restatement of the reference engine (the Rust reference cannot be built here)")
+    return {
+        "metric": METRIC, "value": value, "unit": UNIT, "impl": "reference", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": seconds / args.steps * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": CONFIG,
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+
+
+def main() -> None:
+    parser = argparse.ArgumentParser(description=__doc__.splitlines()[0])
+    parser.add_argument("--gpus", type=int, default=1)
+    parser.add_argument("--steps", type=int, default=200)
+    parser.add_argument("--warmup", type=int, default=5)
+    parser.add_argument("--impl", choices=("ours", "reference"), default="ours")
+    args = parser.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    out = run_reference(args) if args.impl == "reference" else run_ours(args)
+    if out is not None:
+        print(json.dumps(out))
+
+
+if __name__ == "__main__":
+    main()

@@ -123,6 +123,12 @@ struct fo_lsm_call_plan {
     void* h_out = nullptr;
     DevicePlan dp{};
     bool launched = false;
+    cudaEvent_t marks[8] = {};   // per-kernel timing marks (created on first timed launch)
+    bool timing = false;
+    ~fo_lsm_call_plan() {
+        for (cudaEvent_t& e : marks)
+            if (e) cudaEventDestroy(e);
+    }
 };
 
 namespace {
@@ -313,10 +319,13 @@ Error plan_launch(fo_lsm_call_plan* plan) {
     auto* records = reinterpret_cast<FitRecord*>(dev + L.records);
     FO_CUDA_TRY(cudaMemsetAsync(dev + L.out, 0, L.out_bytes, s), "reset");
     FO_CUDA_TRY(cudaMemsetAsync(status, 0xff, kStatusNoneBytes, s), "reset");
+    auto mark = [&](int i) -> cudaError_t { return plan->timing ? cudaEventRecord(plan->marks[i], s) : cudaSuccess; };
+    FO_CUDA_TRY(mark(0), "event");
     // K1 training simulation
     FO_CUDA_TRY(launch_simulate(plan->dp, plan->hp.train_paths, plan->hp.train_seed, plan->hp.train_domain, plan->d_slab,
                                 plan->first_stored_row, plan->hp.escrowed ? 1 : 0, &status->train_sim_fail, s),
                 "training simulation launch");
+    FO_CUDA_TRY(mark(1), "event");
     // K2 backward induction
     BackwardArgs b{};
     b.plan = plan->dp;
@@ -327,8 +336,10 @@ Error plan_launch(fo_lsm_call_plan* plan) {
     b.status = status;
     b.ppt = plan->ppt;
     FO_CUDA_TRY(launch_backward(b, plan->backward_blocks, plan->ppt, s), "backward launch");
+    FO_CUDA_TRY(mark(2), "event");
     // K3 diagnostics
     FO_CUDA_TRY(launch_diagnose(plan->dp, records, s), "diagnose launch");
+    FO_CUDA_TRY(mark(3), "event");
     if (plan->run_eval) {
         EvalArgs a{};
         a.plan = plan->dp;
@@ -338,15 +349,51 @@ Error plan_launch(fo_lsm_call_plan* plan) {
         a.itm_counts = reinterpret_cast<unsigned*>(dev + L.itm_counts);
         a.status = status;
         FO_CUDA_TRY(launch_evaluate(a, plan->eval_blocks, s), "evaluation launch");
+        FO_CUDA_TRY(mark(4), "event");
         FO_CUDA_TRY(launch_finalize(a.partials, plan->eval_blocks, plan->hp.eval_paths,
                                     reinterpret_cast<double*>(dev + L.result), s),
                     "finalize launch");
+        FO_CUDA_TRY(mark(5), "event");
     }
     plan->launched = true;
     return Error{};
 }
 
 uint64_t kernels_per_launch(const fo_lsm_call_plan* plan) { return plan->run_eval ? 5 : 3; }
+
+Error plan_time_launches(fo_lsm_call_plan* plan, uint32_t iterations, double* elapsed_ms, double* kernel_ms,
+                         uint64_t capacity) {
+    cudaStream_t s = plan->ex->stream;
+    for (cudaEvent_t& e : plan->marks)
+        if (!e) FO_CUDA_TRY(cudaEventCreate(&e), "cudaEventCreate");
+    const uint64_t kernels = kernels_per_launch(plan);
+    std::vector<double> sums(kernels, 0.0);
+    cudaEvent_t begin = plan->marks[6], end = plan->marks[7];
+    FO_CUDA_TRY(cudaEventRecord(begin, s), "event");
+    double total = 0.0;
+    for (uint32_t i = 0; i < iterations; ++i) {
+        plan->timing = kernel_ms != nullptr;
+        Error e = plan_launch(plan);
+        plan->timing = false;
+        if (!e.ok()) return e;
+        if (kernel_ms) {
+            FO_CUDA_TRY(cudaEventSynchronize(plan->marks[kernels]), "event");
+            for (uint64_t k = 0; k < kernels; ++k) {
+                float ms = 0.f;
+                FO_CUDA_TRY(cudaEventElapsedTime(&ms, plan->marks[k], plan->marks[k + 1]), "event");
+                sums[k] += ms;
+            }
+        }
+    }
+    FO_CUDA_TRY(cudaEventRecord(end, s), "event");
+    FO_CUDA_TRY(cudaEventSynchronize(end), "event");
+    float ms = 0.f;
+    FO_CUDA_TRY(cudaEventElapsedTime(&ms, begin, end), "event");
+    total = ms;
+    *elapsed_ms = total;
+    for (uint64_t k = 0; kernel_ms && k < kernels && k < capacity; ++k) kernel_ms[k] = sums[k];
+    return Error{};
+}
 
 std::string node_str(uint32_t node) { return std::to_string(node); }
 
@@ -695,6 +742,23 @@ int fo_lsm_call_plan_collect(fo_lsm_call_plan* plan, fo_lsm_call_result* result,
     std::lock_guard<std::mutex> lock(plan->ex->mu);
     cudaSetDevice(plan->ex->device);
     return finish(err, plan_collect(plan, result));
+}
+
+int fo_lsm_call_plan_time_launches(fo_lsm_call_plan* plan, uint32_t iterations, double* elapsed_ms, double* kernel_ms,
+                                   uint64_t kernel_capacity, fo_error* err) {
+    Error e = require(plan, "plan");
+    if (e.ok()) e = require(elapsed_ms, "elapsed_ms");
+    if (!e.ok()) return finish(err, e);
+    std::lock_guard<std::mutex> lock(plan->ex->mu);
+    cudaSetDevice(plan->ex->device);
+    return finish(err, plan_time_launches(plan, iterations, elapsed_ms, kernel_ms, kernel_capacity));
+}
+
+int fo_lsm_call_plan_transfer_bytes(const fo_lsm_call_plan* plan, uint64_t* h2d_bytes, uint64_t* d2h_bytes) {
+    if (!plan || !h2d_bytes || !d2h_bytes) return FO_ERR_EXECUTION;
+    *h2d_bytes = plan->lay.inputs_bytes;
+    *d2h_bytes = plan->lay.out_bytes;
+    return FO_OK;
 }
 
 int fo_lsm_call_plan_kernel_count(const fo_lsm_call_plan* plan, uint64_t* kernels) {

@@ -190,6 +190,8 @@ EXPORTED_SYMBOLS: Final = (
     "fo_lsm_call_plan_create",
     "fo_lsm_call_plan_launch",
     "fo_lsm_call_plan_collect",
+    "fo_lsm_call_plan_time_launches",
+    "fo_lsm_call_plan_transfer_bytes",
     "fo_lsm_call_plan_kernel_count",
     "fo_lsm_call_plan_stream",
     "fo_lsm_call_plan_destroy",
@@ -220,6 +222,10 @@ def _declare(lib: ctypes.CDLL) -> None:
     lib.fo_lsm_call_plan_launch.restype = ctypes.c_int
     lib.fo_lsm_call_plan_collect.argtypes = [vp, ctypes.POINTER(FoLsmCallResult), err]
     lib.fo_lsm_call_plan_collect.restype = ctypes.c_int
+    lib.fo_lsm_call_plan_time_launches.argtypes = [vp, ctypes.c_uint32, c_double_p, c_double_p, ctypes.c_uint64, err]
+    lib.fo_lsm_call_plan_time_launches.restype = ctypes.c_int
+    lib.fo_lsm_call_plan_transfer_bytes.argtypes = [vp, ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ctypes.c_uint64)]
+    lib.fo_lsm_call_plan_transfer_bytes.restype = ctypes.c_int
     lib.fo_lsm_call_plan_kernel_count.argtypes = [vp, ctypes.POINTER(ctypes.c_uint64)]
     lib.fo_lsm_call_plan_kernel_count.restype = ctypes.c_int
     lib.fo_lsm_call_plan_stream.argtypes = [vp, ctypes.POINTER(vp)]

@@ -307,6 +307,14 @@ int fo_lsm_call_plan_create(fo_executor* executor, const fo_lsm_call_request* re
                             fo_lsm_call_plan** out, fo_error* err);
 int fo_lsm_call_plan_launch(fo_lsm_call_plan* plan, fo_error* err);
 int fo_lsm_call_plan_collect(fo_lsm_call_plan* plan, fo_lsm_call_result* result, fo_error* err);
+/* Enqueues `iterations` launches of the plan bracketed by CUDA events on the plan's stream, waits
+ * for them, and returns the elapsed device time in milliseconds. When kernel_ms is not NULL it
+ * receives, per kernel of one launch (in launch order, at most kernel_capacity entries), the device
+ * time summed over the iterations. Results stay on the device; collect reads the last launch. */
+int fo_lsm_call_plan_time_launches(fo_lsm_call_plan* plan, uint32_t iterations, double* elapsed_ms,
+                                   double* kernel_ms, uint64_t kernel_capacity, fo_error* err);
+/* Bytes one fo_price_lsm_call_f64 of this request copies host->device and device->host. */
+int fo_lsm_call_plan_transfer_bytes(const fo_lsm_call_plan* plan, uint64_t* h2d_bytes, uint64_t* d2h_bytes);
 /* Number of kernels one launch enqueues (for launch accounting). */
 int fo_lsm_call_plan_kernel_count(const fo_lsm_call_plan* plan, uint64_t* kernels);
 /* The cudaStream_t (as void*) the plan's kernels run on. */
