@@ -1,0 +1,64 @@
+"""The device regression solve, compiled for the host, against the oracle's sequential
+Stieltjes fit (regression.rs:369-523) on in-the-money populations of realistic shape."""
+
+from __future__ import annotations
+
+import ctypes
+import subprocess
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+import _oracle
+
+HERE = Path(__file__).resolve().parent
+BUILD = HERE.parent / "oracle" / "_build"
+
+
+@pytest.fixture(scope="module")
+def harness() -> ctypes.CDLL:
+    BUILD.mkdir(parents=True, exist_ok=True)
+    lib = BUILD / "libsolve_harness.so"
+    src = HERE / "native" / "solve_harness.cpp"
+    if not lib.is_file() or lib.stat().st_mtime < max(src.stat().st_mtime, (HERE.parent / "finoptions-engine_b200" / "csrc" / "fo_core.cuh").stat().st_mtime):
+        subprocess.run(["g++", "-O2", "-std=c++17", "-ffp-contract=off", "-fPIC", "-shared", str(src), "-o", str(lib)],
+                       check=True)
+    h = ctypes.CDLL(str(lib))
+    h.harness_fit.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint64, ctypes.c_double, ctypes.c_int,
+                              ctypes.c_int, ctypes.c_void_p]
+    return h
+
+
+def population(rng: np.random.Generator, n: int, sigma: float, moneyness: float) -> tuple[np.ndarray, np.ndarray]:
+    s = 100.0 * np.exp(sigma * rng.standard_normal(4 * n))
+    k = 100.0 * moneyness
+    s = s[s > k][:n]
+    y = np.maximum(s * np.exp(0.3 * sigma * rng.standard_normal(s.size)) - k, 0.0) * 0.99
+    return s / k, y
+
+
+@pytest.mark.parametrize("degree", [0, 1, 2, 3, 4])
+def test_one_pass_moment_solve_matches_the_sequential_reference_fit(harness, degree) -> None:
+    rng = np.random.default_rng(17 + degree)
+    worst = 0.0
+    for trial in range(24):
+        n = 40 + trial * 7 if trial % 3 == 0 else 20000
+        x, y = population(rng, n, 0.05 + 0.07 * (trial % 7), 0.7 + 0.1 * (trial % 5))
+        code, model, _ = _oracle.fit_regression(x, y, degree)
+        if code != 0:
+            continue
+        for offset in (-1.5, -0.3, 0.0, 0.4, 1.5):  # pivot distance from the mean, in scales
+            pivot = (1.2 if degree == 0 else model[0]) + offset * model[1]
+            ours = np.zeros(22)
+            status = harness.harness_fit(x.ctypes.data, y.ctypes.data, x.size, pivot, degree, 4, ours.ctypes.data)
+            assert status // 10 == 0 and status % 10 == 0, status
+            assert ours[20] == model[20]  # rank
+            assert abs(ours[21] - model[21]) <= 1e-8 * model[21]
+            if degree:
+                assert abs(ours[0] - model[0]) <= 1e-13 * abs(model[0])
+                assert abs(ours[1] - model[1]) <= 1e-12 * model[1]
+            reference = _oracle.predict(model, degree, x)
+            predicted = _oracle.predict(ours, degree, x)
+            worst = max(worst, float(np.max(np.abs(predicted - reference)) / np.max(np.abs(reference))))
+    assert worst <= 1e-12
