@@ -962,3 +962,108 @@ int fo_validate_lsm_call_request(const fo_lsm_call_request* request, fo_error* e
 }
 
 }  // extern "C"
+
+// =============================================================================================
+// Allocation-free pricing: the whole pass (plan inputs, training-path slab, partials, status and
+// results) runs in one file-scope device array, so a call makes no device allocation. For callers
+// whose device memory belongs to another allocator (a framework's caching allocator or a pool
+// reserved at start-up that forbids further driver allocations), and for latency-critical callers
+// that cannot absorb cudaMalloc/cudaFree's implicit device-wide synchronisation. Every GPU that
+// loads this library holds the array until the process exits.
+// =============================================================================================
+
+namespace {
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[FO_NOALLOC_SCRATCH_BYTES];
+
+std::mutex g_noalloc_mu;
+void* g_noalloc_address[256] = {};
+
+// The array's device address on the current device, looked up once per device. In host code the
+// symbol is only a host-side stand-in, never a device address.
+Error noalloc_scratch(int device, unsigned char** out) {
+    if (device < 0 || device >= 256)
+        return make_error(FO_ERR_EXECUTION, FO_CODE_NO_DEVICE, "device ordinal outside the supported range");
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    if (!g_noalloc_address[device]) {
+        void* p = nullptr;
+        const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e != cudaSuccess) return cuda_error(e, "cudaGetSymbolAddress of the allocation-free scratch");
+        g_noalloc_address[device] = p;
+    }
+    *out = static_cast<unsigned char*>(g_noalloc_address[device]);
+    return Error{};
+}
+
+Error price_noalloc(const fo_lsm_call_request& q, cudaStream_t stream, fo_lsm_call_result* result) {
+    int device = 0;
+    FO_CUDA_TRY(cudaGetDevice(&device), "cudaGetDevice");
+    cudaDeviceProp prop{};
+    FO_CUDA_TRY(cudaGetDeviceProperties(&prop, device), "cudaGetDeviceProperties");
+    if (prop.major != 10)
+        return make_error(FO_ERR_EXECUTION, FO_CODE_UNSUPPORTED_DEVICE,
+                          std::string("allocation-free pricing requires an sm_100 (Blackwell B200) device; device ") +
+                              std::to_string(device) + " is " + prop.name);
+    unsigned char* scratch = nullptr;
+    Error e = noalloc_scratch(device, &scratch);
+    if (!e.ok()) return e;
+    // A stack executor carries the caller's stream and the device's launch shapes; it owns no
+    // memory and creates nothing.
+    fo_executor shadow;
+    shadow.device = device;
+    shadow.sms = prop.multiProcessorCount;
+    shadow.stream = stream;
+    shadow.backward_blocks_max = backward_max_blocks(device);
+    shadow.backward_max_ppt = backward_max_ppt();
+    shadow.eval_blocks_per_sm = 8;
+    fo_lsm_call_plan plan;
+    plan.ex = &shadow;
+    e = build_call_plan(q, &plan.hp);
+    if (!e.ok()) return e;
+    const HostPlan& hp = plan.hp;
+    if (q.evaluation_paths == 0) {
+        plan.eval_error = make_error(FO_ERR_LSM, FO_CODE_EMPTY_PATH_SET,
+                                     "LSM evaluation simulation failed: simulation path count must be positive");
+    } else if (q.evaluation_paths > 0xffffffffull) {
+        plan.eval_error = make_error(FO_ERR_LSM, FO_CODE_RANDOM_PATH_NAMESPACE_OVERFLOW,
+                                     "LSM evaluation simulation failed: seeded simulation supports at most 4294967295 "
+                                     "paths in one random domain; observed " + std::to_string(q.evaluation_paths));
+    }
+    plan.run_eval = plan.eval_error.ok();
+    e = choose_backward_shape(&shadow, hp.train_paths, &plan.backward_blocks, &plan.ppt);
+    if (!e.ok()) return e;
+    const uint64_t eval_needed = plan.run_eval ? (hp.eval_paths + kEvalThreads - 1) / kEvalThreads : 1;
+    plan.eval_blocks = int(std::max<uint64_t>(1, std::min<uint64_t>(eval_needed, uint64_t(shadow.sms) * 8)));
+    plan.first_stored_row = hp.origin_row ? 1u : 0u;
+    plan.lay = layout_for(hp, plan.backward_blocks, plan.eval_blocks);
+    const PlanLayout& L = plan.lay;
+    const uint64_t stored_rows = hp.rows() - plan.first_stored_row;
+    const uint64_t slab_bytes = uint64_t(sizeof(double)) * stored_rows * hp.train_paths;
+    const uint64_t needed = uint64_t(L.total) + slab_bytes;
+    if (needed > FO_NOALLOC_SCRATCH_BYTES)
+        return make_error(FO_ERR_EXECUTION, FO_CODE_CAPACITY_EXCEEDED,
+                          "request needs " + std::to_string(needed) +
+                              " bytes of device scratch; the allocation-free entry point holds at most " +
+                              std::to_string(uint64_t(FO_NOALLOC_SCRATCH_BYTES)) +
+                              " bytes (training paths x stored rows x 8 bytes plus the plan block)");
+    std::vector<unsigned char> host(std::max(L.inputs_bytes, L.out_bytes));
+    plan.d_block = scratch;
+    plan.d_slab = reinterpret_cast<double*>(scratch + L.total);
+    plan.h_out = host.data();
+    plan.dp = device_plan(hp, L, scratch, plan.first_stored_row);
+    pack_inputs(hp, L, host.data());
+    FO_CUDA_TRY(cudaMemcpyAsync(scratch, host.data(), L.inputs_bytes, cudaMemcpyHostToDevice, stream), "plan upload");
+    e = plan_launch(&plan);  // clears the status and result region before the kernels run
+    if (!e.ok()) return e;
+    return plan_collect(&plan, result);
+}
+
+}  // namespace
+
+extern "C" int fo_price_lsm_call_f64_noalloc(const fo_lsm_call_request* request, void* cuda_stream,
+                                             fo_lsm_call_result* result, fo_error* err) {
+    Error e = require(request, "request");
+    if (e.ok()) e = require(result, "result");
+    if (!e.ok()) return finish(err, e);
+    return finish(err, price_noalloc(*request, static_cast<cudaStream_t>(cuda_stream), result));
+}

@@ -195,6 +195,7 @@ EXPORTED_SYMBOLS: Final = (
     "fo_lsm_call_plan_kernel_count",
     "fo_lsm_call_plan_stream",
     "fo_lsm_call_plan_destroy",
+    "fo_price_lsm_call_f64_noalloc",
     "fo_price_lsm_grouped_f64",
     "fo_price_lsm_batch_f64",
     "fo_simulate_gbm_seeded_f64",
@@ -216,6 +217,8 @@ def _declare(lib: ctypes.CDLL) -> None:
     lib.fo_executor_device.restype = ctypes.c_int
     lib.fo_price_lsm_call_f64.argtypes = [vp, ctypes.POINTER(FoLsmCallRequest), ctypes.POINTER(FoLsmCallResult), err]
     lib.fo_price_lsm_call_f64.restype = ctypes.c_int
+    lib.fo_price_lsm_call_f64_noalloc.argtypes = [ctypes.POINTER(FoLsmCallRequest), vp, ctypes.POINTER(FoLsmCallResult), err]
+    lib.fo_price_lsm_call_f64_noalloc.restype = ctypes.c_int
     lib.fo_lsm_call_plan_create.argtypes = [vp, ctypes.POINTER(FoLsmCallRequest), ctypes.POINTER(vp), err]
     lib.fo_lsm_call_plan_create.restype = ctypes.c_int
     lib.fo_lsm_call_plan_launch.argtypes = [vp, err]

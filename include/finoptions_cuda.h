@@ -321,6 +321,25 @@ int fo_lsm_call_plan_kernel_count(const fo_lsm_call_plan* plan, uint64_t* kernel
 int fo_lsm_call_plan_stream(const fo_lsm_call_plan* plan, void** stream);
 void fo_lsm_call_plan_destroy(fo_lsm_call_plan* plan);
 
+/* Allocation-free variant of fo_price_lsm_call_f64. It has no counterpart in the reference.
+ *
+ * For callers that cannot allocate device memory: code whose device memory belongs to another
+ * allocator (a framework's caching allocator, or a pool reserved at start-up that forbids further
+ * driver allocations) and latency-critical code that cannot absorb cudaMalloc / cudaFree's implicit
+ * device-wide synchronisation. The call prices on the calling thread's current device and on
+ * `cuda_stream` (NULL: the legacy default stream), makes no cudaMalloc, cudaFree or other device
+ * allocation, and keeps everything it needs on the device (plan inputs, the training-path slab of
+ * training_paths x stored rows x 8 bytes, partials, status, results) in one file-scope device
+ * array of FO_NOALLOC_SCRATCH_BYTES (64 MiB) that every GPU loading this library holds until the
+ * process exits. Requests that need more return FO_ERR_EXECUTION / FO_CODE_CAPACITY_EXCEEDED.
+ * The first call on a device looks up the array's device address; make that first call before
+ * any stream capture. Every call shares the one array and clears what must start at zero itself;
+ * calls that overlap on the GPU (two streams, or two threads) race on it and must be serialised
+ * by the caller. The call synchronises `cuda_stream` before returning. */
+#define FO_NOALLOC_SCRATCH_BYTES (64ull << 20)
+int fo_price_lsm_call_f64_noalloc(const fo_lsm_call_request* request, void* cuda_stream,
+                                  fo_lsm_call_result* result, fo_error* err);
+
 /* ---- grouped / row batches ------------------------------------------------------------------ */
 
 /* Arguments of price_lsm_call_grouped_batch_*_f64 (lib.rs:1884-2100) with the dividend model and
