@@ -1,14 +1,15 @@
 #!/usr/bin/env python
 """LSM path-steps/s on one B200: the 52-node weekly single-contract workload.
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--paths P]
 
 Workload (one "step" = pricing one contract end to end: training simulation, backward policy fit,
 independent evaluation): S0 = K = 100, T = 1, 53-node weekly grid t_i = i/52, exercise at nodes
 0..51 (the origin is a common decision) plus expiry 52, log-discounts -0.04 t, cumulative
 continuous yield 0.02 t, sigma = 0.25, 2^20 training + 2^20 evaluation paths (Philox seed 11,
 domains 1 / 2), degree-4 regression, rank tolerance 1e-12, condition limit 1e8, strictly-greater
-ties, insufficient support = fail. path-steps per step = (2^20 + 2^20) * 52 intervals.
+ties, insufficient support = fail. path-steps per step = (2^20 + 2^20) * 52 intervals. `--paths`
+shrinks both populations for small profiler captures; the headline run keeps 2^20.
 
 `value` is timed on the device (CUDA events around K launches of a resident plan); `e2e` is the
 same metric through the public API finoptions.price_lsm_call with host inputs and host results.
@@ -58,17 +59,18 @@ def path_steps(paths: int = PATHS) -> int:
     return 2 * paths * STEPS_IN_GRID
 
 
-CONFIG = {
-    "workload": "weekly single-contract LSM call: S0=K=100, T=1, 52 weekly intervals, exercise nodes 0..51 + expiry",
-    "contract": "r=0.04 (log-discount -r t), continuous yield q=0.02, sigma=0.25, degree 4",
-    "training_paths": PATHS,
-    "evaluation_paths": PATHS,
-    "streams": "Philox seed 11, domains 1 (training) / 2 (evaluation)",
-    "global_batch": 1,
-    "path_steps_per_step": path_steps(),
-    "parallelism": "replicas",
-    "l2": "working set > L2: 436 MB of stored training rows per step vs 126 MB L2",
-}
+def config(paths: int = PATHS) -> dict:
+    return {
+        "workload": "weekly single-contract LSM call: S0=K=100, T=1, 52 weekly intervals, exercise nodes 0..51 + expiry",
+        "contract": "r=0.04 (log-discount -r t), continuous yield q=0.02, sigma=0.25, degree 4",
+        "training_paths": paths,
+        "evaluation_paths": paths,
+        "streams": "Philox seed 11, domains 1 (training) / 2 (evaluation)",
+        "global_batch": 1,
+        "path_steps_per_step": path_steps(paths),
+        "parallelism": "replicas",
+        "l2": f"working set vs L2: {8 * STEPS_IN_GRID * paths / 1e6:.0f} MB of stored training rows per step, 126 MB L2",
+    }
 
 
 # ---- helpers -----------------------------------------------------------------------------------
@@ -186,7 +188,8 @@ def run_ours(args: argparse.Namespace) -> dict | None:
 
     lib = _abi.load()
     executor = CudaExecutor(local)
-    kwargs = workload_kwargs()
+    paths = args.paths
+    kwargs = workload_kwargs(paths)
     request = lsm_call_request(**kwargs)
     err = _abi.FoError()
     plan = ctypes.c_void_p()
@@ -245,7 +248,7 @@ def run_ours(args: argparse.Namespace) -> dict | None:
                                                              cumulative_yields=tuple(kwargs["cumulative_dividend_yields"])),
         volatility=fo.ConstantVolatility(kwargs["annualized_volatility"]),
         dividend_policy=fo.DividendPolicy.LIQUIDATOR, executor=fo.CudaExecutor(device=local),
-        method=fo.Lsm(training_paths=PATHS, evaluation_paths=PATHS, training_stream=fo.RandomStream(seed=11, domain=1),
+        method=fo.Lsm(training_paths=paths, evaluation_paths=paths, training_stream=fo.RandomStream(seed=11, domain=1),
                       evaluation_stream=fo.RandomStream(seed=11, domain=2),
                       insufficient_exercise_support=fo.InsufficientExerciseSupportPolicy.FAIL),
     )
@@ -272,11 +275,11 @@ def run_ours(args: argparse.Namespace) -> dict | None:
         return None
 
     ms_per_step = device_ms / args.steps
-    value = world * path_steps() * args.steps / (device_ms / 1e3)
+    value = world * path_steps(paths) * args.steps / (device_ms / 1e3)
     # Roofline of the dominant path-data kernel: stored rows are written once (simulate) and read
     # once (backward); algorithmic bytes = 8 B per stored path-row.
     stored_rows = STEPS_IN_GRID  # rows 1..52 (the origin row is the constant S0, never stored)
-    algorithmic = 8 * stored_rows * PATHS
+    algorithmic = 8 * stored_rows * paths
     hbm_peak, peak_kind = measured_peaks()
     roofline_all = {}
     for name in KERNEL_NAMES[: int(kernels.value)]:
@@ -305,9 +308,9 @@ def run_ours(args: argparse.Namespace) -> dict | None:
         "vs_baseline": None,
         "dtype": "f64",
         "data": "synthetic (seeded Philox paths of the configured contract)",
-        "config": dict(CONFIG, contracts_per_s=world * args.steps / (device_ms / 1e3)),
+        "config": dict(config(paths), contracts_per_s=world * args.steps / (device_ms / 1e3)),
         "e2e": {
-            "value": world * path_steps() * e2e_steps / e2e_s,
+            "value": world * path_steps(paths) * e2e_steps / e2e_s,
             "unit": UNIT,
             "h2d_bytes_per_step": int(h2d.value),
             "d2h_bytes_per_step": int(d2h.value),
@@ -322,27 +325,27 @@ def run_ours(args: argparse.Namespace) -> dict | None:
             "peak_source": peak_kind,
             "unit": "GB/s",
             "frac": round(achieved / hbm_peak, 4),
-            "traffic": None if traffic_unit is None else int(traffic_unit * stored_rows * PATHS),
+            "traffic": None if traffic_unit is None else int(traffic_unit * stored_rows * paths),
         },
         "kernels": roofline_all,
         "clocks": clocks.report(),
         "result": {"price": price, "standard_error": se},
     }
     if world == 1:
-        out["cpu_baseline"] = cpu_baseline()
+        out["cpu_baseline"] = cpu_baseline(paths)
     return out
 
 
-def cpu_baseline() -> dict:
+def cpu_baseline(paths: int = PATHS) -> dict:
     """The CPU restatement of the reference engine (path-parallel simulation on every host thread,
     serial fit and evaluation per contract) on one full contract of the workload."""
     threads = cpu_threads()
-    kwargs = workload_kwargs()
+    kwargs = workload_kwargs(paths)
     oracle_price(workload_kwargs(1 << 14), threads)  # load + warm
     t0 = time.perf_counter()
     oracle_price(kwargs, threads)
     seconds = time.perf_counter() - t0
-    return {"value": path_steps() / seconds, "unit": UNIT, "cores": threads, "kind": "port",
+    return {"value": path_steps(paths) / seconds, "unit": UNIT, "cores": threads, "kind": "port",
             "sample": f"one full contract of the workload ({seconds:.2f} s on {threads} threads)"}
 
 
@@ -368,7 +371,7 @@ def run_reference(args: argparse.Namespace) -> dict | None:
     return {
         "metric": METRIC, "value": value, "unit": UNIT, "impl": "reference", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": seconds / args.steps * 1e3, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": CONFIG,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": config(),
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
@@ -380,7 +383,10 @@ def main() -> None:
     parser.add_argument("--steps", type=int, default=200)
     parser.add_argument("--warmup", type=int, default=5)
     parser.add_argument("--impl", choices=("ours", "reference"), default="ours")
+    parser.add_argument("--paths", type=int, default=PATHS, help="paths per role (profiling captures shrink it)")
     args = parser.parse_args()
+    if args.paths < 2:
+        parser.error("--paths must be at least 2")
     if args.warmup < 3:
         args.warmup = 3
     out = run_reference(args) if args.impl == "reference" else run_ours(args)
