@@ -13,6 +13,7 @@
 #include <vector>
 
 #include "../../include/finoptions_cuda.h"
+#include "executor.h"
 #include "host.h"
 #include "lsm_kernels.h"
 
@@ -26,73 +27,7 @@ namespace {
 
 constexpr unsigned long long kNone = ~0ull;
 
-Error cuda_error(cudaError_t e, const char* what) {
-    return make_error(FO_ERR_EXECUTION, FO_CODE_CUDA_FAILURE,
-                      std::string("CUDA failure in ") + what + ": " + cudaGetErrorName(e) + " (" + cudaGetErrorString(e) + ")");
-}
-
-#define FO_CUDA_TRY(expr, what)                        \
-    do {                                               \
-        cudaError_t _e = (expr);                       \
-        if (_e != cudaSuccess) return cuda_error(_e, what); \
-    } while (0)
-
-// Grow-only device buffer.
-struct DeviceBuffer {
-    void* ptr = nullptr;
-    size_t bytes = 0;
-    Error reserve(size_t need) {
-        if (need <= bytes) return Error{};
-        if (ptr) cudaFree(ptr);
-        ptr = nullptr;
-        bytes = 0;
-        const size_t grow = std::max(need, size_t(1) << 20);
-        cudaError_t e = cudaMalloc(&ptr, grow);
-        if (e != cudaSuccess) return cuda_error(e, "cudaMalloc");
-        bytes = grow;
-        return Error{};
-    }
-    ~DeviceBuffer() {
-        if (ptr) cudaFree(ptr);
-    }
-};
-
-// Grow-only pinned host buffer.
-struct PinnedBuffer {
-    void* ptr = nullptr;
-    size_t bytes = 0;
-    Error reserve(size_t need) {
-        if (need <= bytes) return Error{};
-        if (ptr) cudaFreeHost(ptr);
-        ptr = nullptr;
-        bytes = 0;
-        const size_t grow = std::max(need, size_t(1) << 16);
-        cudaError_t e = cudaMallocHost(&ptr, grow);
-        if (e != cudaSuccess) return cuda_error(e, "cudaMallocHost");
-        bytes = grow;
-        return Error{};
-    }
-    ~PinnedBuffer() {
-        if (ptr) cudaFreeHost(ptr);
-    }
-};
-
-size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
-
 }  // namespace
-
-struct fo_executor {
-    int device = 0;
-    int sms = 0;
-    int backward_blocks_max = 0;
-    int backward_max_ppt = 0;
-    int eval_blocks_per_sm = 0;
-    cudaStream_t stream = nullptr;
-    std::mutex mu;
-    DeviceBuffer slab;        // training path storage shared by this executor's plans (stream-ordered)
-    DeviceBuffer scratch;     // per-call block for one-shot calls
-    PinnedBuffer staging;     // one-shot upload / download staging
-};
 
 // Layout of a plan's device block. Everything the host reads back is contiguous at `out`.
 struct PlanLayout {
@@ -393,77 +328,6 @@ Error plan_time_launches(fo_lsm_call_plan* plan, uint32_t iterations, double* el
     *elapsed_ms = total;
     for (uint64_t k = 0; kernel_ms && k < kernels && k < capacity; ++k) kernel_ms[k] = sums[k];
     return Error{};
-}
-
-std::string node_str(uint32_t node) { return std::to_string(node); }
-
-// Message of a failed fit row (RegressionError Display wrapped in LsmError::RegressionAtNode).
-Error fit_failure(const HostPlan& hp, const FitRecord& rec, uint32_t node) {
-    const int d = hp.degree;
-    const std::string prefix = "continuation regression failed at exercise node " + node_str(node) + ": ";
-    if (rec.itm < uint64_t(d + 1)) {
-        Error e = make_error(FO_ERR_LSM, FO_CODE_INSUFFICIENT_OBSERVATIONS,
-                             prefix + "regression has " + std::to_string(rec.itm) + " observations but degree " +
-                                 std::to_string(d) + " requires at least " + std::to_string(d + 1));
-        e.node = node;
-        return e;
-    }
-    Error e;
-    switch (rec.model.status) {
-        case kFitDegeneratePredictor:
-            e = make_error(FO_ERR_LSM, FO_CODE_DEGENERATE_PREDICTOR,
-                           prefix + "degree " + std::to_string(d) + " regression predictor scale is degenerate; observed " +
-                               fmt_f64(rec.model.aux_value));
-            break;
-        case kFitRankDeficient:
-            e = make_error(FO_ERR_LSM, FO_CODE_RANK_DEFICIENT,
-                           prefix + "degree " + std::to_string(d) + " polynomial design has numerical rank " +
-                               std::to_string(rec.model.aux) + " of " + std::to_string(d + 1) + " at rank tolerance " +
-                               fmt_f64(hp.rank_tolerance));
-            break;
-        case kFitNonFinite:
-            e = make_error(FO_ERR_LSM, FO_CODE_NON_FINITE_FIT,
-                           prefix + "polynomial regression produced non-finite arithmetic at basis degree " +
-                               std::to_string(rec.model.aux));
-            break;
-        default:
-            e = make_error(FO_ERR_LSM, FO_CODE_NON_FINITE_PREDICTOR,
-                           prefix + "regression population contains a non-finite predictor or response");
-            break;
-    }
-    e.node = node;
-    return e;
-}
-
-Error diag_failure(const HostPlan& hp, const FitRecord& rec, uint32_t node) {
-    const int d = hp.degree;
-    const std::string prefix = "continuation regression failed at exercise node " + node_str(node) + ": ";
-    Error e;
-    switch (rec.diag_status) {
-        case kDiagRankDeficient:
-            e = make_error(FO_ERR_LSM, FO_CODE_RANK_DEFICIENT,
-                           prefix + "degree " + std::to_string(d) + " polynomial design has numerical rank " +
-                               std::to_string(rec.diag_rank) + " of " + std::to_string(d + 1) + " at rank tolerance " +
-                               fmt_f64(hp.rank_tolerance));
-            break;
-        case kDiagConditionExceeded:
-            e = make_error(FO_ERR_LSM, FO_CODE_CONDITION_LIMIT_EXCEEDED,
-                           prefix + "degree " + std::to_string(d) + " polynomial design condition number " +
-                               fmt_f64(rec.diag_condition) + " exceeds configured limit " + fmt_f64(hp.condition_limit));
-            break;
-        case kDiagNotConverged:
-            e = make_error(FO_ERR_LSM, FO_CODE_CONDITION_DIAGNOSTIC_DID_NOT_CONVERGE,
-                           prefix + "polynomial condition diagnostic did not converge for " + std::to_string(d + 1) +
-                               " columns after 32 sweeps");
-            break;
-        default:
-            e = make_error(FO_ERR_LSM, FO_CODE_NON_FINITE_FIT,
-                           prefix + "polynomial regression produced non-finite arithmetic at basis degree " +
-                               std::to_string(rec.diag_aux));
-            break;
-    }
-    e.node = node;
-    return e;
 }
 
 Error replay(fo_lsm_call_plan* plan, bool training, uint64_t path, int want_row, SimFailure* out) {

@@ -1,0 +1,84 @@
+// executor.h - the CudaExecutor object behind the C ABI handle and the device / pinned buffers
+// it owns. Shared by the single-contract (capi.cu) and batch (lsm_grouped.cu) entry points.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <mutex>
+#include <string>
+
+#include "../../include/finoptions_cuda.h"
+#include "host.h"
+
+namespace fo {
+
+inline Error cuda_error(cudaError_t e, const char* what) {
+    return make_error(FO_ERR_EXECUTION, FO_CODE_CUDA_FAILURE,
+                      std::string("CUDA failure in ") + what + ": " + cudaGetErrorName(e) + " (" + cudaGetErrorString(e) + ")");
+}
+
+#define FO_CUDA_TRY(expr, what)                             \
+    do {                                                    \
+        cudaError_t _e = (expr);                            \
+        if (_e != cudaSuccess) return ::fo::cuda_error(_e, what); \
+    } while (0)
+
+// Grow-only device buffer.
+struct DeviceBuffer {
+    void* ptr = nullptr;
+    size_t bytes = 0;
+    Error reserve(size_t need) {
+        if (need <= bytes) return Error{};
+        if (ptr) cudaFree(ptr);
+        ptr = nullptr;
+        bytes = 0;
+        const size_t grow = std::max(need, size_t(1) << 20);
+        cudaError_t e = cudaMalloc(&ptr, grow);
+        if (e != cudaSuccess) return cuda_error(e, "cudaMalloc");
+        bytes = grow;
+        return Error{};
+    }
+    ~DeviceBuffer() {
+        if (ptr) cudaFree(ptr);
+    }
+};
+
+// Grow-only pinned host buffer.
+struct PinnedBuffer {
+    void* ptr = nullptr;
+    size_t bytes = 0;
+    Error reserve(size_t need) {
+        if (need <= bytes) return Error{};
+        if (ptr) cudaFreeHost(ptr);
+        ptr = nullptr;
+        bytes = 0;
+        const size_t grow = std::max(need, size_t(1) << 16);
+        cudaError_t e = cudaMallocHost(&ptr, grow);
+        if (e != cudaSuccess) return cuda_error(e, "cudaMallocHost");
+        bytes = grow;
+        return Error{};
+    }
+    ~PinnedBuffer() {
+        if (ptr) cudaFreeHost(ptr);
+    }
+};
+
+inline size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
+
+}  // namespace fo
+
+struct fo_executor {
+    int device = 0;
+    int sms = 0;
+    int backward_blocks_max = 0;
+    int backward_max_ppt = 0;
+    int eval_blocks_per_sm = 0;
+    cudaStream_t stream = nullptr;
+    std::mutex mu;
+    fo::DeviceBuffer slab;        // training path storage shared by this executor's plans (stream-ordered)
+    fo::DeviceBuffer scratch;     // per-call block for one-shot calls
+    fo::PinnedBuffer staging;     // one-shot upload / download staging
+    fo::DeviceBuffer batch;       // batch arena (plans, records, values, outputs)
+    fo::PinnedBuffer batch_host;  // batch upload / download staging
+};

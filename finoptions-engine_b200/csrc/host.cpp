@@ -529,4 +529,76 @@ std::string simulation_failure_message(int code, uint32_t interval, uint64_t pat
     }
 }
 
+// ---- fit failures (RegressionError Display wrapped in LsmError::RegressionAtNode) ------------
+
+std::string node_str(uint32_t node) { return std::to_string(node); }
+
+Error fit_failure(const HostPlan& hp, const FitRecord& rec, uint32_t node) {
+    const int d = hp.degree;
+    const std::string prefix = "continuation regression failed at exercise node " + node_str(node) + ": ";
+    if (rec.itm < uint64_t(d + 1)) {
+        Error e = make_error(FO_ERR_LSM, FO_CODE_INSUFFICIENT_OBSERVATIONS,
+                             prefix + "regression has " + std::to_string(rec.itm) + " observations but degree " +
+                                 std::to_string(d) + " requires at least " + std::to_string(d + 1));
+        e.node = node;
+        return e;
+    }
+    Error e;
+    switch (rec.model.status) {
+        case kFitDegeneratePredictor:
+            e = make_error(FO_ERR_LSM, FO_CODE_DEGENERATE_PREDICTOR,
+                           prefix + "degree " + std::to_string(d) + " regression predictor scale is degenerate; observed " +
+                               fmt_f64(rec.model.aux_value));
+            break;
+        case kFitRankDeficient:
+            e = make_error(FO_ERR_LSM, FO_CODE_RANK_DEFICIENT,
+                           prefix + "degree " + std::to_string(d) + " polynomial design has numerical rank " +
+                               std::to_string(rec.model.aux) + " of " + std::to_string(d + 1) + " at rank tolerance " +
+                               fmt_f64(hp.rank_tolerance));
+            break;
+        case kFitNonFinite:
+            e = make_error(FO_ERR_LSM, FO_CODE_NON_FINITE_FIT,
+                           prefix + "polynomial regression produced non-finite arithmetic at basis degree " +
+                               std::to_string(rec.model.aux));
+            break;
+        default:
+            e = make_error(FO_ERR_LSM, FO_CODE_NON_FINITE_PREDICTOR,
+                           prefix + "regression population contains a non-finite predictor or response");
+            break;
+    }
+    e.node = node;
+    return e;
+}
+
+Error diag_failure(const HostPlan& hp, const FitRecord& rec, uint32_t node) {
+    const int d = hp.degree;
+    const std::string prefix = "continuation regression failed at exercise node " + node_str(node) + ": ";
+    Error e;
+    switch (rec.diag_status) {
+        case kDiagRankDeficient:
+            e = make_error(FO_ERR_LSM, FO_CODE_RANK_DEFICIENT,
+                           prefix + "degree " + std::to_string(d) + " polynomial design has numerical rank " +
+                               std::to_string(rec.diag_rank) + " of " + std::to_string(d + 1) + " at rank tolerance " +
+                               fmt_f64(hp.rank_tolerance));
+            break;
+        case kDiagConditionExceeded:
+            e = make_error(FO_ERR_LSM, FO_CODE_CONDITION_LIMIT_EXCEEDED,
+                           prefix + "degree " + std::to_string(d) + " polynomial design condition number " +
+                               fmt_f64(rec.diag_condition) + " exceeds configured limit " + fmt_f64(hp.condition_limit));
+            break;
+        case kDiagNotConverged:
+            e = make_error(FO_ERR_LSM, FO_CODE_CONDITION_DIAGNOSTIC_DID_NOT_CONVERGE,
+                           prefix + "polynomial condition diagnostic did not converge for " + std::to_string(d + 1) +
+                               " columns after 32 sweeps");
+            break;
+        default:
+            e = make_error(FO_ERR_LSM, FO_CODE_NON_FINITE_FIT,
+                           prefix + "polynomial regression produced non-finite arithmetic at basis degree " +
+                               std::to_string(rec.diag_aux));
+            break;
+    }
+    e.node = node;
+    return e;
+}
+
 }  // namespace fo

@@ -93,4 +93,10 @@ Error finish_discounts(HostPlan* plan);
 std::string simulation_failure_message(int code, uint32_t interval, uint64_t path, double spot, double normal);
 int32_t simulation_failure_code(int code);
 
+// Typed errors of a failed backward row: the regression itself (fit_failure) or its rank /
+// condition diagnostic (diag_failure), at exercise node `node`.
+std::string node_str(uint32_t node);
+Error fit_failure(const HostPlan& hp, const FitRecord& rec, uint32_t node);
+Error diag_failure(const HostPlan& hp, const FitRecord& rec, uint32_t node);
+
 }  // namespace fo

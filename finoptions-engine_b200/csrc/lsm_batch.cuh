@@ -1,0 +1,107 @@
+// lsm_batch.cuh - device layout of grouped and row-addressed LSM batches
+// (crates/finoptions-lsm/src/batch/pricing.rs:422-589, 191-300).
+//
+// A batch is a list of groups; a group owns one training and one evaluation path population
+// (one simulation plan, one random domain per role) shared by its strike rows. Each (group,
+// strike) pair is a "problem": its own backward policy fit over the group's stored training rows
+// and its own fixed-policy evaluation on the group's evaluation paths. A row-addressed batch is
+// the special case of one strike per group.
+#pragma once
+
+#include <stdint.h>
+
+#include "lsm_device.cuh"
+
+namespace fo {
+
+// One group of the launched wave. `plan` points into the batch input block; its strike field is
+// unused (strikes live on the problems).
+struct BatchGroup {
+    DevicePlan plan;
+    uint64_t slab_offset;    // first element of the group's stored training rows in the wave slab
+    uint32_t first_problem;  // wave-local index of the group's first strike problem
+    uint32_t problems;       // strike rows in the group
+};
+
+// One (group, strike) problem of the launched wave.
+struct BatchProblem {
+    double strike;
+    uint32_t group;          // wave-local group index
+    uint32_t records;        // index of its first FitRecord (one per observation row)
+    uint64_t values;         // first element of its training values (train_paths doubles)
+    int32_t skip_fit;        // 1: the host already failed this problem's fit (no backward pass)
+    int32_t pad;
+};
+
+// Failure keys; every word starts as all-ones ("none") and keeps the lowest key with atomicMin.
+struct GroupStatus {
+    unsigned long long train_sim_fail;  // lowest failing training path
+    unsigned long long eval_sim_fail;   // lowest failing evaluation path
+};
+
+struct ProblemStatus {
+    unsigned long long fit_payoff_fail;     // (order << 32) | path: non-finite discounted value
+    unsigned long long fit_predict_fail;    // (order << 32) | path: non-finite prediction
+    unsigned long long fit_nonfinite;       // (order << 32) | path: non-finite ITM predictor/response
+    unsigned long long eval_fail;           // (row << 33) | (path << 1) | type (0 predict, 1 payoff)
+    unsigned long long eval_terminal_fail;  // path: non-finite terminal payoff
+};
+
+// Per-problem outputs: the twelve result columns (BatchLsmCallRowResult::try_from_parts,
+// pricing.rs:1130-1230) and what the host needs to report the problem's first failure.
+struct ProblemSummary {
+    double price;
+    double sample_standard_deviation;
+    double standard_error;
+    double maximum_condition;
+    uint32_t regression_nodes;
+    uint32_t no_support_nodes;
+    uint32_t insufficient_nodes;
+    uint32_t minimum_itm;
+    uint32_t early_paths;
+    uint32_t expiry_paths;
+    uint32_t origin_fitted;
+    uint32_t origin_exercised;
+    uint32_t fit_fail_order;   // first failing backward order (all-ones: none)
+    int32_t fit_fail_kind;     // kFitFail*
+    uint32_t nosupport_row;    // first unsupported row reached by in-the-money evaluation paths
+    uint32_t nosupport_count;  // those paths
+};
+
+enum FitFailKind : int32_t {
+    kFitFailNone = 0,
+    kFitFailPayoff = 1,     // non-finite discounted value (order = row being staged)
+    kFitFailNonFinite = 2,  // non-finite in-the-money predictor or response
+    kFitFailFit = 3,        // the regression itself failed (FitRecord.model.status / population)
+    kFitFailDiagnostic = 4, // rank / condition diagnostic failed
+    kFitFailPredict = 5,    // non-finite continuation prediction in the update
+};
+
+// Strikes evaluated together by one evaluation thread (groups with more run several passes).
+constexpr int kEvalStrikes = 8;
+
+struct BatchArgs {
+    const BatchGroup* groups;
+    const BatchProblem* problems;
+    uint32_t n_groups;
+    uint32_t n_problems;
+    double* slab;
+    double* values;
+    FitRecord* records;
+    GroupStatus* group_status;
+    ProblemStatus* problem_status;
+    unsigned* counts;          // [problems * 2]: early, expiry
+    unsigned* itm_counts;      // [records]: in-the-money evaluation paths at unsupported rows
+    double2* eval_partials;    // [problems * eval_blocks * 2]: (sum, sum of squares) as double-double
+    ProblemSummary* summaries; // [problems]
+    uint64_t train_paths;
+    uint64_t eval_paths;
+    uint32_t eval_blocks;      // evaluation blocks per group
+    int32_t degree;
+    double rank_tolerance;
+    double condition_limit;
+    int32_t tie_rule;
+    int32_t support;
+};
+
+}  // namespace fo

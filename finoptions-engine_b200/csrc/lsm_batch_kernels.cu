@@ -1,0 +1,482 @@
+// lsm_batch_kernels.cu - sm_100a kernels of grouped and row-addressed LSM batches
+// (crates/finoptions-lsm/src/batch/pricing.rs:505-589 for one group; 191-300 for row batches).
+//
+//   batch_simulate_kernel   training paths of every group of the wave, one thread per path, stored
+//                           time-major per group [rows, paths] with coalesced row stores.
+//   batch_backward_kernel   one CTA per (group, strike) problem: backward induction over the
+//                           group's stored rows with the problem's values in HBM, one CTA-wide
+//                           deterministic reduction of in-the-money power sums per row, the
+//                           regression solve by one thread (policy.rs:215-296, 471-601).
+//   batch_diagnose_kernel   rank / condition diagnostic of every regression row of every problem
+//                           (regression.rs:540-577).
+//   batch_evaluate_kernel   re-simulates each group's evaluation paths once and applies the fixed
+//                           policies of up to kEvalStrikes strikes on the fly (policy.rs:642-834).
+//   batch_summarize_kernel  per problem: price / SE from the evaluation partials, the row-result
+//                           columns (pricing.rs:1130-1230) and the first failing backward row.
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "lsm_batch.cuh"
+#include "lsm_batch_kernels.h"
+#include "lsm_common.cuh"
+
+namespace fo {
+
+// CTA reduction of S per-thread doubles to double-double totals in shared memory. Warp sums are
+// formed in double by the transpose reduction; warp w then combines slots w, w + warps, ... over
+// the CTA's warps in double-double in a fixed order, so the totals do not depend on timing.
+template <int S>
+__device__ __forceinline__ void cta_reduce_dd(double (&acc)[S], double* red /* [32 * S] */, dd* out /* [S] */) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, warps = blockDim.x >> 5;
+    const double total = warp_transpose_reduce<S>(acc);
+    if (lane < S) red[warp * S + lane] = total;
+    __syncthreads();
+    for (int slot = warp; slot < S; slot += warps) {
+        dd v = dd_make(lane < warps ? red[lane * S + slot] : 0.0);
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) v = dd_add(v, shfl_dd_down(v, off));
+        if (lane == 0) out[slot] = v;
+    }
+    __syncthreads();
+}
+
+__device__ __forceinline__ bool sim_failed(const unsigned long long* word) {
+    return *(const volatile unsigned long long*)word != kNone;
+}
+
+// ---------------------------------------------------------------------------------------------
+// Training simulation of every group of the wave.
+// ---------------------------------------------------------------------------------------------
+
+__global__ void __launch_bounds__(kBatchSimThreads) batch_simulate_kernel(BatchArgs a) {
+    __shared__ double sx[257], sf[257];
+    load_zig_tables(sx, sf);
+    const SmemZig zig = make_zig(sx, sf);
+    const uint64_t P = a.train_paths;
+    const uint64_t p = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (p >= P) return;
+    const BatchGroup& g = a.groups[blockIdx.y];
+    const DevicePlan plan = g.plan;
+    const uint32_t fsr = plan.first_stored_row;
+    double* out = a.slab + g.slab_offset;
+    const bool escrowed = plan.escrowed != 0;
+    auto store = [&](int row, double value) {
+        if (uint32_t(row) < fsr) return;
+        // Escrowed observations: origin -> S0; otherwise prepaid forward + prepaid cash.
+        if (escrowed) value = plan.row_node[row] == 0 ? plan.initial_spot : value + plan.escrow_cash[row];
+        out[uint64_t(row - fsr) * P + p] = value;
+    };
+    const SimResult r = simulate_path(plan, zig, plan.train_seed, plan.train_domain, uint32_t(p), store);
+    if (r.code != 0) atomicMin(&a.group_status[blockIdx.y].train_sim_fail, (unsigned long long)p);
+}
+
+// ---------------------------------------------------------------------------------------------
+// Backward induction, one CTA per problem.
+// ---------------------------------------------------------------------------------------------
+
+struct BatchBackwardSmem {
+    double red[32 * kSlots];
+    dd total[kSlots];
+    FitModel model;
+    int kind;
+};
+
+__global__ void __launch_bounds__(kBatchBackwardThreads, 2) batch_backward_kernel(BatchArgs a) {
+    __shared__ BatchBackwardSmem sm;
+    const BatchProblem pr = a.problems[blockIdx.x];
+    if (pr.skip_fit) return;
+    if (sim_failed(&a.group_status[pr.group].train_sim_fail)) return;
+    const BatchGroup& g = a.groups[pr.group];
+    const DevicePlan plan = g.plan;
+    ProblemStatus* st = a.problem_status + blockIdx.x;
+    FitRecord* records = a.records + pr.records;
+    double* values = a.values + pr.values;
+    const double* slab = a.slab + g.slab_offset;
+    const uint64_t P = a.train_paths;
+    const unsigned T = blockDim.x;
+    const double K = pr.strike;
+    const int degree = a.degree;
+    const uint32_t E = plan.rows - 1;
+    const uint32_t fsr = plan.first_stored_row;
+    const int lowest = plan.origin_row ? 1 : 0;
+    auto row_ptr = [&](uint32_t row) { return slab + uint64_t(row - fsr) * P; };
+    {
+        const double* terminal = row_ptr(E);
+        for (uint64_t p = threadIdx.x; p < P; p += T) {
+            const double d = terminal[p] - K;
+            values[p] = d > 0.0 ? d : 0.0;
+        }
+    }
+    uint32_t order = 0;
+    int row = int(E) - 1;
+    double pivot = 1.0;
+    RowSums sums;
+#pragma unroll
+    for (int k = 0; k < kSlots; ++k) sums.acc[k] = 0.0;
+    if (row >= lowest) {
+        // Discount into the first fitted row and locate its in-the-money mean (the moment pivot).
+        const double disc = plan.disc_from_later[row];
+        const double* srow = row_ptr(uint32_t(row));
+        double loc[2] = {0.0, 0.0};
+        for (uint64_t p = threadIdx.x; p < P; p += T) {
+            const double v = values[p] * disc;
+            values[p] = v;
+            if (!fo_isfinite(v)) atomicMin(&st->fit_payoff_fail, ((unsigned long long)order << 32) | p);
+            const double sp = srow[p];
+            if (sp > K) {
+                const double x = sp / K;
+                if (fo_isfinite(x)) {
+                    loc[0] += 1.0;
+                    loc[1] += x;
+                }
+            }
+        }
+        cta_reduce_dd<2>(loc, sm.red, sm.total);
+        if (sm.total[0].hi > 0.0) pivot = dd_round(dd_div(sm.total[1], sm.total[0]));
+        for (uint64_t p = threadIdx.x; p < P; p += T) {
+            const double sp = srow[p];
+            if (sp > K) {
+                const double x = sp / K, y = values[p];
+                if (!fo_isfinite(x) || !fo_isfinite(y)) {
+                    sums.acc[14] += 1.0;
+                    atomicMin(&st->fit_nonfinite, ((unsigned long long)order << 32) | p);
+                } else {
+                    accumulate_itm(sums, x, y, pivot);
+                }
+            }
+        }
+    }
+    for (; row >= lowest; --row, ++order) {
+        cta_reduce_dd<kSlots>(sums.acc, sm.red, sm.total);
+        if (threadIdx.x == 0) {
+            const uint64_t itm = uint64_t(sm.total[0].hi);
+            const uint64_t bad = uint64_t(sm.total[14].hi);
+            const uint64_t population = itm + bad;
+            const uint32_t required = uint32_t(degree + 1);
+            int kind;
+            if (population == 0) {
+                kind = a.support == 1 ? kRuleContinue : kRuleNoSupport;
+            } else if (population < required && a.support == 1) {
+                kind = kRuleContinue;
+            } else if (population < required || bad > 0) {
+                kind = kRuleFitFailed;  // InsufficientObservations / non-finite population
+            } else {
+                fit_continuation(sm.total, pivot, itm, degree, a.rank_tolerance, &sm.model);
+                kind = sm.model.status == kFitOk ? kRuleRegression : kRuleFitFailed;
+            }
+            sm.kind = kind;
+            FitRecord& rec = records[row];
+            rec.kind = kind;
+            rec.itm = population;
+            rec.pivot = pivot;
+            rec.model = sm.model;
+            rec.origin_exercise = 0;
+            rec.origin_continuation = 0.0;
+            rec.diag_status = -1;
+        }
+        __syncthreads();
+        const int kind = sm.kind;
+        if (kind == kRuleFitFailed) return;  // the problem's fit raised; the host reports it
+        const bool regression = kind == kRuleRegression;
+        if (regression) pivot = sm.model.mean;
+        const bool stage_next = row - 1 >= lowest;
+        const double disc = stage_next ? plan.disc_from_later[row - 1] : 1.0;
+        const double* cur = row_ptr(uint32_t(row));
+        const double* nxt = stage_next ? row_ptr(uint32_t(row - 1)) : nullptr;
+#pragma unroll
+        for (int k = 0; k < kSlots; ++k) sums.acc[k] = 0.0;
+        for (uint64_t p = threadIdx.x; p < P; p += T) {
+            double v = values[p];
+            if (regression) {
+                const double sp = cur[p];
+                if (sp > K) {
+                    const double intrinsic = sp - K;
+                    double continuation;
+                    if (!predict_continuation(sm.model, degree, sp / K, &continuation)) {
+                        atomicMin(&st->fit_predict_fail, ((unsigned long long)order << 32) | p);
+                    } else if (exercise_rule(a.tie_rule, intrinsic, continuation)) {
+                        v = intrinsic;
+                    }
+                }
+            }
+            if (stage_next) {
+                const double sp = nxt[p];
+                v *= disc;
+                if (!fo_isfinite(v)) atomicMin(&st->fit_payoff_fail, ((unsigned long long)(order + 1) << 32) | p);
+                if (sp > K) {
+                    const double x = sp / K;
+                    if (!fo_isfinite(x) || !fo_isfinite(v)) {
+                        sums.acc[14] += 1.0;
+                        atomicMin(&st->fit_nonfinite, ((unsigned long long)(order + 1) << 32) | p);
+                    } else {
+                        accumulate_itm(sums, x, v, pivot);
+                    }
+                }
+            }
+            values[p] = v;
+        }
+    }
+    // Common origin decision (policy.rs:265-281): mean of the values discounted to the origin.
+    if (plan.origin_row) {
+        double acc[2] = {0.0, 0.0};
+        for (uint64_t p = threadIdx.x; p < P; p += T) {
+            const double w = values[p] * plan.origin_discount;
+            if (!fo_isfinite(w)) atomicMin(&st->fit_payoff_fail, ((unsigned long long)order << 32) | p);
+            acc[0] += 1.0;
+            acc[1] += w;
+        }
+        cta_reduce_dd<2>(acc, sm.red, sm.total);
+        if (threadIdx.x == 0) {
+            const double mean = dd_round(dd_div(sm.total[1], sm.total[0]));
+            const double intrinsic = plan.initial_spot - K > 0.0 ? plan.initial_spot - K : 0.0;
+            FitRecord& rec = records[0];
+            rec.kind = kRuleOrigin;
+            rec.origin_exercise = exercise_rule(a.tie_rule, intrinsic, mean) ? 1 : 0;
+            rec.origin_continuation = mean;
+            rec.itm = 0;
+            rec.diag_status = -1;
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------------------------
+// Diagnostics of every regression row.
+// ---------------------------------------------------------------------------------------------
+
+__global__ void batch_diagnose_kernel(BatchArgs a, uint32_t n_records) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n_records) return;
+    FitRecord& rec = a.records[i];
+    if (rec.kind != kRuleRegression) return;
+    int rank = 0, aux = 0;
+    double condition = 0.0;
+    rec.diag_status = diagnose_design(rec.model, a.degree, a.rank_tolerance, a.condition_limit, &rank, &condition, &aux);
+    rec.diag_rank = rank;
+    rec.diag_condition = condition;
+    rec.diag_aux = aux;
+}
+
+// ---------------------------------------------------------------------------------------------
+// Fused evaluation: one evaluation path per thread, up to kEvalStrikes policies applied on the fly.
+// ---------------------------------------------------------------------------------------------
+
+__global__ void __launch_bounds__(kBatchEvalThreads, 2) batch_evaluate_kernel(BatchArgs a) {
+    __shared__ double sx[257], sf[257];
+    __shared__ double red[32 * 2 * kEvalStrikes];
+    __shared__ dd tot[2 * kEvalStrikes];
+    __shared__ unsigned cnt[2 * kEvalStrikes];
+    __shared__ double strikes[kEvalStrikes];
+    __shared__ uint32_t rbase[kEvalStrikes];
+    const BatchGroup& g = a.groups[blockIdx.y];
+    const uint32_t first = g.first_problem + blockIdx.z * kEvalStrikes;
+    const int ns = min(kEvalStrikes, int(g.problems) - int(blockIdx.z) * kEvalStrikes);
+    if (ns <= 0) return;  // uniform over the block
+    if (sim_failed(&a.group_status[blockIdx.y].train_sim_fail)) return;
+    load_zig_tables(sx, sf);
+    const SmemZig zig = make_zig(sx, sf);
+    if (threadIdx.x < 2 * kEvalStrikes) cnt[threadIdx.x] = 0;
+    if (threadIdx.x < kEvalStrikes) {
+        const bool live = int(threadIdx.x) < ns;
+        strikes[threadIdx.x] = live ? a.problems[first + threadIdx.x].strike : 1.0;
+        rbase[threadIdx.x] = live ? a.problems[first + threadIdx.x].records : 0u;
+    }
+    __syncthreads();
+    const DevicePlan plan = g.plan;
+    const uint64_t P = a.eval_paths;
+    const uint64_t p = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    const uint32_t last = plan.rows - 1;
+    const int degree = a.degree;
+    double payoff[kEvalStrikes];
+#pragma unroll
+    for (int k = 0; k < kEvalStrikes; ++k) payoff[k] = 0.0;
+    unsigned active = p < P ? ((1u << ns) - 1u) : 0u;
+    auto observe = [&](int row, double spot) {
+        if (!active) return;
+        if (plan.escrowed) spot = plan.row_node[row] == 0 ? plan.initial_spot : spot + plan.escrow_cash[row];
+        const double disc = plan.disc_to_origin[row];
+        if (uint32_t(row) == last) {
+#pragma unroll
+            for (int k = 0; k < kEvalStrikes; ++k) {
+                if (!((active >> k) & 1u)) continue;
+                const double d = spot - strikes[k];
+                payoff[k] = (d > 0.0 ? d : 0.0) * disc;
+                if (!fo_isfinite(payoff[k])) atomicMin(&a.problem_status[first + k].eval_terminal_fail, (unsigned long long)p);
+                atomicAdd(&cnt[2 * k + 1], 1u);
+            }
+            active = 0u;
+            return;
+        }
+#pragma unroll
+        for (int k = 0; k < kEvalStrikes; ++k) {
+            if (!((active >> k) & 1u)) continue;
+            const double K = strikes[k];
+            const FitRecord& rec = a.records[rbase[k] + row];
+            const int kind = rec.kind;
+            if (kind == kRuleNoSupport) {
+                if (spot > K) atomicAdd(&a.itm_counts[rbase[k] + row], 1u);
+                continue;
+            }
+            if (kind != kRuleRegression || !(spot > K)) continue;
+            const double intrinsic = spot - K;
+            double continuation;
+            if (!predict_continuation(rec.model, degree, spot / K, &continuation)) {
+                atomicMin(&a.problem_status[first + k].eval_fail, ((unsigned long long)row << 33) | (p << 1));
+                continue;
+            }
+            if (exercise_rule(a.tie_rule, intrinsic, continuation)) {
+                payoff[k] = intrinsic * disc;
+                if (!fo_isfinite(payoff[k]))
+                    atomicMin(&a.problem_status[first + k].eval_fail, ((unsigned long long)row << 33) | (p << 1) | 1ull);
+                active &= ~(1u << k);
+                atomicAdd(&cnt[2 * k], 1u);
+            }
+        }
+    };
+    if (p < P) {
+        const SimResult r = simulate_path(plan, zig, plan.eval_seed, plan.eval_domain, uint32_t(p), observe);
+        if (r.code != 0) atomicMin(&a.group_status[blockIdx.y].eval_sim_fail, (unsigned long long)p);
+    }
+    double acc[2 * kEvalStrikes];
+#pragma unroll
+    for (int k = 0; k < kEvalStrikes; ++k) {
+        acc[2 * k] = payoff[k];
+        acc[2 * k + 1] = payoff[k] * payoff[k];
+    }
+    cta_reduce_dd<2 * kEvalStrikes>(acc, red, tot);
+    if (int(threadIdx.x) < 2 * ns) {
+        const uint32_t k = threadIdx.x >> 1, which = threadIdx.x & 1u;
+        a.eval_partials[(size_t(first + k) * a.eval_blocks + blockIdx.x) * 2 + which] =
+            make_double2(tot[threadIdx.x].hi, tot[threadIdx.x].lo);
+        if (cnt[threadIdx.x]) atomicAdd(&a.counts[size_t(first + k) * 2 + which], cnt[threadIdx.x]);
+    }
+}
+
+// ---------------------------------------------------------------------------------------------
+// Per-problem summary.
+// ---------------------------------------------------------------------------------------------
+
+__global__ void batch_summarize_kernel(BatchArgs a) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= a.n_problems) return;
+    const BatchProblem pr = a.problems[i];
+    const BatchGroup& g = a.groups[pr.group];
+    const uint32_t rows = g.plan.rows;
+    const uint32_t E = rows - 1;
+    const uint32_t lowest = g.plan.origin_row ? 1u : 0u;
+    const FitRecord* rec = a.records + pr.records;
+    const ProblemStatus st = a.problem_status[i];
+    ProblemSummary s{};
+    // First failure of the backward pass in the reference's order: the discount into the row,
+    // then its population, regression, diagnostic and update (policy.rs:215-296).
+    s.fit_fail_order = 0xffffffffu;
+    s.fit_fail_kind = kFitFailNone;
+    if (!pr.skip_fit) {
+        const uint32_t fitted = E > lowest ? E - lowest : 0u;
+        for (uint32_t order = 0; order <= fitted; ++order) {
+            const unsigned long long lo = (unsigned long long)order << 32, hi = lo | 0xffffffffull;
+            int kind = kFitFailNone;
+            if (st.fit_payoff_fail >= lo && st.fit_payoff_fail <= hi) {
+                kind = kFitFailPayoff;
+            } else if (order < fitted) {
+                const FitRecord& r = rec[E - 1 - order];
+                if (st.fit_nonfinite >= lo && st.fit_nonfinite <= hi) kind = kFitFailNonFinite;
+                else if (r.kind == kRuleFitFailed) kind = kFitFailFit;
+                else if (r.kind == kRuleRegression && r.diag_status != kDiagOk) kind = kFitFailDiagnostic;
+                else if (st.fit_predict_fail >= lo && st.fit_predict_fail <= hi) kind = kFitFailPredict;
+            }
+            if (kind != kFitFailNone) {
+                s.fit_fail_order = order;
+                s.fit_fail_kind = kind;
+                break;
+            }
+        }
+    }
+    uint32_t min_itm = 0xffffffffu;
+    double max_condition = 0.0;
+    s.nosupport_row = 0xffffffffu;
+    for (uint32_t r = 0; r < E; ++r) {
+        switch (rec[r].kind) {
+            case kRuleOrigin:
+                s.origin_fitted = 1;
+                s.origin_exercised = uint32_t(rec[r].origin_exercise);
+                break;
+            case kRuleNoSupport:
+                s.no_support_nodes += 1;
+                if (s.nosupport_row == 0xffffffffu && a.itm_counts[pr.records + r] > 0) {
+                    s.nosupport_row = r;
+                    s.nosupport_count = a.itm_counts[pr.records + r];
+                }
+                break;
+            case kRuleContinue: s.insufficient_nodes += 1; break;
+            case kRuleRegression: {
+                s.regression_nodes += 1;
+                const uint32_t itm = uint32_t(rec[r].itm);
+                min_itm = itm < min_itm ? itm : min_itm;
+                max_condition = fmax(max_condition, rec[r].diag_condition);
+                break;
+            }
+            default: break;
+        }
+    }
+    s.minimum_itm = s.regression_nodes == 0 ? 0u : min_itm;
+    s.maximum_condition = max_condition;
+    if (s.origin_exercised) {
+        // LsmEvaluation::deterministic (policy.rs:657-669): every path stops at the origin.
+        const double d = g.plan.initial_spot - pr.strike;
+        s.price = d > 0.0 ? d : 0.0;
+        s.sample_standard_deviation = 0.0;
+        s.standard_error = 0.0;
+        s.early_paths = uint32_t(a.eval_paths);
+        s.expiry_paths = 0;
+    } else {
+        dd sum = dd_make(0.0), sumsq = dd_make(0.0);
+        const double2* part = a.eval_partials + size_t(i) * a.eval_blocks * 2;
+        for (uint32_t b = 0; b < a.eval_blocks; ++b) {
+            sum = dd_add(sum, dd{part[2 * b].x, part[2 * b].y});
+            sumsq = dd_add(sumsq, dd{part[2 * b + 1].x, part[2 * b + 1].y});
+        }
+        const uint64_t n = a.eval_paths;
+        const dd mean = dd_div(sum, dd_make(double(n)));
+        dd m2 = dd_sub(sumsq, dd_mul(sum, mean));
+        if (m2.hi < 0.0) m2 = dd_make(0.0);
+        s.price = dd_round(mean);
+        const double sd = n > 1 ? dd_round(dd_sqrt(dd_div(m2, dd_make(double(n - 1))))) : 0.0;
+        s.sample_standard_deviation = sd;
+        s.standard_error = n > 1 ? sd / sqrt(double(n)) : 0.0;
+        s.early_paths = a.counts[size_t(i) * 2];
+        s.expiry_paths = a.counts[size_t(i) * 2 + 1];
+    }
+    a.summaries[i] = s;
+}
+
+// ---------------------------------------------------------------------------------------------
+// Launchers
+// ---------------------------------------------------------------------------------------------
+
+cudaError_t launch_batch_simulate(const BatchArgs& a, cudaStream_t stream) {
+    const uint64_t blocks = (a.train_paths + kBatchSimThreads - 1) / kBatchSimThreads;
+    batch_simulate_kernel<<<dim3(unsigned(blocks), a.n_groups), kBatchSimThreads, 0, stream>>>(a);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_batch_backward(const BatchArgs& a, cudaStream_t stream) {
+    batch_backward_kernel<<<a.n_problems, kBatchBackwardThreads, 0, stream>>>(a);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_batch_diagnose(const BatchArgs& a, uint32_t n_records, cudaStream_t stream) {
+    batch_diagnose_kernel<<<(n_records + 127) / 128, 128, 0, stream>>>(a, n_records);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_batch_evaluate(const BatchArgs& a, uint32_t strike_chunks, cudaStream_t stream) {
+    batch_evaluate_kernel<<<dim3(a.eval_blocks, a.n_groups, strike_chunks), kBatchEvalThreads, 0, stream>>>(a);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_batch_summarize(const BatchArgs& a, cudaStream_t stream) {
+    batch_summarize_kernel<<<(a.n_problems + 127) / 128, 128, 0, stream>>>(a);
+    return cudaGetLastError();
+}
+
+}  // namespace fo

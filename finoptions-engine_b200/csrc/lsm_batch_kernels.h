@@ -1,0 +1,20 @@
+// lsm_batch_kernels.h - host launchers of the batch LSM kernels (lsm_batch_kernels.cu).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "lsm_batch.cuh"
+
+namespace fo {
+
+constexpr int kBatchSimThreads = 256;
+constexpr int kBatchBackwardThreads = 256;
+constexpr int kBatchEvalThreads = 256;
+
+cudaError_t launch_batch_simulate(const BatchArgs& a, cudaStream_t stream);
+cudaError_t launch_batch_backward(const BatchArgs& a, cudaStream_t stream);
+cudaError_t launch_batch_diagnose(const BatchArgs& a, uint32_t n_records, cudaStream_t stream);
+cudaError_t launch_batch_evaluate(const BatchArgs& a, uint32_t strike_chunks, cudaStream_t stream);
+cudaError_t launch_batch_summarize(const BatchArgs& a, cudaStream_t stream);
+
+}  // namespace fo

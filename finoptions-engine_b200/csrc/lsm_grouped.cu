@@ -1,21 +1,1268 @@
-// lsm_grouped.cu - grouped / row-addressed batches (price_lsm_call_grouped_batch).
+// lsm_grouped.cu - grouped and row-addressed LSM batches on the device
+// (GroupedBatchLsmCallInputs::price and BatchLsmCallInputs::price,
+// crates/finoptions-lsm/src/batch/pricing.rs:191-300, 422-589, 704-1114).
+//
+// Host side: request validation in the reference's order (lib.rs:1302-1415 parse_batch_lsm_method,
+// input.rs try_new, BatchRandomStreams::validate, validate_exercise_mesh_domain), then per group
+// the exact union mesh, curves, event schedule and simulation plan (build_path_plan). Groups are
+// priced in waves sized to the device memory budget; each wave is five kernels
+// (lsm_batch_kernels.cu). The lowest failing group is reported with the typed error its serial
+// replay in the reference would raise (pricing.rs:452-503); no partial result is returned.
 #include <cuda_runtime.h>
 
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <string>
+#include <vector>
+
 #include "../../include/finoptions_cuda.h"
+#include "executor.h"
 #include "host.h"
+#include "lsm_batch.cuh"
+#include "lsm_batch_kernels.h"
+#include "lsm_kernels.h"
 
 using namespace fo;
 
-extern "C" {
+namespace {
 
-int fo_price_lsm_grouped_f64(fo_executor*, const fo_lsm_grouped_request*, fo_batch_result_columns*, fo_error* err) {
-    write_error(err, make_error(FO_ERR_EXECUTION, FO_CODE_INVALID_ARGUMENT, "grouped pricing is not available in this build"));
-    return FO_ERR_EXECUTION;
+constexpr unsigned long long kNone = ~0ull;
+constexpr uint64_t kU32Max = 0xffffffffull;
+
+std::string u(uint64_t v) { return std::to_string(v); }
+
+Error input_error(int32_t code, std::string message) { return make_error(FO_ERR_INPUT, code, std::move(message)); }
+Error lsm_error(int32_t code, std::string message) { return make_error(FO_ERR_LSM, code, std::move(message)); }
+
+bool canonical_nonnegative(double v) { return std::isfinite(v) && !(v < 0.0) && !(v == 0.0 && std::signbit(v)); }
+
+uint64_t bits(double x) {
+    uint64_t b;
+    std::memcpy(&b, &x, sizeof b);
+    return b;
 }
 
-int fo_price_lsm_batch_f64(fo_executor*, const fo_lsm_grouped_request*, fo_batch_result_columns*, fo_error* err) {
-    write_error(err, make_error(FO_ERR_EXECUTION, FO_CODE_INVALID_ARGUMENT, "row batch pricing is not available in this build"));
-    return FO_ERR_EXECUTION;
+// f64::total_cmp on the finite, non-negative values the validated batch columns hold.
+int total_cmp(double a, double b) {
+    if (a < b) return -1;
+    if (a > b) return 1;
+    const bool sa = std::signbit(a), sb = std::signbit(b);
+    if (sa == sb) return 0;
+    return sa ? -1 : 1;
+}
+
+// BatchLsmError wrappers of row-addressed sources (batch/error.rs).
+Error financial_at_row(uint64_t row, const Error& e) {
+    Error w = wrap(e, FO_ERR_INPUT, "LSM batch financial input failed at row " + u(row));
+    w.row = int64_t(row);
+    return w;
+}
+Error plan_at_row(uint64_t row, const Error& e) {
+    Error w = wrap(e, FO_ERR_INPUT, "LSM batch simulation plan failed at row " + u(row));
+    w.row = int64_t(row);
+    return w;
+}
+Error estimator_at_row(uint64_t row, const Error& e) {
+    Error w = wrap(e, FO_ERR_LSM, "LSM batch estimator failed at row " + u(row));
+    w.row = int64_t(row);
+    return w;
+}
+
+// A grouped request or a row batch seen as groups of strike rows.
+struct BatchView {
+    const fo_lsm_grouped_request* q;
+    bool grouped;
+    uint64_t groups() const { return q->n_initial_spots; }
+    uint64_t rows() const { return q->n_strikes; }
+    uint64_t first_row(uint64_t g) const { return grouped ? q->group_offsets[g] : g; }
+    uint64_t end_row(uint64_t g) const { return grouped ? q->group_offsets[g + 1] : g + 1; }
+    bool cash() const { return q->dividend_model != FO_MODEL_CONTINUOUS_YIELD; }
+    uint64_t cash_rows() const { return q->n_dividend_offsets ? q->n_dividend_offsets - 1 : 0; }
+    void cash_row(uint64_t g, const double** times, const double** amounts, uint64_t* n) const {
+        const int64_t base = q->dividend_offsets[0];
+        const int64_t b = q->dividend_offsets[g] - base, e = q->dividend_offsets[g + 1] - base;
+        *times = q->dividend_times + b;
+        *amounts = q->dividend_amounts + b;
+        *n = uint64_t(e - b);
+    }
+    uint64_t explicit_rows() const { return q->n_explicit_exercise_offsets ? q->n_explicit_exercise_offsets - 1 : 0; }
+    void explicit_row(uint64_t g, const double** times, uint64_t* n) const {
+        const int64_t base = q->explicit_exercise_offsets[0];
+        const int64_t b = q->explicit_exercise_offsets[g] - base, e = q->explicit_exercise_offsets[g + 1] - base;
+        *times = q->explicit_exercise_times + b;
+        *n = uint64_t(e - b);
+    }
+};
+
+// ---- method (parse_batch_lsm_method, lib.rs:1302-1415; BatchLsmCallMethod, input.rs:276-437) ---
+
+Error validate_method(const fo_lsm_grouped_request& q) {
+    if (q.polynomial_degree > 4)
+        return lsm_error(FO_CODE_UNSUPPORTED_DEGREE,
+                         "polynomial degree " + u(q.polynomial_degree) + " is unsupported; the validated maximum degree is 4");
+    if (!std::isfinite(q.rank_tolerance) || q.rank_tolerance <= 0.0 || q.rank_tolerance >= 1.0)
+        return lsm_error(FO_CODE_INVALID_RANK_TOLERANCE,
+                         "rank tolerance must be finite and strictly between 0 and 1; observed " + fmt_f64(q.rank_tolerance));
+    const double maximum = 1.0 / q.rank_tolerance;
+    if (!std::isfinite(q.condition_limit) || q.condition_limit < 1.0 || q.condition_limit > maximum)
+        return lsm_error(FO_CODE_INVALID_CONDITION_LIMIT,
+                         "condition limit must be finite, at least 1, and no greater than 1/rank_tolerance (" +
+                             fmt_f64(maximum) + "); observed " + fmt_f64(q.condition_limit));
+    if (q.tie_rule != FO_TIE_STRICTLY_GREATER && q.tie_rule != FO_TIE_GREATER_OR_EQUAL)
+        return input_error(FO_CODE_UNSUPPORTED_ENUM, "unsupported exercise tie rule " + std::to_string(q.tie_rule));
+    if (q.insufficient_exercise_support != FO_SUPPORT_FAIL && q.insufficient_exercise_support != FO_SUPPORT_CONTINUE)
+        return input_error(FO_CODE_UNSUPPORTED_ENUM, "unsupported insufficient exercise support policy " +
+                                                         std::to_string(q.insufficient_exercise_support));
+    const bool has_offsets = q.explicit_exercise_offsets != nullptr, has_times = q.explicit_exercise_times != nullptr;
+    auto origin_ok = [&]() { return q.origin_exercise == FO_ORIGIN_INCLUDED || q.origin_exercise == FO_ORIGIN_EXCLUDED; };
+    switch (q.exercise_mesh) {
+        case FO_MESH_UNIFORM:
+            if (has_offsets || has_times)
+                return input_error(FO_CODE_INVALID_ARGUMENT, "uniform exercise mesh forbids explicit exercise buffers");
+            if (!q.has_base_intervals)
+                return input_error(FO_CODE_INVALID_ARGUMENT, "uniform exercise mesh requires base_intervals");
+            if (!q.has_origin_exercise)
+                return input_error(FO_CODE_INVALID_ARGUMENT, "uniform exercise mesh requires origin_exercise");
+            if (!origin_ok())
+                return input_error(FO_CODE_UNSUPPORTED_ENUM, "unsupported origin exercise convention " +
+                                                                 std::to_string(q.origin_exercise));
+            if (q.base_intervals == 0)
+                return input_error(FO_CODE_EMPTY_BASE_INTERVALS,
+                                   "LSM uniform exercise mesh must contain at least one base interval");
+            break;
+        case FO_MESH_CASH_DIVIDEND_DATES:
+            if (q.has_base_intervals || q.has_origin_exercise || has_offsets || has_times)
+                return input_error(FO_CODE_INVALID_ARGUMENT,
+                                   "cash-dividend-date exercise mesh forbids uniform and explicit mesh fields");
+            break;
+        case FO_MESH_EXPLICIT_TIMES: {
+            if (q.has_base_intervals)
+                return input_error(FO_CODE_INVALID_ARGUMENT, "explicit exercise mesh forbids base_intervals");
+            if (!q.has_origin_exercise)
+                return input_error(FO_CODE_INVALID_ARGUMENT, "explicit exercise mesh requires origin_exercise");
+            if (!has_offsets) return input_error(FO_CODE_INVALID_ARGUMENT, "explicit exercise mesh requires exercise offsets");
+            if (!has_times) return input_error(FO_CODE_INVALID_ARGUMENT, "explicit exercise mesh requires exercise times");
+            Error e = validate_ragged_exercise(q.explicit_exercise_offsets, q.n_explicit_exercise_offsets,
+                                               q.explicit_exercise_times, q.n_explicit_exercise_times);
+            if (!e.ok()) return e;
+            if (!origin_ok())
+                return input_error(FO_CODE_UNSUPPORTED_ENUM, "unsupported origin exercise convention " +
+                                                                 std::to_string(q.origin_exercise));
+            break;
+        }
+        default:
+            return input_error(FO_CODE_UNSUPPORTED_ENUM, "unsupported batched LSM exercise mesh " + std::to_string(q.exercise_mesh));
+    }
+    auto path_count = [](const char* population, uint64_t n) -> Error {
+        if (n == 0 || n > kU32Max)
+            return input_error(FO_CODE_BATCH_PATH_COUNT_OUTSIDE_DOMAIN, std::string("batched LSM ") + population +
+                                                                             " path count " + u(n) +
+                                                                             " exceeds maximum 4294967295");
+        return Error{};
+    };
+    Error e = path_count("training", q.training_paths);
+    if (!e.ok()) return e;
+    e = path_count("evaluation", q.evaluation_paths);
+    if (!e.ok()) return e;
+    if (q.evaluation_paths < 2)
+        return input_error(FO_CODE_INSUFFICIENT_EVALUATION_PATHS,
+                           "batched LSM evaluation requires at least two paths; observed " + u(q.evaluation_paths));
+    return Error{};
+}
+
+// ---- dividend model and columns (input.rs:502-902) ----------------------------------------------
+
+Error validate_dividend_model(const fo_lsm_grouped_request& q) {
+    switch (q.dividend_model) {
+        case FO_MODEL_CONTINUOUS_YIELD:
+            return Error{};
+        case FO_MODEL_CASH_DIVIDENDS:
+            if (q.dividend_policy != FO_DIVIDEND_LIQUIDATOR && q.dividend_policy != FO_DIVIDEND_SURVIVOR)
+                return input_error(FO_CODE_UNSUPPORTED_ENUM, "unsupported dividend policy " + std::to_string(q.dividend_policy));
+            break;
+        case FO_MODEL_ESCROWED_CASH_DIVIDENDS:
+            if (q.volatility_convention != FO_ESCROWED_PREPAID_FORWARD &&
+                q.volatility_convention != FO_ESCROWED_SPOT_MATCHED_AT_ORIGIN)
+                return input_error(FO_CODE_UNSUPPORTED_ENUM, "unsupported escrowed volatility convention " +
+                                                                 std::to_string(q.volatility_convention));
+            break;
+        default:
+            return input_error(FO_CODE_UNSUPPORTED_ENUM, "unsupported batch dividend model " + std::to_string(q.dividend_model));
+    }
+    if (q.maturity_boundary != FO_MATURITY_STRICTLY_BEFORE && q.maturity_boundary != FO_MATURITY_AT_OR_BEFORE)
+        return input_error(FO_CODE_UNSUPPORTED_CASH_MATURITY_BOUNDARY,
+                           "cash-dividend maturity boundary is unsupported by this LSM engine");
+    // RaggedCashDividends::try_new; in the LSM batch context its errors surface as InputError.
+    Error e = validate_ragged_cash(q.dividend_offsets, q.n_dividend_offsets, q.dividend_times, q.n_dividend_times,
+                                   q.dividend_amounts, q.n_dividend_amounts);
+    if (!e.ok()) e.kind = FO_ERR_INPUT;
+    return e;
+}
+
+Error row_count(const char* field, uint64_t expected, uint64_t observed) {
+    if (observed != expected)
+        return input_error(FO_CODE_ROW_COUNT_MISMATCH, std::string("LSM batch field ") + field + " has " + u(observed) +
+                                                           " rows; expected " + u(expected));
+    return Error{};
+}
+
+Error invalid_row_value(const char* field, uint64_t row, double observed) {
+    return input_error(FO_CODE_INVALID_ROW_VALUE, std::string("LSM batch field ") + field + " is invalid at row " + u(row) +
+                                                      ": observed " + fmt_f64(observed));
+}
+Error finite_value(const char* field, uint64_t row, double v) {
+    return std::isfinite(v) ? Error{} : invalid_row_value(field, row, v);
+}
+Error positive_value(const char* field, uint64_t row, double v) {
+    return std::isfinite(v) && v > 0.0 ? Error{} : invalid_row_value(field, row, v);
+}
+Error nonnegative_value(const char* field, uint64_t row, double v) {
+    return canonical_nonnegative(v) ? Error{} : invalid_row_value(field, row, v);
+}
+
+Error validate_cash_schedule(uint64_t row, double maturity, const double* times, uint64_t n, int32_t boundary) {
+    for (uint64_t event = 0; event < n; ++event) {
+        const double time = times[event];
+        const int c = total_cmp(time, maturity);
+        if (c > 0)
+            return input_error(FO_CODE_CASH_DIVIDEND_AFTER_MATURITY,
+                               "cash dividend at batch row " + u(row) + ", event " + u(event) + ", time " + fmt_f64(time) +
+                                   " occurs after maturity " + fmt_f64(maturity));
+        if (c == 0 && boundary == FO_MATURITY_STRICTLY_BEFORE)
+            return input_error(FO_CODE_CASH_DIVIDEND_AT_EXCLUDED_MATURITY,
+                               "cash dividend at batch row " + u(row) + ", event " + u(event) + " equals maturity " +
+                                   fmt_f64(maturity) + ", but the declared boundary is strictly-before");
+        if (event > 0 && bits(times[event - 1]) == bits(time))
+            return input_error(FO_CODE_DUPLICATE_CASH_DIVIDEND_TIME,
+                               "cash-dividend batch row " + u(row) + " repeats exact event time " + fmt_f64(time) +
+                                   " at event " + u(event) + "; aggregation policy is not declared");
+    }
+    return Error{};
+}
+
+// escrowed_origin_prepaid_cash (input.rs:830-850)
+Error escrowed_origin_prepaid_cash(uint64_t row, double rate, const double* times, const double* amounts, uint64_t n,
+                                   double* out) {
+    double prepaid = 0.0;
+    for (uint64_t event = 0; event < n; ++event) {
+        const double discounted = amounts[event] * std::exp(-rate * times[event]);
+        prepaid += discounted;
+        if (!std::isfinite(discounted) || !std::isfinite(prepaid))
+            return input_error(FO_CODE_ESCROWED_NON_FINITE_PREPAID_CASH,
+                               "escrowed prepaid cash is not finite at batch row " + u(row) + ", event " + u(event) +
+                                   ": time=" + fmt_f64(times[event]) + ", amount=" + fmt_f64(amounts[event]) +
+                                   ", rate=" + fmt_f64(rate));
+    }
+    *out = prepaid;
+    return Error{};
+}
+
+Error validate_escrowed_row(uint64_t row, double s0, double rate, double vol, const double* times, const double* amounts,
+                            uint64_t n, int32_t convention) {
+    double prepaid = 0.0;
+    Error e = escrowed_origin_prepaid_cash(row, rate, times, amounts, n, &prepaid);
+    if (!e.ok()) return e;
+    const double forward = s0 - prepaid;
+    if (!std::isfinite(forward) || forward <= 0.0)
+        return input_error(FO_CODE_ESCROWED_NON_POSITIVE_PREPAID_FORWARD,
+                           "escrowed prepaid forward must be strictly positive at batch row " + u(row) + "; initial spot is " +
+                               fmt_f64(s0) + " and origin prepaid cash is " + fmt_f64(prepaid));
+    if (convention == FO_ESCROWED_SPOT_MATCHED_AT_ORIGIN) {
+        const double transformed = vol * s0 / forward;
+        if (!std::isfinite(transformed) || transformed <= 0.0)
+            return input_error(FO_CODE_ESCROWED_INVALID_VOLATILITY,
+                               "escrowed spot-matched volatility is invalid at batch row " + u(row) + ": supplied=" +
+                                   fmt_f64(vol) + ", initial_spot=" + fmt_f64(s0) + ", prepaid_forward=" + fmt_f64(forward) +
+                                   ", transformed=" + fmt_f64(transformed));
+    }
+    return Error{};
+}
+
+// The dividend-model checks of one row (continuous yield, or cash schedule + escrowed row).
+Error validate_row_dividends(const BatchView& v, uint64_t g, uint64_t index) {
+    const fo_lsm_grouped_request& q = *v.q;
+    if (!v.cash()) return nonnegative_value("continuous_dividend_yields", index, q.dividend_yields[g]);
+    const double *times, *amounts;
+    uint64_t n;
+    v.cash_row(g, &times, &amounts, &n);
+    Error e = validate_cash_schedule(index, q.maturities[g], times, n, q.maturity_boundary);
+    if (!e.ok()) return e;
+    if (q.dividend_model == FO_MODEL_ESCROWED_CASH_DIVIDENDS)
+        return validate_escrowed_row(index, q.initial_spots[g], q.rates[g], q.volatilities[g], times, amounts, n,
+                                     q.volatility_convention);
+    return Error{};
+}
+
+uint64_t dividend_model_rows(const BatchView& v) {
+    return v.cash() ? v.cash_rows() : v.q->n_dividend_yields;
+}
+
+// GroupedBatchLsmCallInputs::try_new (input.rs:617-706)
+Error validate_grouped_inputs(const BatchView& v) {
+    const fo_lsm_grouped_request& q = *v.q;
+    const uint64_t groups = q.n_initial_spots;
+    if (groups == 0 || q.n_strikes == 0)
+        return input_error(FO_CODE_EMPTY_BATCH, "LSM call batch must contain at least one contract");
+    Error e = row_count("maturities", groups, q.n_maturities);
+    if (e.ok()) e = row_count("constant_continuously_compounded_rates", groups, q.n_rates);
+    if (e.ok()) e = row_count("constant_volatilities", groups, q.n_volatilities);
+    if (e.ok()) e = row_count("dividend_model", groups, dividend_model_rows(v));
+    if (!e.ok()) return e;
+    // validate_group_offsets (input.rs:761-796)
+    if (q.n_group_offsets != groups + 1)
+        return input_error(FO_CODE_GROUP_OFFSET_COUNT_MISMATCH, "LSM grouped batch offsets contain " + u(q.n_group_offsets) +
+                                                                    " values; expected " + u(groups + 1));
+    if (q.group_offsets[0] != 0)
+        return input_error(FO_CODE_GROUP_OFFSETS_DO_NOT_START_AT_ZERO,
+                           "LSM grouped batch offsets must start at zero; observed " + u(q.group_offsets[0]));
+    for (uint64_t g = 0; g < groups; ++g) {
+        if (q.group_offsets[g] >= q.group_offsets[g + 1])
+            return input_error(FO_CODE_INVALID_GROUP_RANGE, "LSM grouped batch range " + u(g) +
+                                                                " must be nonempty and increasing; observed [" +
+                                                                u(q.group_offsets[g]) + ", " + u(q.group_offsets[g + 1]) + ")");
+    }
+    if (uint64_t(q.group_offsets[groups]) != q.n_strikes)
+        return input_error(FO_CODE_GROUP_OFFSET_END_MISMATCH, "LSM grouped batch terminal offset is " +
+                                                                  u(q.group_offsets[groups]) + "; expected " +
+                                                                  u(q.n_strikes) + " contract rows");
+    for (uint64_t r = 0; r < q.n_strikes; ++r) {
+        e = positive_value("strikes", r, q.strikes[r]);
+        if (!e.ok()) return e;
+    }
+    for (uint64_t g = 0; g < groups; ++g) {
+        e = nonnegative_value("initial_spots", g, q.initial_spots[g]);
+        if (e.ok()) e = positive_value("maturities", g, q.maturities[g]);
+        if (e.ok()) e = finite_value("constant_continuously_compounded_rates", g, q.rates[g]);
+        if (e.ok()) e = positive_value("constant_volatilities", g, q.volatilities[g]);
+        if (e.ok()) e = validate_row_dividends(v, g, g);
+        if (!e.ok()) return e;
+    }
+    return Error{};
+}
+
+// BatchLsmCallInputs::try_new (input.rs:502-585)
+Error validate_row_inputs(const BatchView& v) {
+    const fo_lsm_grouped_request& q = *v.q;
+    const uint64_t rows = q.n_initial_spots;
+    if (rows == 0) return input_error(FO_CODE_EMPTY_BATCH, "LSM call batch must contain at least one contract");
+    Error e = row_count("strikes", rows, q.n_strikes);
+    if (e.ok()) e = row_count("maturities", rows, q.n_maturities);
+    if (e.ok()) e = row_count("constant_continuously_compounded_rates", rows, q.n_rates);
+    if (e.ok()) e = row_count("constant_volatilities", rows, q.n_volatilities);
+    if (e.ok()) e = row_count("dividend_model", rows, dividend_model_rows(v));
+    if (!e.ok()) return e;
+    for (uint64_t r = 0; r < rows; ++r) {
+        e = nonnegative_value("initial_spots", r, q.initial_spots[r]);
+        if (e.ok()) e = positive_value("strikes", r, q.strikes[r]);
+        if (e.ok()) e = positive_value("maturities", r, q.maturities[r]);
+        if (e.ok()) e = finite_value("constant_continuously_compounded_rates", r, q.rates[r]);
+        if (e.ok()) e = positive_value("constant_volatilities", r, q.volatilities[r]);
+        if (e.ok()) e = validate_row_dividends(v, r, r);
+        if (!e.ok()) return e;
+    }
+    return Error{};
+}
+
+// BatchRandomStreams::validate (input.rs:201-255)
+Error validate_streams(const fo_lsm_grouped_request& q, uint64_t rows) {
+    auto end = [&](const char* population, uint32_t start, uint64_t* out) -> Error {
+        const uint64_t e = uint64_t(start) + rows;
+        if (e > kU32Max + 1)
+            return input_error(FO_CODE_RANDOM_DOMAIN_RANGE_OVERFLOW, std::string("batched LSM ") + population +
+                                                                         " random domains starting at " + u(start) +
+                                                                         " cannot address " + u(rows) + " rows");
+        *out = e;
+        return Error{};
+    };
+    uint64_t te = 0, ee = 0;
+    Error e = end("training", q.training_domain_start, &te);
+    if (!e.ok()) return e;
+    e = end("evaluation", q.evaluation_domain_start, &ee);
+    if (!e.ok()) return e;
+    const uint64_t ts = q.training_domain_start, es = q.evaluation_domain_start;
+    if (ts < ee && es < te)
+        return input_error(FO_CODE_RANDOM_DOMAIN_RANGE_COLLISION, "batched LSM training domains [" + u(ts) + ", " + u(te) +
+                                                                      ") overlap evaluation domains [" + u(es) + ", " +
+                                                                      u(ee) + ")");
+    return Error{};
+}
+
+Error cash_mesh_row(uint64_t row, double maturity, double rate, const double* times, uint64_t n) {
+    if (rate < 0.0)
+        return input_error(FO_CODE_NEGATIVE_RATE_FOR_CASH_MESH,
+                           "cash-dividend-date exercise mesh requires a nonnegative continuously compounded rate at batch row " +
+                               u(row) + "; observed " + fmt_f64(rate));
+    for (uint64_t event = 0; event < n; ++event)
+        if (bits(times[event]) == bits(maturity))
+            return input_error(FO_CODE_TERMINAL_CASH_FOR_CASH_MESH,
+                               "cash-dividend-date exercise mesh does not admit terminal cash at batch row " + u(row) +
+                                   ", event " + u(event) + "; event and maturity are " + fmt_f64(maturity));
+    return Error{};
+}
+
+Error explicit_times_row(uint64_t row, double maturity, const double* times, uint64_t n) {
+    for (uint64_t event = 0; event < n; ++event)
+        if (times[event] >= maturity)
+            return input_error(FO_CODE_EXPLICIT_EXERCISE_AT_OR_AFTER_MATURITY,
+                               "explicit exercise time at batch row " + u(row) + ", event " + u(event) + ", time " +
+                                   fmt_f64(times[event]) + " must be strictly before maturity " + fmt_f64(maturity));
+    return Error{};
+}
+
+// validate_exercise_mesh_domain (pricing.rs:356-400 rows, 622-664 groups)
+Error validate_mesh_domain(const BatchView& v) {
+    const fo_lsm_grouped_request& q = *v.q;
+    const uint64_t groups = v.groups();
+    if (q.exercise_mesh == FO_MESH_CASH_DIVIDEND_DATES) {
+        if (!v.cash())
+            return input_error(FO_CODE_CASH_MESH_REQUIRES_CASH_DIVIDENDS,
+                               "cash-dividend-date exercise mesh requires a deterministic cash-dividend model");
+        for (uint64_t g = 0; g < groups; ++g) {
+            const double *times, *amounts;
+            uint64_t n;
+            v.cash_row(g, &times, &amounts, &n);
+            Error e = cash_mesh_row(v.first_row(g), q.maturities[g], q.rates[g], times, n);
+            if (!e.ok()) return e;
+        }
+    } else if (q.exercise_mesh == FO_MESH_EXPLICIT_TIMES) {
+        if (v.explicit_rows() != groups) return row_count("explicit_exercise_times", groups, v.explicit_rows());
+        for (uint64_t g = 0; g < groups; ++g) {
+            const double* times;
+            uint64_t n;
+            v.explicit_row(g, &times, &n);
+            Error e = explicit_times_row(v.first_row(g), q.maturities[g], times, n);
+            if (!e.ok()) return e;
+        }
+    }
+    return Error{};
+}
+
+// ---- per-group plan (build_path_plan, pricing.rs:704-748) -------------------------------------
+
+uint32_t next_base_node(uint32_t node, uint32_t final_node, bool* done) {
+    if (node == final_node) {
+        *done = true;
+        return node;
+    }
+    return node + 1;
+}
+
+// exact_union_times (pricing.rs:967-1047)
+Error exact_union_times(uint64_t row, double maturity, uint32_t base_intervals, const double* cash, uint64_t n_cash,
+                        std::vector<double>* out) {
+    const uint64_t capacity = uint64_t(base_intervals) + 1 + n_cash;
+    if (capacity - 1 > kU32Max)
+        return input_error(FO_CODE_CONTRACT_MESH_SHAPE_OVERFLOW, "LSM batch mesh shape overflow at row " + u(row) + " for " +
+                                                                     u(base_intervals) + " base intervals and " + u(n_cash) +
+                                                                     " cash events");
+    std::vector<double>& times = *out;
+    times.clear();
+    times.reserve(capacity);
+    bool base_done = false;
+    uint32_t base_node = 0;
+    uint64_t event = 0;
+    while (!base_done || event < n_cash) {
+        double base = 0.0;
+        if (!base_done) base = base_node == base_intervals ? maturity : maturity * (double(base_node) / double(base_intervals));
+        if (!base_done && event < n_cash) {
+            const int c = total_cmp(base, cash[event]);
+            if (c < 0) {
+                times.push_back(base);
+                base_node = next_base_node(base_node, base_intervals, &base_done);
+            } else if (c == 0) {
+                times.push_back(base);
+                base_node = next_base_node(base_node, base_intervals, &base_done);
+                event += 1;
+            } else {
+                times.push_back(cash[event]);
+                event += 1;
+            }
+        } else if (!base_done) {
+            times.push_back(base);
+            base_node = next_base_node(base_node, base_intervals, &base_done);
+        } else {
+            times.push_back(cash[event]);
+            event += 1;
+        }
+    }
+    return Error{};
+}
+
+// exact_explicit_union_times (pricing.rs:1049-1114)
+Error exact_explicit_union_times(uint64_t row, double maturity, const double* ex, uint64_t n_ex, const double* cash,
+                                 uint64_t n_cash, std::vector<double>* out) {
+    const uint64_t capacity = n_ex + n_cash + 2;
+    if (capacity - 1 > kU32Max)
+        return input_error(FO_CODE_EXPLICIT_CONTRACT_MESH_SHAPE_OVERFLOW,
+                           "LSM explicit batch mesh shape overflow at row " + u(row) + " for " + u(n_ex) +
+                               " exercise events and " + u(n_cash) + " cash events");
+    std::vector<double>& times = *out;
+    times.clear();
+    times.reserve(capacity);
+    times.push_back(0.0);
+    uint64_t e = 0, c = 0;
+    while (e < n_ex || c < n_cash) {
+        double next;
+        if (e < n_ex && c < n_cash) {
+            const int cmp = total_cmp(ex[e], cash[c]);
+            if (cmp < 0) {
+                next = ex[e++];
+            } else if (cmp == 0) {
+                next = ex[e++];
+                c++;
+            } else {
+                next = cash[c++];
+            }
+        } else if (e < n_ex) {
+            next = ex[e++];
+        } else {
+            next = cash[c++];
+        }
+        if (next < maturity) times.push_back(next);
+    }
+    times.push_back(maturity);
+    return Error{};
+}
+
+// Index of `t` in the strictly increasing grid by total order, or -1.
+int64_t find_exact(const std::vector<double>& grid, double t) {
+    size_t lo = 0, hi = grid.size();
+    while (lo < hi) {
+        const size_t mid = (lo + hi) / 2;
+        const int c = total_cmp(grid[mid], t);
+        if (c == 0) return int64_t(mid);
+        if (c < 0) lo = mid + 1;
+        else hi = mid;
+    }
+    return -1;
+}
+
+// EscrowedGbmPathPlan prepaid cash by node (path.rs:889-944).
+Error escrowed_prepaid_cash(const std::vector<double>& log_discounts, const std::vector<uint32_t>& dividend_nodes,
+                            const std::vector<double>& amounts, std::vector<double>* out) {
+    const size_t n = log_discounts.size();
+    std::vector<double> prepaid(n, 0.0);
+    size_t event = dividend_nodes.size();
+    const size_t last = n - 1;
+    if (event > 0 && dividend_nodes[event - 1] == last) {
+        event -= 1;
+        prepaid[last] = amounts[event];
+    }
+    for (size_t node = n - 1; node-- > 0;) {
+        const double interval = log_discounts[node + 1] - log_discounts[node];
+        const double discounted_future = prepaid[node + 1] * std::exp(interval);
+        double same_node_cash = 0.0;
+        if (event > 0 && dividend_nodes[event - 1] == node) {
+            event -= 1;
+            same_node_cash = amounts[event];
+        }
+        const double value = discounted_future + same_node_cash;
+        if (!std::isfinite(value))
+            return make_error(FO_ERR_SIMULATION, FO_CODE_NON_FINITE_ESCROWED_PREPAID_CASH,
+                              "escrowed-dividend prepaid cash is not finite at node " + u(node) +
+                                  "; discounted later cash is " + fmt_f64(discounted_future) + " and same-node cash is " +
+                                  fmt_f64(same_node_cash));
+        prepaid[node] = value;
+    }
+    double origin = 0.0;
+    for (size_t i = 0; i < dividend_nodes.size(); ++i) {
+        const double discounted_future = amounts[i] * std::exp(log_discounts[dividend_nodes[i]]);
+        origin += discounted_future;
+        if (!std::isfinite(origin))
+            return make_error(FO_ERR_SIMULATION, FO_CODE_NON_FINITE_ESCROWED_PREPAID_CASH,
+                              "escrowed-dividend prepaid cash is not finite at node 0; discounted later cash is " +
+                                  fmt_f64(discounted_future) + " and same-node cash is 0.0");
+    }
+    prepaid[0] = origin;
+    *out = std::move(prepaid);
+    return Error{};
+}
+
+struct GroupWork {
+    HostPlan hp;              // simulation plan + method (strike unused)
+    uint64_t first_row = 0, end_row = 0;
+    Error build;              // build_path_plan failure: the group's error at first_row
+    Error fit;                // discount failure raised by the first strike's fit
+};
+
+Error build_group(const BatchView& v, uint64_t g, GroupWork* w) {
+    const fo_lsm_grouped_request& q = *v.q;
+    const uint64_t row = v.first_row(g);
+    const double maturity = q.maturities[g], rate = q.rates[g], s0 = q.initial_spots[g];
+    const double *cash_times = nullptr, *cash_amounts = nullptr;
+    uint64_t n_cash = 0;
+    if (v.cash()) v.cash_row(g, &cash_times, &cash_amounts, &n_cash);
+    // resolve_exercise_mesh (pricing.rs:750-800)
+    std::vector<double> times;
+    const double* ex_times = nullptr;
+    uint64_t n_ex = 0;
+    bool all_transition = true;
+    int32_t origin = FO_ORIGIN_EXCLUDED;
+    Error e;
+    if (q.exercise_mesh == FO_MESH_UNIFORM) {
+        e = exact_union_times(row, maturity, q.base_intervals, cash_times, n_cash, &times);
+        origin = q.origin_exercise;
+    } else if (q.exercise_mesh == FO_MESH_CASH_DIVIDEND_DATES) {
+        e = cash_mesh_row(row, maturity, rate, cash_times, n_cash);
+        if (e.ok()) e = exact_union_times(row, maturity, 1, cash_times, n_cash, &times);
+    } else {
+        v.explicit_row(g, &ex_times, &n_ex);
+        e = explicit_times_row(row, maturity, ex_times, n_ex);
+        if (e.ok()) e = exact_explicit_union_times(row, maturity, ex_times, n_ex, cash_times, n_cash, &times);
+        all_transition = false;
+        origin = q.origin_exercise;
+    }
+    if (!e.ok()) return e;
+    e = validate_time_grid(times);
+    if (!e.ok()) return financial_at_row(row, e);
+    // build_row_curves (pricing.rs:862-893)
+    const size_t n = times.size();
+    const double yield = v.cash() ? 0.0 : q.dividend_yields[g];
+    std::vector<double> log_discounts(n), yields(n);
+    for (size_t i = 0; i < n; ++i) {
+        log_discounts[i] = i == 0 ? 0.0 : -rate * times[i];
+        yields[i] = i == 0 ? 0.0 : yield * times[i];
+    }
+    e = validate_log_discount_curve(times, log_discounts);
+    if (e.ok()) e = validate_cumulative_yield_curve(times, yields);
+    if (!e.ok()) return financial_at_row(row, e);
+    // build_row_schedule (pricing.rs:895-965)
+    std::vector<uint32_t> dividend_nodes;
+    std::vector<double> dividend_amounts;
+    for (uint64_t event = 0; event < n_cash; ++event) {
+        const int64_t node = find_exact(times, cash_times[event]);
+        if (node < 0)
+            return input_error(FO_CODE_CASH_DIVIDEND_NODE_MISSING, "cash dividend at batch row " + u(row) + ", event " +
+                                                                       u(event) + ", time " + fmt_f64(cash_times[event]) +
+                                                                       " is absent from its exact union mesh");
+        e = validate_cash_dividend(uint32_t(node), cash_amounts[event]);
+        if (!e.ok()) return financial_at_row(row, e);
+        dividend_nodes.push_back(uint32_t(node));
+        dividend_amounts.push_back(cash_amounts[event]);
+    }
+    std::vector<uint32_t> exercise;
+    if (all_transition) {
+        const size_t start = origin == FO_ORIGIN_EXCLUDED ? 1 : 0;
+        for (size_t node = start; node + 1 < n; ++node) exercise.push_back(uint32_t(node));
+    } else {
+        if (origin == FO_ORIGIN_INCLUDED) exercise.push_back(0);
+        for (uint64_t event = 0; event < n_ex; ++event) {
+            const int64_t node = find_exact(times, ex_times[event]);
+            if (node < 0)
+                return input_error(FO_CODE_EXPLICIT_EXERCISE_NODE_MISSING, "exercise time at batch row " + u(row) +
+                                                                               ", event " + u(event) + ", time " +
+                                                                               fmt_f64(ex_times[event]) +
+                                                                               " is absent from its exact union mesh");
+            exercise.push_back(uint32_t(node));
+        }
+    }
+    const uint32_t expiry = uint32_t(n - 1);
+    e = validate_event_schedule(times, dividend_nodes, dividend_amounts, exercise, expiry);
+    if (!e.ok()) return financial_at_row(row, e);
+    // path_volatility (pricing.rs:840-860)
+    double volatility = q.volatilities[g];
+    const bool escrowed = q.dividend_model == FO_MODEL_ESCROWED_CASH_DIVIDENDS;
+    if (escrowed && q.volatility_convention == FO_ESCROWED_SPOT_MATCHED_AT_ORIGIN) {
+        double prepaid = 0.0;
+        e = escrowed_origin_prepaid_cash(row, rate, cash_times, cash_amounts, n_cash, &prepaid);
+        if (!e.ok()) return e;
+        volatility = volatility * s0 / (s0 - prepaid);
+    }
+    e = validate_constant_volatility(volatility);
+    if (!e.ok()) return financial_at_row(row, e);
+    HostPlan& hp = w->hp;
+    if (escrowed) {
+        // Risky prepaid forward: no yield, no cash jumps; the prepaid cash is added back per row.
+        std::vector<double> prepaid;
+        e = escrowed_prepaid_cash(log_discounts, dividend_nodes, dividend_amounts, &prepaid);
+        if (!e.ok()) return plan_at_row(row, e);
+        const std::vector<double> zero(n, 0.0);
+        e = build_gbm_plan(times.data(), n, times.data(), n, log_discounts.data(), n, times.data(), n, zero.data(), n,
+                           nullptr, 0, nullptr, 0, exercise.data(), exercise.size(), expiry, volatility,
+                           FO_DIVIDEND_LIQUIDATOR, &hp);
+        if (!e.ok()) return plan_at_row(row, e);
+        hp.escrowed = true;
+        for (size_t r = 0; r < hp.row_node.size(); ++r) {
+            const uint32_t node = hp.row_node[r];
+            hp.escrow_cash[r] = node == expiry ? 0.0 : prepaid[node];
+        }
+        hp.sim_start = s0 - prepaid[0];
+    } else {
+        const int32_t policy = v.cash() ? q.dividend_policy : int32_t(FO_DIVIDEND_LIQUIDATOR);
+        e = build_gbm_plan(times.data(), n, times.data(), n, log_discounts.data(), n, times.data(), n, yields.data(), n,
+                           dividend_nodes.data(), dividend_nodes.size(), dividend_amounts.data(), dividend_amounts.size(),
+                           exercise.data(), exercise.size(), expiry, volatility, policy, &hp);
+        if (!e.ok()) return plan_at_row(row, e);
+        hp.sim_start = s0;
+    }
+    hp.initial_spot = s0;
+    hp.strike = 0.0;
+    hp.train_paths = q.training_paths;
+    hp.eval_paths = q.evaluation_paths;
+    hp.train_seed = q.training_seed;
+    hp.eval_seed = q.evaluation_seed;
+    hp.train_domain = uint32_t(uint64_t(q.training_domain_start) + g);
+    hp.eval_domain = uint32_t(uint64_t(q.evaluation_domain_start) + g);
+    hp.degree = int32_t(q.polynomial_degree);
+    hp.rank_tolerance = q.rank_tolerance;
+    hp.condition_limit = q.condition_limit;
+    hp.tie_rule = q.tie_rule;
+    hp.support = q.insufficient_exercise_support;
+    // Discounts of the fit (policy.rs:1049-1108): a failure is the first strike's fit error.
+    Error fit = finish_discounts(&hp);
+    if (!fit.ok()) {
+        w->fit = fit;
+        hp.disc_from_later.assign(hp.rows(), 1.0);
+        hp.disc_to_origin.assign(hp.rows(), 1.0);
+        hp.origin_discount = 1.0;
+    }
+    return Error{};
+}
+
+// ---- device layout of one wave ------------------------------------------------------------------
+
+struct WaveLayout {
+    size_t groups, problems, group_status, problem_status, summaries;  // read-back region: group_status..summaries
+    size_t counts, itm_counts, eval_partials, records, values, slab, replay;
+    size_t out_begin, out_bytes, clear_begin, clear_bytes, total;
+};
+
+struct Wave {
+    uint64_t g0 = 0, g1 = 0;     // groups [g0, g1)
+    uint64_t problems = 0;       // strike rows
+    uint64_t records = 0;        // FitRecords (rows per problem)
+    uint64_t slab_elems = 0;     // stored training states
+};
+
+uint32_t eval_blocks_for(uint64_t eval_paths) {
+    return uint32_t((eval_paths + kBatchEvalThreads - 1) / kBatchEvalThreads);
+}
+
+WaveLayout layout_for(const Wave& w, uint64_t train_paths, uint32_t eval_blocks, size_t base) {
+    WaveLayout L{};
+    size_t off = base;
+    auto take = [&](size_t bytes) {
+        off = align_up(off, 256);
+        const size_t at = off;
+        off += bytes;
+        return at;
+    };
+    const uint64_t G = w.g1 - w.g0, P = w.problems;
+    L.groups = take(sizeof(BatchGroup) * G);
+    L.problems = take(sizeof(BatchProblem) * P);
+    off = align_up(off, 256);
+    L.out_begin = off;
+    L.group_status = take(sizeof(GroupStatus) * G);
+    L.problem_status = take(sizeof(ProblemStatus) * P);
+    L.summaries = take(sizeof(ProblemSummary) * P);
+    off = align_up(off, 256);
+    L.out_bytes = off - L.out_begin;
+    L.clear_begin = off;
+    L.counts = take(sizeof(unsigned) * 2 * P);
+    L.itm_counts = take(sizeof(unsigned) * w.records);
+    L.records = take(sizeof(FitRecord) * w.records);
+    off = align_up(off, 256);
+    L.clear_bytes = off - L.clear_begin;
+    L.eval_partials = take(sizeof(double2) * 2 * size_t(eval_blocks) * P);
+    L.replay = take(sizeof(SimFailure));
+    L.values = take(sizeof(double) * train_paths * P);
+    L.slab = take(sizeof(double) * std::max<uint64_t>(w.slab_elems, 1));
+    L.total = align_up(off, 256);
+    return L;
+}
+
+// Offsets of one group's plan arrays inside the batch input block (uploaded once per call).
+struct InputOffsets {
+    size_t steps, events, row_node, disc_from_later, disc_to_origin, escrow_cash;
+};
+
+DevicePlan device_plan(const HostPlan& hp, const InputOffsets& o, unsigned char* dev) {
+    DevicePlan p{};
+    p.intervals = hp.intervals();
+    p.rows = hp.rows();
+    p.first_stored_row = hp.origin_row ? 1u : 0u;
+    p.strike = 0.0;
+    p.sim_start = hp.sim_start;
+    p.initial_spot = hp.initial_spot;
+    p.policy = hp.policy;
+    p.escrowed = hp.escrowed ? 1 : 0;
+    p.degree = hp.degree;
+    p.tie_rule = hp.tie_rule;
+    p.support = hp.support;
+    p.origin_row = hp.origin_row ? 1 : 0;
+    p.rank_tolerance = hp.rank_tolerance;
+    p.condition_limit = hp.condition_limit;
+    p.train_paths = hp.train_paths;
+    p.eval_paths = hp.eval_paths;
+    p.train_seed = hp.train_seed;
+    p.eval_seed = hp.eval_seed;
+    p.train_domain = hp.train_domain;
+    p.eval_domain = hp.eval_domain;
+    p.steps = reinterpret_cast<const StepCoef*>(dev + o.steps);
+    p.events = reinterpret_cast<const NodeEvent*>(dev + o.events);
+    p.row_node = reinterpret_cast<const uint32_t*>(dev + o.row_node);
+    p.disc_from_later = reinterpret_cast<const double*>(dev + o.disc_from_later);
+    p.disc_to_origin = reinterpret_cast<const double*>(dev + o.disc_to_origin);
+    p.escrow_cash = reinterpret_cast<const double*>(dev + o.escrow_cash);
+    p.origin_discount = hp.origin_discount;
+    return p;
+}
+
+// ---- failure reports ------------------------------------------------------------------------------
+
+struct BatchRun {
+    fo_executor* ex;
+    const BatchView* v;
+    std::vector<GroupWork>* work;
+    std::vector<DevicePlan>* plans;
+    const std::vector<uint64_t>* slab_of;  // wave-local group -> first slab element
+    unsigned char* dev;
+    WaveLayout L;
+    Wave w;
+};
+
+Error replay_path(const BatchRun& run, uint64_t g, bool training, uint64_t path, int want_row, SimFailure* out) {
+    const HostPlan& hp = (*run.work)[g].hp;
+    auto* d = reinterpret_cast<SimFailure*>(run.dev + run.L.replay);
+    FO_CUDA_TRY(launch_replay((*run.plans)[g], training ? hp.train_seed : hp.eval_seed,
+                              training ? hp.train_domain : hp.eval_domain, uint32_t(path), want_row, d, run.ex->stream),
+                "replay launch");
+    FO_CUDA_TRY(cudaMemcpyAsync(out, d, sizeof(SimFailure), cudaMemcpyDeviceToHost, run.ex->stream), "replay copy");
+    FO_CUDA_TRY(cudaStreamSynchronize(run.ex->stream), "replay");
+    return Error{};
+}
+
+Error simulation_failure(const BatchRun& run, uint64_t g, bool training, uint64_t path) {
+    SimFailure f{};
+    Error e = replay_path(run, g, training, path, -1, &f);
+    if (!e.ok()) return e;
+    Error out = lsm_error(simulation_failure_code(f.code), std::string("LSM ") + (training ? "training" : "evaluation") +
+                                                               " simulation failed: " +
+                                                               simulation_failure_message(f.code, uint32_t(f.interval), path,
+                                                                                          f.spot, f.normal));
+    out.path = int64_t(path);
+    return estimator_at_row((*run.work)[g].first_row, out);
+}
+
+Error read_record(const BatchRun& run, uint64_t record, FitRecord* out) {
+    FO_CUDA_TRY(cudaMemcpy(out, run.dev + run.L.records + record * sizeof(FitRecord), sizeof(FitRecord),
+                           cudaMemcpyDeviceToHost),
+                "record read");
+    return Error{};
+}
+
+// The fit error of problem `i` (wave-local) at its first failing backward order.
+Error fit_error(const BatchRun& run, uint64_t g, uint64_t row, const BatchProblem& pr, const ProblemStatus& st,
+                const ProblemSummary& s) {
+    const HostPlan& hp = (*run.work)[g].hp;
+    const uint32_t E = hp.rows() - 1;
+    const uint32_t order = s.fit_fail_order;
+    Error e;
+    if (s.fit_fail_kind == kFitFailPayoff) {
+        const uint64_t path = st.fit_payoff_fail & kU32Max;
+        e = lsm_error(FO_CODE_NON_FINITE_DISCOUNTED_PAYOFF, "LSM evaluation produced non-finite discounted payoff at path " + u(path));
+        e.path = int64_t(path);
+        return estimator_at_row(row, e);
+    }
+    const uint32_t r = E - 1 - order;
+    const uint32_t node = hp.row_node[r];
+    FitRecord rec{};
+    Error re = read_record(run, pr.records + r, &rec);
+    if (!re.ok()) return re;
+    switch (s.fit_fail_kind) {
+        case kFitFailNonFinite: {
+            const uint64_t path = st.fit_nonfinite & kU32Max;
+            e = lsm_error(FO_CODE_NON_FINITE_PREDICTOR, "continuation regression failed at exercise node " + node_str(node) +
+                                                            ": regression predictor or response at path " + u(path) +
+                                                            " must be finite");
+            e.node = node;
+            e.path = int64_t(path);
+            break;
+        }
+        case kFitFailFit: e = fit_failure(hp, rec, node); break;
+        case kFitFailDiagnostic: e = diag_failure(hp, rec, node); break;
+        default: {
+            // The stored state of the failing path at the row (time-major group slab).
+            const uint64_t path = st.fit_predict_fail & kU32Max;
+            const uint64_t elem = (*run.slab_of)[g - run.w.g0] + uint64_t(r - (hp.origin_row ? 1u : 0u)) * hp.train_paths + path;
+            double spot = 0.0;
+            FO_CUDA_TRY(cudaMemcpy(&spot, run.dev + run.L.slab + elem * sizeof(double), sizeof(double), cudaMemcpyDeviceToHost),
+                        "state read");
+            e = lsm_error(FO_CODE_NON_FINITE_PREDICTION, "continuation prediction failed at exercise node " + node_str(node) +
+                                                             ", path " + u(path) +
+                                                             ": polynomial regression produced non-finite prediction for predictor " +
+                                                             fmt_f64(spot / pr.strike));
+            e.node = node;
+            e.path = int64_t(path);
+            break;
+        }
+    }
+    return estimator_at_row(row, e);
+}
+
+// The evaluation error of a problem, if any, in the reference's order (policy.rs:642-834).
+Error evaluation_error(const BatchRun& run, uint64_t g, uint64_t row, const BatchProblem& pr, const ProblemStatus& st,
+                       const ProblemSummary& s) {
+    if (s.origin_exercised) return Error{};
+    const HostPlan& hp = (*run.work)[g].hp;
+    const uint64_t eval_row = st.eval_fail != kNone ? (st.eval_fail >> 33) : ~0ull;
+    if (s.nosupport_row != 0xffffffffu && !(eval_row < s.nosupport_row)) {
+        const uint32_t node = hp.row_node[s.nosupport_row];
+        Error e = lsm_error(FO_CODE_EVALUATION_OUTSIDE_TRAINING_SUPPORT,
+                            u(s.nosupport_count) + " active evaluation paths are in the money at node " + node_str(node) +
+                                ", but training had no in-the-money support");
+        e.node = node;
+        return estimator_at_row(row, e);
+    }
+    if (st.eval_fail != kNone) {
+        const uint32_t r = uint32_t(st.eval_fail >> 33);
+        const uint64_t path = (st.eval_fail >> 1) & kU32Max;
+        if (st.eval_fail & 1ull) {
+            Error e = lsm_error(FO_CODE_NON_FINITE_DISCOUNTED_PAYOFF,
+                                "LSM evaluation produced non-finite discounted payoff at path " + u(path));
+            e.path = int64_t(path);
+            return estimator_at_row(row, e);
+        }
+        SimFailure f{};
+        Error re = replay_path(run, g, false, path, int(r), &f);
+        if (!re.ok()) return re;
+        double spot = f.observed;
+        if (hp.escrowed) spot = hp.row_node[r] == 0 ? hp.initial_spot : spot + hp.escrow_cash[r];
+        const uint32_t node = hp.row_node[r];
+        Error e = lsm_error(FO_CODE_NON_FINITE_PREDICTION, "continuation prediction failed at exercise node " + node_str(node) +
+                                                               ", path " + u(path) +
+                                                               ": polynomial regression produced non-finite prediction for predictor " +
+                                                               fmt_f64(spot / pr.strike));
+        e.node = node;
+        e.path = int64_t(path);
+        return estimator_at_row(row, e);
+    }
+    if (st.eval_terminal_fail != kNone) {
+        Error e = lsm_error(FO_CODE_NON_FINITE_DISCOUNTED_PAYOFF,
+                            "LSM evaluation produced non-finite discounted payoff at path " + u(st.eval_terminal_fail));
+        e.path = int64_t(st.eval_terminal_fail);
+        return estimator_at_row(row, e);
+    }
+    if (!std::isfinite(s.price) || !std::isfinite(s.sample_standard_deviation) || !std::isfinite(s.standard_error)) {
+        Error e = lsm_error(FO_CODE_NON_FINITE_DISCOUNTED_PAYOFF, "LSM evaluation produced non-finite discounted payoff at path 0");
+        e.path = 0;
+        return estimator_at_row(row, e);
+    }
+    return Error{};
+}
+
+// ---- orchestration ----------------------------------------------------------------------------------
+
+size_t memory_budget(const fo_executor* ex) {
+    size_t free_bytes = 0, total = 0;
+    if (cudaMemGetInfo(&free_bytes, &total) != cudaSuccess) free_bytes = size_t(8) << 30;
+    const size_t usable = size_t(double(free_bytes + ex->batch.bytes) * 0.8);
+    return std::min<size_t>(usable, size_t(48) << 30);
+}
+
+Error price_batch(fo_executor* ex, const BatchView& v, fo_batch_result_columns* out) {
+    const fo_lsm_grouped_request& q = *v.q;
+    Error e = validate_method(q);
+    if (!e.ok()) return e;
+    e = validate_dividend_model(q);
+    if (!e.ok()) return e;
+    e = v.grouped ? validate_grouped_inputs(v) : validate_row_inputs(v);
+    if (!e.ok()) return e;
+    e = validate_streams(q, v.groups());
+    if (!e.ok()) return e;
+    e = validate_mesh_domain(v);
+    if (!e.ok()) return e;
+    if (out->rows != v.rows())
+        return make_error(FO_ERR_EXECUTION, FO_CODE_INVALID_ARGUMENT,
+                          "result columns hold " + u(out->rows) + " rows; the batch has " + u(v.rows()));
+
+    // Per-group plans on the host. Only groups before the first one whose plan fails can matter.
+    const uint64_t groups = v.groups();
+    std::vector<GroupWork> work(groups);
+    uint64_t launchable = groups;
+    for (uint64_t g = 0; g < groups; ++g) {
+        GroupWork& w = work[g];
+        w.first_row = v.first_row(g);
+        w.end_row = v.end_row(g);
+        w.build = build_group(v, g, &w);
+        if (!w.build.ok()) {
+            launchable = g;
+            break;
+        }
+    }
+
+    // Input block: every launchable group's plan arrays.
+    std::vector<InputOffsets> offsets(launchable);
+    size_t in_bytes = 0;
+    auto take = [&](size_t bytes) {
+        in_bytes = align_up(in_bytes, 16);
+        const size_t at = in_bytes;
+        in_bytes += bytes;
+        return at;
+    };
+    for (uint64_t g = 0; g < launchable; ++g) {
+        const HostPlan& hp = work[g].hp;
+        InputOffsets& o = offsets[g];
+        o.steps = take(sizeof(StepCoef) * std::max<size_t>(hp.steps.size(), 1));
+        o.events = take(sizeof(NodeEvent) * hp.events.size());
+        o.row_node = take(sizeof(uint32_t) * hp.rows());
+        o.disc_from_later = take(sizeof(double) * hp.rows());
+        o.disc_to_origin = take(sizeof(double) * hp.rows());
+        o.escrow_cash = take(sizeof(double) * hp.rows());
+    }
+    in_bytes = align_up(std::max<size_t>(in_bytes, 16), 256);
+
+    // Waves: consecutive groups within the memory budget (and the grid's y extent).
+    const uint64_t P = q.training_paths;
+    const uint32_t eval_blocks = eval_blocks_for(q.evaluation_paths);
+    const size_t budget = memory_budget(ex);
+    std::vector<Wave> waves;
+    {
+        Wave cur;
+        cur.g0 = cur.g1 = 0;
+        size_t bytes = 0;
+        for (uint64_t g = 0; g < launchable; ++g) {
+            const HostPlan& hp = work[g].hp;
+            const uint64_t strikes = work[g].end_row - work[g].first_row;
+            const uint64_t rows = hp.rows();
+            const uint64_t stored = rows - (hp.origin_row ? 1 : 0);
+            const size_t cost = sizeof(double) * (stored * P + strikes * P) +
+                                strikes * (rows * (sizeof(FitRecord) + sizeof(unsigned)) + 2 * size_t(eval_blocks) * sizeof(double2) +
+                                           sizeof(BatchProblem) + sizeof(ProblemStatus) + sizeof(ProblemSummary) + 8) +
+                                sizeof(BatchGroup) + sizeof(GroupStatus) + 1024;
+            if (cur.g1 > cur.g0 && (bytes + cost > budget || cur.g1 - cur.g0 >= 65535)) {
+                waves.push_back(cur);
+                cur = Wave{};
+                cur.g0 = cur.g1 = g;
+                bytes = 0;
+            }
+            cur.g1 = g + 1;
+            cur.problems += strikes;
+            cur.records += strikes * rows;
+            cur.slab_elems += stored * P;
+            bytes += cost;
+        }
+        if (cur.g1 > cur.g0) waves.push_back(cur);
+    }
+    size_t arena = in_bytes;
+    for (const Wave& w : waves) arena = std::max(arena, layout_for(w, P, eval_blocks, in_bytes).total);
+    e = ex->batch.reserve(arena);
+    if (!e.ok()) return e;
+    unsigned char* dev = static_cast<unsigned char*>(ex->batch.ptr);
+    std::vector<DevicePlan> plans(launchable);
+    for (uint64_t g = 0; g < launchable; ++g) plans[g] = device_plan(work[g].hp, offsets[g], dev);
+
+    // Host staging: inputs, then per wave the group / problem tables and the read-back region.
+    size_t stage = in_bytes;
+    for (const Wave& w : waves) {
+        const WaveLayout L = layout_for(w, P, eval_blocks, 0);
+        stage = std::max(stage, std::max(L.out_begin, L.out_bytes));
+    }
+    e = ex->batch_host.reserve(stage);
+    if (!e.ok()) return e;
+    unsigned char* host = static_cast<unsigned char*>(ex->batch_host.ptr);
+    cudaStream_t s = ex->stream;
+    if (launchable > 0) {
+        std::memset(host, 0, in_bytes);
+        for (uint64_t g = 0; g < launchable; ++g) {
+            const HostPlan& hp = work[g].hp;
+            const InputOffsets& o = offsets[g];
+            std::memcpy(host + o.steps, hp.steps.data(), sizeof(StepCoef) * hp.steps.size());
+            std::memcpy(host + o.events, hp.events.data(), sizeof(NodeEvent) * hp.events.size());
+            std::memcpy(host + o.row_node, hp.row_node.data(), sizeof(uint32_t) * hp.rows());
+            std::memcpy(host + o.disc_from_later, hp.disc_from_later.data(), sizeof(double) * hp.rows());
+            std::memcpy(host + o.disc_to_origin, hp.disc_to_origin.data(), sizeof(double) * hp.rows());
+            std::memcpy(host + o.escrow_cash, hp.escrow_cash.data(), sizeof(double) * hp.rows());
+        }
+        FO_CUDA_TRY(cudaMemcpyAsync(dev, host, in_bytes, cudaMemcpyHostToDevice, s), "batch input upload");
+        FO_CUDA_TRY(cudaStreamSynchronize(s), "batch input upload");
+    }
+
+    std::vector<uint64_t> slab_of;
+    for (const Wave& w : waves) {
+        const WaveLayout L = layout_for(w, P, eval_blocks, in_bytes);
+        // Group and problem tables.
+        auto* hg = reinterpret_cast<BatchGroup*>(host + (L.groups - in_bytes));
+        auto* hpb = reinterpret_cast<BatchProblem*>(host + (L.problems - in_bytes));
+        uint64_t slab = 0, record = 0, problem = 0;
+        slab_of.assign(w.g1 - w.g0, 0);
+        for (uint64_t g = w.g0; g < w.g1; ++g) {
+            const HostPlan& hp = work[g].hp;
+            BatchGroup& bg = hg[g - w.g0];
+            bg.plan = plans[g];
+            bg.slab_offset = slab;
+            slab_of[g - w.g0] = slab;
+            bg.first_problem = uint32_t(problem);
+            bg.problems = uint32_t(work[g].end_row - work[g].first_row);
+            for (uint64_t r = work[g].first_row; r < work[g].end_row; ++r) {
+                BatchProblem& pb = hpb[problem];
+                pb.strike = q.strikes[r];
+                pb.group = uint32_t(g - w.g0);
+                pb.records = uint32_t(record);
+                pb.values = problem * P;
+                pb.skip_fit = work[g].fit.ok() ? 0 : 1;
+                pb.pad = 0;
+                record += hp.rows();
+                problem += 1;
+            }
+            slab += uint64_t(hp.rows() - (hp.origin_row ? 1 : 0)) * P;
+        }
+        FO_CUDA_TRY(cudaMemcpyAsync(dev + L.groups, host + (L.groups - in_bytes), L.out_begin - L.groups,
+                                    cudaMemcpyHostToDevice, s),
+                    "batch table upload");
+        FO_CUDA_TRY(cudaMemsetAsync(dev + L.out_begin, 0xff, L.summaries - L.out_begin, s), "batch status reset");
+        FO_CUDA_TRY(cudaMemsetAsync(dev + L.clear_begin, 0, L.clear_bytes, s), "batch reset");
+        BatchArgs a{};
+        a.groups = reinterpret_cast<const BatchGroup*>(dev + L.groups);
+        a.problems = reinterpret_cast<const BatchProblem*>(dev + L.problems);
+        a.n_groups = uint32_t(w.g1 - w.g0);
+        a.n_problems = uint32_t(w.problems);
+        a.slab = reinterpret_cast<double*>(dev + L.slab);
+        a.values = reinterpret_cast<double*>(dev + L.values);
+        a.records = reinterpret_cast<FitRecord*>(dev + L.records);
+        a.group_status = reinterpret_cast<GroupStatus*>(dev + L.group_status);
+        a.problem_status = reinterpret_cast<ProblemStatus*>(dev + L.problem_status);
+        a.counts = reinterpret_cast<unsigned*>(dev + L.counts);
+        a.itm_counts = reinterpret_cast<unsigned*>(dev + L.itm_counts);
+        a.eval_partials = reinterpret_cast<double2*>(dev + L.eval_partials);
+        a.summaries = reinterpret_cast<ProblemSummary*>(dev + L.summaries);
+        a.train_paths = P;
+        a.eval_paths = q.evaluation_paths;
+        a.eval_blocks = eval_blocks;
+        a.degree = int32_t(q.polynomial_degree);
+        a.rank_tolerance = q.rank_tolerance;
+        a.condition_limit = q.condition_limit;
+        a.tie_rule = q.tie_rule;
+        a.support = q.insufficient_exercise_support;
+        uint32_t chunks = 1;
+        for (uint64_t g = w.g0; g < w.g1; ++g)
+            chunks = std::max<uint32_t>(chunks, uint32_t((work[g].end_row - work[g].first_row + kEvalStrikes - 1) / kEvalStrikes));
+        FO_CUDA_TRY(launch_batch_simulate(a, s), "batch training simulation launch");
+        FO_CUDA_TRY(launch_batch_backward(a, s), "batch backward launch");
+        FO_CUDA_TRY(launch_batch_diagnose(a, uint32_t(w.records), s), "batch diagnose launch");
+        FO_CUDA_TRY(launch_batch_evaluate(a, chunks, s), "batch evaluation launch");
+        FO_CUDA_TRY(launch_batch_summarize(a, s), "batch summary launch");
+        FO_CUDA_TRY(cudaMemcpyAsync(host, dev + L.out_begin, L.out_bytes, cudaMemcpyDeviceToHost, s), "batch result copy");
+        FO_CUDA_TRY(cudaStreamSynchronize(s), "batch pricing");
+        const auto* gst = reinterpret_cast<const GroupStatus*>(host + (L.group_status - L.out_begin));
+        const auto* pst = reinterpret_cast<const ProblemStatus*>(host + (L.problem_status - L.out_begin));
+        const auto* sum = reinterpret_cast<const ProblemSummary*>(host + (L.summaries - L.out_begin));
+        BatchRun run{ex, &v, &work, &plans, &slab_of, dev, L, w};
+        // Failure scan in group order (the lowest failing group wins).
+        uint64_t i0 = 0;
+        uint64_t first_record = 0;
+        for (uint64_t g = w.g0; g < w.g1; ++g) {
+            const GroupWork& gw = work[g];
+            const uint64_t strikes = gw.end_row - gw.first_row;
+            const GroupStatus& gs = gst[g - w.g0];
+            bool failed = gs.train_sim_fail != kNone || !gw.fit.ok() || gs.eval_sim_fail != kNone;
+            for (uint64_t k = 0; k < strikes && !failed; ++k) {
+                const ProblemSummary& ps = sum[i0 + k];
+                const ProblemStatus& st = pst[i0 + k];
+                failed = ps.fit_fail_order != 0xffffffffu ||
+                         (!ps.origin_exercised && (ps.nosupport_row != 0xffffffffu || st.eval_fail != kNone ||
+                                                   st.eval_terminal_fail != kNone || !std::isfinite(ps.price) ||
+                                                   !std::isfinite(ps.sample_standard_deviation)));
+            }
+            if (failed) {
+                if (gs.train_sim_fail != kNone) return simulation_failure(run, g, true, gs.train_sim_fail);
+                if (!gw.fit.ok()) return estimator_at_row(gw.first_row, gw.fit);
+                uint64_t rec = first_record;
+                for (uint64_t k = 0; k < strikes; ++k) {
+                    const ProblemSummary& ps = sum[i0 + k];
+                    BatchProblem pr{};
+                    pr.strike = q.strikes[gw.first_row + k];
+                    pr.records = uint32_t(rec);
+                    rec += gw.hp.rows();
+                    if (ps.fit_fail_order != 0xffffffffu) return fit_error(run, g, gw.first_row + k, pr, pst[i0 + k], ps);
+                }
+                if (gs.eval_sim_fail != kNone) return simulation_failure(run, g, false, gs.eval_sim_fail);
+                rec = first_record;
+                for (uint64_t k = 0; k < strikes; ++k) {
+                    BatchProblem pr{};
+                    pr.strike = q.strikes[gw.first_row + k];
+                    pr.records = uint32_t(rec);
+                    rec += gw.hp.rows();
+                    Error ee = evaluation_error(run, g, gw.first_row + k, pr, pst[i0 + k], sum[i0 + k]);
+                    if (!ee.ok()) return ee;
+                }
+                return make_error(FO_ERR_LSM, FO_CODE_INVALID_ARGUMENT,
+                                  "parallel LSM batch reported row " + u(gw.first_row) +
+                                      " as failed, but deterministic serial replay succeeded");
+            }
+            for (uint64_t k = 0; k < strikes; ++k) {
+                const ProblemSummary& ps = sum[i0 + k];
+                const uint64_t r = gw.first_row + k;
+                out->prices[r] = ps.price;
+                out->sample_standard_deviations[r] = ps.sample_standard_deviation;
+                out->standard_errors[r] = ps.standard_error;
+                out->origin_decisions_fitted[r] = uint8_t(ps.origin_fitted);
+                out->origin_exercised[r] = uint8_t(ps.origin_exercised);
+                out->regression_nodes[r] = ps.regression_nodes;
+                out->no_training_support_nodes[r] = ps.no_support_nodes;
+                out->insufficient_exercise_support_nodes[r] = ps.insufficient_nodes;
+                out->minimum_in_the_money_training_paths[r] = ps.minimum_itm;
+                out->maximum_regression_condition_numbers[r] = ps.maximum_condition;
+                out->early_exercise_paths[r] = ps.early_paths;
+                out->expiry_paths[r] = ps.expiry_paths;
+            }
+            i0 += strikes;
+            first_record += strikes * gw.hp.rows();
+        }
+    }
+    if (launchable < groups) return work[launchable].build;
+    return Error{};
+}
+
+int finish(fo_error* err, const Error& e) {
+    if (!e.ok()) write_error(err, e);
+    return e.kind;
+}
+
+Error check_columns(const fo_batch_result_columns* out) {
+    if (!out || !out->prices || !out->sample_standard_deviations || !out->standard_errors || !out->origin_decisions_fitted ||
+        !out->origin_exercised || !out->regression_nodes || !out->no_training_support_nodes ||
+        !out->insufficient_exercise_support_nodes || !out->minimum_in_the_money_training_paths ||
+        !out->maximum_regression_condition_numbers || !out->early_exercise_paths || !out->expiry_paths)
+        return make_error(FO_ERR_EXECUTION, FO_CODE_INVALID_ARGUMENT, "every batch result column must be provided");
+    return Error{};
+}
+
+int entry(fo_executor* ex, const fo_lsm_grouped_request* request, fo_batch_result_columns* out, fo_error* err,
+          bool grouped) {
+    if (!ex || !request)
+        return finish(err, make_error(FO_ERR_EXECUTION, FO_CODE_INVALID_ARGUMENT, "executor and request must not be NULL"));
+    Error e = check_columns(out);
+    if (!e.ok()) return finish(err, e);
+    if (grouped && !request->group_offsets && request->n_group_offsets)
+        return finish(err, make_error(FO_ERR_EXECUTION, FO_CODE_INVALID_ARGUMENT, "group offsets must not be NULL"));
+    if (!grouped && request->group_offsets)
+        return finish(err, make_error(FO_ERR_EXECUTION, FO_CODE_INVALID_ARGUMENT,
+                                      "a row-addressed batch takes no group offsets"));
+    std::lock_guard<std::mutex> lock(ex->mu);
+    cudaError_t ce = cudaSetDevice(ex->device);
+    if (ce != cudaSuccess) return finish(err, cuda_error(ce, "cudaSetDevice"));
+    BatchView v{request, grouped};
+    try {
+        return finish(err, price_batch(ex, v, out));
+    } catch (const std::bad_alloc&) {
+        return finish(err, make_error(FO_ERR_EXECUTION, FO_CODE_CAPACITY_EXCEEDED, "host memory exhausted"));
+    }
+}
+
+}  // namespace
+
+extern "C" {
+
+int fo_price_lsm_grouped_f64(fo_executor* executor, const fo_lsm_grouped_request* request, fo_batch_result_columns* out,
+                             fo_error* err) {
+    return entry(executor, request, out, err, true);
+}
+
+int fo_price_lsm_batch_f64(fo_executor* executor, const fo_lsm_grouped_request* request, fo_batch_result_columns* out,
+                           fo_error* err) {
+    return entry(executor, request, out, err, false);
 }
 
 }  // extern "C"

@@ -4,7 +4,7 @@
 //                          observed rows time-major [rows, paths] with coalesced row stores
 //                          (path/seeded.rs:399-474 fused with the transpose).
 //   K2 backward_kernel     persistent cooperative kernel: backward induction over exercise rows
-//                          with every thread's discounted values held in registers; one grid-wide
+//                          with every thread's discounted values held in shared memory; one grid-wide
 //                          reduction of in-the-money power sums per row, then each CTA solves the
 //                          continuation regression redundantly and applies the exercise rule
 //                          (policy.rs:215-296, 471-601).
@@ -17,31 +17,11 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include "lsm_common.cuh"
 #include "lsm_device.cuh"
 #include "lsm_kernels.h"
 
 namespace fo {
-
-__constant__ uint64_t c_zig_x[257] = FO_ZIG_NORM_X_BITS;
-__constant__ uint64_t c_zig_f[257] = FO_ZIG_NORM_F_BITS;
-
-constexpr unsigned long long kNone = ~0ull;
-
-__device__ __forceinline__ void load_zig_tables(double* sx, double* sf) {
-    for (int i = threadIdx.x; i < 257; i += blockDim.x) {
-        sx[i] = bits_to_double(c_zig_x[i]);
-        sf[i] = bits_to_double(c_zig_f[i]);
-    }
-    __syncthreads();
-}
-
-__device__ __forceinline__ SmemZig make_zig(const double* sx, const double* sf) {
-    SmemZig z;
-    z.xs = sx;
-    z.fs = sf;
-    z.rr = bits_to_double(FO_ZIG_NORM_R_BITS);
-    return z;
-}
 
 __device__ __forceinline__ unsigned ld_acquire_gpu(const unsigned* p) {
     unsigned v;
@@ -126,51 +106,6 @@ __global__ void __launch_bounds__(256) normals_kernel(uint64_t seed, uint32_t do
 // K1: seeded simulation with time-major row stores.
 // ---------------------------------------------------------------------------------------------
 
-struct SimResult {
-    int code;  // 0 ok, kNormalBudget, kNormalRejection, 3 non-finite transition
-    int interval;
-    double spot;
-    double normal;
-};
-
-// Simulates one path; calls store(row, value) at every observation. Mirrors simulate_one_seeded
-// (seeded.rs:399-459) including the terminal-dividend phase order.
-template <typename Store>
-__device__ __forceinline__ SimResult simulate_path(const DevicePlan& plan, const SmemZig& zig, uint64_t seed,
-                                                   uint32_t domain, uint32_t path, Store&& store) {
-    PathStream s;
-    s.init(seed, domain, path, plan.intervals);
-    double spot = plan.sim_start;
-    SimResult r{0, 0, 0.0, 0.0};
-    if (plan.row_node[0] == 0) store(0, spot);
-    for (uint32_t i = 0; i < plan.intervals; ++i) {
-        double z = 0.0;
-        const int status = zig_sample(s, zig, &z);
-        if (status != kNormalOk) {
-            r.code = status;
-            r.interval = int(i);
-            return r;
-        }
-        const StepCoef c = plan.steps[i];
-        const double next = gbm_advance(spot, c.diffusion, c.log_drift, z);
-        if (!fo_isfinite(next)) {
-            r.code = 3;
-            r.interval = int(i);
-            r.spot = spot;
-            r.normal = z;
-            return r;
-        }
-        spot = next;
-        const NodeEvent ev = plan.events[i + 1];
-        const bool dividend = (ev.flags & kEventDividend) != 0;
-        const bool terminal = (ev.flags & kEventTerminal) != 0;
-        if (dividend && terminal) spot = apply_cash_dividend(plan.policy, ev.dividend_amount, spot);
-        if (ev.row >= 0) store(ev.row, spot);
-        if (dividend && !terminal) spot = apply_cash_dividend(plan.policy, ev.dividend_amount, spot);
-    }
-    return r;
-}
-
 __global__ void __launch_bounds__(256) simulate_kernel(DevicePlan plan, uint64_t paths, uint64_t seed,
                                                        uint32_t domain, double* out, uint32_t store_first_row,
                                                        int reconstruct_escrowed, unsigned long long* fail) {
@@ -211,85 +146,6 @@ __global__ void replay_kernel(DevicePlan plan, uint64_t seed, uint32_t domain, u
 }
 
 // ---------------------------------------------------------------------------------------------
-// Reductions
-// ---------------------------------------------------------------------------------------------
-
-constexpr int kSlots = 16;  // T_0..T_8, U_0..U_4, non-finite count, spare
-
-__device__ __forceinline__ dd shfl_dd_down(dd v, int off);
-
-// Butterfly "transpose" reduction of S values across a warp: at each stage a lane keeps half of
-// its remaining values and adds its partner's copy of that half, so S values need S - 1 + log2
-// shuffles instead of 5 S. Lane l ends holding the warp total of value (l % S) (S a power of two
-// no larger than 32).
-template <int S>
-__device__ __forceinline__ double warp_transpose_reduce(double (&v)[S]) {
-    const int lane = threadIdx.x & 31;
-    double buf[S];
-#pragma unroll
-    for (int k = 0; k < S; ++k) buf[k] = v[k];
-#pragma unroll
-    for (int half = S / 2; half >= 1; half >>= 1) {
-        // partner offset = half; lanes with (lane & half) keep the upper half.
-        const bool upper = (lane & half) != 0;
-#pragma unroll
-        for (int k = 0; k < half; ++k) {
-            const double send = upper ? buf[k] : buf[k + half];
-            const double keep = upper ? buf[k + half] : buf[k];
-            buf[k] = keep + __shfl_xor_sync(0xffffffffu, send, half);
-        }
-    }
-    double total = buf[0];
-#pragma unroll
-    for (int off = S; off < 32; off <<= 1) total += __shfl_xor_sync(0xffffffffu, total, off);
-    return total;
-}
-
-__device__ __forceinline__ dd shfl_dd_down(dd v, int off);
-
-// Warp sums in double, then warp k combines slot k across the CTA's warps with a double-double
-// shuffle tree; lane 0 of warp k writes slot k of the CTA partial. Requires S <= warps per CTA.
-template <int S>
-__device__ __forceinline__ void cta_reduce_to(double (&acc)[S], double* smem /* [32 * S] */, double2* dst) {
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, warps = blockDim.x >> 5;
-    const double total = warp_transpose_reduce<S>(acc);
-    // lane l holds value l % S: lanes 0..S-1 publish
-    if (lane < S) smem[warp * S + lane] = total;
-    __syncthreads();
-    if (warp < S) {
-        dd v = dd_make(lane < warps ? smem[lane * S + warp] : 0.0);
-#pragma unroll
-        for (int off = 16; off > 0; off >>= 1) v = dd_add(v, shfl_dd_down(v, off));
-        if (lane == 0) dst[warp] = make_double2(v.hi, v.lo);
-    }
-    __syncthreads();
-}
-
-__device__ __forceinline__ dd shfl_dd_down(dd v, int off) {
-    dd o;
-    o.hi = __shfl_down_sync(0xffffffffu, v.hi, off);
-    o.lo = __shfl_down_sync(0xffffffffu, v.lo, off);
-    return o;
-}
-
-// Sums partials[b * S + k] over b in a fixed order; warp k handles slot k. Identical in every CTA.
-template <int S>
-__device__ __forceinline__ void grid_combine(const double2* partials, int blocks, dd* out /* smem [S] */) {
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    if (warp < S) {
-        dd acc = dd_make(0.0);
-        for (int b = lane; b < blocks; b += 32) {
-            const double2 v = __ldcg(&partials[b * S + warp]);
-            acc = dd_add(acc, dd{v.x, v.y});
-        }
-#pragma unroll
-        for (int off = 16; off > 0; off >>= 1) acc = dd_add(acc, shfl_dd_down(acc, off));
-        if (lane == 0) out[warp] = acc;
-    }
-    __syncthreads();
-}
-
-// ---------------------------------------------------------------------------------------------
 // K2: persistent backward induction.
 // ---------------------------------------------------------------------------------------------
 
@@ -302,32 +158,11 @@ struct BackwardSmem {
     unsigned local_gen;
 };
 
-__device__ __forceinline__ bool exercise_rule(int tie_rule, double intrinsic, double continuation) {
-    return tie_rule == 0 ? intrinsic > continuation : intrinsic >= continuation;
-}
-
 // Each thread owns paths gtid + j * nthreads (j < ppt). Their discounted values, the current
 // row's spots and moneyness x = S/K live in this CTA's shared memory ([j * blockDim + tid]) for the
 // whole backward pass, so the only HBM traffic is one read of each stored row. One pass over the
 // shared arrays per row applies row k's exercise rule and immediately stages row k-1: load its
 // spots, discount the values (policy.rs:1049-1063) and accumulate its in-the-money power sums.
-struct RowSums {
-    double acc[kSlots];
-};
-
-__device__ __forceinline__ void accumulate_itm(RowSums& r, double x, double y, double pivot) {
-    const double t = x - pivot;
-    r.acc[0] += 1.0;
-    double pw = t;
-    r.acc[kPowerSums] += y;
-#pragma unroll
-    for (int k = 1; k < kPowerSums; ++k) {
-        r.acc[k] += pw;
-        if (k < kResponseSums) r.acc[kPowerSums + k] += y * pw;
-        pw *= t;
-    }
-}
-
 __global__ void __launch_bounds__(kBackwardThreads, 1) backward_kernel(BackwardArgs a) {
     __shared__ BackwardSmem sm;
     extern __shared__ double backward_dyn[];

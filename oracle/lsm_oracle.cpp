@@ -1487,8 +1487,9 @@ int orc_price_lsm_call(const fo_lsm_call_request* q, int32_t threads, fo_lsm_cal
 }
 
 // Grouped batch over the oracle: groups run in parallel over `threads` workers (each group's
-// simulation serial), lowest failing group reported (pricing.rs:452-503). Inputs are assumed
-// valid; the product library owns request validation.
+// simulation serial), lowest failing group reported (pricing.rs:452-503). With NULL group offsets
+// the request is a row batch: group g is contract row g, with domains start + g. Inputs are
+// assumed valid; the product library owns request validation.
 int orc_price_lsm_grouped(const fo_lsm_grouped_request* q, int32_t threads, fo_batch_result_columns* out,
                           fo_error* err) {
     const uint64_t groups = q->n_initial_spots;
@@ -1501,7 +1502,9 @@ int orc_price_lsm_grouped(const fo_lsm_grouped_request* q, int32_t threads, fo_b
             const uint64_t g = next.fetch_add(1);
             if (g >= groups) return;
             if (g > first_failure.load()) continue;
-            const uint64_t b = q->group_offsets[g], e = q->group_offsets[g + 1];
+            // Row batches (no offsets) are groups of one contract (pricing.rs:191-300).
+            const uint64_t b = q->group_offsets ? q->group_offsets[g] : g;
+            const uint64_t e = q->group_offsets ? q->group_offsets[g + 1] : g + 1;
             Failure f = price_group(q, g, b, e, 1, rows.data() + b);
             if (!f.ok()) {
                 failures[g] = f;

@@ -1,0 +1,134 @@
+"""Seeded synthetic batch workloads shared by the batch tests and bench.py.
+
+The grouped workload has the shapes of the reference's batched-LSM benchmark case: market states,
+each with a uniform moneyness grid of strikes, exact explicit exercise meshes and exercise-aligned
+cash dividends (crates/finoptions-lsm/src/batch/input.rs:594-723 for the column layout). Market
+draws use NumPy's PCG64 with a fixed seed; the LSM paths themselves come from the engine's Philox
+streams.
+"""
+
+from __future__ import annotations
+
+from dataclasses import dataclass
+
+import numpy as np
+from finoptions._requests import GroupedRequest, lsm_grouped_request
+
+TRAINING_DOMAIN_START = 0
+EVALUATION_DOMAIN_START = 1 << 20
+
+
+@dataclass
+class GroupedColumns:
+    group_offsets: np.ndarray
+    initial_spots: np.ndarray
+    strikes: np.ndarray
+    maturities: np.ndarray
+    rates: np.ndarray
+    volatilities: np.ndarray
+    dividend_offsets: np.ndarray
+    dividend_times: np.ndarray
+    dividend_amounts: np.ndarray
+    exercise_offsets: np.ndarray
+    exercise_times: np.ndarray
+
+    @property
+    def groups(self) -> int:
+        return int(self.initial_spots.size)
+
+    @property
+    def rows(self) -> int:
+        return int(self.strikes.size)
+
+
+def grouped_columns(groups: int, strikes_per_group: int = 8, seed: int = 23, min_exercise: int = 12,
+                    max_exercise: int = 52, max_dividends: int = 4) -> GroupedColumns:
+    """States S0~U[50,150], sigma~U[0.10,0.60], T~U[0.25,2.0], r~U[0,0.06], n~U{min..max}
+    exercise dates at T*k/n (k = 1..n-1), 0..max_dividends cash dividends of U[0.5,3.0] at
+    distinct exercise dates; strikes K = S0 * linspace(0.8, 1.2, strikes_per_group)."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    s0 = rng.uniform(50.0, 150.0, groups)
+    vol = rng.uniform(0.10, 0.60, groups)
+    maturity = rng.uniform(0.25, 2.0, groups)
+    rate = rng.uniform(0.0, 0.06, groups)
+    n_ex = rng.integers(min_exercise, max_exercise + 1, groups)
+    n_div = rng.integers(0, max_dividends + 1, groups)
+    moneyness = np.linspace(0.8, 1.2, strikes_per_group)
+    ex_offsets = [0]
+    ex_times: list[float] = []
+    div_offsets = [0]
+    div_times: list[float] = []
+    div_amounts: list[float] = []
+    for g in range(groups):
+        n = int(n_ex[g])
+        times = [float(maturity[g]) * (k / n) for k in range(1, n)]
+        ex_times.extend(times)
+        ex_offsets.append(len(ex_times))
+        k = min(int(n_div[g]), len(times))
+        picks = np.sort(rng.choice(len(times), size=k, replace=False)) if k else np.array([], dtype=np.int64)
+        div_times.extend(times[int(i)] for i in picks)
+        div_amounts.extend(float(a) for a in rng.uniform(0.5, 3.0, k))
+        div_offsets.append(len(div_times))
+    return GroupedColumns(
+        group_offsets=(np.arange(groups + 1, dtype=np.uint32) * strikes_per_group).astype(np.uint32),
+        initial_spots=s0,
+        strikes=(s0[:, None] * moneyness[None, :]).reshape(-1).copy(),
+        maturities=maturity,
+        rates=rate,
+        volatilities=vol,
+        dividend_offsets=np.asarray(div_offsets, dtype=np.int64),
+        dividend_times=np.asarray(div_times, dtype=np.float64),
+        dividend_amounts=np.asarray(div_amounts, dtype=np.float64),
+        exercise_offsets=np.asarray(ex_offsets, dtype=np.int64),
+        exercise_times=np.asarray(ex_times, dtype=np.float64),
+    )
+
+
+def grouped_request(c: GroupedColumns, paths: int, *, seed: int = 23, support: int = 1, degree: int = 4,
+                    dividend_model: int = 1, grouped: bool = True, origin: int = 0,
+                    volatility_convention: int = 0, maturity_boundary: int = 0) -> GroupedRequest:
+    """Explicit-mesh request over the columns (cash dividends, liquidator, strictly-before maturity
+    unless overridden). support 1 = continue (the reference benchmark's choice), 0 = fail."""
+    cash = dividend_model != 0
+    return lsm_grouped_request(
+        group_offsets=c.group_offsets if grouped else None,
+        initial_spots=c.initial_spots,
+        strikes=c.strikes,
+        maturities=c.maturities,
+        rates=c.rates,
+        volatilities=c.volatilities,
+        dividend_model=dividend_model,
+        dividend_yields=None if cash else np.zeros(c.groups),
+        dividend_offsets=c.dividend_offsets if cash else None,
+        dividend_times=c.dividend_times if cash else None,
+        dividend_amounts=c.dividend_amounts if cash else None,
+        dividend_policy=0,
+        maturity_boundary=maturity_boundary,
+        volatility_convention=volatility_convention,
+        exercise_mesh=2,
+        base_intervals=None,
+        origin_exercise=origin,
+        explicit_exercise_offsets=c.exercise_offsets,
+        explicit_exercise_times=c.exercise_times,
+        training_paths=paths,
+        evaluation_paths=paths,
+        training_seed=seed,
+        training_domain_start=TRAINING_DOMAIN_START,
+        evaluation_seed=seed,
+        evaluation_domain_start=EVALUATION_DOMAIN_START,
+        polynomial_degree=degree,
+        rank_tolerance=1e-12,
+        condition_limit=1e8,
+        tie_rule=0,
+        insufficient_exercise_support=support,
+    )
+
+
+def path_steps(c: GroupedColumns, paths: int) -> int:
+    """Training + evaluation path-steps of a grouped request: paths x union-mesh intervals, both roles."""
+    total = 0
+    for g in range(c.groups):
+        ex = c.exercise_times[c.exercise_offsets[g]:c.exercise_offsets[g + 1]]
+        cash = c.dividend_times[c.dividend_offsets[g]:c.dividend_offsets[g + 1]]
+        total += np.union1d(ex, cash).size + 1  # intervals: interior union times, then maturity
+    return 2 * paths * total
