@@ -333,7 +333,116 @@ def run_ours(args: argparse.Namespace) -> dict | None:
     }
     if world == 1:
         out["cpu_baseline"] = cpu_baseline(paths)
+    if not args.skip_batched:
+        out["batched"] = run_grouped(args, executor)
     return out
+
+
+# ---- batched grouped workload ------------------------------------------------------------------
+
+GROUPED_STATES = 4096
+GROUPED_STRIKES = 8
+GROUPED_PATHS = 32768
+GROUPED_SAMPLE_STATES = 48
+
+
+def grouped_algorithmic_bytes(c, paths: int) -> dict:
+    """Algorithmic HBM bytes per call: the training rows are written once by the simulation; each
+    (state, strike) problem reads its state's rows once and reads + writes its values per row."""
+    import numpy as np
+
+    rows = np.diff(c.exercise_offsets) + 1  # explicit exercise dates + expiry (origin excluded)
+    strikes = np.diff(c.group_offsets.astype(np.int64))
+    return {
+        "batch_simulate_kernel": int((8 * rows * paths).sum()),
+        "batch_backward_kernel": int((strikes * (8 * rows * paths + 16 * (rows - 1) * paths)).sum()),
+    }
+
+
+def run_grouped(args: argparse.Namespace, executor) -> dict:
+    """The grouped batch (4096 states x 8 strikes, 32,768 + 32,768 paths per state) through the C
+    ABI with host columns in and host result columns out, per call."""
+    import _workloads
+    from finoptions import _abi
+    from finoptions._requests import batch_columns
+
+    lib = _abi.load()
+    cols = _workloads.grouped_columns(GROUPED_STATES, GROUPED_STRIKES, seed=23)
+    req = _workloads.grouped_request(cols, GROUPED_PATHS)
+    result = batch_columns(req.rows)
+    err = _abi.FoError()
+
+    def call() -> None:
+        st = lib.fo_price_lsm_grouped_f64(executor.raw, ctypes.byref(req.struct), ctypes.byref(result.struct),
+                                          ctypes.byref(err))
+        if st:
+            raise RuntimeError(err.message.decode())
+
+    steps = max(1, min(args.steps, 5))
+    for _ in range(2):
+        call()
+    clocks = ClockSampler(executor.device)
+    kernel_ms = [0.0] * 5
+    launches = 0
+    ms = (ctypes.c_double * 5)()
+    n_launch = ctypes.c_uint64()
+    with clocks:
+        t0 = time.perf_counter()
+        for _ in range(steps):
+            call()
+            lib.fo_executor_batch_kernel_ms(executor.raw, ms, 5, ctypes.byref(n_launch))
+            kernel_ms = [a + b for a, b in zip(kernel_ms, ms, strict=True)]
+            launches += int(n_launch.value)
+        wall = time.perf_counter() - t0
+    h2d, d2h = ctypes.c_uint64(), ctypes.c_uint64()
+    lib.fo_executor_batch_transfer_bytes(executor.raw, ctypes.byref(h2d), ctypes.byref(d2h))
+    names = ("batch_simulate_kernel", "batch_backward_kernel", "batch_diagnose_kernel", "batch_evaluate_kernel",
+             "batch_summarize_kernel")
+    device_ms = sum(kernel_ms) / steps
+    contracts = req.rows
+    steps_per_call = _workloads.path_steps(cols, GROUPED_PATHS)
+    algorithmic = grouped_algorithmic_bytes(cols, GROUPED_PATHS)
+    hbm_peak, peak_kind = measured_peaks()
+    kernels = {}
+    for name, total in zip(names, kernel_ms, strict=True):
+        per = total / steps
+        b = algorithmic.get(name, 0)
+        kernels[name] = {"ms_per_call": round(per, 4), "share": round(total / sum(kernel_ms), 4),
+                         "algorithmic_bytes": b, "achieved_gbs": round(b / (per / 1e3) / 1e9, 1) if b else 0.0}
+    dominant = max(algorithmic, key=lambda k: kernels[k]["ms_per_call"])
+    achieved = algorithmic[dominant] / (kernels[dominant]["ms_per_call"] / 1e3) / 1e9
+    # CPU restatement of the reference's group-parallel CpuExecutor on a bounded sample of states.
+    threads = cpu_threads()
+    sample = _workloads.grouped_columns(GROUPED_SAMPLE_STATES, GROUPED_STRIKES, seed=23)
+    sample_req = _workloads.grouped_request(sample, GROUPED_PATHS)
+    import _oracle
+
+    t0 = time.perf_counter()
+    _oracle.price_lsm_grouped(sample_req, threads)
+    cpu_s = time.perf_counter() - t0
+    return {
+        "workload": (f"grouped batch: {GROUPED_STATES} states x {GROUPED_STRIKES} strikes (K/S0 0.8..1.2), "
+                     f"{GROUPED_PATHS} + {GROUPED_PATHS} paths per state, explicit meshes of 12-52 dates, "
+                     "0-4 exercise-aligned cash dividends (liquidator), insufficient support = continue, seed 23"),
+        "contracts": contracts,
+        "path_steps_per_call": steps_per_call,
+        "calls": steps,
+        "device_ms_per_call": device_ms,
+        "device_contracts_per_s": contracts / (device_ms / 1e3),
+        "device_path_steps_per_s": steps_per_call / (device_ms / 1e3),
+        "e2e": {"contracts_per_s": contracts * steps / wall, "path_steps_per_s": steps_per_call * steps / wall,
+                "ms_per_call": wall / steps * 1e3, "h2d_bytes_per_step": int(h2d.value),
+                "d2h_bytes_per_step": int(d2h.value), "api": "fo_price_lsm_grouped_f64 (host columns in and out)"},
+        "gpu_launches": launches,
+        "kernels": kernels,
+        "roofline": {"kernel": dominant, "bound": "hbm", "achieved": round(achieved, 1), "peak": hbm_peak,
+                     "peak_source": peak_kind, "unit": "GB/s", "frac": round(achieved / hbm_peak, 4)},
+        "clocks": clocks.report(),
+        "cpu_baseline": {"contracts_per_s": GROUPED_SAMPLE_STATES * GROUPED_STRIKES / cpu_s,
+                         "path_steps_per_s": _workloads.path_steps(sample, GROUPED_PATHS) / cpu_s, "cores": threads,
+                         "kind": "port", "sample": f"the first {GROUPED_SAMPLE_STATES} states of the workload "
+                                                   f"({cpu_s:.2f} s on {threads} threads)"},
+    }
 
 
 def cpu_baseline(paths: int = PATHS) -> dict:
@@ -384,6 +493,7 @@ def main() -> None:
     parser.add_argument("--warmup", type=int, default=5)
     parser.add_argument("--impl", choices=("ours", "reference"), default="ours")
     parser.add_argument("--paths", type=int, default=PATHS, help="paths per role (profiling captures shrink it)")
+    parser.add_argument("--skip-batched", action="store_true", help="omit the grouped-batch section")
     args = parser.parse_args()
     if args.paths < 2:
         parser.error("--paths must be at least 2")

@@ -81,4 +81,12 @@ struct fo_executor {
     fo::PinnedBuffer staging;     // one-shot upload / download staging
     fo::DeviceBuffer batch;       // batch arena (plans, records, values, outputs)
     fo::PinnedBuffer batch_host;  // batch upload / download staging
+    cudaEvent_t batch_marks[FO_BATCH_KERNELS + 1] = {};  // per-kernel timing of batch waves
+    double batch_ms[FO_BATCH_KERNELS] = {};              // last batch call, summed over waves
+    uint64_t batch_launches = 0;
+    uint64_t batch_h2d = 0, batch_d2h = 0;                // bytes copied by the last batch call
+    ~fo_executor() {
+        for (cudaEvent_t& e : batch_marks)
+            if (e) cudaEventDestroy(e);
+    }
 };

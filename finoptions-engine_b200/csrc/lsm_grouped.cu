@@ -1063,6 +1063,11 @@ Error price_batch(fo_executor* ex, const BatchView& v, fo_batch_result_columns* 
     if (!e.ok()) return e;
     unsigned char* host = static_cast<unsigned char*>(ex->batch_host.ptr);
     cudaStream_t s = ex->stream;
+    for (cudaEvent_t& m : ex->batch_marks)
+        if (!m) FO_CUDA_TRY(cudaEventCreate(&m), "cudaEventCreate");
+    for (double& ms : ex->batch_ms) ms = 0.0;
+    ex->batch_launches = 0;
+    ex->batch_h2d = ex->batch_d2h = 0;
     if (launchable > 0) {
         std::memset(host, 0, in_bytes);
         for (uint64_t g = 0; g < launchable; ++g) {
@@ -1076,6 +1081,7 @@ Error price_batch(fo_executor* ex, const BatchView& v, fo_batch_result_columns* 
             std::memcpy(host + o.escrow_cash, hp.escrow_cash.data(), sizeof(double) * hp.rows());
         }
         FO_CUDA_TRY(cudaMemcpyAsync(dev, host, in_bytes, cudaMemcpyHostToDevice, s), "batch input upload");
+        ex->batch_h2d += in_bytes;
         FO_CUDA_TRY(cudaStreamSynchronize(s), "batch input upload");
     }
 
@@ -1111,6 +1117,7 @@ Error price_batch(fo_executor* ex, const BatchView& v, fo_batch_result_columns* 
         FO_CUDA_TRY(cudaMemcpyAsync(dev + L.groups, host + (L.groups - in_bytes), L.out_begin - L.groups,
                                     cudaMemcpyHostToDevice, s),
                     "batch table upload");
+        ex->batch_h2d += L.out_begin - L.groups;
         FO_CUDA_TRY(cudaMemsetAsync(dev + L.out_begin, 0xff, L.summaries - L.out_begin, s), "batch status reset");
         FO_CUDA_TRY(cudaMemsetAsync(dev + L.clear_begin, 0, L.clear_bytes, s), "batch reset");
         BatchArgs a{};
@@ -1138,13 +1145,27 @@ Error price_batch(fo_executor* ex, const BatchView& v, fo_batch_result_columns* 
         uint32_t chunks = 1;
         for (uint64_t g = w.g0; g < w.g1; ++g)
             chunks = std::max<uint32_t>(chunks, uint32_t((work[g].end_row - work[g].first_row + kEvalStrikes - 1) / kEvalStrikes));
+        cudaEvent_t* mark = ex->batch_marks;
+        FO_CUDA_TRY(cudaEventRecord(mark[0], s), "event");
         FO_CUDA_TRY(launch_batch_simulate(a, s), "batch training simulation launch");
+        FO_CUDA_TRY(cudaEventRecord(mark[1], s), "event");
         FO_CUDA_TRY(launch_batch_backward(a, s), "batch backward launch");
+        FO_CUDA_TRY(cudaEventRecord(mark[2], s), "event");
         FO_CUDA_TRY(launch_batch_diagnose(a, uint32_t(w.records), s), "batch diagnose launch");
+        FO_CUDA_TRY(cudaEventRecord(mark[3], s), "event");
         FO_CUDA_TRY(launch_batch_evaluate(a, chunks, s), "batch evaluation launch");
+        FO_CUDA_TRY(cudaEventRecord(mark[4], s), "event");
         FO_CUDA_TRY(launch_batch_summarize(a, s), "batch summary launch");
+        FO_CUDA_TRY(cudaEventRecord(mark[5], s), "event");
+        ex->batch_launches += FO_BATCH_KERNELS;
+        ex->batch_d2h += L.out_bytes;
         FO_CUDA_TRY(cudaMemcpyAsync(host, dev + L.out_begin, L.out_bytes, cudaMemcpyDeviceToHost, s), "batch result copy");
         FO_CUDA_TRY(cudaStreamSynchronize(s), "batch pricing");
+        for (int k = 0; k < FO_BATCH_KERNELS; ++k) {
+            float ms = 0.f;
+            FO_CUDA_TRY(cudaEventElapsedTime(&ms, mark[k], mark[k + 1]), "event");
+            ex->batch_ms[k] += ms;
+        }
         const auto* gst = reinterpret_cast<const GroupStatus*>(host + (L.group_status - L.out_begin));
         const auto* pst = reinterpret_cast<const ProblemStatus*>(host + (L.problem_status - L.out_begin));
         const auto* sum = reinterpret_cast<const ProblemSummary*>(host + (L.summaries - L.out_begin));
@@ -1263,6 +1284,22 @@ int fo_price_lsm_grouped_f64(fo_executor* executor, const fo_lsm_grouped_request
 int fo_price_lsm_batch_f64(fo_executor* executor, const fo_lsm_grouped_request* request, fo_batch_result_columns* out,
                            fo_error* err) {
     return entry(executor, request, out, err, false);
+}
+
+int fo_executor_batch_kernel_ms(fo_executor* executor, double* kernel_ms, uint64_t capacity, uint64_t* launches) {
+    if (!executor) return FO_ERR_EXECUTION;
+    std::lock_guard<std::mutex> lock(executor->mu);
+    for (uint64_t k = 0; kernel_ms && k < capacity && k < FO_BATCH_KERNELS; ++k) kernel_ms[k] = executor->batch_ms[k];
+    if (launches) *launches = executor->batch_launches;
+    return FO_OK;
+}
+
+int fo_executor_batch_transfer_bytes(fo_executor* executor, uint64_t* h2d_bytes, uint64_t* d2h_bytes) {
+    if (!executor) return FO_ERR_EXECUTION;
+    std::lock_guard<std::mutex> lock(executor->mu);
+    if (h2d_bytes) *h2d_bytes = executor->batch_h2d;
+    if (d2h_bytes) *d2h_bytes = executor->batch_d2h;
+    return FO_OK;
 }
 
 }  // extern "C"

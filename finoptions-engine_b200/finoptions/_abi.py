@@ -198,6 +198,8 @@ EXPORTED_SYMBOLS: Final = (
     "fo_price_lsm_call_f64_noalloc",
     "fo_price_lsm_grouped_f64",
     "fo_price_lsm_batch_f64",
+    "fo_executor_batch_kernel_ms",
+    "fo_executor_batch_transfer_bytes",
     "fo_simulate_gbm_seeded_f64",
     "fo_sample_standard_normals_f64",
     "fo_build_info",
@@ -239,6 +241,11 @@ def _declare(lib: ctypes.CDLL) -> None:
         fn = getattr(lib, name)
         fn.argtypes = [vp, ctypes.POINTER(FoLsmGroupedRequest), ctypes.POINTER(FoBatchResultColumns), err]
         fn.restype = ctypes.c_int
+    lib.fo_executor_batch_kernel_ms.argtypes = [vp, c_double_p, ctypes.c_uint64, ctypes.POINTER(ctypes.c_uint64)]
+    lib.fo_executor_batch_kernel_ms.restype = ctypes.c_int
+    u64p = ctypes.POINTER(ctypes.c_uint64)
+    lib.fo_executor_batch_transfer_bytes.argtypes = [vp, u64p, u64p]
+    lib.fo_executor_batch_transfer_bytes.restype = ctypes.c_int
     lib.fo_simulate_gbm_seeded_f64.argtypes = [vp, ctypes.POINTER(FoGbmSeededRequest), c_double_p, ctypes.c_uint64, err]
     lib.fo_simulate_gbm_seeded_f64.restype = ctypes.c_int
     lib.fo_sample_standard_normals_f64.argtypes = [

@@ -403,6 +403,16 @@ int fo_price_lsm_grouped_f64(fo_executor* executor, const fo_lsm_grouped_request
 int fo_price_lsm_batch_f64(fo_executor* executor, const fo_lsm_grouped_request* request,
                            fo_batch_result_columns* out, fo_error* err);
 
+/* Device time of the executor's last grouped / row batch call (no counterpart in the reference; a
+ * measurement hook). kernel_ms[k] receives the milliseconds of batch kernel k summed over the
+ * call's waves, k = 0 training simulation, 1 backward fits, 2 diagnostics, 3 evaluation,
+ * 4 summaries; *launches receives the number of kernel launches. Timed with CUDA events on the
+ * executor's stream. */
+#define FO_BATCH_KERNELS 5
+int fo_executor_batch_kernel_ms(fo_executor* executor, double* kernel_ms, uint64_t capacity, uint64_t* launches);
+/* Host->device and device->host bytes the executor's last batch call copied. */
+int fo_executor_batch_transfer_bytes(fo_executor* executor, uint64_t* h2d_bytes, uint64_t* d2h_bytes);
+
 /* ---- simulation exports --------------------------------------------------------------------- */
 
 typedef struct fo_gbm_seeded_request {
