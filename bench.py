@@ -367,7 +367,8 @@ def run_grouped(args: argparse.Namespace, executor) -> dict:
     from finoptions._requests import batch_columns
 
     lib = _abi.load()
-    cols = _workloads.grouped_columns(GROUPED_STATES, GROUPED_STRIKES, seed=23)
+    states = args.batched_states
+    cols = _workloads.grouped_columns(states, GROUPED_STRIKES, seed=23)
     req = _workloads.grouped_request(cols, GROUPED_PATHS)
     result = batch_columns(req.rows)
     err = _abi.FoError()
@@ -421,7 +422,7 @@ def run_grouped(args: argparse.Namespace, executor) -> dict:
     _oracle.price_lsm_grouped(sample_req, threads)
     cpu_s = time.perf_counter() - t0
     return {
-        "workload": (f"grouped batch: {GROUPED_STATES} states x {GROUPED_STRIKES} strikes (K/S0 0.8..1.2), "
+        "workload": (f"grouped batch: {states} states x {GROUPED_STRIKES} strikes (K/S0 0.8..1.2), "
                      f"{GROUPED_PATHS} + {GROUPED_PATHS} paths per state, explicit meshes of 12-52 dates, "
                      "0-4 exercise-aligned cash dividends (liquidator), insufficient support = continue, seed 23"),
         "contracts": contracts,
@@ -494,6 +495,8 @@ def main() -> None:
     parser.add_argument("--impl", choices=("ours", "reference"), default="ours")
     parser.add_argument("--paths", type=int, default=PATHS, help="paths per role (profiling captures shrink it)")
     parser.add_argument("--skip-batched", action="store_true", help="omit the grouped-batch section")
+    parser.add_argument("--batched-states", type=int, default=GROUPED_STATES,
+                        help="states of the grouped-batch section (profiling captures shrink it)")
     args = parser.parse_args()
     if args.paths < 2:
         parser.error("--paths must be at least 2")

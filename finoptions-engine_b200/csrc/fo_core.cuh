@@ -703,7 +703,9 @@ FO_HD_NOINLINE void fit_continuation(const dd* sums, double pivot, uint64_t coun
 }
 
 // PolynomialModel::predict_for (regression.rs:197-224). Returns false for a non-finite result.
-FO_HD bool predict_continuation(const FitModel& m, int degree, double predictor, double* out) {
+// Model is FitModel or any type with the same mean / scale / alpha / beta / coef fields.
+template <typename Model>
+FO_HD bool predict_continuation(const Model& m, int degree, double predictor, double* out) {
     if (!fo_isfinite(predictor)) return false;
     const double z = degree == 0 ? 0.0 : (predictor - m.mean) / m.scale;
     double prediction = m.coef[0];

@@ -80,6 +80,19 @@ enum FitFailKind : int32_t {
 // Strikes evaluated together by one evaluation thread (groups with more run several passes).
 constexpr int kEvalStrikes = 8;
 
+// The part of a fitted row the evaluation reads, staged in shared memory per (strike, row).
+struct PolicyRule {
+    double mean, scale;
+    double alpha[kMaxDegree];
+    double beta[kMaxDegree];
+    double coef[kMaxColumns];
+    int32_t kind;
+    int32_t pad;
+};
+
+// Shared memory the evaluation may spend on staged rules; larger groups read them from HBM.
+constexpr size_t kEvalRuleSmemBytes = 96 * 1024;
+
 struct BatchArgs {
     const BatchGroup* groups;
     const BatchProblem* problems;

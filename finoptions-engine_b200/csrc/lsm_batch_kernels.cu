@@ -81,6 +81,10 @@ struct BatchBackwardSmem {
     int kind;
 };
 
+// Paths a thread loads together before computing on them: the loads of one batch are independent
+// of each other and of the previous batch's stores, so several memory round trips overlap.
+constexpr int kBackwardBatch = 4;
+
 __global__ void __launch_bounds__(kBatchBackwardThreads, 2) batch_backward_kernel(BatchArgs a) {
     __shared__ BatchBackwardSmem sm;
     const BatchProblem pr = a.problems[blockIdx.x];
@@ -90,10 +94,11 @@ __global__ void __launch_bounds__(kBatchBackwardThreads, 2) batch_backward_kerne
     const DevicePlan plan = g.plan;
     ProblemStatus* st = a.problem_status + blockIdx.x;
     FitRecord* records = a.records + pr.records;
-    double* values = a.values + pr.values;
-    const double* slab = a.slab + g.slab_offset;
+    double* __restrict__ values = a.values + pr.values;
+    const double* __restrict__ slab = a.slab + g.slab_offset;
     const uint64_t P = a.train_paths;
     const unsigned T = blockDim.x;
+    const uint64_t stride = uint64_t(T) * kBackwardBatch;
     const double K = pr.strike;
     const int degree = a.degree;
     const uint32_t E = plan.rows - 1;
@@ -101,10 +106,20 @@ __global__ void __launch_bounds__(kBatchBackwardThreads, 2) batch_backward_kerne
     const int lowest = plan.origin_row ? 1 : 0;
     auto row_ptr = [&](uint32_t row) { return slab + uint64_t(row - fsr) * P; };
     {
-        const double* terminal = row_ptr(E);
-        for (uint64_t p = threadIdx.x; p < P; p += T) {
-            const double d = terminal[p] - K;
-            values[p] = d > 0.0 ? d : 0.0;
+        const double* __restrict__ terminal = row_ptr(E);
+        for (uint64_t base = threadIdx.x; base < P; base += stride) {
+            double s[kBackwardBatch];
+#pragma unroll
+            for (int u = 0; u < kBackwardBatch; ++u) {
+                const uint64_t p = base + uint64_t(u) * T;
+                s[u] = p < P ? __ldg(&terminal[p]) : 0.0;
+            }
+#pragma unroll
+            for (int u = 0; u < kBackwardBatch; ++u) {
+                const uint64_t p = base + uint64_t(u) * T;
+                const double d = s[u] - K;
+                if (p < P) values[p] = d > 0.0 ? d : 0.0;
+            }
         }
     }
     uint32_t order = 0;
@@ -116,32 +131,52 @@ __global__ void __launch_bounds__(kBatchBackwardThreads, 2) batch_backward_kerne
     if (row >= lowest) {
         // Discount into the first fitted row and locate its in-the-money mean (the moment pivot).
         const double disc = plan.disc_from_later[row];
-        const double* srow = row_ptr(uint32_t(row));
+        const double* __restrict__ srow = row_ptr(uint32_t(row));
         double loc[2] = {0.0, 0.0};
-        for (uint64_t p = threadIdx.x; p < P; p += T) {
-            const double v = values[p] * disc;
-            values[p] = v;
-            if (!fo_isfinite(v)) atomicMin(&st->fit_payoff_fail, ((unsigned long long)order << 32) | p);
-            const double sp = srow[p];
-            if (sp > K) {
-                const double x = sp / K;
-                if (fo_isfinite(x)) {
-                    loc[0] += 1.0;
-                    loc[1] += x;
+        for (uint64_t base = threadIdx.x; base < P; base += stride) {
+            double v[kBackwardBatch], s[kBackwardBatch];
+#pragma unroll
+            for (int u = 0; u < kBackwardBatch; ++u) {
+                const uint64_t p = base + uint64_t(u) * T;
+                v[u] = p < P ? values[p] : 0.0;
+                s[u] = p < P ? __ldg(&srow[p]) : 0.0;
+            }
+#pragma unroll
+            for (int u = 0; u < kBackwardBatch; ++u) {
+                const uint64_t p = base + uint64_t(u) * T;
+                if (p >= P) continue;
+                v[u] *= disc;
+                values[p] = v[u];
+                if (!fo_isfinite(v[u])) atomicMin(&st->fit_payoff_fail, ((unsigned long long)order << 32) | p);
+                if (s[u] > K) {
+                    const double x = s[u] / K;
+                    if (fo_isfinite(x)) {
+                        loc[0] += 1.0;
+                        loc[1] += x;
+                    }
                 }
             }
         }
         cta_reduce_dd<2>(loc, sm.red, sm.total);
         if (sm.total[0].hi > 0.0) pivot = dd_round(dd_div(sm.total[1], sm.total[0]));
-        for (uint64_t p = threadIdx.x; p < P; p += T) {
-            const double sp = srow[p];
-            if (sp > K) {
-                const double x = sp / K, y = values[p];
-                if (!fo_isfinite(x) || !fo_isfinite(y)) {
+        for (uint64_t base = threadIdx.x; base < P; base += stride) {
+            double v[kBackwardBatch], s[kBackwardBatch];
+#pragma unroll
+            for (int u = 0; u < kBackwardBatch; ++u) {
+                const uint64_t p = base + uint64_t(u) * T;
+                v[u] = p < P ? values[p] : 0.0;
+                s[u] = p < P ? __ldg(&srow[p]) : 0.0;
+            }
+#pragma unroll
+            for (int u = 0; u < kBackwardBatch; ++u) {
+                const uint64_t p = base + uint64_t(u) * T;
+                if (p >= P || !(s[u] > K)) continue;
+                const double x = s[u] / K;
+                if (!fo_isfinite(x) || !fo_isfinite(v[u])) {
                     sums.acc[14] += 1.0;
                     atomicMin(&st->fit_nonfinite, ((unsigned long long)order << 32) | p);
                 } else {
-                    accumulate_itm(sums, x, y, pivot);
+                    accumulate_itm(sums, x, v[u], pivot);
                 }
             }
         }
@@ -181,49 +216,74 @@ __global__ void __launch_bounds__(kBatchBackwardThreads, 2) batch_backward_kerne
         if (regression) pivot = sm.model.mean;
         const bool stage_next = row - 1 >= lowest;
         const double disc = stage_next ? plan.disc_from_later[row - 1] : 1.0;
-        const double* cur = row_ptr(uint32_t(row));
-        const double* nxt = stage_next ? row_ptr(uint32_t(row - 1)) : nullptr;
+        const double* __restrict__ cur = row_ptr(uint32_t(row));
+        const double* __restrict__ nxt = stage_next ? row_ptr(uint32_t(row - 1)) : cur;
 #pragma unroll
         for (int k = 0; k < kSlots; ++k) sums.acc[k] = 0.0;
-        for (uint64_t p = threadIdx.x; p < P; p += T) {
-            double v = values[p];
-            if (regression) {
-                const double sp = cur[p];
-                if (sp > K) {
-                    const double intrinsic = sp - K;
+        for (uint64_t base = threadIdx.x; base < P; base += stride) {
+            double v[kBackwardBatch], sc[kBackwardBatch], sn[kBackwardBatch];
+#pragma unroll
+            for (int u = 0; u < kBackwardBatch; ++u) {
+                const uint64_t p = base + uint64_t(u) * T;
+                const bool in = p < P;
+                v[u] = in ? values[p] : 0.0;
+                sc[u] = in && regression ? __ldg(&cur[p]) : 0.0;
+                sn[u] = in && stage_next ? __ldg(&nxt[p]) : 0.0;
+            }
+#pragma unroll
+            for (int u = 0; u < kBackwardBatch; ++u) {
+                const uint64_t p = base + uint64_t(u) * T;
+                if (p >= P) continue;
+                if (regression && sc[u] > K) {
+                    const double intrinsic = sc[u] - K;
                     double continuation;
-                    if (!predict_continuation(sm.model, degree, sp / K, &continuation)) {
+                    if (!predict_continuation(sm.model, degree, sc[u] / K, &continuation)) {
                         atomicMin(&st->fit_predict_fail, ((unsigned long long)order << 32) | p);
                     } else if (exercise_rule(a.tie_rule, intrinsic, continuation)) {
-                        v = intrinsic;
+                        v[u] = intrinsic;
+                    }
+                }
+                if (stage_next) {
+                    v[u] *= disc;
+                    if (!fo_isfinite(v[u]))
+                        atomicMin(&st->fit_payoff_fail, ((unsigned long long)(order + 1) << 32) | p);
+                    if (sn[u] > K) {
+                        const double x = sn[u] / K;
+                        if (!fo_isfinite(x) || !fo_isfinite(v[u])) {
+                            sums.acc[14] += 1.0;
+                            atomicMin(&st->fit_nonfinite, ((unsigned long long)(order + 1) << 32) | p);
+                        } else {
+                            accumulate_itm(sums, x, v[u], pivot);
+                        }
                     }
                 }
             }
-            if (stage_next) {
-                const double sp = nxt[p];
-                v *= disc;
-                if (!fo_isfinite(v)) atomicMin(&st->fit_payoff_fail, ((unsigned long long)(order + 1) << 32) | p);
-                if (sp > K) {
-                    const double x = sp / K;
-                    if (!fo_isfinite(x) || !fo_isfinite(v)) {
-                        sums.acc[14] += 1.0;
-                        atomicMin(&st->fit_nonfinite, ((unsigned long long)(order + 1) << 32) | p);
-                    } else {
-                        accumulate_itm(sums, x, v, pivot);
-                    }
-                }
+#pragma unroll
+            for (int u = 0; u < kBackwardBatch; ++u) {
+                const uint64_t p = base + uint64_t(u) * T;
+                if (p < P) values[p] = v[u];
             }
-            values[p] = v;
         }
     }
     // Common origin decision (policy.rs:265-281): mean of the values discounted to the origin.
     if (plan.origin_row) {
         double acc[2] = {0.0, 0.0};
-        for (uint64_t p = threadIdx.x; p < P; p += T) {
-            const double w = values[p] * plan.origin_discount;
-            if (!fo_isfinite(w)) atomicMin(&st->fit_payoff_fail, ((unsigned long long)order << 32) | p);
-            acc[0] += 1.0;
-            acc[1] += w;
+        for (uint64_t base = threadIdx.x; base < P; base += stride) {
+            double v[kBackwardBatch];
+#pragma unroll
+            for (int u = 0; u < kBackwardBatch; ++u) {
+                const uint64_t p = base + uint64_t(u) * T;
+                v[u] = p < P ? values[p] : 0.0;
+            }
+#pragma unroll
+            for (int u = 0; u < kBackwardBatch; ++u) {
+                const uint64_t p = base + uint64_t(u) * T;
+                if (p >= P) continue;
+                const double w = v[u] * plan.origin_discount;
+                if (!fo_isfinite(w)) atomicMin(&st->fit_payoff_fail, ((unsigned long long)order << 32) | p);
+                acc[0] += 1.0;
+                acc[1] += w;
+            }
         }
         cta_reduce_dd<2>(acc, sm.red, sm.total);
         if (threadIdx.x == 0) {
@@ -260,13 +320,17 @@ __global__ void batch_diagnose_kernel(BatchArgs a, uint32_t n_records) {
 // Fused evaluation: one evaluation path per thread, up to kEvalStrikes policies applied on the fly.
 // ---------------------------------------------------------------------------------------------
 
-__global__ void __launch_bounds__(kBatchEvalThreads, 2) batch_evaluate_kernel(BatchArgs a) {
+// kStaged: the group's fitted rules are copied into shared memory ([strike][row]) before the
+// paths run; otherwise each lookup reads the FitRecord from HBM / L2.
+template <bool kStaged>
+__global__ void __launch_bounds__(kBatchEvalThreads, 2) batch_evaluate_kernel(BatchArgs a, uint32_t rule_rows) {
     __shared__ double sx[257], sf[257];
     __shared__ double red[32 * 2 * kEvalStrikes];
     __shared__ dd tot[2 * kEvalStrikes];
     __shared__ unsigned cnt[2 * kEvalStrikes];
     __shared__ double strikes[kEvalStrikes];
     __shared__ uint32_t rbase[kEvalStrikes];
+    extern __shared__ PolicyRule staged[];  // [kEvalStrikes][rule_rows] when kStaged
     const BatchGroup& g = a.groups[blockIdx.y];
     const uint32_t first = g.first_problem + blockIdx.z * kEvalStrikes;
     const int ns = min(kEvalStrikes, int(g.problems) - int(blockIdx.z) * kEvalStrikes);
@@ -282,9 +346,28 @@ __global__ void __launch_bounds__(kBatchEvalThreads, 2) batch_evaluate_kernel(Ba
     }
     __syncthreads();
     const DevicePlan plan = g.plan;
+    const uint32_t rows = plan.rows;
+    if (kStaged) {
+        for (uint32_t i = threadIdx.x; i < uint32_t(ns) * rows; i += blockDim.x) {
+            const uint32_t k = i / rows, r = i % rows;
+            const FitRecord& rec = a.records[rbase[k] + r];
+            PolicyRule& rule = staged[k * rule_rows + r];
+            rule.kind = rec.kind;
+            rule.mean = rec.model.mean;
+            rule.scale = rec.model.scale;
+#pragma unroll
+            for (int j = 0; j < kMaxDegree; ++j) {
+                rule.alpha[j] = rec.model.alpha[j];
+                rule.beta[j] = rec.model.beta[j];
+            }
+#pragma unroll
+            for (int j = 0; j < kMaxColumns; ++j) rule.coef[j] = rec.model.coef[j];
+        }
+        __syncthreads();
+    }
     const uint64_t P = a.eval_paths;
     const uint64_t p = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x;
-    const uint32_t last = plan.rows - 1;
+    const uint32_t last = rows - 1;
     const int degree = a.degree;
     double payoff[kEvalStrikes];
 #pragma unroll
@@ -310,8 +393,7 @@ __global__ void __launch_bounds__(kBatchEvalThreads, 2) batch_evaluate_kernel(Ba
         for (int k = 0; k < kEvalStrikes; ++k) {
             if (!((active >> k) & 1u)) continue;
             const double K = strikes[k];
-            const FitRecord& rec = a.records[rbase[k] + row];
-            const int kind = rec.kind;
+            const int kind = kStaged ? staged[k * rule_rows + row].kind : a.records[rbase[k] + row].kind;
             if (kind == kRuleNoSupport) {
                 if (spot > K) atomicAdd(&a.itm_counts[rbase[k] + row], 1u);
                 continue;
@@ -319,7 +401,9 @@ __global__ void __launch_bounds__(kBatchEvalThreads, 2) batch_evaluate_kernel(Ba
             if (kind != kRuleRegression || !(spot > K)) continue;
             const double intrinsic = spot - K;
             double continuation;
-            if (!predict_continuation(rec.model, degree, spot / K, &continuation)) {
+            const bool ok = kStaged ? predict_continuation(staged[k * rule_rows + row], degree, spot / K, &continuation)
+                                    : predict_continuation(a.records[rbase[k] + row].model, degree, spot / K, &continuation);
+            if (!ok) {
                 atomicMin(&a.problem_status[first + k].eval_fail, ((unsigned long long)row << 33) | (p << 1));
                 continue;
             }
@@ -469,8 +553,17 @@ cudaError_t launch_batch_diagnose(const BatchArgs& a, uint32_t n_records, cudaSt
     return cudaGetLastError();
 }
 
-cudaError_t launch_batch_evaluate(const BatchArgs& a, uint32_t strike_chunks, cudaStream_t stream) {
-    batch_evaluate_kernel<<<dim3(a.eval_blocks, a.n_groups, strike_chunks), kBatchEvalThreads, 0, stream>>>(a);
+cudaError_t launch_batch_evaluate(const BatchArgs& a, uint32_t strike_chunks, uint32_t max_rows, cudaStream_t stream) {
+    const dim3 grid(a.eval_blocks, a.n_groups, strike_chunks);
+    const size_t smem = sizeof(PolicyRule) * kEvalStrikes * max_rows;
+    if (smem <= kEvalRuleSmemBytes) {
+        cudaError_t e = cudaFuncSetAttribute(batch_evaluate_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             int(kEvalRuleSmemBytes));
+        if (e != cudaSuccess) return e;
+        batch_evaluate_kernel<true><<<grid, kBatchEvalThreads, smem, stream>>>(a, max_rows);
+    } else {
+        batch_evaluate_kernel<false><<<grid, kBatchEvalThreads, 0, stream>>>(a, max_rows);
+    }
     return cudaGetLastError();
 }
 

@@ -1142,9 +1142,11 @@ Error price_batch(fo_executor* ex, const BatchView& v, fo_batch_result_columns* 
         a.condition_limit = q.condition_limit;
         a.tie_rule = q.tie_rule;
         a.support = q.insufficient_exercise_support;
-        uint32_t chunks = 1;
-        for (uint64_t g = w.g0; g < w.g1; ++g)
+        uint32_t chunks = 1, max_rows = 1;
+        for (uint64_t g = w.g0; g < w.g1; ++g) {
             chunks = std::max<uint32_t>(chunks, uint32_t((work[g].end_row - work[g].first_row + kEvalStrikes - 1) / kEvalStrikes));
+            max_rows = std::max<uint32_t>(max_rows, work[g].hp.rows());
+        }
         cudaEvent_t* mark = ex->batch_marks;
         FO_CUDA_TRY(cudaEventRecord(mark[0], s), "event");
         FO_CUDA_TRY(launch_batch_simulate(a, s), "batch training simulation launch");
@@ -1153,7 +1155,7 @@ Error price_batch(fo_executor* ex, const BatchView& v, fo_batch_result_columns* 
         FO_CUDA_TRY(cudaEventRecord(mark[2], s), "event");
         FO_CUDA_TRY(launch_batch_diagnose(a, uint32_t(w.records), s), "batch diagnose launch");
         FO_CUDA_TRY(cudaEventRecord(mark[3], s), "event");
-        FO_CUDA_TRY(launch_batch_evaluate(a, chunks, s), "batch evaluation launch");
+        FO_CUDA_TRY(launch_batch_evaluate(a, chunks, max_rows, s), "batch evaluation launch");
         FO_CUDA_TRY(cudaEventRecord(mark[4], s), "event");
         FO_CUDA_TRY(launch_batch_summarize(a, s), "batch summary launch");
         FO_CUDA_TRY(cudaEventRecord(mark[5], s), "event");

@@ -23,6 +23,15 @@
 
 namespace fo {
 
+// Asynchronous 8-byte global -> shared copies (cp.async): issued before a row's reduction, barrier
+// and solve, waited for just before the pass that reads them.
+__device__ __forceinline__ void cp_async8(void* smem, const void* gmem) {
+    const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
 __device__ __forceinline__ unsigned ld_acquire_gpu(const unsigned* p) {
     unsigned v;
     asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
@@ -175,9 +184,11 @@ __global__ void __launch_bounds__(kBackwardThreads, 1) backward_kernel(BackwardA
     }
     const int ppt = a.ppt;
     const int T = blockDim.x;
+    // values, the spots of the row being decided, and the spots of the row being staged (filled
+    // by cp.async while the current row is reduced and solved); the two spot buffers alternate.
     double* values = backward_dyn;
     double* spots = backward_dyn + size_t(ppt) * T;
-    double* xs = backward_dyn + 2 * size_t(ppt) * T;  // S / K when in the money
+    double* spots_next = backward_dyn + 2 * size_t(ppt) * T;
     const uint64_t P = plan.train_paths;
     const uint64_t nthreads = uint64_t(gridDim.x) * T;
     const uint64_t gtid = uint64_t(blockIdx.x) * T + threadIdx.x;
@@ -233,7 +244,6 @@ __global__ void __launch_bounds__(kBackwardThreads, 1) backward_kernel(BackwardA
                 }
             }
             spots[at] = sp;
-            xs[at] = x;
         }
         cta_reduce_to<2>(loc, sm.red, parts + size_t(parity) * a.partial_stride + size_t(blockIdx.x) * 2);
         if (!grid_barrier(&sm.local_gen, a.status)) return;
@@ -243,7 +253,7 @@ __global__ void __launch_bounds__(kBackwardThreads, 1) backward_kernel(BackwardA
         for (int j = 0; j < ppt; ++j) {
             const int at = j * T + threadIdx.x;
             if (spots[at] > K) {
-                const double x = xs[at], y = values[at];
+                const double x = spots[at] / K, y = values[at];
                 if (!fo_isfinite(x) || !fo_isfinite(y)) {
                     sums.acc[14] += 1.0;
                     atomicMin(&a.status->fit_nonfinite, ((unsigned long long)order << 32) | (gtid + uint64_t(j) * nthreads));
@@ -254,8 +264,21 @@ __global__ void __launch_bounds__(kBackwardThreads, 1) backward_kernel(BackwardA
         }
     }
     for (; row >= lowest; --row, ++order) {
+        const bool stage_next = row - 1 >= lowest;
+        if (stage_next) {
+            // Prefetch the next row's spots while this row is reduced, synchronised and solved.
+            const double* srow = row_ptr(uint32_t(row - 1));
+            for (int j = 0; j < ppt; ++j) {
+                const uint64_t p = gtid + uint64_t(j) * nthreads;
+                if (p < P) cp_async8(&spots_next[j * T + threadIdx.x], &srow[p]);
+            }
+            cp_async_commit();
+        }
         cta_reduce_to<kSlots>(sums.acc, sm.red, parts + size_t(parity) * a.partial_stride + size_t(blockIdx.x) * kSlots);
-        if (!grid_barrier(&sm.local_gen, a.status)) return;
+        if (!grid_barrier(&sm.local_gen, a.status)) {
+            cp_async_wait_all();
+            return;
+        }
         grid_combine<kSlots>(parts + size_t(parity) * a.partial_stride, gridDim.x, sm.total);
         parity ^= 1;
         if (threadIdx.x == 0) {
@@ -288,27 +311,27 @@ __global__ void __launch_bounds__(kBackwardThreads, 1) backward_kernel(BackwardA
             }
         }
         __syncthreads();
+        cp_async_wait_all();
         const int kind = sm.kind;
         if (kind == kRuleFitFailed) return;  // identical decision in every CTA
         const bool regression = kind == kRuleRegression;
         const FitModel& model = sm.model;  // read from shared memory
         if (regression) pivot = model.mean;
-        const bool stage_next = row - 1 >= lowest;
         const double disc = stage_next ? plan.disc_from_later[row - 1] : 1.0;
-        const double* srow = stage_next ? row_ptr(uint32_t(row - 1)) : nullptr;
 #pragma unroll
         for (int k = 0; k < kSlots; ++k) sums.acc[k] = 0.0;
 #pragma unroll 2
         for (int j = 0; j < ppt; ++j) {
             const uint64_t p = gtid + uint64_t(j) * nthreads;
             const int at = j * T + threadIdx.x;
+            if (p >= P) continue;
             double v = values[at];
             if (regression) {
                 const double sp = spots[at];
                 if (sp > K) {
                     const double intrinsic = sp - K;
                     double continuation;
-                    if (!predict_continuation(model, degree, xs[at], &continuation)) {
+                    if (!predict_continuation(model, degree, sp / K, &continuation)) {
                         atomicMin(&a.status->fit_predict_fail, ((unsigned long long)order << 32) | p);
                     } else if (exercise_rule(plan.tie_rule, intrinsic, continuation)) {
                         v = intrinsic;
@@ -316,27 +339,25 @@ __global__ void __launch_bounds__(kBackwardThreads, 1) backward_kernel(BackwardA
                 }
             }
             if (stage_next) {
-                double sp = 0.0, x = 0.0;
-                if (p < P) {
-                    sp = __ldcs(&srow[p]);
-                    v *= disc;
-                    if (!fo_isfinite(v))
-                        atomicMin(&a.status->fit_payoff_fail, ((unsigned long long)(order + 1) << 32) | p);
-                    if (sp > K) {
-                        x = sp / K;
-                        if (!fo_isfinite(x) || !fo_isfinite(v)) {
-                            sums.acc[14] += 1.0;
-                            atomicMin(&a.status->fit_nonfinite, ((unsigned long long)(order + 1) << 32) | p);
-                        } else {
-                            accumulate_itm(sums, x, v, pivot);
-                        }
+                const double sp = spots_next[at];
+                v *= disc;
+                if (!fo_isfinite(v))
+                    atomicMin(&a.status->fit_payoff_fail, ((unsigned long long)(order + 1) << 32) | p);
+                if (sp > K) {
+                    const double x = sp / K;
+                    if (!fo_isfinite(x) || !fo_isfinite(v)) {
+                        sums.acc[14] += 1.0;
+                        atomicMin(&a.status->fit_nonfinite, ((unsigned long long)(order + 1) << 32) | p);
+                    } else {
+                        accumulate_itm(sums, x, v, pivot);
                     }
                 }
-                spots[at] = sp;
-                xs[at] = x;
             }
             values[at] = v;
         }
+        double* swap = spots;
+        spots = spots_next;
+        spots_next = swap;
     }
     // Common origin decision (policy.rs:265-281): mean of values discounted to the origin.
     if (plan.origin_row) {
