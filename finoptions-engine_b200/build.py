@@ -22,7 +22,7 @@ CSRC = HERE / "csrc"
 OUT_DIR = HERE / "finoptions" / "_lib"
 OUT = OUT_DIR / "libfinoptions_cuda.so"
 BUILD_DIR = HERE / "_build"
-SOURCES = ("host.cpp", "capi.cu", "lsm_kernels.cu", "lsm_batch_kernels.cu", "lsm_grouped.cu")
+SOURCES = ("host.cpp", "capi.cu", "lsm_kernels.cu", "lsm_greeks.cu", "lsm_batch_kernels.cu", "lsm_grouped.cu")
 NVCC_FLAGS = (
     "-gencode", "arch=compute_100a,code=sm_100a",
     "-lineinfo", "-O3", "--fmad=false", "-std=c++17",

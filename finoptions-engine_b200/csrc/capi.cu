@@ -32,6 +32,9 @@ constexpr unsigned long long kNone = ~0ull;
 // Layout of a plan's device block. Everything the host reads back is contiguous at `out`.
 struct PlanLayout {
     size_t steps, events, row_node, disc_from_later, disc_to_origin, escrow_cash;  // inputs
+    size_t sqrt_dt, dt;       // per-interval sqrt(dt) and dt for the adjoint vega
+    size_t greek_partials;    // eval_blocks * kGreekSlots double2
+    size_t greek_out;         // kGreekSlots doubles (read back)
     size_t partials;          // backward partials: 2 * blocks * 16 double2
     size_t eval_partials;     // eval partials: eval_blocks * 2 double2
     size_t out;               // start of the read-back region
@@ -60,6 +63,10 @@ struct fo_lsm_call_plan {
     bool launched = false;
     cudaEvent_t marks[8] = {};   // per-kernel timing marks (created on first timed launch)
     bool timing = false;
+    bool fitted = false;         // a launch has left a fitted policy in the device records
+    bool greeks = false;         // evaluation also forms the pathwise adjoint Greeks
+    double sigma = 0.0;          // constant volatility of the request
+    GreeksArgs gk{};
     ~fo_lsm_call_plan() {
         for (cudaEvent_t& e : marks)
             if (e) cudaEventDestroy(e);
@@ -131,9 +138,12 @@ PlanLayout layout_for(const HostPlan& hp, int backward_blocks, int eval_blocks) 
     L.disc_from_later = take(sizeof(double) * rows);
     L.disc_to_origin = take(sizeof(double) * rows);
     L.escrow_cash = take(sizeof(double) * rows);
+    L.sqrt_dt = take(sizeof(double) * std::max<size_t>(hp.intervals(), 1));
+    L.dt = take(sizeof(double) * std::max<size_t>(hp.intervals(), 1));
     L.inputs_bytes = off;
     L.partials = take(sizeof(double2) * 2 * size_t(backward_blocks) * 16);
     L.eval_partials = take(sizeof(double2) * size_t(eval_blocks) * 2);
+    L.greek_partials = take(sizeof(double2) * size_t(eval_blocks) * kGreekSlots);
     off = align_up(off, 256);
     L.out = off;
     L.status = take(sizeof(DeviceStatus));
@@ -142,6 +152,7 @@ PlanLayout layout_for(const HostPlan& hp, int backward_blocks, int eval_blocks) 
     L.counts = take(sizeof(unsigned) * rows);
     L.itm_counts = take(sizeof(unsigned) * rows);
     L.replay = take(sizeof(SimFailure));
+    L.greek_out = take(sizeof(double) * kGreekSlots);
     L.out_bytes = align_up(off, 256) - L.out;
     L.total = align_up(off, 256);
     return L;
@@ -156,6 +167,12 @@ void pack_inputs(const HostPlan& hp, const PlanLayout& L, unsigned char* host) {
     std::memcpy(host + L.disc_from_later, hp.disc_from_later.data(), sizeof(double) * hp.rows());
     std::memcpy(host + L.disc_to_origin, hp.disc_to_origin.data(), sizeof(double) * hp.rows());
     std::memcpy(host + L.escrow_cash, hp.escrow_cash.data(), sizeof(double) * hp.rows());
+    auto* sqrt_dt = reinterpret_cast<double*>(host + L.sqrt_dt);
+    auto* dt = reinterpret_cast<double*>(host + L.dt);
+    for (uint32_t i = 0; i < hp.intervals(); ++i) {
+        dt[i] = hp.times[i + 1] - hp.times[i];
+        sqrt_dt[i] = std::sqrt(dt[i]);
+    }
 }
 
 DevicePlan device_plan(const HostPlan& hp, const PlanLayout& L, unsigned char* dev, uint32_t first_stored_row) {
@@ -188,6 +205,26 @@ DevicePlan device_plan(const HostPlan& hp, const PlanLayout& L, unsigned char* d
     p.escrow_cash = reinterpret_cast<const double*>(dev + L.escrow_cash);
     p.origin_discount = hp.origin_discount;
     return p;
+}
+
+// The adjoint's view of the plan: cash dividends in node order, volatility, device arrays.
+void fill_greeks_args(fo_lsm_call_plan* plan) {
+    GreeksArgs& g = plan->gk;
+    g = GreeksArgs{};
+    const HostPlan& hp = plan->hp;
+    for (uint32_t node = 1; node < hp.events.size(); ++node) {
+        if (!(hp.events[node].flags & kEventDividend)) continue;
+        if (g.dividends < uint32_t(kMaxGreekDividends)) {
+            g.div_node[g.dividends] = node;
+            g.div_amount[g.dividends] = hp.events[node].dividend_amount;
+        }
+        g.dividends += 1;
+    }
+    g.sigma = plan->sigma;
+    unsigned char* dev = static_cast<unsigned char*>(plan->d_block);
+    g.sqrt_dt = reinterpret_cast<const double*>(dev + plan->lay.sqrt_dt);
+    g.dt = reinterpret_cast<const double*>(dev + plan->lay.dt);
+    g.partials = reinterpret_cast<double2*>(dev + plan->lay.greek_partials);
 }
 
 Error plan_create(fo_executor* ex, const fo_lsm_call_request& q, bool own_memory, fo_lsm_call_plan** out) {
@@ -237,12 +274,19 @@ Error plan_create(fo_executor* ex, const fo_lsm_call_request& q, bool own_memory
     plan->d_slab = static_cast<double*>(ex->slab.ptr);
     unsigned char* dev = static_cast<unsigned char*>(plan->d_block);
     plan->dp = device_plan(hp, L, dev, plan->first_stored_row);
+    plan->sigma = q.annualized_volatility;
+    fill_greeks_args(plan.get());
     // upload inputs once
     pack_inputs(hp, L, static_cast<unsigned char*>(plan->h_out));
     FO_CUDA_TRY(cudaMemcpyAsync(dev, plan->h_out, L.inputs_bytes, cudaMemcpyHostToDevice, ex->stream), "plan upload");
     FO_CUDA_TRY(cudaStreamSynchronize(ex->stream), "plan upload");
     *out = plan.release();
     return Error{};
+}
+
+cudaError_t launch_evaluation(const fo_lsm_call_plan* plan, const EvalArgs& a) {
+    return plan->greeks ? launch_evaluate_greeks(a, plan->gk, plan->eval_blocks, plan->ex->stream)
+                        : launch_evaluate(a, plan->eval_blocks, plan->ex->stream);
 }
 
 Error plan_launch(fo_lsm_call_plan* plan) {
@@ -283,17 +327,23 @@ Error plan_launch(fo_lsm_call_plan* plan) {
         a.counts = reinterpret_cast<unsigned*>(dev + L.counts);
         a.itm_counts = reinterpret_cast<unsigned*>(dev + L.itm_counts);
         a.status = status;
-        FO_CUDA_TRY(launch_evaluate(a, plan->eval_blocks, s), "evaluation launch");
+        FO_CUDA_TRY(launch_evaluation(plan, a), "evaluation launch");
         FO_CUDA_TRY(mark(4), "event");
         FO_CUDA_TRY(launch_finalize(a.partials, plan->eval_blocks, plan->hp.eval_paths,
                                     reinterpret_cast<double*>(dev + L.result), s),
                     "finalize launch");
+        if (plan->greeks)
+            FO_CUDA_TRY(launch_finalize_greeks(plan->gk.partials, plan->eval_blocks,
+                                               reinterpret_cast<double*>(dev + L.greek_out), s),
+                        "Greeks finalize launch");
         FO_CUDA_TRY(mark(5), "event");
     }
     plan->launched = true;
+    plan->fitted = true;
     return Error{};
 }
 
+// Timed kernel segments of one launch (the Greeks finalize shares the last segment).
 uint64_t kernels_per_launch(const fo_lsm_call_plan* plan) { return plan->run_eval ? 5 : 3; }
 
 Error plan_time_launches(fo_lsm_call_plan* plan, uint32_t iterations, double* elapsed_ms, double* kernel_ms,
@@ -536,6 +586,119 @@ Error plan_collect(fo_lsm_call_plan* plan, fo_lsm_call_result* result) {
     return Error{};
 }
 
+// Pathwise adjoint Greeks of the last collected launch (lsm_greeks.cu for the per-path terms).
+Error plan_greeks(const fo_lsm_call_plan* plan, fo_lsm_call_greeks* g) {
+    if (!plan->greeks)
+        return make_error(FO_ERR_EXECUTION, FO_CODE_INVALID_ARGUMENT, "the plan does not form adjoint Greeks");
+    const HostPlan& hp = plan->hp;
+    const PlanLayout& L = plan->lay;
+    const auto* host = static_cast<const unsigned char*>(plan->h_out);
+    const auto* out = reinterpret_cast<const double*>(host + (L.greek_out - L.out));
+    const auto* counts = reinterpret_cast<const unsigned*>(host + (L.counts - L.out));
+    const auto* records = reinterpret_cast<const FitRecord*>(host + (L.records - L.out));
+    const uint64_t nodes = hp.times.size();
+    const uint32_t n_div = plan->gk.dividends;
+    if ((nodes && (!g->log_discount_sensitivities || g->log_discount_capacity < nodes)) ||
+        (n_div && (!g->dividend_sensitivities || g->dividend_capacity < n_div)))
+        return make_error(FO_ERR_EXECUTION, FO_CODE_INVALID_ARGUMENT,
+                          "Greeks buffers must hold " + std::to_string(nodes) + " log-discount and " +
+                              std::to_string(n_div) + " dividend sensitivities");
+    for (uint64_t i = 0; i < nodes; ++i) g->log_discount_sensitivities[i] = 0.0;
+    for (uint32_t j = 0; j < n_div; ++j) g->dividend_sensitivities[j] = 0.0;
+    const double K = hp.strike;
+    if (hp.origin_row && records[0].kind == kRuleOrigin && records[0].origin_exercise) {
+        // Deterministic origin exercise (policy.rs:657-669): price = max(S0 - K, 0) at node 0.
+        const double d = hp.initial_spot - K;
+        g->delta = d > 0.0 ? 1.0 : 0.0;
+        g->vega = 0.0;
+        g->log_discount_sensitivities[0] = d > 0.0 ? d : 0.0;
+        return Error{};
+    }
+    const double n = double(hp.eval_paths);
+    g->delta = out[kGreekDelta] / n;
+    g->vega = out[kGreekVega] / n;
+    double* dl = g->log_discount_sensitivities;
+    dl[0] += out[kGreekL0] / n;
+    for (uint32_t j = 0; j < n_div; ++j) {
+        dl[plan->gk.div_node[j]] += out[kGreekJump + j] / n;
+        g->dividend_sensitivities[j] = out[kGreekDividend + j] / n;
+    }
+    // Early exercise at row r contributes exactly -K exp(L_node) per stopped path.
+    const uint32_t rows = hp.rows();
+    for (uint32_t r = 0; r + 1 < rows; ++r)
+        if (counts[r]) dl[hp.row_node[r]] += -K * hp.disc_to_origin[r] * double(counts[r]) / n;
+    dl[hp.row_node[rows - 1]] += out[kGreekTerminal] / n;
+    return Error{};
+}
+
+// Re-values the plan's fitted policy on another market of the same contract shape: only the
+// initial spot, log discounts, cumulative yields, cash amounts and volatility may change.
+Error plan_revalue(fo_lsm_call_plan* plan, const fo_lsm_call_request& q, fo_lsm_call_result* result) {
+    if (!plan->fitted)
+        return make_error(FO_ERR_EXECUTION, FO_CODE_INVALID_ARGUMENT, "the plan has no fitted policy; launch it first");
+    HostPlan next;
+    Error e = build_call_plan(q, &next);
+    if (!e.ok()) return e;
+    const HostPlan& hp = plan->hp;
+    bool same = next.times.size() == hp.times.size() && next.row_node == hp.row_node &&
+                next.train_paths == hp.train_paths && next.eval_paths == hp.eval_paths &&
+                next.train_seed == hp.train_seed && next.eval_seed == hp.eval_seed &&
+                next.train_domain == hp.train_domain && next.eval_domain == hp.eval_domain &&
+                next.strike == hp.strike && next.degree == hp.degree && next.tie_rule == hp.tie_rule &&
+                next.support == hp.support && next.policy == hp.policy;
+    for (size_t i = 0; same && i < hp.times.size(); ++i)
+        same = next.times[i] == hp.times[i] && (next.events[i].flags & kEventDividend) == (hp.events[i].flags & kEventDividend);
+    if (!same)
+        return make_error(FO_ERR_EXECUTION, FO_CODE_INVALID_ARGUMENT,
+                          "a revaluation market must keep the plan's schedule, dividend nodes, strike, paths, streams "
+                          "and method");
+    plan->hp = std::move(next);
+    plan->sigma = q.annualized_volatility;
+    const PlanLayout& L = plan->lay;
+    unsigned char* dev = static_cast<unsigned char*>(plan->d_block);
+    plan->dp = device_plan(plan->hp, L, dev, plan->first_stored_row);
+    fill_greeks_args(plan);
+    fo_executor* ex = plan->ex;
+    cudaStream_t s = ex->stream;
+    pack_inputs(plan->hp, L, static_cast<unsigned char*>(plan->h_out));
+    FO_CUDA_TRY(cudaMemcpyAsync(dev, plan->h_out, L.inputs_bytes, cudaMemcpyHostToDevice, s), "revaluation upload");
+    auto* status = reinterpret_cast<DeviceStatus*>(dev + L.status);
+    FO_CUDA_TRY(cudaMemsetAsync(&status->eval_sim_fail, 0xff, sizeof(unsigned long long), s), "reset");
+    FO_CUDA_TRY(cudaMemsetAsync(&status->eval_fail, 0xff, 2 * sizeof(unsigned long long), s), "reset");
+    FO_CUDA_TRY(cudaMemsetAsync(dev + L.result, 0, sizeof(double) * 4, s), "reset");
+    FO_CUDA_TRY(cudaMemsetAsync(dev + L.counts, 0, sizeof(unsigned) * plan->hp.rows(), s), "reset");
+    FO_CUDA_TRY(cudaMemsetAsync(dev + L.itm_counts, 0, sizeof(unsigned) * plan->hp.rows(), s), "reset");
+    FO_CUDA_TRY(cudaMemsetAsync(dev + L.greek_out, 0, sizeof(double) * kGreekSlots, s), "reset");
+    if (plan->run_eval) {
+        EvalArgs a{};
+        a.plan = plan->dp;
+        a.records = reinterpret_cast<const FitRecord*>(dev + L.records);
+        a.partials = reinterpret_cast<double2*>(dev + L.eval_partials);
+        a.counts = reinterpret_cast<unsigned*>(dev + L.counts);
+        a.itm_counts = reinterpret_cast<unsigned*>(dev + L.itm_counts);
+        a.status = status;
+        FO_CUDA_TRY(launch_evaluation(plan, a), "revaluation launch");
+        FO_CUDA_TRY(launch_finalize(a.partials, plan->eval_blocks, plan->hp.eval_paths,
+                                    reinterpret_cast<double*>(dev + L.result), s),
+                    "finalize launch");
+        if (plan->greeks)
+            FO_CUDA_TRY(launch_finalize_greeks(plan->gk.partials, plan->eval_blocks,
+                                               reinterpret_cast<double*>(dev + L.greek_out), s),
+                        "Greeks finalize launch");
+    }
+    plan->launched = true;
+    return plan_collect(plan, result);
+}
+
+Error enable_greeks(fo_lsm_call_plan* plan, bool enabled) {
+    if (enabled && plan->gk.dividends > uint32_t(kMaxGreekDividends))
+        return make_error(FO_ERR_EXECUTION, FO_CODE_CAPACITY_EXCEEDED,
+                          "adjoint Greeks support at most " + std::to_string(kMaxGreekDividends) +
+                              " cash dividends per contract; observed " + std::to_string(plan->gk.dividends));
+    plan->greeks = enabled;
+    return Error{};
+}
+
 int finish(fo_error* err, const Error& e) {
     if (!e.ok()) write_error(err, e);
     return e.kind;
@@ -662,6 +825,52 @@ int fo_price_lsm_call_f64(fo_executor* executor, const fo_lsm_call_request* requ
     e = plan_launch(plan.get());
     if (e.ok()) e = plan_collect(plan.get(), result);
     return finish(err, e);
+}
+
+int fo_price_lsm_call_greeks_f64(fo_executor* executor, const fo_lsm_call_request* request, fo_lsm_call_result* result,
+                                 fo_lsm_call_greeks* greeks, fo_error* err) {
+    Error e = require(executor, "executor");
+    if (e.ok()) e = require(request, "request");
+    if (e.ok()) e = require(result, "result");
+    if (e.ok()) e = require(greeks, "greeks");
+    if (!e.ok()) return finish(err, e);
+    std::lock_guard<std::mutex> lock(executor->mu);
+    cudaSetDevice(executor->device);
+    fo_lsm_call_plan* raw = nullptr;
+    e = plan_create(executor, *request, false, &raw);
+    if (!e.ok()) return finish(err, e);
+    std::unique_ptr<fo_lsm_call_plan> plan(raw);
+    e = enable_greeks(plan.get(), true);
+    if (e.ok()) e = plan_launch(plan.get());
+    if (e.ok()) e = plan_collect(plan.get(), result);
+    if (e.ok()) e = plan_greeks(plan.get(), greeks);
+    return finish(err, e);
+}
+
+int fo_lsm_call_plan_set_greeks(fo_lsm_call_plan* plan, int32_t enabled, fo_error* err) {
+    Error e = require(plan, "plan");
+    if (!e.ok()) return finish(err, e);
+    std::lock_guard<std::mutex> lock(plan->ex->mu);
+    return finish(err, enable_greeks(plan, enabled != 0));
+}
+
+int fo_lsm_call_plan_greeks(fo_lsm_call_plan* plan, fo_lsm_call_greeks* greeks, fo_error* err) {
+    Error e = require(plan, "plan");
+    if (e.ok()) e = require(greeks, "greeks");
+    if (!e.ok()) return finish(err, e);
+    std::lock_guard<std::mutex> lock(plan->ex->mu);
+    return finish(err, plan_greeks(plan, greeks));
+}
+
+int fo_lsm_call_plan_revalue_f64(fo_lsm_call_plan* plan, const fo_lsm_call_request* market, fo_lsm_call_result* result,
+                                 fo_error* err) {
+    Error e = require(plan, "plan");
+    if (e.ok()) e = require(market, "market");
+    if (e.ok()) e = require(result, "result");
+    if (!e.ok()) return finish(err, e);
+    std::lock_guard<std::mutex> lock(plan->ex->mu);
+    cudaSetDevice(plan->ex->device);
+    return finish(err, plan_revalue(plan, *market, result));
 }
 
 int fo_simulate_gbm_seeded_f64(fo_executor* executor, const fo_gbm_seeded_request* q, double* states, uint64_t out_len,

@@ -159,6 +159,24 @@ __device__ __forceinline__ void grid_combine(const double2* partials, int blocks
     __syncthreads();
 }
 
+// CTA reduction of S per-thread doubles to double-double totals in shared memory. Warp sums are
+// formed in double by the transpose reduction; warp w then combines slots w, w + warps, ... over
+// the CTA's warps in double-double in a fixed order, so the totals do not depend on timing.
+template <int S>
+__device__ __forceinline__ void cta_reduce_dd(double (&acc)[S], double* red /* [32 * S] */, dd* out /* [S] */) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, warps = blockDim.x >> 5;
+    const double total = warp_transpose_reduce<S>(acc);
+    if (lane < S) red[warp * S + lane] = total;
+    __syncthreads();
+    for (int slot = warp; slot < S; slot += warps) {
+        dd v = dd_make(lane < warps ? red[lane * S + slot] : 0.0);
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) v = dd_add(v, shfl_dd_down(v, off));
+        if (lane == 0) out[slot] = v;
+    }
+    __syncthreads();
+}
+
 __device__ __forceinline__ bool exercise_rule(int tie_rule, double intrinsic, double continuation) {
     return tie_rule == 0 ? intrinsic > continuation : intrinsic >= continuation;
 }

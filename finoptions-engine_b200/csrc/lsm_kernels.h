@@ -31,6 +31,28 @@ struct EvalArgs {
     DeviceStatus* status;
 };
 
+// Pathwise adjoint Greeks of the fused evaluation (lsm_greeks.cu).
+constexpr int kMaxGreekDividends = 8;
+constexpr int kGreekSlots = 32;
+enum GreekSlot : int {
+    kGreekDelta = 0,     // sum of dP/dS0
+    kGreekVega = 1,      // sum of dP/dsigma
+    kGreekL0 = 2,        // sum of dP/dL_0 (drift of the first step)
+    kGreekTerminal = 3,  // sum of dP/dL_N at expiry stops (discount + last drift)
+    kGreekJump = 4,      // [kMaxGreekDividends]: sums of dP/dL at each cash-dividend node
+    kGreekDividend = kGreekJump + kMaxGreekDividends,  // [kMaxGreekDividends]: sums of dP/dD_j
+};
+
+struct GreeksArgs {
+    uint32_t dividends;                         // cash dividends of the schedule, in node order
+    uint32_t div_node[kMaxGreekDividends];
+    double div_amount[kMaxGreekDividends];
+    double sigma;
+    const double* sqrt_dt;                      // [intervals]
+    const double* dt;                           // [intervals]
+    double2* partials;                          // [blocks][kGreekSlots] double-double block sums
+};
+
 cudaError_t launch_normals(uint64_t seed, uint32_t domain, uint32_t path_start, uint64_t paths, uint32_t count,
                            double* out, unsigned long long* fail, cudaStream_t stream);
 cudaError_t launch_simulate(const DevicePlan& plan, uint64_t paths, uint64_t seed, uint32_t domain, double* out,
@@ -46,5 +68,8 @@ cudaError_t launch_diagnose(const DevicePlan& plan, FitRecord* records, cudaStre
 size_t evaluate_smem_bytes(uint32_t rows);
 cudaError_t launch_evaluate(const EvalArgs& args, int blocks, cudaStream_t stream);
 cudaError_t launch_finalize(const double2* partials, int blocks, uint64_t paths, double* out, cudaStream_t stream);
+size_t evaluate_greeks_smem_bytes(uint32_t rows);
+cudaError_t launch_evaluate_greeks(const EvalArgs& args, const GreeksArgs& greeks, int blocks, cudaStream_t stream);
+cudaError_t launch_finalize_greeks(const double2* partials, int blocks, double* out, cudaStream_t stream);
 
 }  // namespace fo

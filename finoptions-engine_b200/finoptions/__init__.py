@@ -28,6 +28,7 @@ from .batch_lsm import (
     price_lsm_call_grouped_batch,
 )
 from .dividends import BatchError, MaturityBoundary, RaggedCashDividends
+from .greeks import LsmCallContract, LsmGreeks, lsm_call_price, price_lsm_call_greeks
 from .lsm import (
     ExerciseFitDiagnostics,
     ExerciseTieRule,
@@ -104,7 +105,9 @@ __all__ = [
     "LogDiscountCurve",
     "Lsm",
     "LsmBatchResult",
+    "LsmCallContract",
     "LsmError",
+    "LsmGreeks",
     "LsmResult",
     "LsmStrikeGroups",
     "MaturityBoundary",
@@ -119,8 +122,10 @@ __all__ = [
     "UniformExerciseMesh",
     "__version__",
     "build_info",
+    "lsm_call_price",
     "price_lsm_call",
     "price_lsm_call_batch",
+    "price_lsm_call_greeks",
     "price_lsm_call_grouped_batch",
     "simulate_gbm_seeded",
 ]

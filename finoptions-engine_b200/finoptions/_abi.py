@@ -105,6 +105,15 @@ class FoLsmCallResult(ctypes.Structure):
     ]
 
 
+class FoLsmCallGreeks(ctypes.Structure):
+    _fields_ = [
+        ("delta", ctypes.c_double),
+        ("vega", ctypes.c_double),
+        ("log_discount_sensitivities", c_double_p), ("log_discount_capacity", ctypes.c_uint64),
+        ("dividend_sensitivities", c_double_p), ("dividend_capacity", ctypes.c_uint64),
+    ]
+
+
 class FoLsmGroupedRequest(ctypes.Structure):
     _fields_ = [
         ("group_offsets", c_uint32_p), ("n_group_offsets", ctypes.c_uint64),
@@ -196,6 +205,10 @@ EXPORTED_SYMBOLS: Final = (
     "fo_lsm_call_plan_stream",
     "fo_lsm_call_plan_destroy",
     "fo_price_lsm_call_f64_noalloc",
+    "fo_price_lsm_call_greeks_f64",
+    "fo_lsm_call_plan_set_greeks",
+    "fo_lsm_call_plan_greeks",
+    "fo_lsm_call_plan_revalue_f64",
     "fo_price_lsm_grouped_f64",
     "fo_price_lsm_batch_f64",
     "fo_executor_batch_kernel_ms",
@@ -235,6 +248,16 @@ def _declare(lib: ctypes.CDLL) -> None:
     lib.fo_lsm_call_plan_kernel_count.restype = ctypes.c_int
     lib.fo_lsm_call_plan_stream.argtypes = [vp, ctypes.POINTER(vp)]
     lib.fo_lsm_call_plan_stream.restype = ctypes.c_int
+    greeks = ctypes.POINTER(FoLsmCallGreeks)
+    lib.fo_price_lsm_call_greeks_f64.argtypes = [vp, ctypes.POINTER(FoLsmCallRequest), ctypes.POINTER(FoLsmCallResult),
+                                                 greeks, err]
+    lib.fo_price_lsm_call_greeks_f64.restype = ctypes.c_int
+    lib.fo_lsm_call_plan_set_greeks.argtypes = [vp, ctypes.c_int32, err]
+    lib.fo_lsm_call_plan_set_greeks.restype = ctypes.c_int
+    lib.fo_lsm_call_plan_greeks.argtypes = [vp, greeks, err]
+    lib.fo_lsm_call_plan_greeks.restype = ctypes.c_int
+    lib.fo_lsm_call_plan_revalue_f64.argtypes = [vp, ctypes.POINTER(FoLsmCallRequest), ctypes.POINTER(FoLsmCallResult), err]
+    lib.fo_lsm_call_plan_revalue_f64.restype = ctypes.c_int
     lib.fo_lsm_call_plan_destroy.argtypes = [vp]
     lib.fo_lsm_call_plan_destroy.restype = None
     for name in ("fo_price_lsm_grouped_f64", "fo_price_lsm_batch_f64"):

@@ -19,6 +19,7 @@ from ._errors import BatchError, ExecutionError, InputError, LsmError, Simulatio
 from ._requests import (
     batch_columns,
     gbm_seeded_request,
+    lsm_call_greeks,
     lsm_call_request,
     lsm_call_result,
     lsm_grouped_request,
@@ -270,6 +271,57 @@ def price_lsm_call_seeded_f64(  # noqa: PLR0913 - mirrors the reference's native
                 raise InputError(f'{prefix} "{value}"')
     _check(status, err)
     return result.as_tuple()
+
+
+def price_lsm_call_greeks_seeded_f64(  # noqa: PLR0913 - price_lsm_call_seeded_f64's signature
+    initial_spot: float,
+    strike: float,
+    schedule_times: list[float],
+    curve_times: list[float],
+    log_discounts: list[float],
+    dividend_yield_times: list[float],
+    cumulative_dividend_yields: list[float],
+    dividend_nodes: list[int],
+    dividend_amounts: list[float],
+    exercise_nodes: list[int],
+    expiry_node: int,
+    annualized_volatility: float,
+    dividend_policy: str,
+    executor: CudaExecutor,
+    training_paths: int,
+    evaluation_paths: int,
+    training_seed: int,
+    training_domain: int,
+    evaluation_seed: int,
+    evaluation_domain: int,
+    polynomial_degree: int,
+    rank_tolerance: float,
+    condition_limit: float,
+    tie_rule: str,
+    insufficient_exercise_support: str,
+) -> tuple:
+    """(NativeLsmResult, delta, vega, dP/dL per node, dP/dD per cash dividend) of the same request
+    as price_lsm_call_seeded_f64: the fixed-policy pathwise adjoint, formed in the pricing pass."""
+    handle = _executor_handle(executor)
+    request = lsm_call_request(
+        initial_spot=initial_spot, strike=strike, schedule_times=schedule_times, curve_times=curve_times,
+        log_discounts=log_discounts, dividend_yield_times=dividend_yield_times,
+        cumulative_dividend_yields=cumulative_dividend_yields, dividend_nodes=dividend_nodes,
+        dividend_amounts=dividend_amounts, exercise_nodes=exercise_nodes, expiry_node=expiry_node,
+        annualized_volatility=annualized_volatility, dividend_policy=_DIVIDEND_POLICIES.get(dividend_policy, -1),
+        training_paths=training_paths, evaluation_paths=evaluation_paths, training_seed=training_seed,
+        training_domain=training_domain, evaluation_seed=evaluation_seed, evaluation_domain=evaluation_domain,
+        polynomial_degree=polynomial_degree, rank_tolerance=rank_tolerance, condition_limit=condition_limit,
+        tie_rule=_TIE_RULES.get(tie_rule, -1),
+        insufficient_exercise_support=_SUPPORT.get(insufficient_exercise_support, -1),
+    )
+    result = lsm_call_result(request.exercise_rows)
+    greeks, d_log_discounts, d_dividends = lsm_call_greeks(len(schedule_times), len(dividend_nodes))
+    err = _abi.FoError()
+    status = _lib().fo_price_lsm_call_greeks_f64(handle, ctypes.byref(request.struct), ctypes.byref(result.struct),
+                                                 ctypes.byref(greeks), ctypes.byref(err))
+    _check(status, err)
+    return (result.as_tuple(), greeks.delta, greeks.vega, d_log_discounts.tolist(), d_dividends.tolist())
 
 
 def simulate_gbm_seeded_f64(  # noqa: PLR0913 - mirrors the reference's native signature

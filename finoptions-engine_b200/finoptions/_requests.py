@@ -155,6 +155,18 @@ def lsm_call_result(exercise_rows: int) -> CallResult:
     return CallResult(r, nodes, counts, diags)
 
 
+def lsm_call_greeks(nodes: int, dividends: int) -> tuple[_abi.FoLsmCallGreeks, np.ndarray, np.ndarray]:
+    """An fo_lsm_call_greeks with caller-owned sensitivity buffers (keep the arrays alive)."""
+    d_log_discounts = np.zeros(max(nodes, 1))
+    d_dividends = np.zeros(max(dividends, 1))
+    g = _abi.FoLsmCallGreeks()
+    g.log_discount_sensitivities = _ptr(d_log_discounts, ctypes.c_double)
+    g.log_discount_capacity = nodes
+    g.dividend_sensitivities = _ptr(d_dividends, ctypes.c_double)
+    g.dividend_capacity = dividends
+    return g, d_log_discounts[:nodes], d_dividends[:dividends]
+
+
 @dataclass
 class GroupedRequest:
     struct: _abi.FoLsmGroupedRequest

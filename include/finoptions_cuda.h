@@ -321,6 +321,33 @@ int fo_lsm_call_plan_kernel_count(const fo_lsm_call_plan* plan, uint64_t* kernel
 int fo_lsm_call_plan_stream(const fo_lsm_call_plan* plan, void** stream);
 void fo_lsm_call_plan_destroy(fo_lsm_call_plan* plan);
 
+/* ---- pathwise adjoint Greeks ----------------------------------------------------------------
+ * No counterpart in the reference, which obtains sensitivities by bump-and-reprice through
+ * price_lsm_call_seeded_f64. The fitted exercise policy is held fixed and the evaluation paths are
+ * differentiated pathwise in the same pass that prices them (the price and standard error are the
+ * plain entry's, bit for bit): delta = dP/dS0, vega = dP/dsigma, dP/dL_i for every schedule node i
+ * (L the log discounts) and dP/dD_j for every cash dividend j in node order. At most
+ * FO_MAX_GREEK_DIVIDENDS cash dividends per contract. */
+#define FO_MAX_GREEK_DIVIDENDS 8
+typedef struct fo_lsm_call_greeks {
+    double delta;
+    double vega;
+    double* log_discount_sensitivities;  uint64_t log_discount_capacity;  /* one per schedule node */
+    double* dividend_sensitivities;      uint64_t dividend_capacity;      /* one per cash dividend */
+} fo_lsm_call_greeks;
+
+int fo_price_lsm_call_greeks_f64(fo_executor* executor, const fo_lsm_call_request* request,
+                                 fo_lsm_call_result* result, fo_lsm_call_greeks* greeks, fo_error* err);
+/* Resident-plan form: enable the Greeks on a plan, then read them after a successful collect. */
+int fo_lsm_call_plan_set_greeks(fo_lsm_call_plan* plan, int32_t enabled, fo_error* err);
+int fo_lsm_call_plan_greeks(fo_lsm_call_plan* plan, fo_lsm_call_greeks* greeks, fo_error* err);
+/* Re-values the plan's last fitted policy on `market` without refitting: the market must keep the
+ * plan's schedule times, exercise and dividend nodes, strike, path counts, streams and method;
+ * the initial spot, log discounts, cumulative yields, cash amounts and volatility may change.
+ * (Fixed-policy finite differences and scenario revaluation.) Greeks, when enabled, follow. */
+int fo_lsm_call_plan_revalue_f64(fo_lsm_call_plan* plan, const fo_lsm_call_request* market,
+                                 fo_lsm_call_result* result, fo_error* err);
+
 /* Allocation-free variant of fo_price_lsm_call_f64. It has no counterpart in the reference.
  *
  * For callers that cannot allocate device memory: code whose device memory belongs to another

@@ -38,7 +38,8 @@ def test_struct_layouts_match_the_header_field_order() -> None:
     text = (Path(__file__).resolve().parents[1] / "include" / "finoptions_cuda.h").read_text()
     for struct, cls in (("fo_lsm_call_request", _abi.FoLsmCallRequest), ("fo_lsm_grouped_request", _abi.FoLsmGroupedRequest),
                         ("fo_gbm_seeded_request", _abi.FoGbmSeededRequest), ("fo_batch_result_columns", _abi.FoBatchResultColumns),
-                        ("fo_lsm_node_diagnostic", _abi.FoLsmNodeDiagnostic), ("fo_lsm_call_result", _abi.FoLsmCallResult)):
+                        ("fo_lsm_node_diagnostic", _abi.FoLsmNodeDiagnostic), ("fo_lsm_call_result", _abi.FoLsmCallResult),
+                        ("fo_lsm_call_greeks", _abi.FoLsmCallGreeks)):
         body = text[text.index(f"typedef struct {struct} {{"):]
         body = re.sub(r"/\*.*?\*/", "", body[: body.index("}")], flags=re.S)
         names = re.findall(r"\*?\s*(\w+)\s*;", body)
