@@ -335,7 +335,79 @@ def run_ours(args: argparse.Namespace) -> dict | None:
         out["cpu_baseline"] = cpu_baseline(paths)
     if not args.skip_batched:
         out["batched"] = run_grouped(args, executor)
+    if not args.skip_greeks:
+        out["greeks"] = run_greeks(args, executor)
     return out
+
+
+# ---- price + adjoint Greeks ----------------------------------------------------------------------
+
+GREEK_DIVIDENDS = ((13, 1.5), (39, 1.5))
+
+
+def greeks_kwargs(paths: int = PATHS) -> dict:
+    kw = workload_kwargs(paths)
+    kw["dividend_nodes"] = [n for n, _ in GREEK_DIVIDENDS]
+    kw["dividend_amounts"] = [a for _, a in GREEK_DIVIDENDS]
+    return kw
+
+
+def run_greeks(args: argparse.Namespace, executor) -> dict:
+    """The weekly contract with cash dividends of 1.5 at weeks 13 and 39: device time per contract
+    of the plain pricing pass and of the pass that also forms delta, vega, 53 log-discount and 2
+    dividend sensitivities (same evaluation, same standard error)."""
+    from finoptions import _abi
+    from finoptions._requests import lsm_call_greeks, lsm_call_request, lsm_call_result
+
+    lib = _abi.load()
+    paths = args.paths
+    kw = greeks_kwargs(paths)
+    req = lsm_call_request(**kw)
+    err = _abi.FoError()
+    elapsed = ctypes.c_double()
+    kernel_ms = (ctypes.c_double * 8)()
+    steps = max(3, min(args.steps, 50))
+    timings = {}
+    for name, greeks in (("plain", 0), ("price_and_greeks", 1)):
+        plan = ctypes.c_void_p()
+        if lib.fo_lsm_call_plan_create(executor.raw, ctypes.byref(req.struct), ctypes.byref(plan), ctypes.byref(err)):
+            raise RuntimeError(err.message.decode())
+        lib.fo_lsm_call_plan_set_greeks(plan, greeks, ctypes.byref(err))
+        lib.fo_lsm_call_plan_time_launches(plan, args.warmup, ctypes.byref(elapsed), None, 0, ctypes.byref(err))
+        if lib.fo_lsm_call_plan_time_launches(plan, steps, ctypes.byref(elapsed), kernel_ms, 8, ctypes.byref(err)):
+            raise RuntimeError(err.message.decode())
+        res = lsm_call_result(req.exercise_rows)
+        if lib.fo_lsm_call_plan_collect(plan, ctypes.byref(res.struct), ctypes.byref(err)):
+            raise RuntimeError(err.message.decode())
+        entry = {"ms_per_contract": elapsed.value / steps, "evaluate_ms": kernel_ms[3] / steps,
+                 "price": res.as_tuple()[0], "standard_error": res.as_tuple()[3]}
+        if greeks:
+            g, d_l, d_d = lsm_call_greeks(STEPS_IN_GRID + 1, len(GREEK_DIVIDENDS))
+            lib.fo_lsm_call_plan_greeks(plan, ctypes.byref(g), ctypes.byref(err))
+            entry.update(delta=g.delta, vega=g.vega, dividend_sensitivities=d_d.tolist(),
+                         log_discount_sensitivity_sum=float(d_l.sum()))
+        lib.fo_lsm_call_plan_destroy(plan)
+        timings[name] = entry
+    sensitivities = 2 + (STEPS_IN_GRID + 1) + len(GREEK_DIVIDENDS)
+    reprices = 2 * (2 + STEPS_IN_GRID + len(GREEK_DIVIDENDS))  # central bumps; L_0 is pinned at 0
+    threads = cpu_threads()
+    t0 = time.perf_counter()
+    oracle_price(greeks_kwargs(paths), threads)
+    cpu_price_s = time.perf_counter() - t0
+    plain_ms, greeks_ms = timings["plain"]["ms_per_contract"], timings["price_and_greeks"]["ms_per_contract"]
+    return {
+        "workload": "weekly contract of the headline with cash dividends 1.5 at weeks 13 and 39 (liquidator)",
+        "paths": paths,
+        "sensitivities": sensitivities,
+        "plain": timings["plain"],
+        "price_and_greeks": timings["price_and_greeks"],
+        "greeks_overhead": greeks_ms / plain_ms,
+        "contracts_per_s": {"plain": 1e3 / plain_ms, "price_and_greeks": 1e3 / greeks_ms},
+        "bump_and_reprice_gpu_ms": reprices * plain_ms,
+        "cpu_baseline": {"kind": "port", "cores": threads, "one_price_s": cpu_price_s,
+                         "bump_and_reprice_s": (1 + reprices) * cpu_price_s,
+                         "sample": f"one oracle price of this contract timed; {reprices} more for central bumps"},
+    }
 
 
 # ---- batched grouped workload ------------------------------------------------------------------
@@ -495,6 +567,7 @@ def main() -> None:
     parser.add_argument("--impl", choices=("ours", "reference"), default="ours")
     parser.add_argument("--paths", type=int, default=PATHS, help="paths per role (profiling captures shrink it)")
     parser.add_argument("--skip-batched", action="store_true", help="omit the grouped-batch section")
+    parser.add_argument("--skip-greeks", action="store_true", help="omit the price + Greeks section")
     parser.add_argument("--batched-states", type=int, default=GROUPED_STATES,
                         help="states of the grouped-batch section (profiling captures shrink it)")
     args = parser.parse_args()
