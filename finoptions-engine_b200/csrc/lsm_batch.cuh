@@ -107,9 +107,8 @@ struct BatchArgs {
     unsigned* itm_counts;      // [records]: in-the-money evaluation paths at unsupported rows
     double2* eval_partials;    // [problems * eval_blocks * 2]: (sum, sum of squares) as double-double
     ProblemSummary* summaries; // [problems]
-    uint64_t train_paths;
-    uint64_t eval_paths;
-    uint32_t eval_blocks;      // evaluation blocks per group
+    uint32_t train_blocks;     // training-simulation blocks of the largest group (grid x)
+    uint32_t eval_blocks;      // evaluation blocks of the largest group (grid x, partials stride)
     int32_t degree;
     double rank_tolerance;
     double condition_limit;

@@ -34,10 +34,10 @@ __global__ void __launch_bounds__(kBatchSimThreads) batch_simulate_kernel(BatchA
     __shared__ double sx[257], sf[257];
     load_zig_tables(sx, sf);
     const SmemZig zig = make_zig(sx, sf);
-    const uint64_t P = a.train_paths;
+    const BatchGroup& g = a.groups[blockIdx.y];
+    const uint64_t P = g.plan.train_paths;
     const uint64_t p = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x;
     if (p >= P) return;
-    const BatchGroup& g = a.groups[blockIdx.y];
     const DevicePlan plan = g.plan;
     const uint32_t fsr = plan.first_stored_row;
     double* out = a.slab + g.slab_offset;
@@ -78,7 +78,7 @@ __global__ void __launch_bounds__(kBatchBackwardThreads, 2) batch_backward_kerne
     FitRecord* records = a.records + pr.records;
     double* __restrict__ values = a.values + pr.values;
     const double* __restrict__ slab = a.slab + g.slab_offset;
-    const uint64_t P = a.train_paths;
+    const uint64_t P = plan.train_paths;
     const unsigned T = blockDim.x;
     const uint64_t stride = uint64_t(T) * kBackwardBatch;
     const double K = pr.strike;
@@ -317,6 +317,7 @@ __global__ void __launch_bounds__(kBatchEvalThreads, 2) batch_evaluate_kernel(Ba
     const uint32_t first = g.first_problem + blockIdx.z * kEvalStrikes;
     const int ns = min(kEvalStrikes, int(g.problems) - int(blockIdx.z) * kEvalStrikes);
     if (ns <= 0) return;  // uniform over the block
+    if (uint64_t(blockIdx.x) * blockDim.x >= g.plan.eval_paths) return;  // beyond this group's paths
     if (sim_failed(&a.group_status[blockIdx.y].train_sim_fail)) return;
     load_zig_tables(sx, sf);
     const SmemZig zig = make_zig(sx, sf);
@@ -347,7 +348,7 @@ __global__ void __launch_bounds__(kBatchEvalThreads, 2) batch_evaluate_kernel(Ba
         }
         __syncthreads();
     }
-    const uint64_t P = a.eval_paths;
+    const uint64_t P = plan.eval_paths;
     const uint64_t p = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x;
     const uint32_t last = rows - 1;
     const int degree = a.degree;
@@ -492,16 +493,17 @@ __global__ void batch_summarize_kernel(BatchArgs a) {
         s.price = d > 0.0 ? d : 0.0;
         s.sample_standard_deviation = 0.0;
         s.standard_error = 0.0;
-        s.early_paths = uint32_t(a.eval_paths);
+        s.early_paths = uint32_t(g.plan.eval_paths);
         s.expiry_paths = 0;
     } else {
         dd sum = dd_make(0.0), sumsq = dd_make(0.0);
+        const uint64_t n = g.plan.eval_paths;
+        const uint32_t blocks = uint32_t((n + kBatchEvalThreads - 1) / kBatchEvalThreads);
         const double2* part = a.eval_partials + size_t(i) * a.eval_blocks * 2;
-        for (uint32_t b = 0; b < a.eval_blocks; ++b) {
+        for (uint32_t b = 0; b < blocks; ++b) {
             sum = dd_add(sum, dd{part[2 * b].x, part[2 * b].y});
             sumsq = dd_add(sumsq, dd{part[2 * b + 1].x, part[2 * b + 1].y});
         }
-        const uint64_t n = a.eval_paths;
         const dd mean = dd_div(sum, dd_make(double(n)));
         dd m2 = dd_sub(sumsq, dd_mul(sum, mean));
         if (m2.hi < 0.0) m2 = dd_make(0.0);
@@ -520,8 +522,7 @@ __global__ void batch_summarize_kernel(BatchArgs a) {
 // ---------------------------------------------------------------------------------------------
 
 cudaError_t launch_batch_simulate(const BatchArgs& a, cudaStream_t stream) {
-    const uint64_t blocks = (a.train_paths + kBatchSimThreads - 1) / kBatchSimThreads;
-    batch_simulate_kernel<<<dim3(unsigned(blocks), a.n_groups), kBatchSimThreads, 0, stream>>>(a);
+    batch_simulate_kernel<<<dim3(a.train_blocks, a.n_groups), kBatchSimThreads, 0, stream>>>(a);
     return cudaGetLastError();
 }
 

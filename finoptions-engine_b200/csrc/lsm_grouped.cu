@@ -579,6 +579,34 @@ Error escrowed_prepaid_cash(const std::vector<double>& log_discounts, const std:
     return Error{};
 }
 
+// Conventions shared by every group of a batch.
+struct BatchMethod {
+    int32_t mesh = FO_MESH_UNIFORM;
+    uint32_t base_intervals = 0;
+    int32_t origin = FO_ORIGIN_EXCLUDED;
+    bool cash = false;         // cash-dividend schedules (spot or escrowed)
+    bool escrowed = false;
+    int32_t policy = FO_DIVIDEND_LIQUIDATOR;
+    int32_t convention = FO_ESCROWED_PREPAID_FORWARD;
+    uint64_t train_seed = 0, eval_seed = 0;
+    int32_t degree = 4;
+    double rank_tolerance = 1e-12, condition_limit = 1e8;
+    int32_t tie_rule = FO_TIE_STRICTLY_GREATER, support = FO_SUPPORT_FAIL;
+};
+
+// One group: its market, its schedule and its two populations.
+struct GroupSpec {
+    uint64_t first_row = 0, end_row = 0;
+    double s0 = 0.0, maturity = 0.0, rate = 0.0, vol = 0.0, yield = 0.0;
+    const double* cash_times = nullptr;
+    const double* cash_amounts = nullptr;
+    uint64_t n_cash = 0;
+    const double* ex_times = nullptr;  // explicit meshes
+    uint64_t n_ex = 0;
+    uint64_t train_paths = 0, eval_paths = 0;
+    uint32_t train_domain = 0, eval_domain = 0;
+};
+
 struct GroupWork {
     HostPlan hp;              // simulation plan + method (strike unused)
     uint64_t first_row = 0, end_row = 0;
@@ -586,13 +614,50 @@ struct GroupWork {
     Error fit;                // discount failure raised by the first strike's fit
 };
 
-Error build_group(const BatchView& v, uint64_t g, GroupWork* w) {
+BatchMethod method_of(const fo_lsm_grouped_request& q) {
+    BatchMethod m;
+    m.mesh = q.exercise_mesh;
+    m.base_intervals = q.base_intervals;
+    m.origin = q.exercise_mesh == FO_MESH_CASH_DIVIDEND_DATES ? int32_t(FO_ORIGIN_EXCLUDED) : q.origin_exercise;
+    m.cash = q.dividend_model != FO_MODEL_CONTINUOUS_YIELD;
+    m.escrowed = q.dividend_model == FO_MODEL_ESCROWED_CASH_DIVIDENDS;
+    m.policy = q.dividend_model == FO_MODEL_CASH_DIVIDENDS ? q.dividend_policy : int32_t(FO_DIVIDEND_LIQUIDATOR);
+    m.convention = q.volatility_convention;
+    m.train_seed = q.training_seed;
+    m.eval_seed = q.evaluation_seed;
+    m.degree = int32_t(q.polynomial_degree);
+    m.rank_tolerance = q.rank_tolerance;
+    m.condition_limit = q.condition_limit;
+    m.tie_rule = q.tie_rule;
+    m.support = q.insufficient_exercise_support;
+    return m;
+}
+
+GroupSpec spec_of(const BatchView& v, uint64_t g) {
     const fo_lsm_grouped_request& q = *v.q;
-    const uint64_t row = v.first_row(g);
-    const double maturity = q.maturities[g], rate = q.rates[g], s0 = q.initial_spots[g];
-    const double *cash_times = nullptr, *cash_amounts = nullptr;
-    uint64_t n_cash = 0;
-    if (v.cash()) v.cash_row(g, &cash_times, &cash_amounts, &n_cash);
+    GroupSpec s;
+    s.first_row = v.first_row(g);
+    s.end_row = v.end_row(g);
+    s.s0 = q.initial_spots[g];
+    s.maturity = q.maturities[g];
+    s.rate = q.rates[g];
+    s.vol = q.volatilities[g];
+    s.yield = v.cash() ? 0.0 : q.dividend_yields[g];
+    if (v.cash()) v.cash_row(g, &s.cash_times, &s.cash_amounts, &s.n_cash);
+    if (q.exercise_mesh == FO_MESH_EXPLICIT_TIMES) v.explicit_row(g, &s.ex_times, &s.n_ex);
+    s.train_paths = q.training_paths;
+    s.eval_paths = q.evaluation_paths;
+    s.train_domain = uint32_t(uint64_t(q.training_domain_start) + g);
+    s.eval_domain = uint32_t(uint64_t(q.evaluation_domain_start) + g);
+    return s;
+}
+
+Error build_group(const BatchMethod& m, const GroupSpec& gs, GroupWork* w) {
+    const uint64_t row = gs.first_row;
+    const double maturity = gs.maturity, rate = gs.rate, s0 = gs.s0;
+    const double* cash_times = gs.cash_times;
+    const double* cash_amounts = gs.cash_amounts;
+    const uint64_t n_cash = gs.n_cash;
     // resolve_exercise_mesh (pricing.rs:750-800)
     std::vector<double> times;
     const double* ex_times = nullptr;
@@ -600,25 +665,26 @@ Error build_group(const BatchView& v, uint64_t g, GroupWork* w) {
     bool all_transition = true;
     int32_t origin = FO_ORIGIN_EXCLUDED;
     Error e;
-    if (q.exercise_mesh == FO_MESH_UNIFORM) {
-        e = exact_union_times(row, maturity, q.base_intervals, cash_times, n_cash, &times);
-        origin = q.origin_exercise;
-    } else if (q.exercise_mesh == FO_MESH_CASH_DIVIDEND_DATES) {
+    if (m.mesh == FO_MESH_UNIFORM) {
+        e = exact_union_times(row, maturity, m.base_intervals, cash_times, n_cash, &times);
+        origin = m.origin;
+    } else if (m.mesh == FO_MESH_CASH_DIVIDEND_DATES) {
         e = cash_mesh_row(row, maturity, rate, cash_times, n_cash);
         if (e.ok()) e = exact_union_times(row, maturity, 1, cash_times, n_cash, &times);
     } else {
-        v.explicit_row(g, &ex_times, &n_ex);
+        ex_times = gs.ex_times;
+        n_ex = gs.n_ex;
         e = explicit_times_row(row, maturity, ex_times, n_ex);
         if (e.ok()) e = exact_explicit_union_times(row, maturity, ex_times, n_ex, cash_times, n_cash, &times);
         all_transition = false;
-        origin = q.origin_exercise;
+        origin = m.origin;
     }
     if (!e.ok()) return e;
     e = validate_time_grid(times);
     if (!e.ok()) return financial_at_row(row, e);
     // build_row_curves (pricing.rs:862-893)
     const size_t n = times.size();
-    const double yield = v.cash() ? 0.0 : q.dividend_yields[g];
+    const double yield = gs.yield;
     std::vector<double> log_discounts(n), yields(n);
     for (size_t i = 0; i < n; ++i) {
         log_discounts[i] = i == 0 ? 0.0 : -rate * times[i];
@@ -661,9 +727,9 @@ Error build_group(const BatchView& v, uint64_t g, GroupWork* w) {
     e = validate_event_schedule(times, dividend_nodes, dividend_amounts, exercise, expiry);
     if (!e.ok()) return financial_at_row(row, e);
     // path_volatility (pricing.rs:840-860)
-    double volatility = q.volatilities[g];
-    const bool escrowed = q.dividend_model == FO_MODEL_ESCROWED_CASH_DIVIDENDS;
-    if (escrowed && q.volatility_convention == FO_ESCROWED_SPOT_MATCHED_AT_ORIGIN) {
+    double volatility = gs.vol;
+    const bool escrowed = m.escrowed;
+    if (escrowed && m.convention == FO_ESCROWED_SPOT_MATCHED_AT_ORIGIN) {
         double prepaid = 0.0;
         e = escrowed_origin_prepaid_cash(row, rate, cash_times, cash_amounts, n_cash, &prepaid);
         if (!e.ok()) return e;
@@ -689,7 +755,7 @@ Error build_group(const BatchView& v, uint64_t g, GroupWork* w) {
         }
         hp.sim_start = s0 - prepaid[0];
     } else {
-        const int32_t policy = v.cash() ? q.dividend_policy : int32_t(FO_DIVIDEND_LIQUIDATOR);
+        const int32_t policy = m.policy;
         e = build_gbm_plan(times.data(), n, times.data(), n, log_discounts.data(), n, times.data(), n, yields.data(), n,
                            dividend_nodes.data(), dividend_nodes.size(), dividend_amounts.data(), dividend_amounts.size(),
                            exercise.data(), exercise.size(), expiry, volatility, policy, &hp);
@@ -698,17 +764,17 @@ Error build_group(const BatchView& v, uint64_t g, GroupWork* w) {
     }
     hp.initial_spot = s0;
     hp.strike = 0.0;
-    hp.train_paths = q.training_paths;
-    hp.eval_paths = q.evaluation_paths;
-    hp.train_seed = q.training_seed;
-    hp.eval_seed = q.evaluation_seed;
-    hp.train_domain = uint32_t(uint64_t(q.training_domain_start) + g);
-    hp.eval_domain = uint32_t(uint64_t(q.evaluation_domain_start) + g);
-    hp.degree = int32_t(q.polynomial_degree);
-    hp.rank_tolerance = q.rank_tolerance;
-    hp.condition_limit = q.condition_limit;
-    hp.tie_rule = q.tie_rule;
-    hp.support = q.insufficient_exercise_support;
+    hp.train_paths = gs.train_paths;
+    hp.eval_paths = gs.eval_paths;
+    hp.train_seed = m.train_seed;
+    hp.eval_seed = m.eval_seed;
+    hp.train_domain = gs.train_domain;
+    hp.eval_domain = gs.eval_domain;
+    hp.degree = m.degree;
+    hp.rank_tolerance = m.rank_tolerance;
+    hp.condition_limit = m.condition_limit;
+    hp.tie_rule = m.tie_rule;
+    hp.support = m.support;
     // Discounts of the fit (policy.rs:1049-1108): a failure is the first strike's fit error.
     Error fit = finish_discounts(&hp);
     if (!fit.ok()) {
@@ -733,13 +799,16 @@ struct Wave {
     uint64_t problems = 0;       // strike rows
     uint64_t records = 0;        // FitRecords (rows per problem)
     uint64_t slab_elems = 0;     // stored training states
+    uint64_t value_elems = 0;    // training values of every problem
+    uint32_t eval_blocks = 0;    // largest evaluation grid of a group (partials stride per problem)
+    uint32_t train_blocks = 0;   // largest training grid of a group
 };
 
 uint32_t eval_blocks_for(uint64_t eval_paths) {
     return uint32_t((eval_paths + kBatchEvalThreads - 1) / kBatchEvalThreads);
 }
 
-WaveLayout layout_for(const Wave& w, uint64_t train_paths, uint32_t eval_blocks, size_t base) {
+WaveLayout layout_for(const Wave& w, size_t base) {
     WaveLayout L{};
     size_t off = base;
     auto take = [&](size_t bytes) {
@@ -764,9 +833,9 @@ WaveLayout layout_for(const Wave& w, uint64_t train_paths, uint32_t eval_blocks,
     L.records = take(sizeof(FitRecord) * w.records);
     off = align_up(off, 256);
     L.clear_bytes = off - L.clear_begin;
-    L.eval_partials = take(sizeof(double2) * 2 * size_t(eval_blocks) * P);
+    L.eval_partials = take(sizeof(double2) * 2 * size_t(w.eval_blocks) * P);
     L.replay = take(sizeof(SimFailure));
-    L.values = take(sizeof(double) * train_paths * P);
+    L.values = take(sizeof(double) * std::max<uint64_t>(w.value_elems, 1));
     L.slab = take(sizeof(double) * std::max<uint64_t>(w.slab_elems, 1));
     L.total = align_up(off, 256);
     return L;
@@ -813,7 +882,6 @@ DevicePlan device_plan(const HostPlan& hp, const InputOffsets& o, unsigned char*
 
 struct BatchRun {
     fo_executor* ex;
-    const BatchView* v;
     std::vector<GroupWork>* work;
     std::vector<DevicePlan>* plans;
     const std::vector<uint64_t>* slab_of;  // wave-local group -> first slab element
@@ -961,7 +1029,8 @@ size_t memory_budget(const fo_executor* ex) {
     return std::min<size_t>(usable, size_t(48) << 30);
 }
 
-Error price_batch(fo_executor* ex, const BatchView& v, fo_batch_result_columns* out) {
+// Request validation in the reference's order (lib.rs:1302-1415, input.rs, pricing.rs:356-400).
+Error validate_request(const BatchView& v, const fo_batch_result_columns* out) {
     const fo_lsm_grouped_request& q = *v.q;
     Error e = validate_method(q);
     if (!e.ok()) return e;
@@ -976,16 +1045,22 @@ Error price_batch(fo_executor* ex, const BatchView& v, fo_batch_result_columns* 
     if (out->rows != v.rows())
         return make_error(FO_ERR_EXECUTION, FO_CODE_INVALID_ARGUMENT,
                           "result columns hold " + u(out->rows) + " rows; the batch has " + u(v.rows()));
+    return Error{};
+}
 
+// Prices validated groups: host plans, waves within the memory budget, five kernels per wave,
+// the lowest failing group's typed error or the row-aligned result columns.
+Error price_groups(fo_executor* ex, const BatchMethod& m, const std::vector<GroupSpec>& specs, const double* strikes,
+                   fo_batch_result_columns* out) {
     // Per-group plans on the host. Only groups before the first one whose plan fails can matter.
-    const uint64_t groups = v.groups();
+    const uint64_t groups = specs.size();
     std::vector<GroupWork> work(groups);
     uint64_t launchable = groups;
     for (uint64_t g = 0; g < groups; ++g) {
         GroupWork& w = work[g];
-        w.first_row = v.first_row(g);
-        w.end_row = v.end_row(g);
-        w.build = build_group(v, g, &w);
+        w.first_row = specs[g].first_row;
+        w.end_row = specs[g].end_row;
+        w.build = build_group(m, specs[g], &w);
         if (!w.build.ok()) {
             launchable = g;
             break;
@@ -1014,22 +1089,22 @@ Error price_batch(fo_executor* ex, const BatchView& v, fo_batch_result_columns* 
     in_bytes = align_up(std::max<size_t>(in_bytes, 16), 256);
 
     // Waves: consecutive groups within the memory budget (and the grid's y extent).
-    const uint64_t P = q.training_paths;
-    const uint32_t eval_blocks = eval_blocks_for(q.evaluation_paths);
     const size_t budget = memory_budget(ex);
     std::vector<Wave> waves;
     {
         Wave cur;
-        cur.g0 = cur.g1 = 0;
         size_t bytes = 0;
         for (uint64_t g = 0; g < launchable; ++g) {
             const HostPlan& hp = work[g].hp;
-            const uint64_t strikes = work[g].end_row - work[g].first_row;
+            const uint64_t strikes_g = work[g].end_row - work[g].first_row;
             const uint64_t rows = hp.rows();
             const uint64_t stored = rows - (hp.origin_row ? 1 : 0);
-            const size_t cost = sizeof(double) * (stored * P + strikes * P) +
-                                strikes * (rows * (sizeof(FitRecord) + sizeof(unsigned)) + 2 * size_t(eval_blocks) * sizeof(double2) +
-                                           sizeof(BatchProblem) + sizeof(ProblemStatus) + sizeof(ProblemSummary) + 8) +
+            const uint32_t eval_blocks = eval_blocks_for(hp.eval_paths);
+            const uint32_t train_blocks = eval_blocks_for(hp.train_paths);
+            const size_t cost = sizeof(double) * (stored + strikes_g) * hp.train_paths +
+                                strikes_g * (rows * (sizeof(FitRecord) + sizeof(unsigned)) +
+                                             2 * size_t(std::max(eval_blocks, cur.eval_blocks)) * sizeof(double2) +
+                                             sizeof(BatchProblem) + sizeof(ProblemStatus) + sizeof(ProblemSummary) + 8) +
                                 sizeof(BatchGroup) + sizeof(GroupStatus) + 1024;
             if (cur.g1 > cur.g0 && (bytes + cost > budget || cur.g1 - cur.g0 >= 65535)) {
                 waves.push_back(cur);
@@ -1038,16 +1113,19 @@ Error price_batch(fo_executor* ex, const BatchView& v, fo_batch_result_columns* 
                 bytes = 0;
             }
             cur.g1 = g + 1;
-            cur.problems += strikes;
-            cur.records += strikes * rows;
-            cur.slab_elems += stored * P;
+            cur.problems += strikes_g;
+            cur.records += strikes_g * rows;
+            cur.slab_elems += stored * hp.train_paths;
+            cur.value_elems += strikes_g * hp.train_paths;
+            cur.eval_blocks = std::max(cur.eval_blocks, eval_blocks);
+            cur.train_blocks = std::max(cur.train_blocks, train_blocks);
             bytes += cost;
         }
         if (cur.g1 > cur.g0) waves.push_back(cur);
     }
     size_t arena = in_bytes;
-    for (const Wave& w : waves) arena = std::max(arena, layout_for(w, P, eval_blocks, in_bytes).total);
-    e = ex->batch.reserve(arena);
+    for (const Wave& w : waves) arena = std::max(arena, layout_for(w, in_bytes).total);
+    Error e = ex->batch.reserve(arena);
     if (!e.ok()) return e;
     unsigned char* dev = static_cast<unsigned char*>(ex->batch.ptr);
     std::vector<DevicePlan> plans(launchable);
@@ -1056,15 +1134,15 @@ Error price_batch(fo_executor* ex, const BatchView& v, fo_batch_result_columns* 
     // Host staging: inputs, then per wave the group / problem tables and the read-back region.
     size_t stage = in_bytes;
     for (const Wave& w : waves) {
-        const WaveLayout L = layout_for(w, P, eval_blocks, 0);
+        const WaveLayout L = layout_for(w, 0);
         stage = std::max(stage, std::max(L.out_begin, L.out_bytes));
     }
     e = ex->batch_host.reserve(stage);
     if (!e.ok()) return e;
     unsigned char* host = static_cast<unsigned char*>(ex->batch_host.ptr);
     cudaStream_t s = ex->stream;
-    for (cudaEvent_t& m : ex->batch_marks)
-        if (!m) FO_CUDA_TRY(cudaEventCreate(&m), "cudaEventCreate");
+    for (cudaEvent_t& mk : ex->batch_marks)
+        if (!mk) FO_CUDA_TRY(cudaEventCreate(&mk), "cudaEventCreate");
     for (double& ms : ex->batch_ms) ms = 0.0;
     ex->batch_launches = 0;
     ex->batch_h2d = ex->batch_d2h = 0;
@@ -1087,12 +1165,13 @@ Error price_batch(fo_executor* ex, const BatchView& v, fo_batch_result_columns* 
 
     std::vector<uint64_t> slab_of;
     for (const Wave& w : waves) {
-        const WaveLayout L = layout_for(w, P, eval_blocks, in_bytes);
+        const WaveLayout L = layout_for(w, in_bytes);
         // Group and problem tables.
         auto* hg = reinterpret_cast<BatchGroup*>(host + (L.groups - in_bytes));
         auto* hpb = reinterpret_cast<BatchProblem*>(host + (L.problems - in_bytes));
-        uint64_t slab = 0, record = 0, problem = 0;
+        uint64_t slab = 0, record = 0, problem = 0, values = 0;
         slab_of.assign(w.g1 - w.g0, 0);
+        uint32_t chunks = 1, max_rows = 1;
         for (uint64_t g = w.g0; g < w.g1; ++g) {
             const HostPlan& hp = work[g].hp;
             BatchGroup& bg = hg[g - w.g0];
@@ -1103,16 +1182,19 @@ Error price_batch(fo_executor* ex, const BatchView& v, fo_batch_result_columns* 
             bg.problems = uint32_t(work[g].end_row - work[g].first_row);
             for (uint64_t r = work[g].first_row; r < work[g].end_row; ++r) {
                 BatchProblem& pb = hpb[problem];
-                pb.strike = q.strikes[r];
+                pb.strike = strikes[r];
                 pb.group = uint32_t(g - w.g0);
                 pb.records = uint32_t(record);
-                pb.values = problem * P;
+                pb.values = values;
                 pb.skip_fit = work[g].fit.ok() ? 0 : 1;
                 pb.pad = 0;
                 record += hp.rows();
+                values += hp.train_paths;
                 problem += 1;
             }
-            slab += uint64_t(hp.rows() - (hp.origin_row ? 1 : 0)) * P;
+            slab += uint64_t(hp.rows() - (hp.origin_row ? 1 : 0)) * hp.train_paths;
+            chunks = std::max<uint32_t>(chunks, uint32_t((bg.problems + kEvalStrikes - 1) / kEvalStrikes));
+            max_rows = std::max<uint32_t>(max_rows, hp.rows());
         }
         FO_CUDA_TRY(cudaMemcpyAsync(dev + L.groups, host + (L.groups - in_bytes), L.out_begin - L.groups,
                                     cudaMemcpyHostToDevice, s),
@@ -1134,19 +1216,13 @@ Error price_batch(fo_executor* ex, const BatchView& v, fo_batch_result_columns* 
         a.itm_counts = reinterpret_cast<unsigned*>(dev + L.itm_counts);
         a.eval_partials = reinterpret_cast<double2*>(dev + L.eval_partials);
         a.summaries = reinterpret_cast<ProblemSummary*>(dev + L.summaries);
-        a.train_paths = P;
-        a.eval_paths = q.evaluation_paths;
-        a.eval_blocks = eval_blocks;
-        a.degree = int32_t(q.polynomial_degree);
-        a.rank_tolerance = q.rank_tolerance;
-        a.condition_limit = q.condition_limit;
-        a.tie_rule = q.tie_rule;
-        a.support = q.insufficient_exercise_support;
-        uint32_t chunks = 1, max_rows = 1;
-        for (uint64_t g = w.g0; g < w.g1; ++g) {
-            chunks = std::max<uint32_t>(chunks, uint32_t((work[g].end_row - work[g].first_row + kEvalStrikes - 1) / kEvalStrikes));
-            max_rows = std::max<uint32_t>(max_rows, work[g].hp.rows());
-        }
+        a.train_blocks = w.train_blocks;
+        a.eval_blocks = w.eval_blocks;
+        a.degree = m.degree;
+        a.rank_tolerance = m.rank_tolerance;
+        a.condition_limit = m.condition_limit;
+        a.tie_rule = m.tie_rule;
+        a.support = m.support;
         cudaEvent_t* mark = ex->batch_marks;
         FO_CUDA_TRY(cudaEventRecord(mark[0], s), "event");
         FO_CUDA_TRY(launch_batch_simulate(a, s), "batch training simulation launch");
@@ -1160,8 +1236,8 @@ Error price_batch(fo_executor* ex, const BatchView& v, fo_batch_result_columns* 
         FO_CUDA_TRY(launch_batch_summarize(a, s), "batch summary launch");
         FO_CUDA_TRY(cudaEventRecord(mark[5], s), "event");
         ex->batch_launches += FO_BATCH_KERNELS;
-        ex->batch_d2h += L.out_bytes;
         FO_CUDA_TRY(cudaMemcpyAsync(host, dev + L.out_begin, L.out_bytes, cudaMemcpyDeviceToHost, s), "batch result copy");
+        ex->batch_d2h += L.out_bytes;
         FO_CUDA_TRY(cudaStreamSynchronize(s), "batch pricing");
         for (int k = 0; k < FO_BATCH_KERNELS; ++k) {
             float ms = 0.f;
@@ -1171,16 +1247,16 @@ Error price_batch(fo_executor* ex, const BatchView& v, fo_batch_result_columns* 
         const auto* gst = reinterpret_cast<const GroupStatus*>(host + (L.group_status - L.out_begin));
         const auto* pst = reinterpret_cast<const ProblemStatus*>(host + (L.problem_status - L.out_begin));
         const auto* sum = reinterpret_cast<const ProblemSummary*>(host + (L.summaries - L.out_begin));
-        BatchRun run{ex, &v, &work, &plans, &slab_of, dev, L, w};
+        BatchRun run{ex, &work, &plans, &slab_of, dev, L, w};
         // Failure scan in group order (the lowest failing group wins).
         uint64_t i0 = 0;
         uint64_t first_record = 0;
         for (uint64_t g = w.g0; g < w.g1; ++g) {
             const GroupWork& gw = work[g];
-            const uint64_t strikes = gw.end_row - gw.first_row;
+            const uint64_t strikes_g = gw.end_row - gw.first_row;
             const GroupStatus& gs = gst[g - w.g0];
             bool failed = gs.train_sim_fail != kNone || !gw.fit.ok() || gs.eval_sim_fail != kNone;
-            for (uint64_t k = 0; k < strikes && !failed; ++k) {
+            for (uint64_t k = 0; k < strikes_g && !failed; ++k) {
                 const ProblemSummary& ps = sum[i0 + k];
                 const ProblemStatus& st = pst[i0 + k];
                 failed = ps.fit_fail_order != 0xffffffffu ||
@@ -1192,19 +1268,19 @@ Error price_batch(fo_executor* ex, const BatchView& v, fo_batch_result_columns* 
                 if (gs.train_sim_fail != kNone) return simulation_failure(run, g, true, gs.train_sim_fail);
                 if (!gw.fit.ok()) return estimator_at_row(gw.first_row, gw.fit);
                 uint64_t rec = first_record;
-                for (uint64_t k = 0; k < strikes; ++k) {
+                for (uint64_t k = 0; k < strikes_g; ++k) {
                     const ProblemSummary& ps = sum[i0 + k];
                     BatchProblem pr{};
-                    pr.strike = q.strikes[gw.first_row + k];
+                    pr.strike = strikes[gw.first_row + k];
                     pr.records = uint32_t(rec);
                     rec += gw.hp.rows();
                     if (ps.fit_fail_order != 0xffffffffu) return fit_error(run, g, gw.first_row + k, pr, pst[i0 + k], ps);
                 }
                 if (gs.eval_sim_fail != kNone) return simulation_failure(run, g, false, gs.eval_sim_fail);
                 rec = first_record;
-                for (uint64_t k = 0; k < strikes; ++k) {
+                for (uint64_t k = 0; k < strikes_g; ++k) {
                     BatchProblem pr{};
-                    pr.strike = q.strikes[gw.first_row + k];
+                    pr.strike = strikes[gw.first_row + k];
                     pr.records = uint32_t(rec);
                     rec += gw.hp.rows();
                     Error ee = evaluation_error(run, g, gw.first_row + k, pr, pst[i0 + k], sum[i0 + k]);
@@ -1214,7 +1290,7 @@ Error price_batch(fo_executor* ex, const BatchView& v, fo_batch_result_columns* 
                                   "parallel LSM batch reported row " + u(gw.first_row) +
                                       " as failed, but deterministic serial replay succeeded");
             }
-            for (uint64_t k = 0; k < strikes; ++k) {
+            for (uint64_t k = 0; k < strikes_g; ++k) {
                 const ProblemSummary& ps = sum[i0 + k];
                 const uint64_t r = gw.first_row + k;
                 out->prices[r] = ps.price;
@@ -1230,12 +1306,145 @@ Error price_batch(fo_executor* ex, const BatchView& v, fo_batch_result_columns* 
                 out->early_exercise_paths[r] = ps.early_paths;
                 out->expiry_paths[r] = ps.expiry_paths;
             }
-            i0 += strikes;
-            first_record += strikes * gw.hp.rows();
+            i0 += strikes_g;
+            first_record += strikes_g * gw.hp.rows();
         }
     }
     if (launchable < groups) return work[launchable].build;
     return Error{};
+}
+
+Error price_batch(fo_executor* ex, const BatchView& v, fo_batch_result_columns* out) {
+    Error e = validate_request(v, out);
+    if (!e.ok()) return e;
+    std::vector<GroupSpec> specs(v.groups());
+    for (uint64_t g = 0; g < specs.size(); ++g) specs[g] = spec_of(v, g);
+    return price_groups(ex, method_of(*v.q), specs, v.q->strikes, out);
+}
+
+// ---- ragged batches (per-contract path counts; no reference counterpart) -----------------------
+
+Error validate_ragged(const fo_lsm_ragged_request& q, const fo_batch_result_columns* out) {
+    // The regression method first, as parse_batch_lsm_method does for the batch routes.
+    fo_lsm_grouped_request m{};
+    m.polynomial_degree = q.polynomial_degree;
+    m.rank_tolerance = q.rank_tolerance;
+    m.condition_limit = q.condition_limit;
+    m.tie_rule = q.tie_rule;
+    m.insufficient_exercise_support = q.insufficient_exercise_support;
+    m.exercise_mesh = FO_MESH_CASH_DIVIDEND_DATES;  // no mesh fields to check here
+    m.training_paths = 1;
+    m.evaluation_paths = 2;
+    Error e = validate_method(m);
+    if (!e.ok()) return e;
+    const uint64_t rows = q.rows;
+    if (rows == 0) return input_error(FO_CODE_EMPTY_BATCH, "LSM call batch must contain at least one contract");
+    if (!q.initial_spots || !q.strikes || !q.maturities || !q.rates || !q.volatilities || !q.exercise_offsets ||
+        (!q.exercise_times && q.n_exercise_times) || !q.training_paths || !q.evaluation_paths)
+        return make_error(FO_ERR_EXECUTION, FO_CODE_INVALID_ARGUMENT,
+                          "ragged batch columns (spots, strikes, maturities, rates, volatilities, exercise offsets, "
+                          "path counts) must not be NULL");
+    if (q.origin_exercise != FO_ORIGIN_INCLUDED && q.origin_exercise != FO_ORIGIN_EXCLUDED)
+        return input_error(FO_CODE_UNSUPPORTED_ENUM, "unsupported origin exercise convention " + std::to_string(q.origin_exercise));
+    e = validate_ragged_exercise(q.exercise_offsets, q.n_exercise_offsets, q.exercise_times, q.n_exercise_times);
+    if (!e.ok()) return e;
+    if (q.n_exercise_offsets != rows + 1) return row_count("exercise_times", rows, q.n_exercise_offsets - 1);
+    const bool cash = q.dividend_offsets != nullptr;
+    if (cash) {
+        if (q.dividend_policy != FO_DIVIDEND_LIQUIDATOR && q.dividend_policy != FO_DIVIDEND_SURVIVOR)
+            return input_error(FO_CODE_UNSUPPORTED_ENUM, "unsupported dividend policy " + std::to_string(q.dividend_policy));
+        if (q.maturity_boundary != FO_MATURITY_STRICTLY_BEFORE && q.maturity_boundary != FO_MATURITY_AT_OR_BEFORE)
+            return input_error(FO_CODE_UNSUPPORTED_CASH_MATURITY_BOUNDARY,
+                               "cash-dividend maturity boundary is unsupported by this LSM engine");
+        e = validate_ragged_cash(q.dividend_offsets, q.n_dividend_offsets, q.dividend_times, q.n_dividend_events,
+                                 q.dividend_amounts, q.n_dividend_events);
+        if (!e.ok()) {
+            e.kind = FO_ERR_INPUT;
+            return e;
+        }
+        if (q.n_dividend_offsets != rows + 1) return row_count("dividend_model", rows, q.n_dividend_offsets - 1);
+    }
+    auto path_count = [](const char* population, uint64_t row, uint64_t n, uint64_t minimum) -> Error {
+        if (n < minimum || n > kU32Max)
+            return input_error(FO_CODE_BATCH_PATH_COUNT_OUTSIDE_DOMAIN,
+                               std::string("batched LSM ") + population + " path count " + u(n) + " at row " + u(row) +
+                                   " is outside [" + u(minimum) + ", 4294967295]");
+        return Error{};
+    };
+    const int64_t ex_base = q.exercise_offsets[0];
+    const int64_t cash_base = cash ? q.dividend_offsets[0] : 0;
+    for (uint64_t r = 0; r < rows; ++r) {
+        e = nonnegative_value("initial_spots", r, q.initial_spots[r]);
+        if (e.ok()) e = positive_value("strikes", r, q.strikes[r]);
+        if (e.ok()) e = positive_value("maturities", r, q.maturities[r]);
+        if (e.ok()) e = finite_value("constant_continuously_compounded_rates", r, q.rates[r]);
+        if (e.ok()) e = positive_value("constant_volatilities", r, q.volatilities[r]);
+        if (e.ok() && q.dividend_yields) e = nonnegative_value("continuous_dividend_yields", r, q.dividend_yields[r]);
+        if (e.ok() && cash) {
+            const int64_t b = q.dividend_offsets[r] - cash_base, en = q.dividend_offsets[r + 1] - cash_base;
+            e = validate_cash_schedule(r, q.maturities[r], q.dividend_times + b, uint64_t(en - b), q.maturity_boundary);
+        }
+        if (e.ok()) {
+            const int64_t b = q.exercise_offsets[r] - ex_base, en = q.exercise_offsets[r + 1] - ex_base;
+            e = explicit_times_row(r, q.maturities[r], q.exercise_times + b, uint64_t(en - b));
+        }
+        if (e.ok()) e = path_count("training", r, q.training_paths[r], 1);
+        if (e.ok()) e = path_count("evaluation", r, q.evaluation_paths[r], 2);
+        if (!e.ok()) return e;
+    }
+    fo_lsm_grouped_request streams{};
+    streams.training_domain_start = q.training_domain_start;
+    streams.evaluation_domain_start = q.evaluation_domain_start;
+    e = validate_streams(streams, rows);
+    if (!e.ok()) return e;
+    if (out->rows != rows)
+        return make_error(FO_ERR_EXECUTION, FO_CODE_INVALID_ARGUMENT,
+                          "result columns hold " + u(out->rows) + " rows; the batch has " + u(rows));
+    return Error{};
+}
+
+Error price_ragged(fo_executor* ex, const fo_lsm_ragged_request& q, fo_batch_result_columns* out) {
+    Error e = validate_ragged(q, out);
+    if (!e.ok()) return e;
+    BatchMethod m;
+    m.mesh = FO_MESH_EXPLICIT_TIMES;
+    m.origin = q.origin_exercise;
+    m.cash = q.dividend_offsets != nullptr;
+    m.policy = m.cash ? q.dividend_policy : int32_t(FO_DIVIDEND_LIQUIDATOR);
+    m.train_seed = q.training_seed;
+    m.eval_seed = q.evaluation_seed;
+    m.degree = int32_t(q.polynomial_degree);
+    m.rank_tolerance = q.rank_tolerance;
+    m.condition_limit = q.condition_limit;
+    m.tie_rule = q.tie_rule;
+    m.support = q.insufficient_exercise_support;
+    std::vector<GroupSpec> specs(q.rows);
+    const int64_t ex_base = q.exercise_offsets[0];
+    const int64_t cash_base = m.cash ? q.dividend_offsets[0] : 0;
+    for (uint64_t r = 0; r < q.rows; ++r) {
+        GroupSpec& s = specs[r];
+        s.first_row = r;
+        s.end_row = r + 1;
+        s.s0 = q.initial_spots[r];
+        s.maturity = q.maturities[r];
+        s.rate = q.rates[r];
+        s.vol = q.volatilities[r];
+        s.yield = q.dividend_yields ? q.dividend_yields[r] : 0.0;
+        if (m.cash) {
+            const int64_t b = q.dividend_offsets[r] - cash_base, en = q.dividend_offsets[r + 1] - cash_base;
+            s.cash_times = q.dividend_times + b;
+            s.cash_amounts = q.dividend_amounts + b;
+            s.n_cash = uint64_t(en - b);
+        }
+        const int64_t b = q.exercise_offsets[r] - ex_base, en = q.exercise_offsets[r + 1] - ex_base;
+        s.ex_times = q.exercise_times + b;
+        s.n_ex = uint64_t(en - b);
+        s.train_paths = q.training_paths[r];
+        s.eval_paths = q.evaluation_paths[r];
+        s.train_domain = uint32_t(uint64_t(q.training_domain_start) + r);
+        s.eval_domain = uint32_t(uint64_t(q.evaluation_domain_start) + r);
+    }
+    return price_groups(ex, m, specs, q.strikes, out);
 }
 
 int finish(fo_error* err, const Error& e) {
@@ -1286,6 +1495,25 @@ int fo_price_lsm_grouped_f64(fo_executor* executor, const fo_lsm_grouped_request
 int fo_price_lsm_batch_f64(fo_executor* executor, const fo_lsm_grouped_request* request, fo_batch_result_columns* out,
                            fo_error* err) {
     return entry(executor, request, out, err, false);
+}
+
+int fo_price_lsm_ragged_f64(fo_executor* executor, const fo_lsm_ragged_request* request, fo_batch_result_columns* out,
+                            fo_ragged_greeks_columns* greeks, fo_error* err) {
+    if (!executor || !request)
+        return finish(err, make_error(FO_ERR_EXECUTION, FO_CODE_INVALID_ARGUMENT, "executor and request must not be NULL"));
+    Error e = check_columns(out);
+    if (!e.ok()) return finish(err, e);
+    if (greeks)
+        return finish(err, make_error(FO_ERR_EXECUTION, FO_CODE_INVALID_ARGUMENT,
+                                      "ragged-batch Greeks are not available in this build"));
+    std::lock_guard<std::mutex> lock(executor->mu);
+    cudaError_t ce = cudaSetDevice(executor->device);
+    if (ce != cudaSuccess) return finish(err, cuda_error(ce, "cudaSetDevice"));
+    try {
+        return finish(err, price_ragged(executor, *request, out));
+    } catch (const std::bad_alloc&) {
+        return finish(err, make_error(FO_ERR_EXECUTION, FO_CODE_CAPACITY_EXCEEDED, "host memory exhausted"));
+    }
 }
 
 int fo_executor_batch_kernel_ms(fo_executor* executor, double* kernel_ms, uint64_t capacity, uint64_t* launches) {

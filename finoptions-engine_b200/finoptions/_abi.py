@@ -149,6 +149,46 @@ class FoLsmGroupedRequest(ctypes.Structure):
     ]
 
 
+class FoLsmRaggedRequest(ctypes.Structure):
+    _fields_ = [
+        ("rows", ctypes.c_uint64),
+        ("initial_spots", c_double_p),
+        ("strikes", c_double_p),
+        ("maturities", c_double_p),
+        ("rates", c_double_p),
+        ("volatilities", c_double_p),
+        ("dividend_yields", c_double_p),
+        ("dividend_offsets", ctypes.POINTER(ctypes.c_int64)), ("n_dividend_offsets", ctypes.c_uint64),
+        ("dividend_times", c_double_p), ("dividend_amounts", c_double_p), ("n_dividend_events", ctypes.c_uint64),
+        ("dividend_policy", ctypes.c_int32),
+        ("maturity_boundary", ctypes.c_int32),
+        ("exercise_offsets", ctypes.POINTER(ctypes.c_int64)), ("n_exercise_offsets", ctypes.c_uint64),
+        ("exercise_times", c_double_p), ("n_exercise_times", ctypes.c_uint64),
+        ("origin_exercise", ctypes.c_int32),
+        ("training_paths", ctypes.POINTER(ctypes.c_uint64)),
+        ("evaluation_paths", ctypes.POINTER(ctypes.c_uint64)),
+        ("training_seed", ctypes.c_uint64),
+        ("training_domain_start", ctypes.c_uint32),
+        ("evaluation_seed", ctypes.c_uint64),
+        ("evaluation_domain_start", ctypes.c_uint32),
+        ("polynomial_degree", ctypes.c_uint32),
+        ("rank_tolerance", ctypes.c_double),
+        ("condition_limit", ctypes.c_double),
+        ("tie_rule", ctypes.c_int32),
+        ("insufficient_exercise_support", ctypes.c_int32),
+    ]
+
+
+class FoRaggedGreeksColumns(ctypes.Structure):
+    _fields_ = [
+        ("delta", c_double_p),
+        ("vega", c_double_p),
+        ("log_discount_sensitivities", c_double_p), ("log_discount_capacity", ctypes.c_uint64),
+        ("log_discount_offsets", ctypes.POINTER(ctypes.c_int64)),
+        ("dividend_sensitivities", c_double_p),
+    ]
+
+
 class FoBatchResultColumns(ctypes.Structure):
     _fields_ = [
         ("rows", ctypes.c_uint64),
@@ -211,6 +251,7 @@ EXPORTED_SYMBOLS: Final = (
     "fo_lsm_call_plan_revalue_f64",
     "fo_price_lsm_grouped_f64",
     "fo_price_lsm_batch_f64",
+    "fo_price_lsm_ragged_f64",
     "fo_executor_batch_kernel_ms",
     "fo_executor_batch_transfer_bytes",
     "fo_simulate_gbm_seeded_f64",
@@ -264,6 +305,9 @@ def _declare(lib: ctypes.CDLL) -> None:
         fn = getattr(lib, name)
         fn.argtypes = [vp, ctypes.POINTER(FoLsmGroupedRequest), ctypes.POINTER(FoBatchResultColumns), err]
         fn.restype = ctypes.c_int
+    lib.fo_price_lsm_ragged_f64.argtypes = [vp, ctypes.POINTER(FoLsmRaggedRequest), ctypes.POINTER(FoBatchResultColumns),
+                                            ctypes.POINTER(FoRaggedGreeksColumns), err]
+    lib.fo_price_lsm_ragged_f64.restype = ctypes.c_int
     lib.fo_executor_batch_kernel_ms.argtypes = [vp, c_double_p, ctypes.c_uint64, ctypes.POINTER(ctypes.c_uint64)]
     lib.fo_executor_batch_kernel_ms.restype = ctypes.c_int
     u64p = ctypes.POINTER(ctypes.c_uint64)

@@ -168,6 +168,77 @@ def lsm_call_greeks(nodes: int, dividends: int) -> tuple[_abi.FoLsmCallGreeks, n
 
 
 @dataclass
+class RaggedRequest:
+    struct: _abi.FoLsmRaggedRequest
+    keepalive: tuple[Any, ...]
+    rows: int
+
+
+def lsm_ragged_request(
+    *,
+    initial_spots: np.ndarray,
+    strikes: np.ndarray,
+    maturities: np.ndarray,
+    rates: np.ndarray,
+    volatilities: np.ndarray,
+    dividend_yields: np.ndarray | None,
+    dividend_offsets: np.ndarray | None,
+    dividend_times: np.ndarray | None,
+    dividend_amounts: np.ndarray | None,
+    dividend_policy: int,
+    maturity_boundary: int,
+    exercise_offsets: np.ndarray,
+    exercise_times: np.ndarray,
+    origin_exercise: int,
+    training_paths: np.ndarray,
+    evaluation_paths: np.ndarray,
+    training_seed: int,
+    training_domain_start: int,
+    evaluation_seed: int,
+    evaluation_domain_start: int,
+    polynomial_degree: int,
+    rank_tolerance: float,
+    condition_limit: float,
+    tie_rule: int,
+    insufficient_exercise_support: int,
+) -> RaggedRequest:
+    q = _abi.FoLsmRaggedRequest()
+    keep = (initial_spots, strikes, maturities, rates, volatilities, dividend_yields, dividend_offsets, dividend_times,
+            dividend_amounts, exercise_offsets, exercise_times, training_paths, evaluation_paths)
+    q.rows = int(initial_spots.size)
+    q.initial_spots = _ptr(initial_spots, ctypes.c_double)
+    q.strikes = _ptr(strikes, ctypes.c_double)
+    q.maturities = _ptr(maturities, ctypes.c_double)
+    q.rates = _ptr(rates, ctypes.c_double)
+    q.volatilities = _ptr(volatilities, ctypes.c_double)
+    q.dividend_yields = _ptr(dividend_yields, ctypes.c_double)
+    q.dividend_offsets = _ptr(dividend_offsets, ctypes.c_int64)
+    q.n_dividend_offsets = 0 if dividend_offsets is None else int(dividend_offsets.size)
+    q.dividend_times = _ptr(dividend_times, ctypes.c_double)
+    q.dividend_amounts = _ptr(dividend_amounts, ctypes.c_double)
+    q.n_dividend_events = 0 if dividend_times is None else int(dividend_times.size)
+    q.dividend_policy = dividend_policy
+    q.maturity_boundary = maturity_boundary
+    q.exercise_offsets = _ptr(exercise_offsets, ctypes.c_int64)
+    q.n_exercise_offsets = int(exercise_offsets.size)
+    q.exercise_times = _ptr(exercise_times, ctypes.c_double)
+    q.n_exercise_times = int(exercise_times.size)
+    q.origin_exercise = origin_exercise
+    q.training_paths = _ptr(training_paths, ctypes.c_uint64)
+    q.evaluation_paths = _ptr(evaluation_paths, ctypes.c_uint64)
+    q.training_seed = training_seed
+    q.training_domain_start = training_domain_start
+    q.evaluation_seed = evaluation_seed
+    q.evaluation_domain_start = evaluation_domain_start
+    q.polynomial_degree = polynomial_degree
+    q.rank_tolerance = rank_tolerance
+    q.condition_limit = condition_limit
+    q.tie_rule = tie_rule
+    q.insufficient_exercise_support = insufficient_exercise_support
+    return RaggedRequest(q, keep, q.rows)
+
+
+@dataclass
 class GroupedRequest:
     struct: _abi.FoLsmGroupedRequest
     keepalive: tuple[Any, ...]

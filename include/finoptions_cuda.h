@@ -430,6 +430,58 @@ int fo_price_lsm_grouped_f64(fo_executor* executor, const fo_lsm_grouped_request
 int fo_price_lsm_batch_f64(fo_executor* executor, const fo_lsm_grouped_request* request,
                            fo_batch_result_columns* out, fo_error* err);
 
+/* ---- ragged batches --------------------------------------------------------------------------
+ * Independent contracts with their own path counts: no counterpart in the reference, whose batch
+ * methods take one training and one evaluation path count per request (input.rs:259-267). Row r
+ * is priced like a one-row explicit-mesh batch with domains training_domain_start + r and
+ * evaluation_domain_start + r: its own exercise times (strictly inside (0, maturity)), a
+ * continuous yield and/or a cash-dividend schedule (exact times merged into the mesh), and its
+ * own training / evaluation path counts. */
+typedef struct fo_lsm_ragged_request {
+    uint64_t rows;
+    const double* initial_spots;      /* each column: one entry per contract */
+    const double* strikes;
+    const double* maturities;
+    const double* rates;              /* constant continuously compounded rate: L(t) = -r t */
+    const double* volatilities;
+    const double* dividend_yields;    /* continuous yields, NULL for none */
+    const int64_t* dividend_offsets;  uint64_t n_dividend_offsets;  /* rows + 1, NULL for none */
+    const double* dividend_times;     const double* dividend_amounts;  uint64_t n_dividend_events;
+    int32_t dividend_policy;          /* fo_dividend_policy of the cash jumps */
+    int32_t maturity_boundary;        /* fo_maturity_boundary of the cash schedules */
+    const int64_t* exercise_offsets;  uint64_t n_exercise_offsets;  /* rows + 1 */
+    const double* exercise_times;     uint64_t n_exercise_times;
+    int32_t origin_exercise;          /* fo_origin_exercise */
+    const uint64_t* training_paths;   /* per contract */
+    const uint64_t* evaluation_paths; /* per contract */
+    uint64_t training_seed;
+    uint32_t training_domain_start;
+    uint64_t evaluation_seed;
+    uint32_t evaluation_domain_start;
+    uint32_t polynomial_degree;
+    double rank_tolerance;
+    double condition_limit;
+    int32_t tie_rule;
+    int32_t insufficient_exercise_support;
+} fo_lsm_ragged_request;
+
+/* Per-contract adjoint Greeks of a ragged batch (fixed fitted policies, as fo_lsm_call_greeks):
+ * delta and vega per row; dP/dL per node of row r's union mesh at
+ * log_discount_sensitivities[log_discount_offsets[r] .. log_discount_offsets[r + 1]) (offsets
+ * written by the call; node i of the mesh is 0, the merged exercise / cash times, maturity);
+ * dP/dD per cash event, aligned with dividend_times. */
+typedef struct fo_ragged_greeks_columns {
+    double* delta;
+    double* vega;
+    double* log_discount_sensitivities;  uint64_t log_discount_capacity;
+    int64_t* log_discount_offsets;       /* rows + 1 */
+    double* dividend_sensitivities;      /* n_dividend_events */
+} fo_ragged_greeks_columns;
+
+/* greeks may be NULL (prices only). */
+int fo_price_lsm_ragged_f64(fo_executor* executor, const fo_lsm_ragged_request* request,
+                            fo_batch_result_columns* out, fo_ragged_greeks_columns* greeks, fo_error* err);
+
 /* Device time of the executor's last grouped / row batch call (no counterpart in the reference; a
  * measurement hook). kernel_ms[k] receives the milliseconds of batch kernel k summed over the
  * call's waves, k = 0 training simulation, 1 backward fits, 2 diagnostics, 3 evaluation,

@@ -132,3 +132,104 @@ def path_steps(c: GroupedColumns, paths: int) -> int:
         cash = c.dividend_times[c.dividend_offsets[g]:c.dividend_offsets[g + 1]]
         total += np.union1d(ex, cash).size + 1  # intervals: interior union times, then maturity
     return 2 * paths * total
+
+
+@dataclass
+class RaggedColumns:
+    initial_spots: np.ndarray
+    strikes: np.ndarray
+    maturities: np.ndarray
+    rates: np.ndarray
+    volatilities: np.ndarray
+    dividend_yields: np.ndarray
+    dividend_offsets: np.ndarray
+    dividend_times: np.ndarray
+    dividend_amounts: np.ndarray
+    exercise_offsets: np.ndarray
+    exercise_times: np.ndarray
+    paths: np.ndarray
+
+    @property
+    def rows(self) -> int:
+        return int(self.initial_spots.size)
+
+
+def ragged_columns(contracts: int, seed: int = 41, min_paths: int = 8192, max_paths: int = 262144,
+                   min_exercise: int = 4, max_exercise: int = 104) -> RaggedColumns:
+    """Independent contracts: P = floor(exp(U[ln min, ln max])) paths per role, n~U{min..max}
+    exercise dates at T*k/n (k = 1..n-1), S0~U[20,500], K/S0~U[0.7,1.3], sigma~U[0.05,0.8],
+    T~U[0.1,3], r~U[0,0.08]; even rows carry a continuous yield q~U[0,0.05], odd rows 1-6 cash
+    dividends of U[0.1,5] at distinct exercise dates."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    paths = np.floor(np.exp(rng.uniform(np.log(min_paths), np.log(max_paths), contracts))).astype(np.uint64)
+    n_ex = rng.integers(min_exercise, max_exercise + 1, contracts)
+    s0 = rng.uniform(20.0, 500.0, contracts)
+    moneyness = rng.uniform(0.7, 1.3, contracts)
+    vol = rng.uniform(0.05, 0.8, contracts)
+    maturity = rng.uniform(0.1, 3.0, contracts)
+    rate = rng.uniform(0.0, 0.08, contracts)
+    yields = np.where(np.arange(contracts) % 2 == 0, rng.uniform(0.0, 0.05, contracts), 0.0)
+    ex_offsets, ex_times, div_offsets, div_times, div_amounts = [0], [], [0], [], []
+    for r in range(contracts):
+        n = int(n_ex[r])
+        times = [float(maturity[r]) * (k / n) for k in range(1, n)]
+        ex_times.extend(times)
+        ex_offsets.append(len(ex_times))
+        if r % 2 == 1 and times:
+            k = min(int(rng.integers(1, 7)), len(times))
+            picks = np.sort(rng.choice(len(times), size=k, replace=False))
+            div_times.extend(times[int(i)] for i in picks)
+            div_amounts.extend(float(a) for a in rng.uniform(0.1, 5.0, k))
+        div_offsets.append(len(div_times))
+    return RaggedColumns(
+        initial_spots=s0, strikes=s0 * moneyness, maturities=maturity, rates=rate, volatilities=vol,
+        dividend_yields=yields, dividend_offsets=np.asarray(div_offsets, dtype=np.int64),
+        dividend_times=np.asarray(div_times, dtype=np.float64), dividend_amounts=np.asarray(div_amounts, dtype=np.float64),
+        exercise_offsets=np.asarray(ex_offsets, dtype=np.int64), exercise_times=np.asarray(ex_times, dtype=np.float64),
+        paths=paths)
+
+
+def ragged_request(c: RaggedColumns, *, seed: int = 41, support: int = 1, training_domain_start: int = 0,
+                   evaluation_domain_start: int = 1 << 20):
+    from finoptions._requests import lsm_ragged_request
+
+    return lsm_ragged_request(
+        initial_spots=c.initial_spots, strikes=c.strikes, maturities=c.maturities, rates=c.rates,
+        volatilities=c.volatilities, dividend_yields=c.dividend_yields, dividend_offsets=c.dividend_offsets,
+        dividend_times=c.dividend_times, dividend_amounts=c.dividend_amounts, dividend_policy=0, maturity_boundary=0,
+        exercise_offsets=c.exercise_offsets, exercise_times=c.exercise_times, origin_exercise=0,
+        training_paths=c.paths, evaluation_paths=c.paths, training_seed=seed,
+        training_domain_start=training_domain_start, evaluation_seed=seed,
+        evaluation_domain_start=evaluation_domain_start, polynomial_degree=4, rank_tolerance=1e-12,
+        condition_limit=1e8, tie_rule=0, insufficient_exercise_support=support)
+
+
+def ragged_row_as_call(c: RaggedColumns, r: int, *, seed: int = 41, support: int = 1, training_domain: int = 0,
+                       evaluation_domain: int = 1 << 20) -> dict:
+    """Row r of a ragged batch as single-contract arguments (the union mesh of its exercise and cash
+    times, domains start + r)."""
+    T, rate, q = float(c.maturities[r]), float(c.rates[r]), float(c.dividend_yields[r])
+    ex = c.exercise_times[c.exercise_offsets[r]:c.exercise_offsets[r + 1]]
+    cash = c.dividend_times[c.dividend_offsets[r]:c.dividend_offsets[r + 1]]
+    amounts = c.dividend_amounts[c.dividend_offsets[r]:c.dividend_offsets[r + 1]]
+    times = [0.0, *np.union1d(ex, cash[cash < T]).tolist(), T]
+    node = {t: i for i, t in enumerate(times)}
+    return dict(
+        initial_spot=float(c.initial_spots[r]), strike=float(c.strikes[r]), schedule_times=times, curve_times=times,
+        log_discounts=[0.0 if i == 0 else -rate * t for i, t in enumerate(times)], dividend_yield_times=times,
+        cumulative_dividend_yields=[0.0 if i == 0 else q * t for i, t in enumerate(times)],
+        dividend_nodes=[node[t] for t in cash.tolist()], dividend_amounts=amounts.tolist(),
+        exercise_nodes=[node[t] for t in ex.tolist()], expiry_node=len(times) - 1,
+        annualized_volatility=float(c.volatilities[r]), dividend_policy=0, training_paths=int(c.paths[r]),
+        evaluation_paths=int(c.paths[r]), training_seed=seed, training_domain=training_domain + r,
+        evaluation_seed=seed, evaluation_domain=evaluation_domain + r, polynomial_degree=4, rank_tolerance=1e-12,
+        condition_limit=1e8, tie_rule=0, insufficient_exercise_support=support)
+
+
+def ragged_path_steps(c: RaggedColumns) -> int:
+    total = 0
+    for r in range(c.rows):
+        ex = c.exercise_times[c.exercise_offsets[r]:c.exercise_offsets[r + 1]]
+        cash = c.dividend_times[c.dividend_offsets[r]:c.dividend_offsets[r + 1]]
+        total += 2 * int(c.paths[r]) * (np.union1d(ex, cash).size + 1)
+    return total

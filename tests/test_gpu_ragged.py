@@ -1,0 +1,76 @@
+"""Ragged batches (fo_price_lsm_ragged_f64): independent contracts with their own path counts.
+
+Row r of a ragged batch is the contract of price_lsm_call on the union mesh of its exercise and
+cash-dividend times with domains start + r; it is checked against the oracle's single-contract
+restatement of the reference (prices / SD / SE within 1e-9 relative, stopping counts identical).
+"""
+
+from __future__ import annotations
+
+import ctypes
+
+import _oracle
+import numpy as np
+import pytest
+from _workloads import ragged_columns, ragged_request, ragged_row_as_call
+from finoptions import _abi
+from finoptions._requests import batch_columns, lsm_call_request
+
+pytestmark = pytest.mark.gpu
+
+RTOL = 1e-9
+
+
+def gpu_ragged(native_executor, req):
+    cols = batch_columns(req.rows)
+    err = _abi.FoError()
+    status = _abi.load().fo_price_lsm_ragged_f64(native_executor.raw, ctypes.byref(req.struct),
+                                                 ctypes.byref(cols.struct), None, ctypes.byref(err))
+    return status, err, (cols.as_tuple() if status == 0 else None)
+
+
+def test_ragged_rows_match_single_contract_oracle_prices(native_executor) -> None:
+    c = ragged_columns(16, seed=41, min_paths=1024, max_paths=16384, min_exercise=4, max_exercise=30)
+    status, err, out = gpu_ragged(native_executor, ragged_request(c))
+    assert status == 0, err.message
+    for r in range(c.rows):
+        want = _oracle.price_lsm_call(lsm_call_request(**ragged_row_as_call(c, r)), 8)
+        price, _, sd, se, _, counts, diags = want
+        assert out[0][r] == pytest.approx(price, rel=RTOL, abs=1e-13), r
+        assert out[1][r] == pytest.approx(sd, rel=RTOL, abs=1e-13), r
+        assert out[2][r] == pytest.approx(se, rel=RTOL, abs=1e-13), r
+        assert out[10][r] == sum(counts[:-1]) and out[11][r] == counts[-1], r
+        assert out[5][r] == sum(1 for d in diags if d[1] == "regression"), r
+
+
+def _row(c, r: int):
+    one = ragged_columns(1, seed=1, min_paths=2, max_paths=3, min_exercise=4, max_exercise=4)
+    for name in ("initial_spots", "strikes", "maturities", "rates", "volatilities", "dividend_yields", "paths"):
+        setattr(one, name, getattr(c, name)[r:r + 1].copy())
+    one.exercise_times = c.exercise_times[c.exercise_offsets[r]:c.exercise_offsets[r + 1]].copy()
+    one.exercise_offsets = np.array([0, one.exercise_times.size], dtype=np.int64)
+    one.dividend_times = c.dividend_times[c.dividend_offsets[r]:c.dividend_offsets[r + 1]].copy()
+    one.dividend_amounts = c.dividend_amounts[c.dividend_offsets[r]:c.dividend_offsets[r + 1]].copy()
+    one.dividend_offsets = np.array([0, one.dividend_times.size], dtype=np.int64)
+    return one
+
+
+def test_ragged_row_equals_the_contract_priced_alone(native_executor) -> None:
+    """A ragged row and the same contract alone (domains shifted to the row's) agree bit for bit."""
+    c = ragged_columns(6, seed=43, min_paths=2048, max_paths=8192, min_exercise=4, max_exercise=20)
+    status, err, out = gpu_ragged(native_executor, ragged_request(c))
+    assert status == 0, err.message
+    for r in (1, 4):
+        status, err, single = gpu_ragged(native_executor, ragged_request(_row(c, r), training_domain_start=r,
+                                                                         evaluation_domain_start=(1 << 20) + r))
+        assert status == 0, err.message
+        for column, values in zip(out, single, strict=True):
+            assert column[r] == values[0]
+
+
+def test_ragged_validation_reports_the_row(native_executor) -> None:
+    c = ragged_columns(4, seed=47, min_paths=256, max_paths=512, min_exercise=4, max_exercise=6)
+    c.paths[2] = 1
+    status, err, _ = gpu_ragged(native_executor, ragged_request(c))
+    assert status == _abi.FO_ERR_INPUT
+    assert err.message.decode() == "batched LSM evaluation path count 1 at row 2 is outside [2, 4294967295]"
