@@ -21,6 +21,7 @@ struct BatchGroup {
     uint64_t slab_offset;    // first element of the group's stored training rows in the wave slab
     uint32_t first_problem;  // wave-local index of the group's first strike problem
     uint32_t problems;       // strike rows in the group
+    double sigma;            // the plan's constant volatility (adjoint vega)
 };
 
 // One (group, strike) problem of the launched wave.
@@ -30,7 +31,7 @@ struct BatchProblem {
     uint32_t records;        // index of its first FitRecord (one per observation row)
     uint64_t values;         // first element of its training values (train_paths doubles)
     int32_t skip_fit;        // 1: the host already failed this problem's fit (no backward pass)
-    int32_t pad;
+    uint32_t partial_base;   // first of its evaluation blocks' partial slots (one per block)
 };
 
 // Failure keys; every word starts as all-ones ("none") and keeps the lowest key with atomicMin.
@@ -105,8 +106,13 @@ struct BatchArgs {
     ProblemStatus* problem_status;
     unsigned* counts;          // [problems * 2]: early, expiry
     unsigned* itm_counts;      // [records]: in-the-money evaluation paths at unsupported rows
-    double2* eval_partials;    // [problems * eval_blocks * 2]: (sum, sum of squares) as double-double
+    double2* eval_partials;    // [evaluation blocks of all problems][2]: (sum, sum of squares), double-double
     ProblemSummary* summaries; // [problems]
+    // Adjoint Greeks (ragged batches): per-block slot partials, per-problem slot sums, per-record
+    // stopping counts. greek_partials is NULL when the batch prices without Greeks.
+    double2* greek_partials;   // [evaluation blocks of all problems][kGreekSlots]
+    double* greek_sums;        // [problems][kGreekSlots]
+    unsigned* stop_counts;     // [records]
     uint32_t train_blocks;     // training-simulation blocks of the largest group (grid x)
     uint32_t eval_blocks;      // evaluation blocks of the largest group (grid x, partials stride)
     int32_t degree;

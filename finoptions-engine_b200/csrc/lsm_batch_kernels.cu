@@ -16,6 +16,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include "lsm_adjoint.cuh"
 #include "lsm_batch.cuh"
 #include "lsm_batch_kernels.h"
 #include "lsm_common.cuh"
@@ -312,6 +313,7 @@ __global__ void __launch_bounds__(kBatchEvalThreads, 2) batch_evaluate_kernel(Ba
     __shared__ unsigned cnt[2 * kEvalStrikes];
     __shared__ double strikes[kEvalStrikes];
     __shared__ uint32_t rbase[kEvalStrikes];
+    __shared__ uint32_t pbase[kEvalStrikes];
     extern __shared__ PolicyRule staged[];  // [kEvalStrikes][rule_rows] when kStaged
     const BatchGroup& g = a.groups[blockIdx.y];
     const uint32_t first = g.first_problem + blockIdx.z * kEvalStrikes;
@@ -326,6 +328,7 @@ __global__ void __launch_bounds__(kBatchEvalThreads, 2) batch_evaluate_kernel(Ba
         const bool live = int(threadIdx.x) < ns;
         strikes[threadIdx.x] = live ? a.problems[first + threadIdx.x].strike : 1.0;
         rbase[threadIdx.x] = live ? a.problems[first + threadIdx.x].records : 0u;
+        pbase[threadIdx.x] = live ? a.problems[first + threadIdx.x].partial_base : 0u;
     }
     __syncthreads();
     const DevicePlan plan = g.plan;
@@ -412,10 +415,157 @@ __global__ void __launch_bounds__(kBatchEvalThreads, 2) batch_evaluate_kernel(Ba
     cta_reduce_dd<2 * kEvalStrikes>(acc, red, tot);
     if (int(threadIdx.x) < 2 * ns) {
         const uint32_t k = threadIdx.x >> 1, which = threadIdx.x & 1u;
-        a.eval_partials[(size_t(first + k) * a.eval_blocks + blockIdx.x) * 2 + which] =
-            make_double2(tot[threadIdx.x].hi, tot[threadIdx.x].lo);
+        a.eval_partials[(size_t(pbase[k]) + blockIdx.x) * 2 + which] = make_double2(tot[threadIdx.x].hi, tot[threadIdx.x].lo);
         if (cnt[threadIdx.x]) atomicAdd(&a.counts[size_t(first + k) * 2 + which], cnt[threadIdx.x]);
     }
+}
+
+// ---------------------------------------------------------------------------------------------
+// Fused evaluation with pathwise adjoint Greeks: one strike per block (grid z = strike in group).
+// ---------------------------------------------------------------------------------------------
+
+__global__ void __launch_bounds__(kBatchEvalThreads, 2) batch_evaluate_greeks_kernel(BatchArgs a, uint32_t rule_rows) {
+    __shared__ double sx[257], sf[257];
+    __shared__ double red[32 * 2];
+    __shared__ dd tot[2];
+    __shared__ double gred[32 * kGreekSlots];
+    __shared__ dd gtot[kGreekSlots];
+    __shared__ unsigned cnt[2];
+    extern __shared__ unsigned char batch_greeks_smem[];  // PolicyRule[rule_rows], unsigned stops[rule_rows]
+    const BatchGroup& g = a.groups[blockIdx.y];
+    const uint32_t k = blockIdx.z;
+    if (k >= g.problems) return;                                          // uniform over the block
+    if (uint64_t(blockIdx.x) * blockDim.x >= g.plan.eval_paths) return;   // beyond this group's paths
+    if (sim_failed(&a.group_status[blockIdx.y].train_sim_fail)) return;
+    const uint32_t problem = g.first_problem + k;
+    const BatchProblem pr = a.problems[problem];
+    PolicyRule* rules = reinterpret_cast<PolicyRule*>(batch_greeks_smem);
+    unsigned* stops = reinterpret_cast<unsigned*>(rules + rule_rows);
+    load_zig_tables(sx, sf);
+    const SmemZig zig = make_zig(sx, sf);
+    const DevicePlan plan = g.plan;
+    const uint32_t rows = plan.rows;
+    for (uint32_t r = threadIdx.x; r < rows; r += blockDim.x) {
+        const FitRecord& rec = a.records[pr.records + r];
+        PolicyRule& rule = rules[r];
+        rule.kind = rec.kind;
+        rule.mean = rec.model.mean;
+        rule.scale = rec.model.scale;
+#pragma unroll
+        for (int j = 0; j < kMaxDegree; ++j) {
+            rule.alpha[j] = rec.model.alpha[j];
+            rule.beta[j] = rec.model.beta[j];
+        }
+#pragma unroll
+        for (int j = 0; j < kMaxColumns; ++j) rule.coef[j] = rec.model.coef[j];
+        stops[r] = 0;
+    }
+    if (threadIdx.x < 2) cnt[threadIdx.x] = 0;
+    __syncthreads();
+    const double K = pr.strike;
+    const uint64_t P = plan.eval_paths;
+    const uint64_t p = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    const uint32_t last = rows - 1;
+    const int degree = a.degree;
+    const double sens_scale = 1.0 / g.sigma;  // (Z diffusion - diffusion^2) / sigma = Z sqrt(dt) - sigma dt
+    double payoff = 0.0;
+    bool active = p < P;
+    GreekSums gs;
+    gs.reset();
+    PathAdjoint adj;
+    adj.reset();
+    auto observe = [&](int row, double spot) {
+        if (!active) return;
+        const double disc = plan.disc_to_origin[row];
+        if (uint32_t(row) == last) {
+            const double d = spot - K;
+            payoff = (d > 0.0 ? d : 0.0) * disc;
+            if (!fo_isfinite(payoff)) atomicMin(&a.problem_status[problem].eval_terminal_fail, (unsigned long long)p);
+            atomicAdd(&cnt[1], 1u);
+            adj.stop(gs, plan.row_node[row], spot, payoff, disc, true, plan.policy, sens_scale);
+            active = false;
+            return;
+        }
+        const PolicyRule& rule = rules[row];
+        if (rule.kind == kRuleNoSupport) {
+            if (spot > K) atomicAdd(&a.itm_counts[pr.records + row], 1u);
+            return;
+        }
+        if (rule.kind != kRuleRegression || !(spot > K)) return;
+        const double intrinsic = spot - K;
+        double continuation;
+        if (!predict_continuation(rule, degree, spot / K, &continuation)) {
+            atomicMin(&a.problem_status[problem].eval_fail, ((unsigned long long)row << 33) | (p << 1));
+            return;
+        }
+        if (exercise_rule(a.tie_rule, intrinsic, continuation)) {
+            payoff = intrinsic * disc;
+            if (!fo_isfinite(payoff))
+                atomicMin(&a.problem_status[problem].eval_fail, ((unsigned long long)row << 33) | (p << 1) | 1ull);
+            atomicAdd(&cnt[0], 1u);
+            atomicAdd(&stops[row], 1u);
+            adj.stop(gs, plan.row_node[row], spot, payoff, disc, false, plan.policy, sens_scale);
+            active = false;
+        }
+    };
+    if (p < P) {
+        // simulate_path's arithmetic and event phases, with the segment bookkeeping.
+        PathStream s;
+        s.init(plan.eval_seed, plan.eval_domain, uint32_t(p), plan.intervals);
+        double spot = plan.sim_start;
+        if (plan.row_node[0] == 0) observe(0, spot);
+        bool failed = false;
+        for (uint32_t i = 0; i < plan.intervals; ++i) {
+            double z = 0.0;
+            if (zig_sample(s, zig, &z) != kNormalOk) {
+                failed = true;
+                break;
+            }
+            const StepCoef c = plan.steps[i];
+            double next = 0.0, growth = 1.0;
+            if (spot != 0.0) {
+                growth = fo_exp(fo_fma(c.diffusion, z, c.log_drift));
+                next = spot * growth;
+            }
+            if (!fo_isfinite(next)) {
+                failed = true;
+                break;
+            }
+            if (active) adj.step(growth, z * c.diffusion - c.diffusion * c.diffusion);
+            spot = next;
+            const uint32_t at = i + 1;
+            const NodeEvent ev = plan.events[at];
+            const bool dividend = (ev.flags & kEventDividend) != 0;
+            const bool terminal = (ev.flags & kEventTerminal) != 0;
+            if (dividend && terminal) {
+                const double before = spot;
+                spot = apply_cash_dividend(plan.policy, ev.dividend_amount, before);
+                if (active) adj.cash(at, before, ev.dividend_amount);
+            }
+            if (ev.row >= 0) observe(ev.row, spot);
+            if (dividend && !terminal) {
+                const double before = spot;
+                spot = apply_cash_dividend(plan.policy, ev.dividend_amount, before);
+                if (active) adj.cash(at, before, ev.dividend_amount);
+            }
+        }
+        if (failed) atomicMin(&a.group_status[blockIdx.y].eval_sim_fail, (unsigned long long)p);
+    }
+    double acc[2] = {payoff, payoff * payoff};
+    cta_reduce_dd<2>(acc, red, tot);
+    if (threadIdx.x < 2) {
+        a.eval_partials[(size_t(pr.partial_base) + blockIdx.x) * 2 + threadIdx.x] =
+            make_double2(tot[threadIdx.x].hi, tot[threadIdx.x].lo);
+        if (cnt[threadIdx.x]) atomicAdd(&a.counts[size_t(problem) * 2 + threadIdx.x], cnt[threadIdx.x]);
+    }
+    for (uint32_t r = threadIdx.x; r < rows; r += blockDim.x)
+        if (stops[r]) atomicAdd(&a.stop_counts[pr.records + r], stops[r]);
+    double gacc[kGreekSlots];
+    gs.to_slots(gacc);
+    cta_reduce_dd<kGreekSlots>(gacc, gred, gtot);
+    if (threadIdx.x < kGreekSlots)
+        a.greek_partials[(size_t(pr.partial_base) + blockIdx.x) * kGreekSlots + threadIdx.x] =
+            make_double2(gtot[threadIdx.x].hi, gtot[threadIdx.x].lo);
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -499,7 +649,7 @@ __global__ void batch_summarize_kernel(BatchArgs a) {
         dd sum = dd_make(0.0), sumsq = dd_make(0.0);
         const uint64_t n = g.plan.eval_paths;
         const uint32_t blocks = uint32_t((n + kBatchEvalThreads - 1) / kBatchEvalThreads);
-        const double2* part = a.eval_partials + size_t(i) * a.eval_blocks * 2;
+        const double2* part = a.eval_partials + size_t(pr.partial_base) * 2;
         for (uint32_t b = 0; b < blocks; ++b) {
             sum = dd_add(sum, dd{part[2 * b].x, part[2 * b].y});
             sumsq = dd_add(sumsq, dd{part[2 * b + 1].x, part[2 * b + 1].y});
@@ -513,6 +663,16 @@ __global__ void batch_summarize_kernel(BatchArgs a) {
         s.standard_error = n > 1 ? sd / sqrt(double(n)) : 0.0;
         s.early_paths = a.counts[size_t(i) * 2];
         s.expiry_paths = a.counts[size_t(i) * 2 + 1];
+        if (a.greek_partials) {
+            // Greek slot sums over the problem's blocks in a fixed order.
+            const double2* gp = a.greek_partials + size_t(pr.partial_base) * kGreekSlots;
+            for (int slot = 0; slot < kGreekSlots; ++slot) {
+                dd acc = dd_make(0.0);
+                for (uint32_t b = 0; b < blocks; ++b) acc = dd_add(acc, dd{gp[size_t(b) * kGreekSlots + slot].x,
+                                                                           gp[size_t(b) * kGreekSlots + slot].y});
+                a.greek_sums[size_t(i) * kGreekSlots + slot] = dd_round(acc);
+            }
+        }
     }
     a.summaries[i] = s;
 }
@@ -547,6 +707,19 @@ cudaError_t launch_batch_evaluate(const BatchArgs& a, uint32_t strike_chunks, ui
     } else {
         batch_evaluate_kernel<false><<<grid, kBatchEvalThreads, 0, stream>>>(a, max_rows);
     }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_batch_evaluate_greeks(const BatchArgs& a, uint32_t max_strikes, uint32_t max_rows,
+                                         cudaStream_t stream) {
+    const dim3 grid(a.eval_blocks, a.n_groups, max_strikes);
+    const size_t smem = (sizeof(PolicyRule) + sizeof(unsigned)) * max_rows;
+    if (smem > 48 * 1024) {
+        cudaError_t e = cudaFuncSetAttribute(batch_evaluate_greeks_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             int(smem));
+        if (e != cudaSuccess) return e;
+    }
+    batch_evaluate_greeks_kernel<<<grid, kBatchEvalThreads, smem, stream>>>(a, max_rows);
     return cudaGetLastError();
 }
 

@@ -20,6 +20,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include "lsm_adjoint.cuh"
 #include "lsm_common.cuh"
 #include "lsm_device.cuh"
 #include "lsm_kernels.h"
@@ -64,57 +65,14 @@ __global__ void __launch_bounds__(kEvalThreads, 2) evaluate_greeks_kernel(EvalAr
     const uint64_t P = plan.eval_paths;
     const int degree = plan.degree;
     const uint32_t last = rows - 1;
-    const int n_div = int(gk.dividends);
     double sum = 0.0, sumsq = 0.0;
-    double g_delta = 0.0, g_vega = 0.0, g_l0 = 0.0, g_terminal = 0.0;
-    double g_jump[kMaxGreekDividends], g_div[kMaxGreekDividends];
-#pragma unroll
-    for (int j = 0; j < kMaxGreekDividends; ++j) g_jump[j] = g_div[j] = 0.0;
+    GreekSums gs;
+    gs.reset();
     for (uint64_t p = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; p < P; p += uint64_t(gridDim.x) * blockDim.x) {
         bool active = true;
         double payoff = 0.0;
-        // Segment bookkeeping: seg = cash dividends applied so far; growth[s] = product of the step
-        // factors of segment s, sens[s] = its sum of (Z sqrt(dt) - sigma dt); pre[j] = S before cash j.
-        int seg = 0;
-        double growth[kMaxGreekDividends + 1], sens[kMaxGreekDividends + 1], pre[kMaxGreekDividends];
-        growth[0] = 1.0;
-        sens[0] = 0.0;
-        // Contribution of a path stopping at `row` with observed state s_obs and payoff `pay`.
-        auto adjoint = [&](uint32_t row, double s_obs, double pay, bool terminal) {
-            if (!(pay > 0.0)) return;
-            const double ad = rules[row].discount;  // dP/dS_obs for an in-the-money stop
-            int s = seg;
-            double a_end = ad, s_end = s_obs;
-            if (terminal && s > 0 && gk.div_node[s - 1] == plan.row_node[row]) {
-                // Cash jump at expiry precedes the record: S_obs = h(S-).
-                const int j = s - 1;
-                const bool above = pre[j] > gk.div_amount[j];
-                g_div[j] += above ? -ad : 0.0;
-                a_end = plan.policy == 0 && !above ? 0.0 : ad;
-                s_end = pre[j];
-                s = j;
-            }
-            double w = a_end * s_end;
-            if (terminal) g_terminal += pay - w;
-            for (;;) {
-                g_vega += w * sens[s];
-                const double a_start = a_end * growth[s];
-                if (s == 0) {
-                    g_delta += a_start;
-                    g_l0 += w;
-                    break;
-                }
-                const int j = s - 1;  // the cash dividend that opened segment s
-                const bool above = pre[j] > gk.div_amount[j];
-                g_div[j] += above ? -a_start : 0.0;
-                const double a_prev = plan.policy == 0 && !above ? 0.0 : a_start;
-                const double w_prev = a_prev * pre[j];
-                g_jump[j] += w - w_prev;
-                a_end = a_prev;
-                w = w_prev;
-                s = j;
-            }
-        };
+        PathAdjoint adj;
+        adj.reset();
         auto observe = [&](int row, double spot) {
             if (!active) return;
             const GreeksEvalRow& er = rules[row];
@@ -124,7 +82,7 @@ __global__ void __launch_bounds__(kEvalThreads, 2) evaluate_greeks_kernel(EvalAr
                 if (!fo_isfinite(payoff)) atomicMin(&a.status->eval_terminal_fail, (unsigned long long)p);
                 active = false;
                 atomicAdd(&counts[row], 1u);
-                adjoint(uint32_t(row), spot, payoff, true);
+                adj.stop(gs, plan.row_node[row], spot, payoff, er.discount, true, plan.policy, 1.0);
                 return;
             }
             if (er.kind == kRuleNoSupport) {
@@ -144,17 +102,7 @@ __global__ void __launch_bounds__(kEvalThreads, 2) evaluate_greeks_kernel(EvalAr
                     atomicMin(&a.status->eval_fail, ((unsigned long long)row << 33) | (p << 1) | 1ull);
                 active = false;
                 atomicAdd(&counts[row], 1u);
-                adjoint(uint32_t(row), spot, payoff, false);
-            }
-        };
-        auto cash = [&](const NodeEvent& ev, double* spot) {
-            const double before = *spot;
-            *spot = apply_cash_dividend(plan.policy, ev.dividend_amount, before);
-            if (active && seg < n_div) {
-                pre[seg] = before;
-                seg += 1;
-                growth[seg] = 1.0;
-                sens[seg] = 0.0;
+                adj.stop(gs, plan.row_node[row], spot, payoff, er.discount, false, plan.policy, 1.0);
             }
         };
         // The path: simulate_path's arithmetic and event phases, with the segment bookkeeping.
@@ -171,23 +119,32 @@ __global__ void __launch_bounds__(kEvalThreads, 2) evaluate_greeks_kernel(EvalAr
             }
             const StepCoef c = plan.steps[i];
             double next = 0.0;
+            double g = 1.0;
             if (spot != 0.0) {
-                const double g = fo_exp(fo_fma(c.diffusion, z, c.log_drift));
+                g = fo_exp(fo_fma(c.diffusion, z, c.log_drift));
                 next = spot * g;
-                if (active) growth[seg] *= g;
             }
             if (!fo_isfinite(next)) {
                 failed = true;
                 break;
             }
-            if (active) sens[seg] += z * gk.sqrt_dt[i] - gk.sigma * gk.dt[i];
+            if (active) adj.step(g, z * gk.sqrt_dt[i] - gk.sigma * gk.dt[i]);
             spot = next;
-            const NodeEvent ev = plan.events[i + 1];
+            const uint32_t at = i + 1;
+            const NodeEvent ev = plan.events[at];
             const bool dividend = (ev.flags & kEventDividend) != 0;
             const bool terminal = (ev.flags & kEventTerminal) != 0;
-            if (dividend && terminal) cash(ev, &spot);
+            if (dividend && terminal) {
+                const double before = spot;
+                spot = apply_cash_dividend(plan.policy, ev.dividend_amount, before);
+                if (active) adj.cash(at, before, ev.dividend_amount);
+            }
             if (ev.row >= 0) observe(ev.row, spot);
-            if (dividend && !terminal) cash(ev, &spot);
+            if (dividend && !terminal) {
+                const double before = spot;
+                spot = apply_cash_dividend(plan.policy, ev.dividend_amount, before);
+                if (active) adj.cash(at, before, ev.dividend_amount);
+            }
         }
         if (failed) atomicMin(&a.status->eval_sim_fail, (unsigned long long)p);
         sum += payoff;
@@ -201,17 +158,7 @@ __global__ void __launch_bounds__(kEvalThreads, 2) evaluate_greeks_kernel(EvalAr
         if (itm_counts[r]) atomicAdd(&a.itm_counts[r], itm_counts[r]);
     }
     double gacc[kGreekSlots];
-#pragma unroll
-    for (int k = 0; k < kGreekSlots; ++k) gacc[k] = 0.0;
-    gacc[kGreekDelta] = g_delta;
-    gacc[kGreekVega] = g_vega;
-    gacc[kGreekL0] = g_l0;
-    gacc[kGreekTerminal] = g_terminal;
-#pragma unroll
-    for (int j = 0; j < kMaxGreekDividends; ++j) {
-        gacc[kGreekJump + j] = g_jump[j];
-        gacc[kGreekDividend + j] = g_div[j];
-    }
+    gs.to_slots(gacc);
     cta_reduce_dd<kGreekSlots>(gacc, gred, gtot);
     if (threadIdx.x < kGreekSlots)
         gk.partials[size_t(blockIdx.x) * kGreekSlots + threadIdx.x] = make_double2(gtot[threadIdx.x].hi, gtot[threadIdx.x].lo);

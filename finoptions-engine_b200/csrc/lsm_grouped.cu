@@ -609,6 +609,7 @@ struct GroupSpec {
 
 struct GroupWork {
     HostPlan hp;              // simulation plan + method (strike unused)
+    double sigma = 0.0;       // the simulated constant volatility
     uint64_t first_row = 0, end_row = 0;
     Error build;              // build_path_plan failure: the group's error at first_row
     Error fit;                // discount failure raised by the first strike's fit
@@ -737,6 +738,7 @@ Error build_group(const BatchMethod& m, const GroupSpec& gs, GroupWork* w) {
     }
     e = validate_constant_volatility(volatility);
     if (!e.ok()) return financial_at_row(row, e);
+    w->sigma = volatility;
     HostPlan& hp = w->hp;
     if (escrowed) {
         // Risky prepaid forward: no yield, no cash jumps; the prepaid cash is added back per row.
@@ -790,7 +792,8 @@ Error build_group(const BatchMethod& m, const GroupSpec& gs, GroupWork* w) {
 
 struct WaveLayout {
     size_t groups, problems, group_status, problem_status, summaries;  // read-back region: group_status..summaries
-    size_t counts, itm_counts, eval_partials, records, values, slab, replay;
+    size_t greek_sums;                                                  // (read back, Greeks only)
+    size_t counts, itm_counts, stop_counts, eval_partials, greek_partials, records, values, slab, replay;
     size_t out_begin, out_bytes, clear_begin, clear_bytes, total;
 };
 
@@ -800,8 +803,10 @@ struct Wave {
     uint64_t records = 0;        // FitRecords (rows per problem)
     uint64_t slab_elems = 0;     // stored training states
     uint64_t value_elems = 0;    // training values of every problem
-    uint32_t eval_blocks = 0;    // largest evaluation grid of a group (partials stride per problem)
+    uint32_t eval_blocks = 0;    // largest evaluation grid of a group
     uint32_t train_blocks = 0;   // largest training grid of a group
+    uint64_t partial_slots = 0;  // evaluation blocks summed over the problems (one partial slot each)
+    bool greeks = false;         // adjoint Greeks buffers
 };
 
 uint32_t eval_blocks_for(uint64_t eval_paths) {
@@ -825,15 +830,18 @@ WaveLayout layout_for(const Wave& w, size_t base) {
     L.group_status = take(sizeof(GroupStatus) * G);
     L.problem_status = take(sizeof(ProblemStatus) * P);
     L.summaries = take(sizeof(ProblemSummary) * P);
+    L.greek_sums = take(w.greeks ? sizeof(double) * kGreekSlots * P : 0);
     off = align_up(off, 256);
     L.out_bytes = off - L.out_begin;
     L.clear_begin = off;
     L.counts = take(sizeof(unsigned) * 2 * P);
     L.itm_counts = take(sizeof(unsigned) * w.records);
+    L.stop_counts = take(w.greeks ? sizeof(unsigned) * w.records : 0);
     L.records = take(sizeof(FitRecord) * w.records);
     off = align_up(off, 256);
     L.clear_bytes = off - L.clear_begin;
-    L.eval_partials = take(sizeof(double2) * 2 * size_t(w.eval_blocks) * P);
+    L.eval_partials = take(sizeof(double2) * 2 * std::max<uint64_t>(w.partial_slots, 1));
+    L.greek_partials = take(w.greeks ? sizeof(double2) * kGreekSlots * w.partial_slots : 0);
     L.replay = take(sizeof(SimFailure));
     L.values = take(sizeof(double) * std::max<uint64_t>(w.value_elems, 1));
     L.slab = take(sizeof(double) * std::max<uint64_t>(w.slab_elems, 1));
@@ -1048,10 +1056,54 @@ Error validate_request(const BatchView& v, const fo_batch_result_columns* out) {
     return Error{};
 }
 
+// Where the adjoint Greeks of a batch go (ragged batches): the caller's columns and, per contract
+// row, the index of its first cash event in dividend_sensitivities.
+struct GreeksSink {
+    fo_ragged_greeks_columns* cols = nullptr;
+    std::vector<uint64_t> cash_first;
+};
+
+// Writes one problem's Greeks from its slot sums and per-row stopping counts (the host half of
+// the adjoint; the per-path half is PathAdjoint in lsm_adjoint.cuh).
+void write_greeks(const GreeksSink& sink, uint64_t row, const GroupWork& gw, double strike, const ProblemSummary& ps,
+                  const double* sums, const unsigned* stops) {
+    const HostPlan& hp = gw.hp;
+    fo_ragged_greeks_columns& c = *sink.cols;
+    double* dl = c.log_discount_sensitivities + c.log_discount_offsets[row];
+    double* dd_out = c.dividend_sensitivities ? c.dividend_sensitivities + sink.cash_first[row] : nullptr;
+    const uint64_t nodes = hp.times.size();
+    std::vector<uint32_t> div_nodes;
+    for (uint32_t node = 1; node < hp.events.size(); ++node)
+        if (hp.events[node].flags & kEventDividend) div_nodes.push_back(node);
+    for (uint64_t i = 0; i < nodes; ++i) dl[i] = 0.0;
+    for (size_t j = 0; j < div_nodes.size() && dd_out; ++j) dd_out[j] = 0.0;
+    if (ps.origin_exercised) {
+        const double d = hp.initial_spot - strike;
+        c.delta[row] = d > 0.0 ? 1.0 : 0.0;
+        c.vega[row] = 0.0;
+        dl[0] = d > 0.0 ? d : 0.0;
+        return;
+    }
+    const double n = double(hp.eval_paths);
+    c.delta[row] = sums[kGreekDelta] / n;
+    c.vega[row] = sums[kGreekVega] / n;
+    dl[0] += sums[kGreekL0] / n;
+    for (size_t j = 0; j < div_nodes.size(); ++j) {
+        dl[div_nodes[j]] += sums[kGreekJump + j] / n;
+        if (dd_out) dd_out[j] = sums[kGreekDividend + j] / n;
+    }
+    const uint32_t rows = hp.rows();
+    for (uint32_t r = 0; r + 1 < rows; ++r)
+        if (stops[r]) dl[hp.row_node[r]] += -strike * hp.disc_to_origin[r] * double(stops[r]) / n;
+    dl[hp.row_node[rows - 1]] += sums[kGreekTerminal] / n;
+}
+
 // Prices validated groups: host plans, waves within the memory budget, five kernels per wave,
-// the lowest failing group's typed error or the row-aligned result columns.
+// the lowest failing group's typed error or the row-aligned result columns (and, with a sink,
+// the adjoint Greeks of every row).
 Error price_groups(fo_executor* ex, const BatchMethod& m, const std::vector<GroupSpec>& specs, const double* strikes,
-                   fo_batch_result_columns* out) {
+                   fo_batch_result_columns* out, const GreeksSink* sink = nullptr) {
+    const bool greeks = sink != nullptr;
     // Per-group plans on the host. Only groups before the first one whose plan fails can matter.
     const uint64_t groups = specs.size();
     std::vector<GroupWork> work(groups);
@@ -1087,6 +1139,20 @@ Error price_groups(fo_executor* ex, const BatchMethod& m, const std::vector<Grou
         o.escrow_cash = take(sizeof(double) * hp.rows());
     }
     in_bytes = align_up(std::max<size_t>(in_bytes, 16), 256);
+    if (greeks && launchable == groups) {
+        // Ragged log-discount offsets: one sensitivity per node of each row's mesh.
+        int64_t at = 0;
+        for (uint64_t g = 0; g < groups; ++g)
+            for (uint64_t r = work[g].first_row; r < work[g].end_row; ++r) {
+                sink->cols->log_discount_offsets[r] = at;
+                at += int64_t(work[g].hp.times.size());
+            }
+        sink->cols->log_discount_offsets[out->rows] = at;
+        if (uint64_t(at) > sink->cols->log_discount_capacity)
+            return make_error(FO_ERR_EXECUTION, FO_CODE_INVALID_ARGUMENT,
+                              "log-discount sensitivities need " + u(uint64_t(at)) + " entries; capacity is " +
+                                  u(sink->cols->log_discount_capacity));
+    }
 
     // Waves: consecutive groups within the memory budget (and the grid's y extent).
     const size_t budget = memory_budget(ex);
@@ -1102,9 +1168,10 @@ Error price_groups(fo_executor* ex, const BatchMethod& m, const std::vector<Grou
             const uint32_t eval_blocks = eval_blocks_for(hp.eval_paths);
             const uint32_t train_blocks = eval_blocks_for(hp.train_paths);
             const size_t cost = sizeof(double) * (stored + strikes_g) * hp.train_paths +
-                                strikes_g * (rows * (sizeof(FitRecord) + sizeof(unsigned)) +
-                                             2 * size_t(std::max(eval_blocks, cur.eval_blocks)) * sizeof(double2) +
-                                             sizeof(BatchProblem) + sizeof(ProblemStatus) + sizeof(ProblemSummary) + 8) +
+                                strikes_g * (rows * (sizeof(FitRecord) + 2 * sizeof(unsigned)) +
+                                             size_t(eval_blocks) * sizeof(double2) * (2 + (greeks ? kGreekSlots : 0)) +
+                                             sizeof(BatchProblem) + sizeof(ProblemStatus) + sizeof(ProblemSummary) +
+                                             sizeof(double) * kGreekSlots + 8) +
                                 sizeof(BatchGroup) + sizeof(GroupStatus) + 1024;
             if (cur.g1 > cur.g0 && (bytes + cost > budget || cur.g1 - cur.g0 >= 65535)) {
                 waves.push_back(cur);
@@ -1119,6 +1186,8 @@ Error price_groups(fo_executor* ex, const BatchMethod& m, const std::vector<Grou
             cur.value_elems += strikes_g * hp.train_paths;
             cur.eval_blocks = std::max(cur.eval_blocks, eval_blocks);
             cur.train_blocks = std::max(cur.train_blocks, train_blocks);
+            cur.partial_slots += strikes_g * eval_blocks;
+            cur.greeks = greeks;
             bytes += cost;
         }
         if (cur.g1 > cur.g0) waves.push_back(cur);
@@ -1169,9 +1238,9 @@ Error price_groups(fo_executor* ex, const BatchMethod& m, const std::vector<Grou
         // Group and problem tables.
         auto* hg = reinterpret_cast<BatchGroup*>(host + (L.groups - in_bytes));
         auto* hpb = reinterpret_cast<BatchProblem*>(host + (L.problems - in_bytes));
-        uint64_t slab = 0, record = 0, problem = 0, values = 0;
+        uint64_t slab = 0, record = 0, problem = 0, values = 0, partial = 0;
         slab_of.assign(w.g1 - w.g0, 0);
-        uint32_t chunks = 1, max_rows = 1;
+        uint32_t chunks = 1, max_rows = 1, max_strikes = 1;
         for (uint64_t g = w.g0; g < w.g1; ++g) {
             const HostPlan& hp = work[g].hp;
             BatchGroup& bg = hg[g - w.g0];
@@ -1180,6 +1249,8 @@ Error price_groups(fo_executor* ex, const BatchMethod& m, const std::vector<Grou
             slab_of[g - w.g0] = slab;
             bg.first_problem = uint32_t(problem);
             bg.problems = uint32_t(work[g].end_row - work[g].first_row);
+            bg.sigma = work[g].sigma;
+            max_strikes = std::max(max_strikes, bg.problems);
             for (uint64_t r = work[g].first_row; r < work[g].end_row; ++r) {
                 BatchProblem& pb = hpb[problem];
                 pb.strike = strikes[r];
@@ -1187,7 +1258,8 @@ Error price_groups(fo_executor* ex, const BatchMethod& m, const std::vector<Grou
                 pb.records = uint32_t(record);
                 pb.values = values;
                 pb.skip_fit = work[g].fit.ok() ? 0 : 1;
-                pb.pad = 0;
+                pb.partial_base = uint32_t(partial);
+                partial += eval_blocks_for(hp.eval_paths);
                 record += hp.rows();
                 values += hp.train_paths;
                 problem += 1;
@@ -1216,6 +1288,9 @@ Error price_groups(fo_executor* ex, const BatchMethod& m, const std::vector<Grou
         a.itm_counts = reinterpret_cast<unsigned*>(dev + L.itm_counts);
         a.eval_partials = reinterpret_cast<double2*>(dev + L.eval_partials);
         a.summaries = reinterpret_cast<ProblemSummary*>(dev + L.summaries);
+        a.greek_partials = greeks ? reinterpret_cast<double2*>(dev + L.greek_partials) : nullptr;
+        a.greek_sums = greeks ? reinterpret_cast<double*>(dev + L.greek_sums) : nullptr;
+        a.stop_counts = greeks ? reinterpret_cast<unsigned*>(dev + L.stop_counts) : nullptr;
         a.train_blocks = w.train_blocks;
         a.eval_blocks = w.eval_blocks;
         a.degree = m.degree;
@@ -1231,7 +1306,10 @@ Error price_groups(fo_executor* ex, const BatchMethod& m, const std::vector<Grou
         FO_CUDA_TRY(cudaEventRecord(mark[2], s), "event");
         FO_CUDA_TRY(launch_batch_diagnose(a, uint32_t(w.records), s), "batch diagnose launch");
         FO_CUDA_TRY(cudaEventRecord(mark[3], s), "event");
-        FO_CUDA_TRY(launch_batch_evaluate(a, chunks, max_rows, s), "batch evaluation launch");
+        if (greeks)
+            FO_CUDA_TRY(launch_batch_evaluate_greeks(a, max_strikes, max_rows, s), "batch Greeks evaluation launch");
+        else
+            FO_CUDA_TRY(launch_batch_evaluate(a, chunks, max_rows, s), "batch evaluation launch");
         FO_CUDA_TRY(cudaEventRecord(mark[4], s), "event");
         FO_CUDA_TRY(launch_batch_summarize(a, s), "batch summary launch");
         FO_CUDA_TRY(cudaEventRecord(mark[5], s), "event");
@@ -1247,6 +1325,14 @@ Error price_groups(fo_executor* ex, const BatchMethod& m, const std::vector<Grou
         const auto* gst = reinterpret_cast<const GroupStatus*>(host + (L.group_status - L.out_begin));
         const auto* pst = reinterpret_cast<const ProblemStatus*>(host + (L.problem_status - L.out_begin));
         const auto* sum = reinterpret_cast<const ProblemSummary*>(host + (L.summaries - L.out_begin));
+        const auto* greek_sums = reinterpret_cast<const double*>(host + (L.greek_sums - L.out_begin));
+        std::vector<unsigned> stops;
+        if (greeks) {
+            stops.resize(w.records);
+            FO_CUDA_TRY(cudaMemcpy(stops.data(), dev + L.stop_counts, sizeof(unsigned) * w.records, cudaMemcpyDeviceToHost),
+                        "stopping counts copy");
+            ex->batch_d2h += sizeof(unsigned) * w.records;
+        }
         BatchRun run{ex, &work, &plans, &slab_of, dev, L, w};
         // Failure scan in group order (the lowest failing group wins).
         uint64_t i0 = 0;
@@ -1305,6 +1391,9 @@ Error price_groups(fo_executor* ex, const BatchMethod& m, const std::vector<Grou
                 out->maximum_regression_condition_numbers[r] = ps.maximum_condition;
                 out->early_exercise_paths[r] = ps.early_paths;
                 out->expiry_paths[r] = ps.expiry_paths;
+                if (greeks)
+                    write_greeks(*sink, r, gw, strikes[r], ps, greek_sums + (i0 + k) * kGreekSlots,
+                                 stops.data() + first_record + k * gw.hp.rows());
             }
             i0 += strikes_g;
             first_record += strikes_g * gw.hp.rows();
@@ -1403,9 +1492,26 @@ Error validate_ragged(const fo_lsm_ragged_request& q, const fo_batch_result_colu
     return Error{};
 }
 
-Error price_ragged(fo_executor* ex, const fo_lsm_ragged_request& q, fo_batch_result_columns* out) {
+Error price_ragged(fo_executor* ex, const fo_lsm_ragged_request& q, fo_batch_result_columns* out,
+                   fo_ragged_greeks_columns* greeks) {
     Error e = validate_ragged(q, out);
     if (!e.ok()) return e;
+    GreeksSink sink;
+    if (greeks) {
+        if (!greeks->delta || !greeks->vega || !greeks->log_discount_sensitivities || !greeks->log_discount_offsets ||
+            (q.n_dividend_events && !greeks->dividend_sensitivities))
+            return make_error(FO_ERR_EXECUTION, FO_CODE_INVALID_ARGUMENT, "every requested Greeks column must be provided");
+        sink.cols = greeks;
+        sink.cash_first.assign(q.rows, 0);
+        for (uint64_t r = 0; r < q.rows && q.dividend_offsets; ++r) {
+            sink.cash_first[r] = uint64_t(q.dividend_offsets[r] - q.dividend_offsets[0]);
+            const uint64_t events = uint64_t(q.dividend_offsets[r + 1] - q.dividend_offsets[r]);
+            if (events > uint64_t(kMaxGreekDividends))
+                return make_error(FO_ERR_EXECUTION, FO_CODE_CAPACITY_EXCEEDED,
+                                  "adjoint Greeks support at most " + std::to_string(kMaxGreekDividends) +
+                                      " cash dividends per contract; row " + u(r) + " has " + u(events));
+        }
+    }
     BatchMethod m;
     m.mesh = FO_MESH_EXPLICIT_TIMES;
     m.origin = q.origin_exercise;
@@ -1444,7 +1550,7 @@ Error price_ragged(fo_executor* ex, const fo_lsm_ragged_request& q, fo_batch_res
         s.train_domain = uint32_t(uint64_t(q.training_domain_start) + r);
         s.eval_domain = uint32_t(uint64_t(q.evaluation_domain_start) + r);
     }
-    return price_groups(ex, m, specs, q.strikes, out);
+    return price_groups(ex, m, specs, q.strikes, out, greeks ? &sink : nullptr);
 }
 
 int finish(fo_error* err, const Error& e) {
@@ -1503,14 +1609,11 @@ int fo_price_lsm_ragged_f64(fo_executor* executor, const fo_lsm_ragged_request* 
         return finish(err, make_error(FO_ERR_EXECUTION, FO_CODE_INVALID_ARGUMENT, "executor and request must not be NULL"));
     Error e = check_columns(out);
     if (!e.ok()) return finish(err, e);
-    if (greeks)
-        return finish(err, make_error(FO_ERR_EXECUTION, FO_CODE_INVALID_ARGUMENT,
-                                      "ragged-batch Greeks are not available in this build"));
     std::lock_guard<std::mutex> lock(executor->mu);
     cudaError_t ce = cudaSetDevice(executor->device);
     if (ce != cudaSuccess) return finish(err, cuda_error(ce, "cudaSetDevice"));
     try {
-        return finish(err, price_ragged(executor, *request, out));
+        return finish(err, price_ragged(executor, *request, out, greeks));
     } catch (const std::bad_alloc&) {
         return finish(err, make_error(FO_ERR_EXECUTION, FO_CODE_CAPACITY_EXCEEDED, "host memory exhausted"));
     }

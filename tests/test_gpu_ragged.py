@@ -74,3 +74,50 @@ def test_ragged_validation_reports_the_row(native_executor) -> None:
     status, err, _ = gpu_ragged(native_executor, ragged_request(c))
     assert status == _abi.FO_ERR_INPUT
     assert err.message.decode() == "batched LSM evaluation path count 1 at row 2 is outside [2, 4294967295]"
+
+
+def gpu_ragged_greeks(native_executor, req, c):
+    nodes = [len(ragged_row_as_call(c, r)["schedule_times"]) for r in range(c.rows)]
+    g = _abi.FoRaggedGreeksColumns()
+    delta, vega = np.zeros(c.rows), np.zeros(c.rows)
+    d_l, offsets = np.zeros(sum(nodes)), np.zeros(c.rows + 1, dtype=np.int64)
+    d_d = np.zeros(max(c.dividend_times.size, 1))
+    g.delta = delta.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+    g.vega = vega.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+    g.log_discount_sensitivities = d_l.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+    g.log_discount_capacity = d_l.size
+    g.log_discount_offsets = offsets.ctypes.data_as(ctypes.POINTER(ctypes.c_int64))
+    g.dividend_sensitivities = d_d.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+    cols = batch_columns(req.rows)
+    err = _abi.FoError()
+    status = _abi.load().fo_price_lsm_ragged_f64(native_executor.raw, ctypes.byref(req.struct),
+                                                 ctypes.byref(cols.struct), ctypes.byref(g), ctypes.byref(err))
+    assert status == 0, err.message
+    assert offsets.tolist() == [0, *np.cumsum(nodes).tolist()]
+    return cols.as_tuple(), delta, vega, d_l, offsets, d_d
+
+
+def test_ragged_greeks_match_the_single_contract_greeks(native_executor) -> None:
+    from finoptions._requests import lsm_call_greeks, lsm_call_result
+
+    c = ragged_columns(10, seed=53, min_paths=2048, max_paths=16384, min_exercise=4, max_exercise=24)
+    out, delta, vega, d_l, offsets, d_d = gpu_ragged_greeks(native_executor, ragged_request(c), c)
+    _, _, plain = gpu_ragged(native_executor, ragged_request(c))
+    np.testing.assert_allclose(out[0], plain[0], rtol=1e-13, atol=1e-14)
+    for r in range(c.rows):
+        kw = ragged_row_as_call(c, r)
+        req = lsm_call_request(**kw)
+        res = lsm_call_result(req.exercise_rows)
+        n_div = len(kw["dividend_nodes"])
+        g, g_l, g_d = lsm_call_greeks(len(kw["schedule_times"]), n_div)
+        err = _abi.FoError()
+        assert _abi.load().fo_price_lsm_call_greeks_f64(native_executor.raw, ctypes.byref(req.struct),
+                                                        ctypes.byref(res.struct), ctypes.byref(g),
+                                                        ctypes.byref(err)) == 0, err.message
+        assert out[0][r] == pytest.approx(res.as_tuple()[0], rel=1e-12, abs=1e-13), r
+        scale = max(abs(g.delta), 1.0)
+        assert delta[r] == pytest.approx(g.delta, rel=1e-10, abs=1e-12 * scale), r
+        assert vega[r] == pytest.approx(g.vega, rel=1e-10, abs=1e-10), r
+        np.testing.assert_allclose(d_l[offsets[r]:offsets[r + 1]], g_l, rtol=1e-9, atol=1e-10, err_msg=str(r))
+        first = int(c.dividend_offsets[r])
+        np.testing.assert_allclose(d_d[first:first + n_div], g_d, rtol=1e-9, atol=1e-10, err_msg=str(r))
