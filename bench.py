@@ -337,6 +337,87 @@ def run_ours(args: argparse.Namespace) -> dict | None:
         out["batched"] = run_grouped(args, executor)
     if not args.skip_greeks:
         out["greeks"] = run_greeks(args, executor)
+    if not args.skip_ragged:
+        out["ragged"] = run_ragged(args, executor)
+    return out
+
+
+# ---- ragged batch with per-contract path counts + Greeks -----------------------------------------
+
+RAGGED_CONTRACTS = 1024
+RAGGED_SAMPLE = 16
+
+
+def run_ragged(args: argparse.Namespace, executor) -> dict:
+    """1024 independent contracts, path counts log-uniform in [8192, 262144] (same per role), 4-104
+    exercise dates, half continuous yield / half 1-6 cash dividends, seed 41: one batch call priced
+    alone and with the adjoint Greeks (delta, vega, dP/dL per mesh node, dP/dD per cash event)."""
+    import _oracle
+    import _workloads
+    import numpy as np
+    from finoptions import _abi
+    from finoptions._requests import batch_columns, lsm_call_request
+
+    lib = _abi.load()
+    c = _workloads.ragged_columns(args.ragged_contracts, seed=41)
+    req = _workloads.ragged_request(c)
+    nodes = sum(len(_workloads.ragged_row_as_call(c, r)["schedule_times"]) for r in range(c.rows))
+    result = batch_columns(req.rows)
+    err = _abi.FoError()
+    g = _abi.FoRaggedGreeksColumns()
+    arrays = {"delta": np.zeros(c.rows), "vega": np.zeros(c.rows), "d_l": np.zeros(nodes),
+              "offsets": np.zeros(c.rows + 1, dtype=np.int64), "d_d": np.zeros(max(c.dividend_times.size, 1))}
+    dp = lambda a: a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))  # noqa: E731
+    g.delta, g.vega, g.log_discount_sensitivities = dp(arrays["delta"]), dp(arrays["vega"]), dp(arrays["d_l"])
+    g.log_discount_capacity = nodes
+    g.log_discount_offsets = arrays["offsets"].ctypes.data_as(ctypes.POINTER(ctypes.c_int64))
+    g.dividend_sensitivities = dp(arrays["d_d"])
+    steps = _workloads.ragged_path_steps(c)
+    ms = (ctypes.c_double * 5)()
+    launches = ctypes.c_uint64()
+    names = ("batch_simulate_kernel", "batch_backward_kernel", "batch_diagnose_kernel", "batch_evaluate_kernel",
+             "batch_summarize_kernel")
+    out = {"workload": (f"ragged batch: {c.rows} contracts, paths per role log-uniform in [8192, 262144] "
+                        f"(mean {float(c.paths.mean()):.0f}), 4-104 exercise dates, S0~U[20,500], K/S0~U[0.7,1.3], "
+                        "sigma~U[0.05,0.8], T~U[0.1,3], r~U[0,0.08], even rows yield q~U[0,0.05], odd rows 1-6 cash "
+                        "dividends, seed 41"),
+           "contracts": c.rows, "path_steps_per_call": steps, "log_discount_sensitivities": nodes}
+    calls = max(1, min(args.steps, 3))
+    for name, greeks in (("plain", None), ("price_and_greeks", ctypes.byref(g))):
+        def call() -> None:
+            if lib.fo_price_lsm_ragged_f64(executor.raw, ctypes.byref(req.struct), ctypes.byref(result.struct), greeks,
+                                           ctypes.byref(err)):
+                raise RuntimeError(err.message.decode())
+        call()
+        kernel_ms = [0.0] * 5
+        t0 = time.perf_counter()
+        for _ in range(calls):
+            call()
+            lib.fo_executor_batch_kernel_ms(executor.raw, ms, 5, ctypes.byref(launches))
+            kernel_ms = [a + b for a, b in zip(kernel_ms, ms, strict=True)]
+        wall = time.perf_counter() - t0
+        device_ms = sum(kernel_ms) / calls
+        out[name] = {"device_ms_per_call": device_ms, "device_contracts_per_s": c.rows / (device_ms / 1e3),
+                     "device_path_steps_per_s": steps / (device_ms / 1e3),
+                     "e2e_contracts_per_s": c.rows * calls / wall, "e2e_ms_per_call": wall / calls * 1e3,
+                     "kernels_ms": {n: round(v / calls, 3) for n, v in zip(names, kernel_ms, strict=True)},
+                     "gpu_launches_per_call": int(launches.value)}
+    out["greeks_overhead"] = out["price_and_greeks"]["device_ms_per_call"] / out["plain"]["device_ms_per_call"]
+    out["sample_greeks"] = {"delta_row0": float(arrays["delta"][0]), "vega_row0": float(arrays["vega"][0])}
+    threads = cpu_threads()
+    t0 = time.perf_counter()
+    sample_steps = 0
+    for r in range(RAGGED_SAMPLE):
+        kw = _workloads.ragged_row_as_call(c, r)
+        _oracle.price_lsm_call(lsm_call_request(**kw), threads)
+        sample_steps += 2 * int(c.paths[r]) * (len(kw["schedule_times"]) - 1)
+    cpu_s = time.perf_counter() - t0
+    rate = sample_steps / cpu_s
+    out["cpu_baseline"] = {"kind": "port", "cores": threads, "path_steps_per_s": rate,
+                           "contracts_per_s": c.rows / (steps / rate),
+                           "sample": f"the first {RAGGED_SAMPLE} contracts priced one by one ({cpu_s:.2f} s); the "
+                                     "whole batch scaled by path-steps; Greeks by bump-and-reprice would multiply it "
+                                     "by 2 x (2 + mesh nodes + cash events) + 1"}
     return out
 
 
@@ -568,6 +649,9 @@ def main() -> None:
     parser.add_argument("--paths", type=int, default=PATHS, help="paths per role (profiling captures shrink it)")
     parser.add_argument("--skip-batched", action="store_true", help="omit the grouped-batch section")
     parser.add_argument("--skip-greeks", action="store_true", help="omit the price + Greeks section")
+    parser.add_argument("--skip-ragged", action="store_true", help="omit the ragged-batch section")
+    parser.add_argument("--ragged-contracts", type=int, default=RAGGED_CONTRACTS,
+                        help="contracts of the ragged-batch section (profiling captures shrink it)")
     parser.add_argument("--batched-states", type=int, default=GROUPED_STATES,
                         help="states of the grouped-batch section (profiling captures shrink it)")
     args = parser.parse_args()

@@ -20,12 +20,16 @@ from .batch_lsm import (
     ExerciseMesh,
     ExplicitExerciseMesh,
     LsmBatchResult,
+    LsmRaggedContracts,
+    LsmRaggedGreeks,
     LsmStrikeGroups,
     OriginExercise,
     RaggedExerciseTimes,
     UniformExerciseMesh,
     price_lsm_call_batch,
     price_lsm_call_grouped_batch,
+    price_lsm_call_ragged,
+    price_lsm_call_ragged_greeks,
 )
 from .dividends import BatchError, MaturityBoundary, RaggedCashDividends
 from .greeks import LsmCallContract, LsmGreeks, lsm_call_price, price_lsm_call_greeks
@@ -108,6 +112,8 @@ __all__ = [
     "LsmCallContract",
     "LsmError",
     "LsmGreeks",
+    "LsmRaggedContracts",
+    "LsmRaggedGreeks",
     "LsmResult",
     "LsmStrikeGroups",
     "MaturityBoundary",
@@ -127,5 +133,7 @@ __all__ = [
     "price_lsm_call_batch",
     "price_lsm_call_greeks",
     "price_lsm_call_grouped_batch",
+    "price_lsm_call_ragged",
+    "price_lsm_call_ragged_greeks",
     "simulate_gbm_seeded",
 ]

@@ -23,6 +23,7 @@ from ._requests import (
     lsm_call_request,
     lsm_call_result,
     lsm_grouped_request,
+    lsm_ragged_request,
 )
 
 __all__ = [
@@ -568,3 +569,53 @@ def price_lsm_call_batch_escrowed_cash_dividends_f64(  # noqa: PLR0913
                     mesh, executor, training_paths, evaluation_paths, training_seed, training_domain_start,
                     evaluation_seed, evaluation_domain_start, polynomial_degree, rank_tolerance, condition_limit,
                     tie_rule, insufficient_exercise_support)
+
+
+def price_lsm_call_ragged_f64(  # noqa: PLR0913 - one argument per ragged column
+    initial_spots, strikes, maturities, rates, volatilities, dividend_yields, dividend_offsets, dividend_times,
+    dividend_amounts, dividend_policy, maturity_boundary, exercise_offsets, exercise_times, origin_exercise,
+    training_paths, evaluation_paths, executor, training_seed, training_domain_start, evaluation_seed,
+    evaluation_domain_start, polynomial_degree, rank_tolerance, condition_limit, tie_rule,
+    insufficient_exercise_support, log_discount_nodes=None,
+) -> tuple:
+    """Ragged batch (per-contract path counts; no reference counterpart): NativeBatchLsmResult, and
+    with log_discount_nodes (mesh nodes per row) also (delta, vega, dP/dL, offsets, dP/dD)."""
+    handle = _executor_handle(executor)
+    request = lsm_ragged_request(
+        initial_spots=initial_spots, strikes=strikes, maturities=maturities, rates=rates, volatilities=volatilities,
+        dividend_yields=dividend_yields, dividend_offsets=dividend_offsets, dividend_times=dividend_times,
+        dividend_amounts=dividend_amounts, dividend_policy=_parse(_DIVIDEND_POLICIES, dividend_policy, "dividend policy"),
+        maturity_boundary=_parse(_MATURITY, maturity_boundary, "maturity boundary", BatchError),
+        exercise_offsets=exercise_offsets, exercise_times=exercise_times,
+        origin_exercise=_parse(_ORIGIN, origin_exercise, "origin exercise convention"),
+        training_paths=training_paths, evaluation_paths=evaluation_paths, training_seed=training_seed,
+        training_domain_start=training_domain_start, evaluation_seed=evaluation_seed,
+        evaluation_domain_start=evaluation_domain_start, polynomial_degree=polynomial_degree,
+        rank_tolerance=rank_tolerance, condition_limit=condition_limit,
+        tie_rule=_parse(_TIE_RULES, tie_rule, "exercise tie rule"),
+        insufficient_exercise_support=_parse(_SUPPORT, insufficient_exercise_support,
+                                             "insufficient exercise support policy"),
+    )
+    columns = batch_columns(request.rows)
+    err = _abi.FoError()
+    greeks = None
+    if log_discount_nodes is not None:
+        rows = request.rows
+        arrays = {"delta": np.zeros(rows), "vega": np.zeros(rows), "d_l": np.zeros(max(int(log_discount_nodes), 1)),
+                  "offsets": np.zeros(rows + 1, dtype=np.int64),
+                  "d_d": np.zeros(max(0 if dividend_times is None else int(dividend_times.size), 1))}
+        greeks = _abi.FoRaggedGreeksColumns()
+        greeks.delta = _dp(arrays["delta"])
+        greeks.vega = _dp(arrays["vega"])
+        greeks.log_discount_sensitivities = _dp(arrays["d_l"])
+        greeks.log_discount_capacity = int(log_discount_nodes)
+        greeks.log_discount_offsets = _ip(arrays["offsets"])
+        greeks.dividend_sensitivities = _dp(arrays["d_d"])
+    status = _lib().fo_price_lsm_ragged_f64(handle, ctypes.byref(request.struct), ctypes.byref(columns.struct),
+                                            None if greeks is None else ctypes.byref(greeks), ctypes.byref(err))
+    _check(status, err)
+    if greeks is None:
+        return columns.as_tuple()
+    n_events = 0 if dividend_times is None else int(dividend_times.size)
+    return (columns.as_tuple(), arrays["delta"], arrays["vega"], arrays["d_l"][: int(log_discount_nodes)],
+            arrays["offsets"], arrays["d_d"][:n_events])

@@ -16,13 +16,15 @@ import numpy.typing as npt
 
 from . import _native
 from .dividends import MaturityBoundary, RaggedCashDividends
-from .lsm import Lsm, LsmError
+from .lsm import ExerciseTieRule, InsufficientExerciseSupportPolicy, Lsm, LsmError
 from .model import DividendPolicy, InputError
+from .simulation import RandomStream
 from .simulation import CpuExecutor, CudaExecutor, native_executor
 
 Float64Vector = npt.NDArray[np.float64]
 Int64Vector = npt.NDArray[np.int64]
 UInt32Vector = npt.NDArray[np.uint32]
+UInt64Vector = npt.NDArray[np.uint64]
 BoolVector = npt.NDArray[np.bool_]
 
 _MAX_U32: Final = (2**32) - 1
@@ -410,6 +412,142 @@ def price_lsm_call_batch(  # noqa: PLR0913 - each financial column is independen
     return _check_partition(_freeze(raw), method.evaluation_paths, "batched LSM")
 
 
+# ---- ragged batches (no reference counterpart) ---------------------------------------------------
+
+
+@dataclass(frozen=True, slots=True)
+class LsmRaggedContracts:
+    """Independent call contracts, each with its own training and evaluation path count.
+
+    Every column has one entry per contract. Row r is priced like a one-row explicit-mesh batch with
+    domains ``training_stream.domain + r`` / ``evaluation_stream.domain + r``: its exercise times,
+    a continuous yield (``dividend_yields``, optional) and/or cash dividends (optional) merged into
+    its exact mesh. The reference's batch methods take one path count per request.
+    """
+
+    initial_spots: Float64Vector
+    strikes: Float64Vector
+    maturities: Float64Vector
+    rates: Float64Vector
+    volatilities: Float64Vector
+    exercise: RaggedExerciseTimes
+    training_paths: UInt64Vector
+    evaluation_paths: UInt64Vector
+    dividend_yields: Float64Vector | None = None
+    cash_dividends: RaggedCashDividends | None = None
+
+    def __post_init__(self) -> None:
+        """Require directly borrowable columns; the engine validates every value."""
+        for name in ("initial_spots", "strikes", "maturities", "rates", "volatilities"):
+            _validate_vector(getattr(self, name), field=name, dtype="float64")
+        for name in ("training_paths", "evaluation_paths"):
+            _validate_vector(getattr(self, name), field=name, dtype="uint64")
+        if self.dividend_yields is not None:
+            _validate_vector(self.dividend_yields, field="dividend_yields", dtype="float64")
+        if type(self.exercise) is not RaggedExerciseTimes:
+            raise InputError("exercise must be RaggedExerciseTimes")
+        if self.cash_dividends is not None and type(self.cash_dividends) is not RaggedCashDividends:
+            raise InputError("cash_dividends must be RaggedCashDividends")
+
+    @property
+    def rows(self) -> int:
+        """Contract count."""
+        return int(self.initial_spots.size)
+
+    def mesh_nodes(self) -> int:
+        """Nodes of every row's exact mesh (origin, merged exercise and cash times, maturity)."""
+        total = 0
+        ex, cash = self.exercise, self.cash_dividends
+        for r in range(self.rows):
+            times = ex.times[ex.offsets[r] - ex.offsets[0]:ex.offsets[r + 1] - ex.offsets[0]]
+            if cash is not None:
+                c = cash.times[cash.offsets[r] - cash.offsets[0]:cash.offsets[r + 1] - cash.offsets[0]]
+                times = np.union1d(times, c)
+            total += int(np.unique(times[times < self.maturities[r]]).size) + 2
+        return total
+
+
+@dataclass(frozen=True, slots=True, eq=False)
+class LsmRaggedGreeks:
+    """Fixed-policy pathwise Greeks of a ragged batch: per row delta and vega; dPrice/dL for every
+    node of row r's mesh at ``log_discount_sensitivities[log_discount_offsets[r]:log_discount_offsets[r + 1]]``
+    (L the log discounts -r t); dPrice/dD per cash event, aligned with the cash-dividend times."""
+
+    delta: Float64Vector
+    vega: Float64Vector
+    log_discount_sensitivities: Float64Vector
+    log_discount_offsets: Int64Vector
+    dividend_sensitivities: Float64Vector
+
+
+def _ragged_arguments(contracts: LsmRaggedContracts, origin_exercise: OriginExercise, dividend_policy: DividendPolicy,
+                      maturity_boundary: MaturityBoundary, executor: object, training_stream: RandomStream,
+                      evaluation_stream: RandomStream, insufficient_exercise_support: InsufficientExerciseSupportPolicy,
+                      polynomial_degree: int, rank_tolerance: float, condition_limit: float,
+                      tie_rule: ExerciseTieRule) -> tuple:
+    if type(contracts) is not LsmRaggedContracts:
+        raise InputError("contracts must be LsmRaggedContracts")
+    cash = contracts.cash_dividends
+    return (
+        contracts.initial_spots, contracts.strikes, contracts.maturities, contracts.rates, contracts.volatilities,
+        contracts.dividend_yields, None if cash is None else cash.offsets, None if cash is None else cash.times,
+        None if cash is None else cash.amounts, dividend_policy.value, maturity_boundary.value,
+        contracts.exercise.offsets, contracts.exercise.times, origin_exercise.value, contracts.training_paths,
+        contracts.evaluation_paths, native_executor(executor), training_stream.seed, training_stream.domain,
+        evaluation_stream.seed, evaluation_stream.domain, polynomial_degree, rank_tolerance, condition_limit,
+        tie_rule.value, insufficient_exercise_support.value,
+    )
+
+
+def price_lsm_call_ragged(  # noqa: PLR0913 - method settings stay explicit keywords
+    *,
+    contracts: LsmRaggedContracts,
+    origin_exercise: OriginExercise,
+    executor: CudaExecutor,
+    training_stream: RandomStream,
+    evaluation_stream: RandomStream,
+    insufficient_exercise_support: InsufficientExerciseSupportPolicy,
+    dividend_policy: DividendPolicy = DividendPolicy.LIQUIDATOR,
+    maturity_boundary: MaturityBoundary = MaturityBoundary.STRICTLY_BEFORE,
+    polynomial_degree: int = 4,
+    rank_tolerance: float = 1.0e-12,
+    condition_limit: float = 1.0e8,
+    tie_rule: ExerciseTieRule = ExerciseTieRule.STRICTLY_GREATER,
+) -> LsmBatchResult:
+    """Price independent contracts with their own path counts in one batch."""
+    raw = _native.price_lsm_call_ragged_f64(*_ragged_arguments(
+        contracts, origin_exercise, dividend_policy, maturity_boundary, executor, training_stream, evaluation_stream,
+        insufficient_exercise_support, polynomial_degree, rank_tolerance, condition_limit, tie_rule))
+    return _freeze(raw)
+
+
+def price_lsm_call_ragged_greeks(  # noqa: PLR0913 - method settings stay explicit keywords
+    *,
+    contracts: LsmRaggedContracts,
+    origin_exercise: OriginExercise,
+    executor: CudaExecutor,
+    training_stream: RandomStream,
+    evaluation_stream: RandomStream,
+    insufficient_exercise_support: InsufficientExerciseSupportPolicy,
+    dividend_policy: DividendPolicy = DividendPolicy.LIQUIDATOR,
+    maturity_boundary: MaturityBoundary = MaturityBoundary.STRICTLY_BEFORE,
+    polynomial_degree: int = 4,
+    rank_tolerance: float = 1.0e-12,
+    condition_limit: float = 1.0e8,
+    tie_rule: ExerciseTieRule = ExerciseTieRule.STRICTLY_GREATER,
+) -> tuple[LsmBatchResult, LsmRaggedGreeks]:
+    """Price independent contracts and their fixed-policy adjoint Greeks in the same pass."""
+    raw, delta, vega, d_l, offsets, d_d = _native.price_lsm_call_ragged_f64(
+        *_ragged_arguments(contracts, origin_exercise, dividend_policy, maturity_boundary, executor, training_stream,
+                           evaluation_stream, insufficient_exercise_support, polynomial_degree, rank_tolerance,
+                           condition_limit, tie_rule),
+        log_discount_nodes=contracts.mesh_nodes())
+    for array in (delta, vega, d_l, offsets, d_d):
+        array.flags.writeable = False
+    return _freeze(raw), LsmRaggedGreeks(delta=delta, vega=vega, log_discount_sensitivities=d_l,
+                                         log_discount_offsets=offsets, dividend_sensitivities=d_d)
+
+
 __all__ = [
     "BatchDividends",
     "CashDividendBatch",
@@ -420,10 +558,14 @@ __all__ = [
     "ExerciseMesh",
     "ExplicitExerciseMesh",
     "LsmBatchResult",
+    "LsmRaggedContracts",
+    "LsmRaggedGreeks",
     "LsmStrikeGroups",
     "OriginExercise",
     "RaggedExerciseTimes",
     "UniformExerciseMesh",
     "price_lsm_call_batch",
     "price_lsm_call_grouped_batch",
+    "price_lsm_call_ragged",
+    "price_lsm_call_ragged_greeks",
 ]

@@ -121,3 +121,29 @@ def test_ragged_greeks_match_the_single_contract_greeks(native_executor) -> None
         np.testing.assert_allclose(d_l[offsets[r]:offsets[r + 1]], g_l, rtol=1e-9, atol=1e-10, err_msg=str(r))
         first = int(c.dividend_offsets[r])
         np.testing.assert_allclose(d_d[first:first + n_div], g_d, rtol=1e-9, atol=1e-10, err_msg=str(r))
+
+
+def test_public_ragged_api_matches_the_c_abi(executor, native_executor) -> None:
+    import finoptions as fo
+
+    c = ragged_columns(6, seed=59, min_paths=1024, max_paths=4096, min_exercise=4, max_exercise=12)
+    contracts = fo.LsmRaggedContracts(
+        initial_spots=c.initial_spots, strikes=c.strikes, maturities=c.maturities, rates=c.rates,
+        volatilities=c.volatilities, exercise=fo.RaggedExerciseTimes(offsets=c.exercise_offsets, times=c.exercise_times),
+        training_paths=c.paths, evaluation_paths=c.paths, dividend_yields=c.dividend_yields,
+        cash_dividends=fo.RaggedCashDividends(offsets=c.dividend_offsets, times=c.dividend_times,
+                                              amounts=c.dividend_amounts))
+    kwargs = dict(contracts=contracts, origin_exercise=fo.OriginExercise.EXCLUDED, executor=executor,
+                  training_stream=fo.RandomStream(seed=41, domain=0), evaluation_stream=fo.RandomStream(seed=41, domain=1 << 20),
+                  insufficient_exercise_support=fo.InsufficientExerciseSupportPolicy.CONTINUE)
+    prices = fo.price_lsm_call_ragged(**kwargs)
+    result, greeks = fo.price_lsm_call_ragged_greeks(**kwargs)
+    out, delta, vega, d_l, offsets, d_d = gpu_ragged_greeks(native_executor, ragged_request(c), c)
+    _, _, plain = gpu_ragged(native_executor, ragged_request(c))
+    np.testing.assert_array_equal(prices.prices, plain[0])
+    np.testing.assert_array_equal(result.prices, out[0])
+    np.testing.assert_array_equal(greeks.delta, delta)
+    np.testing.assert_array_equal(greeks.log_discount_sensitivities, d_l)
+    np.testing.assert_array_equal(greeks.log_discount_offsets, offsets)
+    np.testing.assert_array_equal(greeks.dividend_sensitivities, d_d[:c.dividend_times.size])
+    assert not greeks.delta.flags.writeable and not result.prices.flags.writeable
