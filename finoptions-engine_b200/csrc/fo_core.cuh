@@ -256,6 +256,35 @@ FO_HD int zig_sample(PathStream& s, const Tables& t, double* out) {
 }
 
 // ----------------------------------------------------------------------------------------------
+// Division by a divisor used many times (the strike, a fitted scale): the reciprocal y = 1/b is
+// formed once and each quotient takes Markstein's correction step (P. Markstein, "Computation of
+// elementary functions on the IBM RISC System/6000 processor", IBM J. Res. Dev. 34(1), 1990;
+// M. Cornea, J. Harrison, P. Tang, "Scientific Computing on Itanium-based Systems", 2002):
+//   q0 = a * y,   r = a - b * q0 (exact in one fma),   q = q0 + r * y (one fma).
+// The residual of q0 is exact and the corrected quotient lies within a tiny fraction of an ulp of
+// a / b before its final rounding, so q is the correctly rounded quotient except when a / b falls
+// within about 2^-51 ulp of a rounding boundary. Operands outside [2^-960, 2^960] divide.
+// ----------------------------------------------------------------------------------------------
+
+struct Divisor {
+    double b;
+    double inv;  // 1 / b, or 0 when b is outside the corrected range
+};
+
+FO_HD Divisor make_divisor(double b) {
+    const double m = fo_fabs(b);
+    return Divisor{b, (m > 0x1p-960 && m < 0x1p960) ? 1.0 / b : 0.0};
+}
+
+FO_HD double divide(double a, const Divisor& d) {
+    const double m = fo_fabs(a);
+    if (d.inv == 0.0 || !(m > 0x1p-960 && m < 0x1p960)) return a / d.b;
+    const double q0 = a * d.inv;
+    const double r = fo_fma(-d.b, q0, a);
+    return fo_fma(r, d.inv, q0);
+}
+
+// ----------------------------------------------------------------------------------------------
 // GBM step and cash-dividend policies.
 // ----------------------------------------------------------------------------------------------
 
@@ -376,6 +405,7 @@ enum FitStatus : int {
 
 struct FitModel {
     double mean, scale;
+    double inv_scale;  // 1 / scale for the prediction's corrected division (see Divisor)
     double alpha[kMaxDegree];
     double beta[kMaxDegree];
     double coef[kMaxColumns];
@@ -405,6 +435,7 @@ FO_HD_NOINLINE void fit_from_moments(const dd* sums, double pivot, uint64_t coun
     if (degree == 0) {
         m->mean = 0.0;
         m->scale = 1.0;
+        m->inv_scale = make_divisor(m->scale).inv;
         mom[0] = dd_make(n);
         for (int k = 1; k < kPowerSums; ++k) mom[k] = dd_make(0.0);
         resp[0] = sums[kPowerSums + 0];
@@ -421,6 +452,7 @@ FO_HD_NOINLINE void fit_from_moments(const dd* sums, double pivot, uint64_t coun
         const double scale_d = dd_round(sd);
         m->mean = mean_d;
         m->scale = scale_d;
+        m->inv_scale = make_divisor(m->scale).inv;
         if (!fo_isfinite(mean_d) || !fo_isfinite(scale_d) || !(scale_d > 0.0)) {
             m->status = kFitDegeneratePredictor;
             m->aux_value = scale_d;
@@ -571,6 +603,7 @@ FO_HD bool fit_near_pivot(const dd* sums, double pivot, uint64_t count, double r
     m->aux_value = 0.0;
     m->mean = mean;
     m->scale = scale;
+    m->inv_scale = make_divisor(m->scale).inv;
     if (!fo_isfinite(mean) || !fo_isfinite(scale) || !(scale > 0.0)) {
         m->status = kFitDegeneratePredictor;
         m->aux_value = scale;
@@ -707,7 +740,7 @@ FO_HD_NOINLINE void fit_continuation(const dd* sums, double pivot, uint64_t coun
 template <typename Model>
 FO_HD bool predict_continuation(const Model& m, int degree, double predictor, double* out) {
     if (!fo_isfinite(predictor)) return false;
-    const double z = degree == 0 ? 0.0 : (predictor - m.mean) / m.scale;
+    const double z = degree == 0 ? 0.0 : divide(predictor - m.mean, Divisor{m.scale, m.inv_scale});
     double prediction = m.coef[0];
     double previous = 0.0, current = 1.0;
     for (int j = 0; j < degree; ++j) {

@@ -83,7 +83,7 @@ constexpr int kEvalStrikes = 8;
 
 // The part of a fitted row the evaluation reads, staged in shared memory per (strike, row).
 struct PolicyRule {
-    double mean, scale;
+    double mean, scale, inv_scale;
     double alpha[kMaxDegree];
     double beta[kMaxDegree];
     double coef[kMaxColumns];

@@ -83,6 +83,7 @@ __global__ void __launch_bounds__(kBatchBackwardThreads, 2) batch_backward_kerne
     const unsigned T = blockDim.x;
     const uint64_t stride = uint64_t(T) * kBackwardBatch;
     const double K = pr.strike;
+    const Divisor Kd = make_divisor(K);
     const int degree = a.degree;
     const uint32_t E = plan.rows - 1;
     const uint32_t fsr = plan.first_stored_row;
@@ -132,7 +133,7 @@ __global__ void __launch_bounds__(kBatchBackwardThreads, 2) batch_backward_kerne
                 values[p] = v[u];
                 if (!fo_isfinite(v[u])) atomicMin(&st->fit_payoff_fail, ((unsigned long long)order << 32) | p);
                 if (s[u] > K) {
-                    const double x = s[u] / K;
+                    const double x = divide(s[u], Kd);
                     if (fo_isfinite(x)) {
                         loc[0] += 1.0;
                         loc[1] += x;
@@ -154,7 +155,7 @@ __global__ void __launch_bounds__(kBatchBackwardThreads, 2) batch_backward_kerne
             for (int u = 0; u < kBackwardBatch; ++u) {
                 const uint64_t p = base + uint64_t(u) * T;
                 if (p >= P || !(s[u] > K)) continue;
-                const double x = s[u] / K;
+                const double x = divide(s[u], Kd);
                 if (!fo_isfinite(x) || !fo_isfinite(v[u])) {
                     sums.acc[14] += 1.0;
                     atomicMin(&st->fit_nonfinite, ((unsigned long long)order << 32) | p);
@@ -220,7 +221,7 @@ __global__ void __launch_bounds__(kBatchBackwardThreads, 2) batch_backward_kerne
                 if (regression && sc[u] > K) {
                     const double intrinsic = sc[u] - K;
                     double continuation;
-                    if (!predict_continuation(sm.model, degree, sc[u] / K, &continuation)) {
+                    if (!predict_continuation(sm.model, degree, divide(sc[u], Kd), &continuation)) {
                         atomicMin(&st->fit_predict_fail, ((unsigned long long)order << 32) | p);
                     } else if (exercise_rule(a.tie_rule, intrinsic, continuation)) {
                         v[u] = intrinsic;
@@ -231,7 +232,7 @@ __global__ void __launch_bounds__(kBatchBackwardThreads, 2) batch_backward_kerne
                     if (!fo_isfinite(v[u]))
                         atomicMin(&st->fit_payoff_fail, ((unsigned long long)(order + 1) << 32) | p);
                     if (sn[u] > K) {
-                        const double x = sn[u] / K;
+                        const double x = divide(sn[u], Kd);
                         if (!fo_isfinite(x) || !fo_isfinite(v[u])) {
                             sums.acc[14] += 1.0;
                             atomicMin(&st->fit_nonfinite, ((unsigned long long)(order + 1) << 32) | p);
@@ -312,6 +313,7 @@ __global__ void __launch_bounds__(kBatchEvalThreads, 2) batch_evaluate_kernel(Ba
     __shared__ dd tot[2 * kEvalStrikes];
     __shared__ unsigned cnt[2 * kEvalStrikes];
     __shared__ double strikes[kEvalStrikes];
+    __shared__ double inv_strikes[kEvalStrikes];
     __shared__ uint32_t rbase[kEvalStrikes];
     __shared__ uint32_t pbase[kEvalStrikes];
     extern __shared__ PolicyRule staged[];  // [kEvalStrikes][rule_rows] when kStaged
@@ -327,6 +329,7 @@ __global__ void __launch_bounds__(kBatchEvalThreads, 2) batch_evaluate_kernel(Ba
     if (threadIdx.x < kEvalStrikes) {
         const bool live = int(threadIdx.x) < ns;
         strikes[threadIdx.x] = live ? a.problems[first + threadIdx.x].strike : 1.0;
+        inv_strikes[threadIdx.x] = make_divisor(strikes[threadIdx.x]).inv;
         rbase[threadIdx.x] = live ? a.problems[first + threadIdx.x].records : 0u;
         pbase[threadIdx.x] = live ? a.problems[first + threadIdx.x].partial_base : 0u;
     }
@@ -341,6 +344,7 @@ __global__ void __launch_bounds__(kBatchEvalThreads, 2) batch_evaluate_kernel(Ba
             rule.kind = rec.kind;
             rule.mean = rec.model.mean;
             rule.scale = rec.model.scale;
+            rule.inv_scale = rec.model.inv_scale;
 #pragma unroll
             for (int j = 0; j < kMaxDegree; ++j) {
                 rule.alpha[j] = rec.model.alpha[j];
@@ -387,8 +391,8 @@ __global__ void __launch_bounds__(kBatchEvalThreads, 2) batch_evaluate_kernel(Ba
             if (kind != kRuleRegression || !(spot > K)) continue;
             const double intrinsic = spot - K;
             double continuation;
-            const bool ok = kStaged ? predict_continuation(staged[k * rule_rows + row], degree, spot / K, &continuation)
-                                    : predict_continuation(a.records[rbase[k] + row].model, degree, spot / K, &continuation);
+            const bool ok = kStaged ? predict_continuation(staged[k * rule_rows + row], degree, divide(spot, Divisor{K, inv_strikes[k]}), &continuation)
+                                    : predict_continuation(a.records[rbase[k] + row].model, degree, divide(spot, Divisor{K, inv_strikes[k]}), &continuation);
             if (!ok) {
                 atomicMin(&a.problem_status[first + k].eval_fail, ((unsigned long long)row << 33) | (p << 1));
                 continue;
@@ -451,6 +455,7 @@ __global__ void __launch_bounds__(kBatchEvalThreads, 2) batch_evaluate_greeks_ke
         rule.kind = rec.kind;
         rule.mean = rec.model.mean;
         rule.scale = rec.model.scale;
+            rule.inv_scale = rec.model.inv_scale;
 #pragma unroll
         for (int j = 0; j < kMaxDegree; ++j) {
             rule.alpha[j] = rec.model.alpha[j];
@@ -463,6 +468,7 @@ __global__ void __launch_bounds__(kBatchEvalThreads, 2) batch_evaluate_greeks_ke
     if (threadIdx.x < 2) cnt[threadIdx.x] = 0;
     __syncthreads();
     const double K = pr.strike;
+    const Divisor Kd = make_divisor(K);
     const uint64_t P = plan.eval_paths;
     const uint64_t p = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x;
     const uint32_t last = rows - 1;
@@ -494,7 +500,7 @@ __global__ void __launch_bounds__(kBatchEvalThreads, 2) batch_evaluate_greeks_ke
         if (rule.kind != kRuleRegression || !(spot > K)) return;
         const double intrinsic = spot - K;
         double continuation;
-        if (!predict_continuation(rule, degree, spot / K, &continuation)) {
+        if (!predict_continuation(rule, degree, divide(spot, Kd), &continuation)) {
             atomicMin(&a.problem_status[problem].eval_fail, ((unsigned long long)row << 33) | (p << 1));
             return;
         }

@@ -147,10 +147,22 @@ template <int S>
 __device__ __forceinline__ void grid_combine(const double2* partials, int blocks, dd* out /* smem [S] */) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     if (warp < S) {
+        // Issue the first eight partials of this lane before adding any, so their L2 latencies
+        // overlap; the additions keep the fixed block order.
+        constexpr int kBatch = 8;
+        double2 v[kBatch];
+#pragma unroll
+        for (int i = 0; i < kBatch; ++i) {
+            const int b = lane + 32 * i;
+            v[i] = b < blocks ? __ldcg(&partials[b * S + warp]) : make_double2(0.0, 0.0);
+        }
         dd acc = dd_make(0.0);
-        for (int b = lane; b < blocks; b += 32) {
-            const double2 v = __ldcg(&partials[b * S + warp]);
-            acc = dd_add(acc, dd{v.x, v.y});
+#pragma unroll
+        for (int i = 0; i < kBatch; ++i)
+            if (lane + 32 * i < blocks) acc = dd_add(acc, dd{v[i].x, v[i].y});
+        for (int b = lane + 32 * kBatch; b < blocks; b += 32) {
+            const double2 w = __ldcg(&partials[b * S + warp]);
+            acc = dd_add(acc, dd{w.x, w.y});
         }
 #pragma unroll
         for (int off = 16; off > 0; off >>= 1) acc = dd_add(acc, shfl_dd_down(acc, off));

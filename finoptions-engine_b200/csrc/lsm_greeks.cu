@@ -62,6 +62,7 @@ __global__ void __launch_bounds__(kEvalThreads, 2) evaluate_greeks_kernel(EvalAr
     load_zig_tables(sx, sf);
     const SmemZig zig = make_zig(sx, sf);
     const double K = plan.strike;
+    const Divisor Kd = make_divisor(K);
     const uint64_t P = plan.eval_paths;
     const int degree = plan.degree;
     const uint32_t last = rows - 1;
@@ -92,7 +93,7 @@ __global__ void __launch_bounds__(kEvalThreads, 2) evaluate_greeks_kernel(EvalAr
             if (er.kind != kRuleRegression || !(spot > K)) return;
             const double intrinsic = spot - K;
             double continuation;
-            if (!predict_continuation(er.model, degree, spot / K, &continuation)) {
+            if (!predict_continuation(er.model, degree, divide(spot, Kd), &continuation)) {
                 atomicMin(&a.status->eval_fail, ((unsigned long long)row << 33) | (p << 1));
                 return;
             }

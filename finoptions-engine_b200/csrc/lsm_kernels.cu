@@ -193,6 +193,7 @@ __global__ void __launch_bounds__(kBackwardThreads, 1) backward_kernel(BackwardA
     const uint64_t nthreads = uint64_t(gridDim.x) * T;
     const uint64_t gtid = uint64_t(blockIdx.x) * T + threadIdx.x;
     const double K = plan.strike;
+    const Divisor Kd = make_divisor(K);
     const int degree = plan.degree;
     const uint32_t rows = plan.rows;
     const uint32_t E = rows - 1;
@@ -236,7 +237,7 @@ __global__ void __launch_bounds__(kBackwardThreads, 1) backward_kernel(BackwardA
                 values[at] = v;
                 if (!fo_isfinite(v)) atomicMin(&a.status->fit_payoff_fail, ((unsigned long long)order << 32) | p);
                 if (sp > K) {
-                    x = sp / K;
+                    x = divide(sp, Kd);
                     if (fo_isfinite(x)) {
                         loc[0] += 1.0;
                         loc[1] += x;
@@ -253,7 +254,7 @@ __global__ void __launch_bounds__(kBackwardThreads, 1) backward_kernel(BackwardA
         for (int j = 0; j < ppt; ++j) {
             const int at = j * T + threadIdx.x;
             if (spots[at] > K) {
-                const double x = spots[at] / K, y = values[at];
+                const double x = divide(spots[at], Kd), y = values[at];
                 if (!fo_isfinite(x) || !fo_isfinite(y)) {
                     sums.acc[14] += 1.0;
                     atomicMin(&a.status->fit_nonfinite, ((unsigned long long)order << 32) | (gtid + uint64_t(j) * nthreads));
@@ -331,7 +332,7 @@ __global__ void __launch_bounds__(kBackwardThreads, 1) backward_kernel(BackwardA
                 if (sp > K) {
                     const double intrinsic = sp - K;
                     double continuation;
-                    if (!predict_continuation(model, degree, sp / K, &continuation)) {
+                    if (!predict_continuation(model, degree, divide(sp, Kd), &continuation)) {
                         atomicMin(&a.status->fit_predict_fail, ((unsigned long long)order << 32) | p);
                     } else if (exercise_rule(plan.tie_rule, intrinsic, continuation)) {
                         v = intrinsic;
@@ -344,7 +345,7 @@ __global__ void __launch_bounds__(kBackwardThreads, 1) backward_kernel(BackwardA
                 if (!fo_isfinite(v))
                     atomicMin(&a.status->fit_payoff_fail, ((unsigned long long)(order + 1) << 32) | p);
                 if (sp > K) {
-                    const double x = sp / K;
+                    const double x = divide(sp, Kd);
                     if (!fo_isfinite(x) || !fo_isfinite(v)) {
                         sums.acc[14] += 1.0;
                         atomicMin(&a.status->fit_nonfinite, ((unsigned long long)(order + 1) << 32) | p);
@@ -443,6 +444,7 @@ __global__ void __launch_bounds__(kEvalThreads, 3) evaluate_kernel(EvalArgs a) {
     load_zig_tables(sx, sf);
     const SmemZig zig = make_zig(sx, sf);
     const double K = plan.strike;
+    const Divisor Kd = make_divisor(K);
     const uint64_t P = plan.eval_paths;
     const int degree = plan.degree;
     double sum = 0.0, sumsq = 0.0;
@@ -467,7 +469,7 @@ __global__ void __launch_bounds__(kEvalThreads, 3) evaluate_kernel(EvalArgs a) {
             if (er.kind != kRuleRegression || !(spot > K)) return;
             const double intrinsic = spot - K;
             double continuation;
-            if (!predict_continuation(er.model, degree, spot / K, &continuation)) {
+            if (!predict_continuation(er.model, degree, divide(spot, Kd), &continuation)) {
                 atomicMin(&a.status->eval_fail, ((unsigned long long)row << 33) | (p << 1));
                 return;
             }
