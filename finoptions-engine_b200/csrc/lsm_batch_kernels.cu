@@ -304,29 +304,31 @@ __global__ void batch_diagnose_kernel(BatchArgs a, uint32_t n_records) {
 // Fused evaluation: one evaluation path per thread, up to kEvalStrikes policies applied on the fly.
 // ---------------------------------------------------------------------------------------------
 
-// kStaged: the group's fitted rules are copied into shared memory ([strike][row]) before the
-// paths run; otherwise each lookup reads the FitRecord from HBM / L2.
-template <bool kStaged>
+// S: strikes per block (1, 2, 4 or 8; the launcher picks the smallest that covers the widest
+// group, so row and ragged batches run the one-strike body). kStaged: the group's fitted rules are
+// copied into shared memory ([strike][row]) before the paths run; otherwise each lookup reads the
+// FitRecord from HBM / L2.
+template <int S, bool kStaged>
 __global__ void __launch_bounds__(kBatchEvalThreads, 2) batch_evaluate_kernel(BatchArgs a, uint32_t rule_rows) {
     __shared__ double sx[257], sf[257];
-    __shared__ double red[32 * 2 * kEvalStrikes];
-    __shared__ dd tot[2 * kEvalStrikes];
-    __shared__ unsigned cnt[2 * kEvalStrikes];
-    __shared__ double strikes[kEvalStrikes];
-    __shared__ double inv_strikes[kEvalStrikes];
-    __shared__ uint32_t rbase[kEvalStrikes];
-    __shared__ uint32_t pbase[kEvalStrikes];
-    extern __shared__ PolicyRule staged[];  // [kEvalStrikes][rule_rows] when kStaged
+    __shared__ double red[32 * 2 * S];
+    __shared__ dd tot[2 * S];
+    __shared__ unsigned cnt[2 * S];
+    __shared__ double strikes[S];
+    __shared__ double inv_strikes[S];
+    __shared__ uint32_t rbase[S];
+    __shared__ uint32_t pbase[S];
+    extern __shared__ PolicyRule staged[];  // [S][rule_rows] when kStaged
     const BatchGroup& g = a.groups[blockIdx.y];
-    const uint32_t first = g.first_problem + blockIdx.z * kEvalStrikes;
-    const int ns = min(kEvalStrikes, int(g.problems) - int(blockIdx.z) * kEvalStrikes);
+    const uint32_t first = g.first_problem + blockIdx.z * S;
+    const int ns = min(S, int(g.problems) - int(blockIdx.z) * S);
     if (ns <= 0) return;  // uniform over the block
     if (uint64_t(blockIdx.x) * blockDim.x >= g.plan.eval_paths) return;  // beyond this group's paths
     if (sim_failed(&a.group_status[blockIdx.y].train_sim_fail)) return;
     load_zig_tables(sx, sf);
     const SmemZig zig = make_zig(sx, sf);
-    if (threadIdx.x < 2 * kEvalStrikes) cnt[threadIdx.x] = 0;
-    if (threadIdx.x < kEvalStrikes) {
+    if (threadIdx.x < 2 * S) cnt[threadIdx.x] = 0;
+    if (threadIdx.x < S) {
         const bool live = int(threadIdx.x) < ns;
         strikes[threadIdx.x] = live ? a.problems[first + threadIdx.x].strike : 1.0;
         inv_strikes[threadIdx.x] = make_divisor(strikes[threadIdx.x]).inv;
@@ -359,9 +361,9 @@ __global__ void __launch_bounds__(kBatchEvalThreads, 2) batch_evaluate_kernel(Ba
     const uint64_t p = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x;
     const uint32_t last = rows - 1;
     const int degree = a.degree;
-    double payoff[kEvalStrikes];
+    double payoff[S];
 #pragma unroll
-    for (int k = 0; k < kEvalStrikes; ++k) payoff[k] = 0.0;
+    for (int k = 0; k < S; ++k) payoff[k] = 0.0;
     unsigned active = p < P ? ((1u << ns) - 1u) : 0u;
     auto observe = [&](int row, double spot) {
         if (!active) return;
@@ -369,7 +371,7 @@ __global__ void __launch_bounds__(kBatchEvalThreads, 2) batch_evaluate_kernel(Ba
         const double disc = plan.disc_to_origin[row];
         if (uint32_t(row) == last) {
 #pragma unroll
-            for (int k = 0; k < kEvalStrikes; ++k) {
+            for (int k = 0; k < S; ++k) {
                 if (!((active >> k) & 1u)) continue;
                 const double d = spot - strikes[k];
                 payoff[k] = (d > 0.0 ? d : 0.0) * disc;
@@ -380,7 +382,7 @@ __global__ void __launch_bounds__(kBatchEvalThreads, 2) batch_evaluate_kernel(Ba
             return;
         }
 #pragma unroll
-        for (int k = 0; k < kEvalStrikes; ++k) {
+        for (int k = 0; k < S; ++k) {
             if (!((active >> k) & 1u)) continue;
             const double K = strikes[k];
             const int kind = kStaged ? staged[k * rule_rows + row].kind : a.records[rbase[k] + row].kind;
@@ -410,13 +412,13 @@ __global__ void __launch_bounds__(kBatchEvalThreads, 2) batch_evaluate_kernel(Ba
         const SimResult r = simulate_path(plan, zig, plan.eval_seed, plan.eval_domain, uint32_t(p), observe);
         if (r.code != 0) atomicMin(&a.group_status[blockIdx.y].eval_sim_fail, (unsigned long long)p);
     }
-    double acc[2 * kEvalStrikes];
+    double acc[2 * S];
 #pragma unroll
-    for (int k = 0; k < kEvalStrikes; ++k) {
+    for (int k = 0; k < S; ++k) {
         acc[2 * k] = payoff[k];
         acc[2 * k + 1] = payoff[k] * payoff[k];
     }
-    cta_reduce_dd<2 * kEvalStrikes>(acc, red, tot);
+    cta_reduce_dd<2 * S>(acc, red, tot);
     if (int(threadIdx.x) < 2 * ns) {
         const uint32_t k = threadIdx.x >> 1, which = threadIdx.x & 1u;
         a.eval_partials[(size_t(pbase[k]) + blockIdx.x) * 2 + which] = make_double2(tot[threadIdx.x].hi, tot[threadIdx.x].lo);
@@ -702,18 +704,26 @@ cudaError_t launch_batch_diagnose(const BatchArgs& a, uint32_t n_records, cudaSt
     return cudaGetLastError();
 }
 
-cudaError_t launch_batch_evaluate(const BatchArgs& a, uint32_t strike_chunks, uint32_t max_rows, cudaStream_t stream) {
-    const dim3 grid(a.eval_blocks, a.n_groups, strike_chunks);
-    const size_t smem = sizeof(PolicyRule) * kEvalStrikes * max_rows;
+template <int S>
+cudaError_t launch_batch_evaluate_width(const BatchArgs& a, uint32_t max_strikes, uint32_t max_rows, cudaStream_t stream) {
+    const dim3 grid(a.eval_blocks, a.n_groups, (max_strikes + S - 1) / S);
+    const size_t smem = sizeof(PolicyRule) * S * max_rows;
     if (smem <= kEvalRuleSmemBytes) {
-        cudaError_t e = cudaFuncSetAttribute(batch_evaluate_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        cudaError_t e = cudaFuncSetAttribute(batch_evaluate_kernel<S, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                              int(kEvalRuleSmemBytes));
         if (e != cudaSuccess) return e;
-        batch_evaluate_kernel<true><<<grid, kBatchEvalThreads, smem, stream>>>(a, max_rows);
+        batch_evaluate_kernel<S, true><<<grid, kBatchEvalThreads, smem, stream>>>(a, max_rows);
     } else {
-        batch_evaluate_kernel<false><<<grid, kBatchEvalThreads, 0, stream>>>(a, max_rows);
+        batch_evaluate_kernel<S, false><<<grid, kBatchEvalThreads, 0, stream>>>(a, max_rows);
     }
     return cudaGetLastError();
+}
+
+cudaError_t launch_batch_evaluate(const BatchArgs& a, uint32_t max_strikes, uint32_t max_rows, cudaStream_t stream) {
+    if (max_strikes <= 1) return launch_batch_evaluate_width<1>(a, max_strikes, max_rows, stream);
+    if (max_strikes <= 2) return launch_batch_evaluate_width<2>(a, max_strikes, max_rows, stream);
+    if (max_strikes <= 4) return launch_batch_evaluate_width<4>(a, max_strikes, max_rows, stream);
+    return launch_batch_evaluate_width<kEvalStrikes>(a, max_strikes, max_rows, stream);
 }
 
 cudaError_t launch_batch_evaluate_greeks(const BatchArgs& a, uint32_t max_strikes, uint32_t max_rows,

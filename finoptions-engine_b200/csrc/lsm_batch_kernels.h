@@ -14,8 +14,9 @@ constexpr int kBatchEvalThreads = 256;
 cudaError_t launch_batch_simulate(const BatchArgs& a, cudaStream_t stream);
 cudaError_t launch_batch_backward(const BatchArgs& a, cudaStream_t stream);
 cudaError_t launch_batch_diagnose(const BatchArgs& a, uint32_t n_records, cudaStream_t stream);
-// max_rows: the largest observation-row count of the wave's groups (sizes the staged rules).
-cudaError_t launch_batch_evaluate(const BatchArgs& a, uint32_t strike_chunks, uint32_t max_rows, cudaStream_t stream);
+// max_strikes: strikes of the widest group; max_rows: the largest observation-row count of the
+// wave's groups (sizes the staged rules).
+cudaError_t launch_batch_evaluate(const BatchArgs& a, uint32_t max_strikes, uint32_t max_rows, cudaStream_t stream);
 // One block per (path block, group, strike): the adjoint Greeks variant of the evaluation.
 cudaError_t launch_batch_evaluate_greeks(const BatchArgs& a, uint32_t max_strikes, uint32_t max_rows,
                                          cudaStream_t stream);

@@ -1240,7 +1240,7 @@ Error price_groups(fo_executor* ex, const BatchMethod& m, const std::vector<Grou
         auto* hpb = reinterpret_cast<BatchProblem*>(host + (L.problems - in_bytes));
         uint64_t slab = 0, record = 0, problem = 0, values = 0, partial = 0;
         slab_of.assign(w.g1 - w.g0, 0);
-        uint32_t chunks = 1, max_rows = 1, max_strikes = 1;
+        uint32_t max_rows = 1, max_strikes = 1;
         for (uint64_t g = w.g0; g < w.g1; ++g) {
             const HostPlan& hp = work[g].hp;
             BatchGroup& bg = hg[g - w.g0];
@@ -1265,7 +1265,6 @@ Error price_groups(fo_executor* ex, const BatchMethod& m, const std::vector<Grou
                 problem += 1;
             }
             slab += uint64_t(hp.rows() - (hp.origin_row ? 1 : 0)) * hp.train_paths;
-            chunks = std::max<uint32_t>(chunks, uint32_t((bg.problems + kEvalStrikes - 1) / kEvalStrikes));
             max_rows = std::max<uint32_t>(max_rows, hp.rows());
         }
         FO_CUDA_TRY(cudaMemcpyAsync(dev + L.groups, host + (L.groups - in_bytes), L.out_begin - L.groups,
@@ -1309,7 +1308,7 @@ Error price_groups(fo_executor* ex, const BatchMethod& m, const std::vector<Grou
         if (greeks)
             FO_CUDA_TRY(launch_batch_evaluate_greeks(a, max_strikes, max_rows, s), "batch Greeks evaluation launch");
         else
-            FO_CUDA_TRY(launch_batch_evaluate(a, chunks, max_rows, s), "batch evaluation launch");
+            FO_CUDA_TRY(launch_batch_evaluate(a, max_strikes, max_rows, s), "batch evaluation launch");
         FO_CUDA_TRY(cudaEventRecord(mark[4], s), "event");
         FO_CUDA_TRY(launch_batch_summarize(a, s), "batch summary launch");
         FO_CUDA_TRY(cudaEventRecord(mark[5], s), "event");
