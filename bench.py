@@ -512,6 +512,18 @@ def grouped_algorithmic_bytes(c, paths: int) -> dict:
     }
 
 
+def batch_traffic(kernel: str, algorithmic_bytes: int) -> int | None:
+    """DRAM bytes per call of a batch kernel: the ncu-measured ratio of DRAM to algorithmic bytes
+    (profiles/traffic.json) times this call's algorithmic bytes."""
+    path = ROOT / "profiles" / "traffic.json"
+    if not path.is_file():
+        return None
+    entry = json.loads(path.read_text()).get(kernel)
+    if entry is None or "dram_bytes_per_algorithmic_byte" not in entry:
+        return None
+    return int(entry["dram_bytes_per_algorithmic_byte"] * algorithmic_bytes)
+
+
 def run_grouped(args: argparse.Namespace, executor) -> dict:
     """The grouped batch (4096 states x 8 strikes, 32,768 + 32,768 paths per state) through the C
     ABI with host columns in and host result columns out, per call."""
@@ -590,7 +602,8 @@ def run_grouped(args: argparse.Namespace, executor) -> dict:
         "gpu_launches": launches,
         "kernels": kernels,
         "roofline": {"kernel": dominant, "bound": "hbm", "achieved": round(achieved, 1), "peak": hbm_peak,
-                     "peak_source": peak_kind, "unit": "GB/s", "frac": round(achieved / hbm_peak, 4)},
+                     "peak_source": peak_kind, "unit": "GB/s", "frac": round(achieved / hbm_peak, 4),
+                     "traffic": batch_traffic(dominant, algorithmic[dominant])},
         "clocks": clocks.report(),
         "cpu_baseline": {"contracts_per_s": GROUPED_SAMPLE_STATES * GROUPED_STRIKES / cpu_s,
                          "path_steps_per_s": _workloads.path_steps(sample, GROUPED_PATHS) / cpu_s, "cores": threads,
