@@ -9,7 +9,7 @@
 
 namespace fo {
 
-constexpr int kBackwardThreads = 512;
+constexpr int kBackwardThreads = 1024;
 constexpr int kEvalThreads = 256;
 
 struct BackwardArgs {
