@@ -415,6 +415,19 @@ struct FitModel {
     double aux_value;  // scale for kFitDegeneratePredictor
 };
 
+// Binomial coefficients C(k, j) for k, j <= 8 (exact in binary64; zero above the diagonal). The
+// binomial shift reads them as constants instead of forming them by a chain of divisions; device
+// code reads the __constant__ copy.
+static constexpr double kBinomialHost[9][9] = {{1.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0}, {1.0, 1.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0}, {1.0, 2.0, 1.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0}, {1.0, 3.0, 3.0, 1.0, 0.0, 0.0, 0.0, 0.0, 0.0}, {1.0, 4.0, 6.0, 4.0, 1.0, 0.0, 0.0, 0.0, 0.0}, {1.0, 5.0, 10.0, 10.0, 5.0, 1.0, 0.0, 0.0, 0.0}, {1.0, 6.0, 15.0, 20.0, 15.0, 6.0, 1.0, 0.0, 0.0}, {1.0, 7.0, 21.0, 35.0, 35.0, 21.0, 7.0, 1.0, 0.0}, {1.0, 8.0, 28.0, 56.0, 70.0, 56.0, 28.0, 8.0, 1.0}};
+#ifdef __CUDACC__
+static __constant__ double kBinomialDevice[9][9] = {{1.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0}, {1.0, 1.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0}, {1.0, 2.0, 1.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0}, {1.0, 3.0, 3.0, 1.0, 0.0, 0.0, 0.0, 0.0, 0.0}, {1.0, 4.0, 6.0, 4.0, 1.0, 0.0, 0.0, 0.0, 0.0}, {1.0, 5.0, 10.0, 10.0, 5.0, 1.0, 0.0, 0.0, 0.0}, {1.0, 6.0, 15.0, 20.0, 15.0, 6.0, 1.0, 0.0, 0.0}, {1.0, 7.0, 21.0, 35.0, 35.0, 21.0, 7.0, 1.0, 0.0}, {1.0, 8.0, 28.0, 56.0, 70.0, 56.0, 28.0, 8.0, 1.0}};
+#endif
+#ifdef __CUDA_ARCH__
+#define FO_BINOMIAL kBinomialDevice
+#else
+#define FO_BINOMIAL kBinomialHost
+#endif
+
 // sums[k] for k in 0..8 are T_k (T_0 = count), sums[9 + k] for k in 0..4 are U_k.
 FO_HD_NOINLINE void fit_from_moments(const dd* sums, double pivot, uint64_t count, int degree, double rank_tolerance,
                             FitModel* m) {
@@ -468,21 +481,16 @@ FO_HD_NOINLINE void fit_from_moments(const dd* sums, double pivot, uint64_t coun
         dd spow = dd_make(1.0);
         for (int k = 0; k <= top; ++k) {
             dd acc = dd_make(0.0);
-            double binom = 1.0;
             for (int j = k; j >= 0; --j) {
                 // term: C(k, j) * delta^(k - j) * T_j
                 const dd tj = j == 0 ? T0 : sums[j];
-                acc = dd_add(acc, dd_mul_d(dd_mul(dpow[k - j], tj), binom));
-                binom = binom * double(j) / double(k - j + 1);
+                acc = dd_add(acc, dd_mul_d(dd_mul(dpow[k - j], tj), FO_BINOMIAL[k][j]));
             }
             mom[k] = dd_mul(acc, spow);
             if (k <= degree) {
                 dd racc = dd_make(0.0);
-                double rb = 1.0;
-                for (int j = k; j >= 0; --j) {
-                    racc = dd_add(racc, dd_mul_d(dd_mul(dpow[k - j], sums[kPowerSums + j]), rb));
-                    rb = rb * double(j) / double(k - j + 1);
-                }
+                for (int j = k; j >= 0; --j)
+                    racc = dd_add(racc, dd_mul_d(dd_mul(dpow[k - j], sums[kPowerSums + j]), FO_BINOMIAL[k][j]));
                 resp[k] = dd_mul(racc, spow);
             }
             spow = dd_mul(spow, inv_scale);
@@ -630,20 +638,14 @@ FO_HD bool fit_near_pivot(const dd* sums, double pivot, uint64_t count, double r
         double spow = 1.0;
 #pragma unroll
         for (int k = 0; k <= 2 * D; ++k) {
-            double acc = 0.0, binom = 1.0;
+            double acc = 0.0;
 #pragma unroll
-            for (int j = k; j >= 0; --j) {
-                acc += binom * dpow[k - j] * T[j];
-                binom = binom * double(j) / double(k - j + 1);
-            }
+            for (int j = k; j >= 0; --j) acc += FO_BINOMIAL[k][j] * dpow[k - j] * T[j];
             mom[k] = acc * spow;
             if (k <= D) {
-                double racc = 0.0, rb = 1.0;
+                double racc = 0.0;
 #pragma unroll
-                for (int j = k; j >= 0; --j) {
-                    racc += rb * dpow[k - j] * U[j];
-                    rb = rb * double(j) / double(k - j + 1);
-                }
+                for (int j = k; j >= 0; --j) racc += FO_BINOMIAL[k][j] * dpow[k - j] * U[j];
                 resp[k] = racc * spow;
             }
             spow *= inv_scale;
