@@ -40,21 +40,15 @@ constexpr uint32_t kPhiloxM1 = 0xcd9e8d57u;
 constexpr uint32_t kPhiloxW0 = 0x9e3779b9u;
 constexpr uint32_t kPhiloxW1 = 0xbb67ae85u;
 
-FO_HD uint32_t mulhi32(uint32_t a, uint32_t b) {
-#if defined(__CUDA_ARCH__)
-    return __umulhi(a, b);
-#else
-    return uint32_t((uint64_t(a) * b) >> 32);
-#endif
-}
-
 // Ten rounds; round r uses key + r * (W0, W1). Output words are the Random123 ordering.
 FO_HD void philox4x32_10(uint32_t c0, uint32_t c1, uint32_t c2, uint32_t c3, uint32_t k0, uint32_t k1,
                          uint32_t out[4]) {
 #pragma unroll
     for (int r = 0; r < 10; ++r) {
-        const uint32_t hi0 = mulhi32(kPhiloxM0, c0), lo0 = kPhiloxM0 * c0;
-        const uint32_t hi1 = mulhi32(kPhiloxM1, c2), lo1 = kPhiloxM1 * c2;
+        // One widening multiply gives both halves of each product.
+        const uint64_t p0 = uint64_t(kPhiloxM0) * c0, p1 = uint64_t(kPhiloxM1) * c2;
+        const uint32_t hi0 = uint32_t(p0 >> 32), lo0 = uint32_t(p0);
+        const uint32_t hi1 = uint32_t(p1 >> 32), lo1 = uint32_t(p1);
         const uint32_t n0 = hi1 ^ c1 ^ k0;
         const uint32_t n2 = hi0 ^ c3 ^ k1;
         c0 = n0;
@@ -70,14 +64,21 @@ FO_HD void philox4x32_10(uint32_t c0, uint32_t c1, uint32_t c2, uint32_t c3, uin
     out[3] = c3;
 }
 
-// Words are consumed as u64 pairs (low word first). A fresh block is generated only when the
-// 4-word buffer is exhausted, so a path's word sequence does not depend on how it is consumed.
+// Words are consumed as u64 pairs (low word first); one Philox block yields two. The next words
+// wait in a small FIFO (b0 first, up to three). Before every odd-numbered normal (the 1st, 3rd,
+// ...) the stream appends a block while at most one word is queued: the fast path of the sampler
+// takes exactly one word per normal, so in the common case every lane of a warp generates its
+// block at the same normal, even after rejections have shifted lanes against each other within
+// their blocks. A block is also generated whenever a word is wanted from an empty FIFO (only after
+// a rejection). Blocks are generated in counter order and words leave in order, so a path's word
+// sequence does not depend on when its blocks are generated.
 struct PathStream {
     uint32_t k0, k1, domain, path;
     uint64_t next_block;
-    uint32_t w[4];
-    uint32_t pos;
-    uint32_t remaining;
+    uint64_t b0, b1, b2;
+    uint32_t count;      // queued words
+    uint32_t remaining;  // normals left in the budget
+    uint32_t drawn;      // normals begun
 
     FO_HD void init(uint64_t seed, uint32_t domain_, uint32_t path_, uint32_t budget) {
         k0 = uint32_t(seed);
@@ -85,36 +86,40 @@ struct PathStream {
         domain = domain_;
         path = path_;
         next_block = 0;
-        pos = 4;
+        b0 = b1 = b2 = 0;
+        count = 0;
         remaining = budget;
-        w[0] = w[1] = w[2] = w[3] = 0;
+        drawn = 0;
     }
-    FO_HD void refill() {
+    // Appends one block; requires count <= 1.
+    FO_HD void append_block() {
+        uint32_t w[4];
         philox4x32_10(uint32_t(next_block), uint32_t(next_block >> 32), path, domain, k0, k1, w);
-        pos = 0;
         next_block += 1;
-    }
-    FO_HD uint32_t next_u32() {
-        if (pos == 4) refill();
-        uint32_t v;
-        // Indexing through a switch keeps the buffer in registers on the device.
-        switch (pos) {
-            case 0: v = w[0]; break;
-            case 1: v = w[1]; break;
-            case 2: v = w[2]; break;
-            default: v = w[3]; break;
+        const uint64_t n0 = uint64_t(w[0]) | (uint64_t(w[1]) << 32);
+        const uint64_t n1 = uint64_t(w[2]) | (uint64_t(w[3]) << 32);
+        if (count == 0) {
+            b0 = n0;
+            b1 = n1;
+        } else {
+            b1 = n0;
+            b2 = n1;
         }
-        pos += 1;
-        return v;
+        count += 2;
     }
     FO_HD uint64_t next_u64() {
-        const uint64_t lo = next_u32();
-        const uint64_t hi = next_u32();
-        return lo | (hi << 32);
+        if (count == 0) append_block();
+        const uint64_t v = b0;
+        b0 = b1;
+        b1 = b2;
+        count -= 1;
+        return v;
     }
     FO_HD bool begin_normal() {
         if (remaining == 0) return false;
         remaining -= 1;
+        if ((drawn & 1u) == 0 && count <= 1) append_block();
+        drawn += 1;
         return true;
     }
 };
