@@ -157,7 +157,7 @@ __global__ void __launch_bounds__(kBatchBackwardThreads, 2) batch_backward_kerne
                 if (p >= P || !(s[u] > K)) continue;
                 const double x = divide(s[u], Kd);
                 if (!fo_isfinite(x) || !fo_isfinite(v[u])) {
-                    sums.acc[14] += 1.0;
+                    sums.acc[kBadSlot] += 1.0;
                     atomicMin(&st->fit_nonfinite, ((unsigned long long)order << 32) | p);
                 } else {
                     accumulate_itm(sums, x, v[u], pivot);
@@ -169,7 +169,7 @@ __global__ void __launch_bounds__(kBatchBackwardThreads, 2) batch_backward_kerne
         cta_reduce_dd<kSlots>(sums.acc, sm.red, sm.total);
         if (threadIdx.x == 0) {
             const uint64_t itm = uint64_t(sm.total[0].hi);
-            const uint64_t bad = uint64_t(sm.total[14].hi);
+            const uint64_t bad = uint64_t(sm.total[kBadSlot].hi);
             const uint64_t population = itm + bad;
             const uint32_t required = uint32_t(degree + 1);
             int kind;
@@ -234,7 +234,7 @@ __global__ void __launch_bounds__(kBatchBackwardThreads, 2) batch_backward_kerne
                     if (sn[u] > K) {
                         const double x = divide(sn[u], Kd);
                         if (!fo_isfinite(x) || !fo_isfinite(v[u])) {
-                            sums.acc[14] += 1.0;
+                            sums.acc[kBadSlot] += 1.0;
                             atomicMin(&st->fit_nonfinite, ((unsigned long long)(order + 1) << 32) | p);
                         } else {
                             accumulate_itm(sums, x, v[u], pivot);

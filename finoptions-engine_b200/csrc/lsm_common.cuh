@@ -85,6 +85,7 @@ __device__ __forceinline__ SimResult simulate_path(const DevicePlan& plan, const
 // ---------------------------------------------------------------------------------------------
 
 constexpr int kSlots = 16;  // T_0..T_8, U_0..U_4, non-finite count, spare
+constexpr int kBadSlot = kMomentSlots;  // in-the-money paths with a non-finite predictor or response
 
 __device__ __forceinline__ dd shfl_dd_down(dd v, int off);
 
@@ -206,6 +207,28 @@ __device__ __forceinline__ void accumulate_itm(RowSums& r, double x, double y, d
     for (int k = 1; k < kPowerSums; ++k) {
         r.acc[k] += pw;
         if (k < kResponseSums) r.acc[kPowerSums + k] += y * pw;
+        pw *= t;
+    }
+}
+
+// The halves of accumulate_itm: count and T_1..T_8 of t = x - pivot (they do not depend on the
+// response), and U_0..U_4 of the response y.
+__device__ __forceinline__ void accumulate_powers(RowSums& r, double t) {
+    r.acc[0] += 1.0;
+    double pw = t;
+#pragma unroll
+    for (int k = 1; k < kPowerSums; ++k) {
+        r.acc[k] += pw;
+        pw *= t;
+    }
+}
+
+__device__ __forceinline__ void accumulate_responses(RowSums& r, double t, double y) {
+    r.acc[kPowerSums] += y;
+    double pw = t;
+#pragma unroll
+    for (int k = 1; k < kResponseSums; ++k) {
+        r.acc[kPowerSums + k] += y * pw;
         pw *= t;
     }
 }

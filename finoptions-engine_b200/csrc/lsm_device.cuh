@@ -64,9 +64,8 @@ struct DeviceStatus {
     unsigned long long eval_terminal_fail;  // path: non-finite terminal payoff
     unsigned long long fit_nonfinite;    // (order << 32) | path: non-finite ITM predictor/response
     unsigned int fit_failed_order;       // first backward order whose fit failed
-    unsigned int barrier_timeout;        // zero-initialised
-    unsigned int arrive;                 // grid barrier arrival counter, zero-initialised
-    unsigned int generation;             // grid barrier generation, zero-initialised
+    unsigned int barrier_timeout;        // zero-initialised: a grid wait timed out
+    unsigned int arrivals;               // zero-initialised: backward CTA partials published so far
 };
 constexpr size_t kStatusNoneBytes = 7 * sizeof(unsigned long long) + sizeof(unsigned int);
 

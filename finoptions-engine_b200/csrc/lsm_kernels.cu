@@ -48,41 +48,104 @@ __device__ __forceinline__ unsigned long long global_timer_ns() {
     return t;
 }
 
-// Bounded grid-wide barrier for a cooperatively launched grid (all CTAs co-resident). A waiting
-// CTA gives up after kBarrierTimeoutNs, raising status->barrier_timeout; every CTA then leaves.
-constexpr unsigned long long kBarrierTimeoutNs = 2000000000ull;
+__device__ __forceinline__ void red_release_add_gpu(unsigned* p, unsigned v) {
+    asm volatile("red.release.gpu.global.add.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
 
-__device__ bool grid_barrier(unsigned* local_gen, DeviceStatus* st) {
-    unsigned* arrive = &st->arrive;
-    unsigned* generation = &st->generation;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        const unsigned gen = *local_gen;
-        __threadfence();
-        const unsigned prev = atomicAdd(arrive, 1u);
-        if (prev == gridDim.x - 1) {
-            atomicExch(arrive, 0u);
-            __threadfence();
-            atomicExch(generation, gen + 1);
-        } else {
-            unsigned long long spins = 0;
-            const unsigned long long start = global_timer_ns();
-            while (ld_acquire_gpu(generation) == gen) {
-                if ((++spins & 1023u) == 0) {
-                    if (ld_volatile_u32(&st->barrier_timeout) != 0) break;
-                    if (global_timer_ns() - start > kBarrierTimeoutNs) {
-                        atomicExch(&st->barrier_timeout, 1u);
-                        break;
-                    }
-                    __nanosleep(32);
+__device__ __forceinline__ unsigned ld_relaxed_gpu(const unsigned* p) {
+    unsigned v;
+    asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+__device__ __forceinline__ void named_barrier_sync(int id, int threads) {
+    asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(threads) : "memory");
+}
+
+// Grid synchronisation of the backward pass (all CTAs co-resident: cooperative launch). There is
+// no grid barrier. When its partial for sync point `seq` is written (cta_reduce_to ends with a CTA
+// barrier), thread 0 adds one to the grid's arrival counter with release semantics and moves on
+// without waiting for a reply. Warp 0 of every CTA reads the counter until it reaches
+// seq * gridDim.x, fences once, and the combine warps read the partials. A partial buffer is
+// reused two sync points later: a CTA arrives at seq + 2 only after combining seq + 1, which needs
+// every CTA to have arrived at seq + 1, which each does only after it has read the partials of
+// seq. A waiting warp gives up after kBarrierTimeoutNs, raising status->barrier_timeout; every CTA
+// then leaves at its next wait.
+constexpr unsigned long long kBarrierTimeoutNs = 2000000000ull;
+constexpr int kCombineWarps = kSlots;  // warps 0..15 wait for and combine the CTA partials
+constexpr int kCombineThreads = kCombineWarps * 32;
+
+__device__ __forceinline__ void publish_partial(DeviceStatus* st) {
+    if (threadIdx.x == 0) red_release_add_gpu(&st->arrivals, 1u);
+}
+
+// Warp-wide wait until the arrival counter reaches `target`. Lane 0 reads the counter and every
+// decision is taken on its broadcast value, so the lanes leave the loop together however they
+// entered it. Returns false (in every lane) on timeout.
+__device__ bool wait_arrivals(DeviceStatus* st, unsigned target) {
+    const int lane = threadIdx.x & 31;
+    unsigned spins = 0;
+    unsigned long long start = 0;
+    __syncwarp();
+    for (;;) {
+        unsigned seen = 0;
+        if (lane == 0) seen = ld_relaxed_gpu(&st->arrivals);
+        seen = __shfl_sync(0xffffffffu, seen, 0);
+        if (seen >= target) break;
+        if ((++spins & 255u) == 0) {
+            int give_up = 0;
+            if (lane == 0) {
+                give_up = ld_volatile_u32(&st->barrier_timeout) != 0;
+                const unsigned long long now = global_timer_ns();
+                if (start == 0) {
+                    start = now;
+                } else if (now - start > kBarrierTimeoutNs) {
+                    atomicExch(&st->barrier_timeout, 1u);
+                    give_up = 1;
                 }
             }
+            if (__shfl_sync(0xffffffffu, give_up, 0)) return false;
         }
-        __threadfence();
-        *local_gen = gen + 1;
     }
-    __syncthreads();
-    return ld_volatile_u32(&st->barrier_timeout) == 0;
+    __threadfence();
+    return true;
+}
+
+// Run by the combine warps only (they meet at named barrier 1). Warp 0 waits for every CTA's arrival;
+// then warp k < S sums slot k of the partials over the CTAs in block order (double-double, the
+// same fixed order in every CTA). *wait_failed is 1 when the wait timed out (out is not written).
+template <int S>
+__device__ __forceinline__ void combine_published(const double2* partials, unsigned seq, DeviceStatus* st, dd* out,
+                                                  int* wait_failed) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int blocks = int(gridDim.x);
+    if (warp == 0) {
+        const bool ok = wait_arrivals(st, seq * unsigned(blocks));
+        if (lane == 0) *wait_failed = ok ? 0 : 1;
+    }
+    named_barrier_sync(1, kCombineThreads);
+    if (*wait_failed) return;
+    if (warp < S) {
+        constexpr int kBatch = 8;  // first eight partials of the lane in flight together
+        double2 v[kBatch];
+#pragma unroll
+        for (int i = 0; i < kBatch; ++i) {
+            const int b = lane + 32 * i;
+            v[i] = b < blocks ? __ldcg(&partials[b * S + warp]) : make_double2(0.0, 0.0);
+        }
+        dd acc = dd_make(0.0);
+#pragma unroll
+        for (int i = 0; i < kBatch; ++i)
+            if (lane + 32 * i < blocks) acc = dd_add(acc, dd{v[i].x, v[i].y});
+        for (int b = lane + 32 * kBatch; b < blocks; b += 32) {
+            const double2 w = __ldcg(&partials[b * S + warp]);
+            acc = dd_add(acc, dd{w.x, w.y});
+        }
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) acc = dd_add(acc, shfl_dd_down(acc, off));
+        if (lane == 0) out[warp] = acc;
+    }
+    named_barrier_sync(1, kCombineThreads);
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -163,27 +226,34 @@ struct BackwardSmem {
     dd total[kSlots];
     FitModel model;
     int kind;
-    int stop;
-    unsigned local_gen;
+    int wait_failed;
 };
 
 // Each thread owns paths gtid + j * nthreads (j < ppt). Their discounted values, the current
-// row's spots and moneyness x = S/K live in this CTA's shared memory ([j * blockDim + tid]) for the
-// whole backward pass, so the only HBM traffic is one read of each stored row. One pass over the
-// shared arrays per row applies row k's exercise rule and immediately stages row k-1: load its
-// spots, discount the values (policy.rs:1049-1063) and accumulate its in-the-money power sums.
+// row's spots and the staged row's spots live in this CTA's shared memory ([j * blockDim + tid])
+// for the whole backward pass, so the only HBM traffic is one read of each stored row.
+//
+// Per exercise row k the CTA reduces its in-the-money power sums of row k and publishes them;
+// then the warps split. Warps 0..15 wait for every CTA's partial, combine them and thread 0 fits
+// row k's continuation. Meanwhile warps 16..31 take row k-1, whose spots were prefetched with
+// cp.async: its in-the-money test and the power sums T_0..T_8 of its moneyness do not depend on
+// row k's exercise decision, so they are accumulated while the grid synchronises and the fit
+// runs. After a CTA barrier every thread applies row k's exercise rule to its paths, discounts
+// them to row k-1 (policy.rs:1049-1063) and adds the response sums U_0..U_4, which need the
+// decided values. Row k-1's sums are taken about the mean of the latest fitted row available when
+// its staging starts (two rows later than row k-1); any pivot near the in-the-money mean serves.
 __global__ void __launch_bounds__(kBackwardThreads, 1) backward_kernel(BackwardArgs a) {
     __shared__ BackwardSmem sm;
     extern __shared__ double backward_dyn[];
     const DevicePlan& plan = a.plan;
     if (*(const volatile unsigned long long*)&a.status->train_sim_fail != kNone)
         return;  // training simulation failed: every CTA reads the same word and leaves
-    if (threadIdx.x == 0) {
-        sm.local_gen = 0;
-        sm.stop = 0;
-    }
     const int ppt = a.ppt;
     const int T = blockDim.x;
+    const int warp = threadIdx.x >> 5;
+    const bool stager = warp >= kCombineWarps;
+    const int stage_threads = T - kCombineThreads;
+    const int stage_tid = int(threadIdx.x) - kCombineThreads;
     // values, the spots of the row being decided, and the spots of the row being staged (filled
     // by cp.async while the current row is reduced and solved); the two spot buffers alternate.
     double* values = backward_dyn;
@@ -191,7 +261,8 @@ __global__ void __launch_bounds__(kBackwardThreads, 1) backward_kernel(BackwardA
     double* spots_next = backward_dyn + 2 * size_t(ppt) * T;
     const uint64_t P = plan.train_paths;
     const uint64_t nthreads = uint64_t(gridDim.x) * T;
-    const uint64_t gtid = uint64_t(blockIdx.x) * T + threadIdx.x;
+    const uint64_t block_first = uint64_t(blockIdx.x) * T;
+    const uint64_t gtid = block_first + threadIdx.x;
     const double K = plan.strike;
     const Divisor Kd = make_divisor(K);
     const int degree = plan.degree;
@@ -215,9 +286,11 @@ __global__ void __launch_bounds__(kBackwardThreads, 1) backward_kernel(BackwardA
     }
     double2* parts = a.partials;
     int parity = 0;
+    unsigned seq = 0;
     uint32_t order = 0;
     int row = int(E) - 1;
-    double pivot = 1.0;
+    double fit_pivot = 1.0;    // pivot of the sums being reduced
+    double latest_mean = 1.0;  // mean of the latest fitted row: pivot of the row staged next
     RowSums sums;
 #pragma unroll
     for (int k = 0; k < kSlots; ++k) sums.acc[k] = 0.0;
@@ -247,80 +320,108 @@ __global__ void __launch_bounds__(kBackwardThreads, 1) backward_kernel(BackwardA
             spots[at] = sp;
         }
         cta_reduce_to<2>(loc, sm.red, parts + size_t(parity) * a.partial_stride + size_t(blockIdx.x) * 2);
-        if (!grid_barrier(&sm.local_gen, a.status)) return;
-        grid_combine<2>(parts + size_t(parity) * a.partial_stride, gridDim.x, sm.total);
+        publish_partial(a.status);
+        ++seq;
+        if (!stager)
+            combine_published<2>(parts + size_t(parity) * a.partial_stride, seq, a.status, sm.total,
+                                 &sm.wait_failed);
+        __syncthreads();
+        if (sm.wait_failed) return;
         parity ^= 1;
-        if (sm.total[0].hi > 0.0) pivot = dd_round(dd_div(sm.total[1], sm.total[0]));
+        if (sm.total[0].hi > 0.0) fit_pivot = dd_round(dd_div(sm.total[1], sm.total[0]));
+        latest_mean = fit_pivot;
         for (int j = 0; j < ppt; ++j) {
             const int at = j * T + threadIdx.x;
             if (spots[at] > K) {
                 const double x = divide(spots[at], Kd), y = values[at];
                 if (!fo_isfinite(x) || !fo_isfinite(y)) {
-                    sums.acc[14] += 1.0;
+                    sums.acc[kBadSlot] += 1.0;
                     atomicMin(&a.status->fit_nonfinite, ((unsigned long long)order << 32) | (gtid + uint64_t(j) * nthreads));
                 } else {
-                    accumulate_itm(sums, x, y, pivot);
+                    accumulate_itm(sums, x, y, fit_pivot);
                 }
             }
         }
     }
     for (; row >= lowest; --row, ++order) {
         const bool stage_next = row - 1 >= lowest;
-        if (stage_next) {
-            // Prefetch the next row's spots while this row is reduced, synchronised and solved.
+        const double stage_pivot = latest_mean;
+        cta_reduce_to<kSlots>(sums.acc, sm.red, parts + size_t(parity) * a.partial_stride + size_t(blockIdx.x) * kSlots);
+        publish_partial(a.status);
+        ++seq;
+#pragma unroll
+        for (int k = 0; k < kSlots; ++k) sums.acc[k] = 0.0;
+        if (stage_next && stager) {
+            // Load the next row's spots for the positions this thread stages (after the release
+            // above, which would otherwise wait for these loads).
             const double* srow = row_ptr(uint32_t(row - 1));
             for (int j = 0; j < ppt; ++j) {
-                const uint64_t p = gtid + uint64_t(j) * nthreads;
-                if (p < P) cp_async8(&spots_next[j * T + threadIdx.x], &srow[p]);
+                for (int t = stage_tid; t < T; t += stage_threads) {
+                    const uint64_t p = block_first + uint64_t(t) + uint64_t(j) * nthreads;
+                    if (p < P) cp_async8(&spots_next[j * T + t], &srow[p]);
+                }
             }
             cp_async_commit();
         }
-        cta_reduce_to<kSlots>(sums.acc, sm.red, parts + size_t(parity) * a.partial_stride + size_t(blockIdx.x) * kSlots);
-        if (!grid_barrier(&sm.local_gen, a.status)) {
-            cp_async_wait_all();
-            return;
-        }
-        grid_combine<kSlots>(parts + size_t(parity) * a.partial_stride, gridDim.x, sm.total);
-        parity ^= 1;
-        if (threadIdx.x == 0) {
-            const uint64_t itm = uint64_t(sm.total[0].hi);
-            const uint64_t bad = uint64_t(sm.total[14].hi);
-            const uint64_t population = itm + bad;
-            const uint32_t required = uint32_t(degree + 1);
-            int kind;
-            if (population == 0) {
-                kind = plan.support == 1 ? kRuleContinue : kRuleNoSupport;
-            } else if (population < required && plan.support == 1) {
-                kind = kRuleContinue;
-            } else if (population < required || bad > 0) {
-                kind = kRuleFitFailed;  // InsufficientObservations / non-finite population
-            } else {
-                fit_continuation(sm.total, pivot, itm, degree, plan.rank_tolerance, &sm.model);
-                kind = sm.model.status == kFitOk ? kRuleRegression : kRuleFitFailed;
+        if (!stager) {
+            combine_published<kSlots>(parts + size_t(parity) * a.partial_stride, seq, a.status, sm.total,
+                                      &sm.wait_failed);
+            if (threadIdx.x == 0 && !sm.wait_failed) {
+                const uint64_t itm = uint64_t(sm.total[0].hi);
+                const uint64_t bad = uint64_t(sm.total[kBadSlot].hi);
+                const uint64_t population = itm + bad;
+                const uint32_t required = uint32_t(degree + 1);
+                int kind;
+                if (population == 0) {
+                    kind = plan.support == 1 ? kRuleContinue : kRuleNoSupport;
+                } else if (population < required && plan.support == 1) {
+                    kind = kRuleContinue;
+                } else if (population < required || bad > 0) {
+                    kind = kRuleFitFailed;  // InsufficientObservations / non-finite population
+                } else {
+                    fit_continuation(sm.total, fit_pivot, itm, degree, plan.rank_tolerance, &sm.model);
+                    kind = sm.model.status == kFitOk ? kRuleRegression : kRuleFitFailed;
+                }
+                sm.kind = kind;
+                if (blockIdx.x == 0) {
+                    FitRecord& rec = a.records[row];
+                    rec.kind = kind;
+                    rec.itm = population;
+                    rec.pivot = fit_pivot;
+                    rec.model = sm.model;
+                    rec.origin_exercise = 0;
+                    rec.origin_continuation = 0.0;
+                    rec.diag_status = -1;
+                    if (kind == kRuleFitFailed) atomicMin(&a.status->fit_failed_order, order);
+                }
             }
-            sm.kind = kind;
-            if (blockIdx.x == 0) {
-                FitRecord& rec = a.records[row];
-                rec.kind = kind;
-                rec.itm = population;
-                rec.pivot = pivot;
-                rec.model = sm.model;
-                rec.origin_exercise = 0;
-                rec.origin_continuation = 0.0;
-                rec.diag_status = -1;
-                if (kind == kRuleFitFailed) atomicMin(&a.status->fit_failed_order, order);
+        } else if (stage_next) {
+            // Row k-1: in-the-money test and power sums, independent of row k's decision.
+            cp_async_wait_all();
+            for (int j = 0; j < ppt; ++j) {
+                for (int t = stage_tid; t < T; t += stage_threads) {
+                    const uint64_t p = block_first + uint64_t(t) + uint64_t(j) * nthreads;
+                    if (p >= P) continue;
+                    const double sp = spots_next[j * T + t];
+                    if (sp > K) {
+                        const double x = divide(sp, Kd);
+                        if (!fo_isfinite(x)) {
+                            sums.acc[kBadSlot] += 1.0;
+                            atomicMin(&a.status->fit_nonfinite, ((unsigned long long)(order + 1) << 32) | p);
+                        } else {
+                            accumulate_powers(sums, x - stage_pivot);
+                        }
+                    }
+                }
             }
         }
         __syncthreads();
-        cp_async_wait_all();
+        if (sm.wait_failed) return;
         const int kind = sm.kind;
         if (kind == kRuleFitFailed) return;  // identical decision in every CTA
         const bool regression = kind == kRuleRegression;
         const FitModel& model = sm.model;  // read from shared memory
-        if (regression) pivot = model.mean;
         const double disc = stage_next ? plan.disc_from_later[row - 1] : 1.0;
-#pragma unroll
-        for (int k = 0; k < kSlots; ++k) sums.acc[k] = 0.0;
 #pragma unroll 2
         for (int j = 0; j < ppt; ++j) {
             const uint64_t p = gtid + uint64_t(j) * nthreads;
@@ -346,11 +447,15 @@ __global__ void __launch_bounds__(kBackwardThreads, 1) backward_kernel(BackwardA
                     atomicMin(&a.status->fit_payoff_fail, ((unsigned long long)(order + 1) << 32) | p);
                 if (sp > K) {
                     const double x = divide(sp, Kd);
-                    if (!fo_isfinite(x) || !fo_isfinite(v)) {
-                        sums.acc[14] += 1.0;
-                        atomicMin(&a.status->fit_nonfinite, ((unsigned long long)(order + 1) << 32) | p);
-                    } else {
-                        accumulate_itm(sums, x, v, pivot);
+                    if (fo_isfinite(x)) {  // a non-finite x was counted by the staging warps
+                        if (!fo_isfinite(v)) {
+                            // excluded from the regression: move the path from the count to the bad slot
+                            sums.acc[0] -= 1.0;
+                            sums.acc[kBadSlot] += 1.0;
+                            atomicMin(&a.status->fit_nonfinite, ((unsigned long long)(order + 1) << 32) | p);
+                        } else {
+                            accumulate_responses(sums, x - stage_pivot, v);
+                        }
                     }
                 }
             }
@@ -359,6 +464,8 @@ __global__ void __launch_bounds__(kBackwardThreads, 1) backward_kernel(BackwardA
         double* swap = spots;
         spots = spots_next;
         spots_next = swap;
+        fit_pivot = stage_pivot;
+        if (regression) latest_mean = model.mean;
     }
     // Common origin decision (policy.rs:265-281): mean of values discounted to the origin.
     if (plan.origin_row) {
@@ -374,9 +481,12 @@ __global__ void __launch_bounds__(kBackwardThreads, 1) backward_kernel(BackwardA
             }
         }
         cta_reduce_to<2>(acc, sm.red, parts + size_t(parity) * a.partial_stride + size_t(blockIdx.x) * 2);
-        if (!grid_barrier(&sm.local_gen, a.status)) return;
-        grid_combine<2>(parts + size_t(parity) * a.partial_stride, gridDim.x, sm.total);
-        if (blockIdx.x == 0 && threadIdx.x == 0) {
+        publish_partial(a.status);
+        ++seq;
+        if (!stager)
+            combine_published<2>(parts + size_t(parity) * a.partial_stride, seq, a.status, sm.total,
+                                 &sm.wait_failed);
+        if (blockIdx.x == 0 && threadIdx.x == 0 && !sm.wait_failed) {
             const double mean = dd_round(dd_div(sm.total[1], sm.total[0]));
             const double intrinsic = plan.initial_spot - K > 0.0 ? plan.initial_spot - K : 0.0;
             FitRecord& rec = a.records[0];
