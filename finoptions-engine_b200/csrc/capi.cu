@@ -10,6 +10,7 @@
 #include <memory>
 #include <mutex>
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "../../include/finoptions_cuda.h"
@@ -61,7 +62,10 @@ struct fo_lsm_call_plan {
     void* h_out = nullptr;
     DevicePlan dp{};
     bool launched = false;
-    cudaEvent_t marks[8] = {};   // per-kernel timing marks (created on first timed launch)
+    // Per-kernel timing marks (created on first timed launch): [0..4] on the plan's stream around
+    // simulate, backward, evaluate and finalize; [5], [6] around the diagnostic on whichever stream
+    // runs it; [8], [9] bracket a timed series.
+    cudaEvent_t marks[10] = {};
     bool timing = false;
     bool fitted = false;         // a launch has left a fitted policy in the device records
     bool greeks = false;         // evaluation also forms the pathwise adjoint Greeks
@@ -98,6 +102,11 @@ Error open_device(int device, fo_executor* ex) {
     ex->device = device;
     ex->sms = prop.multiProcessorCount;
     FO_CUDA_TRY(cudaStreamCreateWithFlags(&ex->stream, cudaStreamNonBlocking), "cudaStreamCreate");
+    int least = 0, greatest = 0;
+    FO_CUDA_TRY(cudaDeviceGetStreamPriorityRange(&least, &greatest), "cudaDeviceGetStreamPriorityRange");
+    FO_CUDA_TRY(cudaStreamCreateWithPriority(&ex->side, cudaStreamNonBlocking, greatest), "cudaStreamCreate");
+    FO_CUDA_TRY(cudaEventCreateWithFlags(&ex->fork, cudaEventDisableTiming), "cudaEventCreate");
+    FO_CUDA_TRY(cudaEventCreateWithFlags(&ex->join, cudaEventDisableTiming), "cudaEventCreate");
     ex->backward_blocks_max = backward_max_blocks(device);
     ex->backward_max_ppt = backward_max_ppt();
     ex->eval_blocks_per_sm = 8;
@@ -316,9 +325,17 @@ Error plan_launch(fo_lsm_call_plan* plan) {
     b.ppt = plan->ppt;
     FO_CUDA_TRY(launch_backward(b, plan->backward_blocks, plan->ppt, s), "backward launch");
     FO_CUDA_TRY(mark(2), "event");
-    // K3 diagnostics
-    FO_CUDA_TRY(launch_diagnose(plan->dp, records, s), "diagnose launch");
-    FO_CUDA_TRY(mark(3), "event");
+    // K3 diagnostics: nothing on the device reads them, so they run on the side stream next to
+    // the evaluation (inline for a stack executor).
+    cudaStream_t ds = ex->side ? ex->side : s;
+    if (ex->side) {
+        FO_CUDA_TRY(cudaEventRecord(ex->fork, s), "event");
+        FO_CUDA_TRY(cudaStreamWaitEvent(ex->side, ex->fork, 0), "event");
+    }
+    if (plan->timing) FO_CUDA_TRY(cudaEventRecord(plan->marks[5], ds), "event");
+    FO_CUDA_TRY(launch_diagnose(plan->dp, records, ds), "diagnose launch");
+    if (plan->timing) FO_CUDA_TRY(cudaEventRecord(plan->marks[6], ds), "event");
+    if (ex->side) FO_CUDA_TRY(cudaEventRecord(ex->join, ex->side), "event");
     if (plan->run_eval) {
         EvalArgs a{};
         a.plan = plan->dp;
@@ -328,7 +345,7 @@ Error plan_launch(fo_lsm_call_plan* plan) {
         a.itm_counts = reinterpret_cast<unsigned*>(dev + L.itm_counts);
         a.status = status;
         FO_CUDA_TRY(launch_evaluation(plan, a), "evaluation launch");
-        FO_CUDA_TRY(mark(4), "event");
+        FO_CUDA_TRY(mark(3), "event");
         FO_CUDA_TRY(launch_finalize(a.partials, plan->eval_blocks, plan->hp.eval_paths,
                                     reinterpret_cast<double*>(dev + L.result), s),
                     "finalize launch");
@@ -336,8 +353,9 @@ Error plan_launch(fo_lsm_call_plan* plan) {
             FO_CUDA_TRY(launch_finalize_greeks(plan->gk.partials, plan->eval_blocks,
                                                reinterpret_cast<double*>(dev + L.greek_out), s),
                         "Greeks finalize launch");
-        FO_CUDA_TRY(mark(5), "event");
+        FO_CUDA_TRY(mark(4), "event");
     }
+    if (ex->side) FO_CUDA_TRY(cudaStreamWaitEvent(s, ex->join, 0), "event");
     plan->launched = true;
     plan->fitted = true;
     return Error{};
@@ -353,7 +371,12 @@ Error plan_time_launches(fo_lsm_call_plan* plan, uint32_t iterations, double* el
         if (!e) FO_CUDA_TRY(cudaEventCreate(&e), "cudaEventCreate");
     const uint64_t kernels = kernels_per_launch(plan);
     std::vector<double> sums(kernels, 0.0);
-    cudaEvent_t begin = plan->marks[6], end = plan->marks[7];
+    cudaEvent_t begin = plan->marks[8], end = plan->marks[9];
+    // Segments in the order simulate, backward, diagnose, evaluate, finalize. The diagnostic runs
+    // beside the evaluation on the side stream, so the evaluation starts where the backward pass
+    // ends; inline, it starts where the diagnostic ends.
+    const bool side = plan->ex->side != nullptr;
+    const std::pair<int, int> segments[5] = {{0, 1}, {1, 2}, {5, 6}, {side ? 2 : 6, 3}, {3, 4}};
     FO_CUDA_TRY(cudaEventRecord(begin, s), "event");
     double total = 0.0;
     for (uint32_t i = 0; i < iterations; ++i) {
@@ -362,10 +385,12 @@ Error plan_time_launches(fo_lsm_call_plan* plan, uint32_t iterations, double* el
         plan->timing = false;
         if (!e.ok()) return e;
         if (kernel_ms) {
-            FO_CUDA_TRY(cudaEventSynchronize(plan->marks[kernels]), "event");
+            FO_CUDA_TRY(cudaEventSynchronize(plan->marks[plan->run_eval ? 4 : 2]), "event");
+            FO_CUDA_TRY(cudaEventSynchronize(plan->marks[6]), "event");
             for (uint64_t k = 0; k < kernels; ++k) {
                 float ms = 0.f;
-                FO_CUDA_TRY(cudaEventElapsedTime(&ms, plan->marks[k], plan->marks[k + 1]), "event");
+                FO_CUDA_TRY(cudaEventElapsedTime(&ms, plan->marks[segments[k].first], plan->marks[segments[k].second]),
+                            "event");
                 sums[k] += ms;
             }
         }
@@ -733,6 +758,10 @@ void fo_executor_destroy(fo_executor* executor) {
     if (executor->stream) {
         cudaStreamSynchronize(executor->stream);
         cudaStreamDestroy(executor->stream);
+    }
+    if (executor->side) {
+        cudaStreamSynchronize(executor->side);
+        cudaStreamDestroy(executor->side);
     }
     delete executor;
 }

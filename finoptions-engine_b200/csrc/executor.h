@@ -75,6 +75,11 @@ struct fo_executor {
     int backward_max_ppt = 0;
     int eval_blocks_per_sm = 0;
     cudaStream_t stream = nullptr;
+    // Higher-priority side stream for work no later kernel reads on the device (the per-row
+    // diagnostic), forked after the backward pass and joined before results are read back; null
+    // for stack executors, which run it inline.
+    cudaStream_t side = nullptr;
+    cudaEvent_t fork = nullptr, join = nullptr;
     std::mutex mu;
     fo::DeviceBuffer slab;        // training path storage shared by this executor's plans (stream-ordered)
     fo::DeviceBuffer scratch;     // per-call block for one-shot calls
@@ -88,5 +93,7 @@ struct fo_executor {
     ~fo_executor() {
         for (cudaEvent_t& e : batch_marks)
             if (e) cudaEventDestroy(e);
+        if (fork) cudaEventDestroy(fork);
+        if (join) cudaEventDestroy(join);
     }
 };

@@ -528,7 +528,7 @@ struct EvalRow {
     double discount;
 };
 
-__global__ void __launch_bounds__(kEvalThreads, 3) evaluate_kernel(EvalArgs a) {
+__global__ void __launch_bounds__(kEvalThreads, 4) evaluate_kernel(EvalArgs a) {
     extern __shared__ unsigned char eval_smem_raw[];
     const DevicePlan& plan = a.plan;
     const uint32_t rows = plan.rows;
