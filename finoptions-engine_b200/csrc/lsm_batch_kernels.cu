@@ -31,7 +31,7 @@ __device__ __forceinline__ bool sim_failed(const unsigned long long* word) {
 // Training simulation of every group of the wave.
 // ---------------------------------------------------------------------------------------------
 
-__global__ void __launch_bounds__(kBatchSimThreads) batch_simulate_kernel(BatchArgs a) {
+__global__ void __launch_bounds__(kBatchSimThreads, 6) batch_simulate_kernel(BatchArgs a) {
     __shared__ double sx[257], sf[257];
     load_zig_tables(sx, sf);
     const SmemZig zig = make_zig(sx, sf);
@@ -309,7 +309,7 @@ __global__ void batch_diagnose_kernel(BatchArgs a, uint32_t n_records) {
 // copied into shared memory ([strike][row]) before the paths run; otherwise each lookup reads the
 // FitRecord from HBM / L2.
 template <int S, bool kStaged>
-__global__ void __launch_bounds__(kBatchEvalThreads, 2) batch_evaluate_kernel(BatchArgs a, uint32_t rule_rows) {
+__global__ void __launch_bounds__(kBatchEvalThreads, 3) batch_evaluate_kernel(BatchArgs a, uint32_t rule_rows) {
     __shared__ double sx[257], sf[257];
     __shared__ double red[32 * 2 * S];
     __shared__ dd tot[2 * S];
