@@ -64,11 +64,14 @@ struct BatchBackwardSmem {
     int kind;
 };
 
-// Paths a thread loads together before computing on them: the loads of one batch are independent
-// of each other and of the previous batch's stores, so several memory round trips overlap.
-constexpr int kBackwardBatch = 4;
-
-__global__ void __launch_bounds__(kBatchBackwardThreads, 2) batch_backward_kernel(BatchArgs a) {
+// kLoads: paths a thread loads together before computing on them (the loads of one batch are
+// independent of each other and of the previous batch's stores, so several memory round trips
+// overlap). kMinBlocks: resident CTAs per SM the register budget is cut for. Problems of up to
+// 64Ki paths run two loads at three CTAs per SM; larger ones, whose single CTA is a long tail,
+// four loads at two CTAs per SM.
+template <int kLoads, int kMinBlocks>
+__global__ void __launch_bounds__(kBatchBackwardThreads, kMinBlocks) batch_backward_kernel(BatchArgs a) {
+    constexpr int kBackwardBatch = kLoads;
     __shared__ BatchBackwardSmem sm;
     const BatchProblem pr = a.problems[blockIdx.x];
     if (pr.skip_fit) return;
@@ -695,7 +698,11 @@ cudaError_t launch_batch_simulate(const BatchArgs& a, cudaStream_t stream) {
 }
 
 cudaError_t launch_batch_backward(const BatchArgs& a, cudaStream_t stream) {
-    batch_backward_kernel<<<a.n_problems, kBatchBackwardThreads, 0, stream>>>(a);
+    const uint64_t max_paths = uint64_t(a.train_blocks) * kBatchSimThreads;
+    if (max_paths <= 65536)
+        batch_backward_kernel<2, 3><<<a.n_problems, kBatchBackwardThreads, 0, stream>>>(a);
+    else
+        batch_backward_kernel<4, 2><<<a.n_problems, kBatchBackwardThreads, 0, stream>>>(a);
     return cudaGetLastError();
 }
 
