@@ -97,6 +97,7 @@ constexpr size_t kEvalRuleSmemBytes = 96 * 1024;
 struct BatchArgs {
     const BatchGroup* groups;
     const BatchProblem* problems;
+    const uint32_t* backward_order;  // [problems]: problem of backward CTA i, largest work first
     uint32_t n_groups;
     uint32_t n_problems;
     double* slab;

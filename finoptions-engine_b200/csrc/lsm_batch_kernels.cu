@@ -73,12 +73,14 @@ template <int kLoads, int kMinBlocks>
 __global__ void __launch_bounds__(kBatchBackwardThreads, kMinBlocks) batch_backward_kernel(BatchArgs a) {
     constexpr int kBackwardBatch = kLoads;
     __shared__ BatchBackwardSmem sm;
-    const BatchProblem pr = a.problems[blockIdx.x];
+    // Problems are dispatched largest first (paths x rows), so the longest ones do not start last.
+    const uint32_t pi = a.backward_order[blockIdx.x];
+    const BatchProblem pr = a.problems[pi];
     if (pr.skip_fit) return;
     if (sim_failed(&a.group_status[pr.group].train_sim_fail)) return;
     const BatchGroup& g = a.groups[pr.group];
     const DevicePlan plan = g.plan;
-    ProblemStatus* st = a.problem_status + blockIdx.x;
+    ProblemStatus* st = a.problem_status + pi;
     FitRecord* records = a.records + pr.records;
     double* __restrict__ values = a.values + pr.values;
     const double* __restrict__ slab = a.slab + g.slab_offset;

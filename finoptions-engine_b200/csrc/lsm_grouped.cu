@@ -11,6 +11,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <utility>
 #include <cmath>
 #include <cstring>
 #include <string>
@@ -791,7 +792,7 @@ Error build_group(const BatchMethod& m, const GroupSpec& gs, GroupWork* w) {
 // ---- device layout of one wave ------------------------------------------------------------------
 
 struct WaveLayout {
-    size_t groups, problems, group_status, problem_status, summaries;  // read-back region: group_status..summaries
+    size_t groups, problems, order, group_status, problem_status, summaries;  // read-back region: group_status..summaries
     size_t greek_sums;                                                  // (read back, Greeks only)
     size_t counts, itm_counts, stop_counts, eval_partials, greek_partials, records, values, slab, replay;
     size_t out_begin, out_bytes, clear_begin, clear_bytes, total;
@@ -825,6 +826,7 @@ WaveLayout layout_for(const Wave& w, size_t base) {
     const uint64_t G = w.g1 - w.g0, P = w.problems;
     L.groups = take(sizeof(BatchGroup) * G);
     L.problems = take(sizeof(BatchProblem) * P);
+    L.order = take(sizeof(uint32_t) * P);
     off = align_up(off, 256);
     L.out_begin = off;
     L.group_status = take(sizeof(GroupStatus) * G);
@@ -1171,7 +1173,7 @@ Error price_groups(fo_executor* ex, const BatchMethod& m, const std::vector<Grou
                                 strikes_g * (rows * (sizeof(FitRecord) + 2 * sizeof(unsigned)) +
                                              size_t(eval_blocks) * sizeof(double2) * (2 + (greeks ? kGreekSlots : 0)) +
                                              sizeof(BatchProblem) + sizeof(ProblemStatus) + sizeof(ProblemSummary) +
-                                             sizeof(double) * kGreekSlots + 8) +
+                                             sizeof(double) * kGreekSlots + sizeof(uint32_t) + 8) +
                                 sizeof(BatchGroup) + sizeof(GroupStatus) + 1024;
             if (cur.g1 > cur.g0 && (bytes + cost > budget || cur.g1 - cur.g0 >= 65535)) {
                 waves.push_back(cur);
@@ -1267,6 +1269,19 @@ Error price_groups(fo_executor* ex, const BatchMethod& m, const std::vector<Grou
             slab += uint64_t(hp.rows() - (hp.origin_row ? 1 : 0)) * hp.train_paths;
             max_rows = std::max<uint32_t>(max_rows, hp.rows());
         }
+        // Backward dispatch order: largest training work (paths x rows) first, ties in problem order.
+        {
+            auto* order = reinterpret_cast<uint32_t*>(host + (L.order - in_bytes));
+            std::vector<std::pair<uint64_t, uint32_t>> work_of;
+            work_of.reserve(w.problems);
+            for (uint64_t i = 0; i < w.problems; ++i) {
+                const HostPlan& hp = work[w.g0 + hpb[i].group].hp;
+                work_of.emplace_back(uint64_t(hp.train_paths) * hp.rows(), uint32_t(i));
+            }
+            std::stable_sort(work_of.begin(), work_of.end(),
+                             [](const auto& x, const auto& y) { return x.first > y.first; });
+            for (uint64_t i = 0; i < w.problems; ++i) order[i] = work_of[i].second;
+        }
         FO_CUDA_TRY(cudaMemcpyAsync(dev + L.groups, host + (L.groups - in_bytes), L.out_begin - L.groups,
                                     cudaMemcpyHostToDevice, s),
                     "batch table upload");
@@ -1276,6 +1291,7 @@ Error price_groups(fo_executor* ex, const BatchMethod& m, const std::vector<Grou
         BatchArgs a{};
         a.groups = reinterpret_cast<const BatchGroup*>(dev + L.groups);
         a.problems = reinterpret_cast<const BatchProblem*>(dev + L.problems);
+        a.backward_order = reinterpret_cast<const uint32_t*>(dev + L.order);
         a.n_groups = uint32_t(w.g1 - w.g0);
         a.n_problems = uint32_t(w.problems);
         a.slab = reinterpret_cast<double*>(dev + L.slab);
