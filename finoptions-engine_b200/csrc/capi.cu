@@ -288,7 +288,10 @@ Error plan_create(fo_executor* ex, const fo_lsm_call_request& q, bool own_memory
     // upload inputs once
     pack_inputs(hp, L, static_cast<unsigned char*>(plan->h_out));
     FO_CUDA_TRY(cudaMemcpyAsync(dev, plan->h_out, L.inputs_bytes, cudaMemcpyHostToDevice, ex->stream), "plan upload");
-    FO_CUDA_TRY(cudaStreamSynchronize(ex->stream), "plan upload");
+    // A plan of its own may be packed again (revaluation) while this copy is pending, so it waits
+    // here. A one-shot plan borrows the executor's staging, which nothing rewrites before the
+    // call's read-back has synchronised the stream: its kernels simply queue behind the copy.
+    if (own_memory) FO_CUDA_TRY(cudaStreamSynchronize(ex->stream), "plan upload");
     *out = plan.release();
     return Error{};
 }
@@ -853,6 +856,7 @@ int fo_price_lsm_call_f64(fo_executor* executor, const fo_lsm_call_request* requ
     std::unique_ptr<fo_lsm_call_plan> plan(raw);
     e = plan_launch(plan.get());
     if (e.ok()) e = plan_collect(plan.get(), result);
+    else cudaStreamSynchronize(executor->stream);  // the input upload may still read the staging
     return finish(err, e);
 }
 
@@ -872,6 +876,7 @@ int fo_price_lsm_call_greeks_f64(fo_executor* executor, const fo_lsm_call_reques
     e = enable_greeks(plan.get(), true);
     if (e.ok()) e = plan_launch(plan.get());
     if (e.ok()) e = plan_collect(plan.get(), result);
+    else cudaStreamSynchronize(executor->stream);  // the input upload may still read the staging
     if (e.ok()) e = plan_greeks(plan.get(), greeks);
     return finish(err, e);
 }
