@@ -13,6 +13,7 @@
 //                           policies of up to kEvalStrikes strikes on the fly (policy.rs:642-834).
 //   batch_summarize_kernel  per problem: price / SE from the evaluation partials, the row-result
 //                           columns (pricing.rs:1130-1230) and the first failing backward row.
+#include <cooperative_groups.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -60,21 +61,43 @@ __global__ void __launch_bounds__(kBatchSimThreads, 6) batch_simulate_kernel(Bat
 struct BatchBackwardSmem {
     double red[32 * kSlots];
     dd total[kSlots];
+    dd exchange[kSlots];  // this CTA's totals, read by the other CTAs of its cluster
     FitModel model;
     int kind;
 };
 
+// Sums slots 0..S-1 of the CTA totals over the CTAs of the cluster in rank order (double-double),
+// leaving the same cluster totals in every CTA. Called by every thread after cta_reduce_dd.
+template <int S, int C>
+__device__ __forceinline__ void cluster_combine(BatchBackwardSmem& sm) {
+    namespace cg = cooperative_groups;
+    cg::cluster_group cluster = cg::this_cluster();
+    if (threadIdx.x < S) sm.exchange[threadIdx.x] = sm.total[threadIdx.x];
+    cluster.sync();
+    if (threadIdx.x < S) {
+        dd acc = cluster.map_shared_rank(&sm, 0)->exchange[threadIdx.x];
+#pragma unroll
+        for (int r = 1; r < C; ++r) acc = dd_add(acc, cluster.map_shared_rank(&sm, r)->exchange[threadIdx.x]);
+        sm.total[threadIdx.x] = acc;
+    }
+    cluster.sync();  // remote reads done before any CTA writes its exchange slots again
+}
+
 // kLoads: paths a thread loads together before computing on them (the loads of one batch are
 // independent of each other and of the previous batch's stores, so several memory round trips
-// overlap). kMinBlocks: resident CTAs per SM the register budget is cut for. Problems of up to
-// 64Ki paths run two loads at three CTAs per SM; larger ones, whose single CTA is a long tail,
-// four loads at two CTAs per SM.
-template <int kLoads, int kMinBlocks>
+// overlap). kMinBlocks: resident CTAs per SM the register budget is cut for. kCluster: CTAs that
+// share one problem (a thread-block cluster): CTA rank c takes the path blocks c, c + kCluster, ...
+// of kLoads x blockDim paths, and the row sums are combined across the cluster through
+// distributed shared memory. Problems of up to 64Ki paths run alone in a CTA with two loads at three
+// CTAs per SM; larger ones, whose single CTA would be a long tail, in clusters of four with four
+// loads at two CTAs per SM.
+template <int kLoads, int kMinBlocks, int kCluster>
 __global__ void __launch_bounds__(kBatchBackwardThreads, kMinBlocks) batch_backward_kernel(BatchArgs a) {
     constexpr int kBackwardBatch = kLoads;
     __shared__ BatchBackwardSmem sm;
+    const unsigned rank = kCluster > 1 ? cooperative_groups::this_cluster().block_rank() : 0u;
     // Problems are dispatched largest first (paths x rows), so the longest ones do not start last.
-    const uint32_t pi = a.backward_order[blockIdx.x];
+    const uint32_t pi = a.backward_order[blockIdx.x / kCluster];
     const BatchProblem pr = a.problems[pi];
     if (pr.skip_fit) return;
     if (sim_failed(&a.group_status[pr.group].train_sim_fail)) return;
@@ -87,6 +110,8 @@ __global__ void __launch_bounds__(kBatchBackwardThreads, kMinBlocks) batch_backw
     const uint64_t P = plan.train_paths;
     const unsigned T = blockDim.x;
     const uint64_t stride = uint64_t(T) * kBackwardBatch;
+    const uint64_t first = uint64_t(rank) * stride + threadIdx.x;  // this thread's first path block
+    const uint64_t step = stride * kCluster;
     const double K = pr.strike;
     const Divisor Kd = make_divisor(K);
     const int degree = a.degree;
@@ -96,7 +121,7 @@ __global__ void __launch_bounds__(kBatchBackwardThreads, kMinBlocks) batch_backw
     auto row_ptr = [&](uint32_t row) { return slab + uint64_t(row - fsr) * P; };
     {
         const double* __restrict__ terminal = row_ptr(E);
-        for (uint64_t base = threadIdx.x; base < P; base += stride) {
+        for (uint64_t base = first; base < P; base += step) {
             double s[kBackwardBatch];
 #pragma unroll
             for (int u = 0; u < kBackwardBatch; ++u) {
@@ -122,7 +147,7 @@ __global__ void __launch_bounds__(kBatchBackwardThreads, kMinBlocks) batch_backw
         const double disc = plan.disc_from_later[row];
         const double* __restrict__ srow = row_ptr(uint32_t(row));
         double loc[2] = {0.0, 0.0};
-        for (uint64_t base = threadIdx.x; base < P; base += stride) {
+        for (uint64_t base = first; base < P; base += step) {
             double v[kBackwardBatch], s[kBackwardBatch];
 #pragma unroll
             for (int u = 0; u < kBackwardBatch; ++u) {
@@ -147,8 +172,9 @@ __global__ void __launch_bounds__(kBatchBackwardThreads, kMinBlocks) batch_backw
             }
         }
         cta_reduce_dd<2>(loc, sm.red, sm.total);
+        if constexpr (kCluster > 1) cluster_combine<2, kCluster>(sm);
         if (sm.total[0].hi > 0.0) pivot = dd_round(dd_div(sm.total[1], sm.total[0]));
-        for (uint64_t base = threadIdx.x; base < P; base += stride) {
+        for (uint64_t base = first; base < P; base += step) {
             double v[kBackwardBatch], s[kBackwardBatch];
 #pragma unroll
             for (int u = 0; u < kBackwardBatch; ++u) {
@@ -172,6 +198,7 @@ __global__ void __launch_bounds__(kBatchBackwardThreads, kMinBlocks) batch_backw
     }
     for (; row >= lowest; --row, ++order) {
         cta_reduce_dd<kSlots>(sums.acc, sm.red, sm.total);
+        if constexpr (kCluster > 1) cluster_combine<kSlots, kCluster>(sm);
         if (threadIdx.x == 0) {
             const uint64_t itm = uint64_t(sm.total[0].hi);
             const uint64_t bad = uint64_t(sm.total[kBadSlot].hi);
@@ -189,14 +216,16 @@ __global__ void __launch_bounds__(kBatchBackwardThreads, kMinBlocks) batch_backw
                 kind = sm.model.status == kFitOk ? kRuleRegression : kRuleFitFailed;
             }
             sm.kind = kind;
-            FitRecord& rec = records[row];
-            rec.kind = kind;
-            rec.itm = population;
-            rec.pivot = pivot;
-            rec.model = sm.model;
-            rec.origin_exercise = 0;
-            rec.origin_continuation = 0.0;
-            rec.diag_status = -1;
+            if (rank == 0) {  // every CTA of a cluster fits the same model; one writes the record
+                FitRecord& rec = records[row];
+                rec.kind = kind;
+                rec.itm = population;
+                rec.pivot = pivot;
+                rec.model = sm.model;
+                rec.origin_exercise = 0;
+                rec.origin_continuation = 0.0;
+                rec.diag_status = -1;
+            }
         }
         __syncthreads();
         const int kind = sm.kind;
@@ -209,7 +238,7 @@ __global__ void __launch_bounds__(kBatchBackwardThreads, kMinBlocks) batch_backw
         const double* __restrict__ nxt = stage_next ? row_ptr(uint32_t(row - 1)) : cur;
 #pragma unroll
         for (int k = 0; k < kSlots; ++k) sums.acc[k] = 0.0;
-        for (uint64_t base = threadIdx.x; base < P; base += stride) {
+        for (uint64_t base = first; base < P; base += step) {
             double v[kBackwardBatch], sc[kBackwardBatch], sn[kBackwardBatch];
 #pragma unroll
             for (int u = 0; u < kBackwardBatch; ++u) {
@@ -257,7 +286,7 @@ __global__ void __launch_bounds__(kBatchBackwardThreads, kMinBlocks) batch_backw
     // Common origin decision (policy.rs:265-281): mean of the values discounted to the origin.
     if (plan.origin_row) {
         double acc[2] = {0.0, 0.0};
-        for (uint64_t base = threadIdx.x; base < P; base += stride) {
+        for (uint64_t base = first; base < P; base += step) {
             double v[kBackwardBatch];
 #pragma unroll
             for (int u = 0; u < kBackwardBatch; ++u) {
@@ -275,7 +304,8 @@ __global__ void __launch_bounds__(kBatchBackwardThreads, kMinBlocks) batch_backw
             }
         }
         cta_reduce_dd<2>(acc, sm.red, sm.total);
-        if (threadIdx.x == 0) {
+        if constexpr (kCluster > 1) cluster_combine<2, kCluster>(sm);
+        if (threadIdx.x == 0 && rank == 0) {
             const double mean = dd_round(dd_div(sm.total[1], sm.total[0]));
             const double intrinsic = plan.initial_spot - K > 0.0 ? plan.initial_spot - K : 0.0;
             FitRecord& rec = records[0];
@@ -699,13 +729,46 @@ cudaError_t launch_batch_simulate(const BatchArgs& a, cudaStream_t stream) {
     return cudaGetLastError();
 }
 
-cudaError_t launch_batch_backward(const BatchArgs& a, cudaStream_t stream) {
-    const uint64_t max_paths = uint64_t(a.train_blocks) * kBatchSimThreads;
-    if (max_paths <= 65536)
-        batch_backward_kernel<2, 3><<<a.n_problems, kBatchBackwardThreads, 0, stream>>>(a);
-    else
-        batch_backward_kernel<4, 2><<<a.n_problems, kBatchBackwardThreads, 0, stream>>>(a);
-    return cudaGetLastError();
+cudaError_t launch_batch_backward(const BatchArgs& a, uint32_t n_large, cudaStream_t stream, cudaStream_t side,
+                                  cudaEvent_t fork, cudaEvent_t join) {
+    // backward_order lists the problems above 64Ki paths first (clusters of four CTAs), then the
+    // rest (one CTA each); the two launches run side by side when a second stream is given.
+    constexpr int kCluster = 4;
+    const uint32_t n_small = a.n_problems - n_large;
+    cudaStream_t small_stream = side ? side : stream;
+    if (n_small > 0 && side) {
+        cudaError_t e = cudaEventRecord(fork, stream);
+        if (e == cudaSuccess) e = cudaStreamWaitEvent(side, fork, 0);
+        if (e != cudaSuccess) return e;
+    }
+    if (n_large > 0) {
+        cudaLaunchConfig_t cfg{};
+        cfg.gridDim = dim3(n_large * kCluster);
+        cfg.blockDim = dim3(kBatchBackwardThreads);
+        cfg.stream = stream;
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeClusterDimension;
+        attr[0].val.clusterDim.x = kCluster;
+        attr[0].val.clusterDim.y = 1;
+        attr[0].val.clusterDim.z = 1;
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+        cudaError_t e = cudaLaunchKernelEx(&cfg, batch_backward_kernel<4, 2, kCluster>, a);
+        if (e != cudaSuccess) return e;
+    }
+    if (n_small > 0) {
+        BatchArgs s = a;
+        s.backward_order = a.backward_order + n_large;
+        batch_backward_kernel<2, 3, 1><<<n_small, kBatchBackwardThreads, 0, small_stream>>>(s);
+        cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+        if (side) {
+            e = cudaEventRecord(join, side);
+            if (e == cudaSuccess) e = cudaStreamWaitEvent(stream, join, 0);
+            if (e != cudaSuccess) return e;
+        }
+    }
+    return cudaSuccess;
 }
 
 cudaError_t launch_batch_diagnose(const BatchArgs& a, uint32_t n_records, cudaStream_t stream) {

@@ -12,7 +12,10 @@ constexpr int kBatchBackwardThreads = 256;
 constexpr int kBatchEvalThreads = 256;
 
 cudaError_t launch_batch_simulate(const BatchArgs& a, cudaStream_t stream);
-cudaError_t launch_batch_backward(const BatchArgs& a, cudaStream_t stream);
+// backward_order holds the n_large problems above 64Ki paths first (clusters of four CTAs on
+// `stream`), then the rest (one CTA each, on `side` between fork and join when side is not null).
+cudaError_t launch_batch_backward(const BatchArgs& a, uint32_t n_large, cudaStream_t stream, cudaStream_t side,
+                                  cudaEvent_t fork, cudaEvent_t join);
 cudaError_t launch_batch_diagnose(const BatchArgs& a, uint32_t n_records, cudaStream_t stream);
 // max_strikes: strikes of the widest group; max_rows: the largest observation-row count of the
 // wave's groups (sizes the staged rules).

@@ -1269,17 +1269,26 @@ Error price_groups(fo_executor* ex, const BatchMethod& m, const std::vector<Grou
             slab += uint64_t(hp.rows() - (hp.origin_row ? 1 : 0)) * hp.train_paths;
             max_rows = std::max<uint32_t>(max_rows, hp.rows());
         }
-        // Backward dispatch order: largest training work (paths x rows) first, ties in problem order.
+        // Backward dispatch order: the problems above 64Ki training paths (run by clusters of CTAs)
+        // first, then the rest; within each, largest training work (paths x rows) first, ties in
+        // problem order.
+        uint32_t n_large = 0;
         {
             auto* order = reinterpret_cast<uint32_t*>(host + (L.order - in_bytes));
             std::vector<std::pair<uint64_t, uint32_t>> work_of;
             work_of.reserve(w.problems);
             for (uint64_t i = 0; i < w.problems; ++i) {
                 const HostPlan& hp = work[w.g0 + hpb[i].group].hp;
+                const bool large = hp.train_paths > 65536;
+                n_large += large ? 1u : 0u;
                 work_of.emplace_back(uint64_t(hp.train_paths) * hp.rows(), uint32_t(i));
             }
-            std::stable_sort(work_of.begin(), work_of.end(),
-                             [](const auto& x, const auto& y) { return x.first > y.first; });
+            std::stable_sort(work_of.begin(), work_of.end(), [&](const auto& x, const auto& y) {
+                const bool lx = work[w.g0 + hpb[x.second].group].hp.train_paths > 65536;
+                const bool ly = work[w.g0 + hpb[y.second].group].hp.train_paths > 65536;
+                if (lx != ly) return lx;
+                return x.first > y.first;
+            });
             for (uint64_t i = 0; i < w.problems; ++i) order[i] = work_of[i].second;
         }
         FO_CUDA_TRY(cudaMemcpyAsync(dev + L.groups, host + (L.groups - in_bytes), L.out_begin - L.groups,
@@ -1317,7 +1326,7 @@ Error price_groups(fo_executor* ex, const BatchMethod& m, const std::vector<Grou
         FO_CUDA_TRY(cudaEventRecord(mark[0], s), "event");
         FO_CUDA_TRY(launch_batch_simulate(a, s), "batch training simulation launch");
         FO_CUDA_TRY(cudaEventRecord(mark[1], s), "event");
-        FO_CUDA_TRY(launch_batch_backward(a, s), "batch backward launch");
+        FO_CUDA_TRY(launch_batch_backward(a, n_large, s, ex->side, ex->fork, ex->join), "batch backward launch");
         FO_CUDA_TRY(cudaEventRecord(mark[2], s), "event");
         FO_CUDA_TRY(launch_batch_diagnose(a, uint32_t(w.records), s), "batch diagnose launch");
         FO_CUDA_TRY(cudaEventRecord(mark[3], s), "event");

@@ -43,6 +43,23 @@ def test_ragged_rows_match_single_contract_oracle_prices(native_executor) -> Non
         assert out[5][r] == sum(1 for d in diags if d[1] == "regression"), r
 
 
+def test_rows_above_64ki_paths_match_the_oracle(native_executor) -> None:
+    """Rows above 65,536 training paths are fitted by a cluster of four CTAs (the rest by one CTA
+    each, in a concurrent launch); both kinds of row must still price like the single contract."""
+    c = ragged_columns(6, seed=67, min_paths=40000, max_paths=140000, min_exercise=4, max_exercise=8)
+    assert (c.paths > 65536).any() and (c.paths <= 65536).any()
+    status, err, out = gpu_ragged(native_executor, ragged_request(c))
+    assert status == 0, err.message
+    for r in range(c.rows):
+        want = _oracle.price_lsm_call(lsm_call_request(**ragged_row_as_call(c, r)), 8)
+        price, _, sd, se, _, counts, diags = want
+        assert out[0][r] == pytest.approx(price, rel=RTOL, abs=1e-13), r
+        assert out[1][r] == pytest.approx(sd, rel=RTOL, abs=1e-13), r
+        assert out[2][r] == pytest.approx(se, rel=RTOL, abs=1e-13), r
+        assert out[10][r] == sum(counts[:-1]) and out[11][r] == counts[-1], r
+        assert out[5][r] == sum(1 for d in diags if d[1] == "regression"), r
+
+
 def _row(c, r: int):
     one = ragged_columns(1, seed=1, min_paths=2, max_paths=3, min_exercise=4, max_exercise=4)
     for name in ("initial_spots", "strikes", "maturities", "rates", "volatilities", "dividend_yields", "paths"):
