@@ -439,7 +439,7 @@ enum FitStatus : int {
     kFitNonFinite = 3,
 };
 
-struct FitModel {
+struct alignas(16) FitModel {  // 16-byte aligned: pairs of fields load together
     double mean, scale;
     double inv_scale;  // 1 / scale for the prediction's corrected division (see Divisor)
     double alpha[kMaxDegree];

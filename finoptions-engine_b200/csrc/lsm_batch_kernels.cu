@@ -472,7 +472,7 @@ __global__ void __launch_bounds__(kBatchEvalThreads, 3) batch_evaluate_greeks_ke
     __shared__ double gred[32 * kGreekSlots];
     __shared__ dd gtot[kGreekSlots];
     __shared__ unsigned cnt[2];
-    extern __shared__ unsigned char batch_greeks_smem[];  // PolicyRule[rule_rows], unsigned stops[rule_rows]
+    extern __shared__ __align__(16) unsigned char batch_greeks_smem[];  // PolicyRule[rule_rows], unsigned stops[rule_rows]
     const BatchGroup& g = a.groups[blockIdx.y];
     const uint32_t k = blockIdx.z;
     if (k >= g.problems) return;                                          // uniform over the block

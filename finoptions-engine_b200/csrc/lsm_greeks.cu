@@ -35,7 +35,7 @@ struct GreeksEvalRow {
 };
 
 __global__ void __launch_bounds__(kEvalThreads, 3) evaluate_greeks_kernel(EvalArgs a, GreeksArgs gk) {
-    extern __shared__ unsigned char greeks_smem_raw[];
+    extern __shared__ __align__(16) unsigned char greeks_smem_raw[];
     __shared__ double gred[32 * kGreekSlots];
     __shared__ dd gtot[kGreekSlots];
     const DevicePlan& plan = a.plan;

@@ -529,7 +529,7 @@ struct EvalRow {
 };
 
 __global__ void __launch_bounds__(kEvalThreads, 4) evaluate_kernel(EvalArgs a) {
-    extern __shared__ unsigned char eval_smem_raw[];
+    extern __shared__ __align__(16) unsigned char eval_smem_raw[];
     const DevicePlan& plan = a.plan;
     const uint32_t rows = plan.rows;
     double* sx = reinterpret_cast<double*>(eval_smem_raw);
