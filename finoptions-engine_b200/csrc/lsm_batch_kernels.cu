@@ -416,7 +416,8 @@ __global__ void __launch_bounds__(kBatchEvalThreads, 3) batch_evaluate_kernel(Ba
             active = 0u;
             return;
         }
-#pragma unroll
+        // Two strikes per iteration: the fully unrolled eight-strike body stalled on instruction fetch.
+#pragma unroll 2
         for (int k = 0; k < S; ++k) {
             if (!((active >> k) & 1u)) continue;
             const double K = strikes[k];
