@@ -453,7 +453,7 @@ Error plan_collect(fo_lsm_call_plan* plan, fo_lsm_call_result* result) {
     const uint32_t E = rows - 1;
     if (status->barrier_timeout)
         return make_error(FO_ERR_EXECUTION, FO_CODE_BARRIER_TIMEOUT,
-                          "backward-induction grid barrier timed out; the device result was discarded");
+                          "backward-induction grid synchronisation timed out; the device result was discarded");
     if (status->train_sim_fail != kNone) return simulation_error(plan, true, status->train_sim_fail);
     // Fit failures in backward order: discount, population, regression, diagnostic, update.
     const uint32_t lowest = hp.origin_row ? 1u : 0u;
