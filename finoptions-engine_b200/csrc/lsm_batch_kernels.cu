@@ -466,7 +466,7 @@ __global__ void __launch_bounds__(kBatchEvalThreads, 3) batch_evaluate_kernel(Ba
 // Fused evaluation with pathwise adjoint Greeks: one strike per block (grid z = strike in group).
 // ---------------------------------------------------------------------------------------------
 
-__global__ void __launch_bounds__(kBatchEvalThreads, 3) batch_evaluate_greeks_kernel(BatchArgs a, uint32_t rule_rows) {
+__global__ void __launch_bounds__(kBatchEvalThreads, 4) batch_evaluate_greeks_kernel(BatchArgs a, uint32_t rule_rows) {
     __shared__ double sx[257], sf[257];
     __shared__ double red[32 * 2];
     __shared__ dd tot[2];

@@ -34,7 +34,7 @@ struct GreeksEvalRow {
     double discount;
 };
 
-__global__ void __launch_bounds__(kEvalThreads, 3) evaluate_greeks_kernel(EvalArgs a, GreeksArgs gk) {
+__global__ void __launch_bounds__(kEvalThreads, 4) evaluate_greeks_kernel(EvalArgs a, GreeksArgs gk) {
     extern __shared__ __align__(16) unsigned char greeks_smem_raw[];
     __shared__ double gred[32 * kGreekSlots];
     __shared__ dd gtot[kGreekSlots];
