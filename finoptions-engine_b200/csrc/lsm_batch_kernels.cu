@@ -344,7 +344,7 @@ __global__ void batch_diagnose_kernel(BatchArgs a, uint32_t n_records) {
 // copied into shared memory ([strike][row]) before the paths run; otherwise each lookup reads the
 // FitRecord from HBM / L2.
 template <int S, bool kStaged>
-__global__ void __launch_bounds__(kBatchEvalThreads, 3) batch_evaluate_kernel(BatchArgs a, uint32_t rule_rows) {
+__global__ void __launch_bounds__(kBatchEvalThreads, S <= 1 ? 4 : 3) batch_evaluate_kernel(BatchArgs a, uint32_t rule_rows) {
     __shared__ double sx[257], sf[257];
     __shared__ double red[32 * 2 * S];
     __shared__ dd tot[2 * S];
