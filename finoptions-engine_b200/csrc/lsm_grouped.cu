@@ -11,6 +11,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <thread>
 #include <utility>
 #include <cmath>
 #include <cstring>
@@ -1108,14 +1109,31 @@ Error price_groups(fo_executor* ex, const BatchMethod& m, const std::vector<Grou
     const bool greeks = sink != nullptr;
     // Per-group plans on the host. Only groups before the first one whose plan fails can matter.
     const uint64_t groups = specs.size();
+    // Groups plan independently (build_group reads only its inputs), so large batches spread them
+    // over host threads; the first failing group in order still bounds what is launched.
     std::vector<GroupWork> work(groups);
+    auto build_range = [&](uint64_t lo, uint64_t hi) {
+        for (uint64_t g = lo; g < hi; ++g) {
+            GroupWork& w = work[g];
+            w.first_row = specs[g].first_row;
+            w.end_row = specs[g].end_row;
+            w.build = build_group(m, specs[g], &w);
+        }
+    };
+    const uint64_t hw = std::max(1u, std::thread::hardware_concurrency());
+    const uint64_t threads = std::min<uint64_t>(std::min<uint64_t>(hw, 32), (groups + 63) / 64);
+    if (threads <= 1) {
+        build_range(0, groups);
+    } else {
+        std::vector<std::thread> pool;
+        pool.reserve(threads);
+        for (uint64_t t = 0; t < threads; ++t)
+            pool.emplace_back(build_range, groups * t / threads, groups * (t + 1) / threads);
+        for (std::thread& th : pool) th.join();
+    }
     uint64_t launchable = groups;
     for (uint64_t g = 0; g < groups; ++g) {
-        GroupWork& w = work[g];
-        w.first_row = specs[g].first_row;
-        w.end_row = specs[g].end_row;
-        w.build = build_group(m, specs[g], &w);
-        if (!w.build.ok()) {
+        if (!work[g].build.ok()) {
             launchable = g;
             break;
         }
