@@ -13,11 +13,11 @@ from . import _abi
 
 
 def _f64(values: Sequence[float] | np.ndarray) -> np.ndarray:
-    return np.ascontiguousarray(np.asarray(values, dtype=np.float64))
+    return np.ascontiguousarray(values, dtype=np.float64)
 
 
 def _u32(values: Sequence[int] | np.ndarray) -> np.ndarray:
-    return np.ascontiguousarray(np.asarray(values, dtype=np.uint32))
+    return np.ascontiguousarray(values, dtype=np.uint32)
 
 
 def _ptr(array: np.ndarray | None, ctype: type) -> Any:

@@ -173,8 +173,28 @@ def _required[T](value: T | None, *, field: str) -> T:
     return value
 
 
+# Regression rows are most of a result; their frozen records are filled through the slot
+# descriptors (the same objects the constructor makes, without its per-field frozen-setattr path).
+_new_record = object.__new__
+(_set_node, _set_itm, _set_observations, _set_columns, _set_rank, _set_condition, _set_mean,
+ _set_scale) = (getattr(RegressionFitDiagnostics, name).__set__ for name in (
+    "node", "in_the_money_paths", "observations", "columns", "rank", "condition_number", "predictor_mean",
+    "predictor_scale"))
+
+
 def _fit_diagnostic(raw: tuple) -> ExerciseFitDiagnostics:
     (node, kind, exercise, continuation, itm, observations, columns, rank, condition, mean, scale) = raw
+    if kind == "regression" and None not in (itm, observations, columns, rank, condition, mean, scale):
+        record = _new_record(RegressionFitDiagnostics)
+        _set_node(record, node)
+        _set_itm(record, itm)
+        _set_observations(record, observations)
+        _set_columns(record, columns)
+        _set_rank(record, rank)
+        _set_condition(record, condition)
+        _set_mean(record, mean)
+        _set_scale(record, scale)
+        return record
     if kind == "origin_decision":
         return OriginDecisionDiagnostics(
             node=node,
