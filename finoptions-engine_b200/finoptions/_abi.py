@@ -45,17 +45,19 @@ class FoError(ctypes.Structure):
 
 
 class FoLsmCallRequest(ctypes.Structure):
+    # The single-contract call is latency-bound on the host: its array fields take plain addresses
+    # (set from integers) into buffers that the request object keeps alive.
     _fields_ = [
         ("initial_spot", ctypes.c_double),
         ("strike", ctypes.c_double),
-        ("schedule_times", c_double_p), ("n_schedule_times", ctypes.c_uint64),
-        ("curve_times", c_double_p), ("n_curve_times", ctypes.c_uint64),
-        ("log_discounts", c_double_p), ("n_log_discounts", ctypes.c_uint64),
-        ("dividend_yield_times", c_double_p), ("n_dividend_yield_times", ctypes.c_uint64),
-        ("cumulative_dividend_yields", c_double_p), ("n_cumulative_dividend_yields", ctypes.c_uint64),
-        ("dividend_nodes", c_uint32_p), ("n_dividend_nodes", ctypes.c_uint64),
-        ("dividend_amounts", c_double_p), ("n_dividend_amounts", ctypes.c_uint64),
-        ("exercise_nodes", c_uint32_p), ("n_exercise_nodes", ctypes.c_uint64),
+        ("schedule_times", ctypes.c_void_p), ("n_schedule_times", ctypes.c_uint64),
+        ("curve_times", ctypes.c_void_p), ("n_curve_times", ctypes.c_uint64),
+        ("log_discounts", ctypes.c_void_p), ("n_log_discounts", ctypes.c_uint64),
+        ("dividend_yield_times", ctypes.c_void_p), ("n_dividend_yield_times", ctypes.c_uint64),
+        ("cumulative_dividend_yields", ctypes.c_void_p), ("n_cumulative_dividend_yields", ctypes.c_uint64),
+        ("dividend_nodes", ctypes.c_void_p), ("n_dividend_nodes", ctypes.c_uint64),
+        ("dividend_amounts", ctypes.c_void_p), ("n_dividend_amounts", ctypes.c_uint64),
+        ("exercise_nodes", ctypes.c_void_p), ("n_exercise_nodes", ctypes.c_uint64),
         ("expiry_node", ctypes.c_uint32),
         ("annualized_volatility", ctypes.c_double),
         ("dividend_policy", ctypes.c_int32),
@@ -90,6 +92,7 @@ class FoLsmNodeDiagnostic(ctypes.Structure):
 
 
 class FoLsmCallResult(ctypes.Structure):
+    # Caller-owned buffers, given by address like the request's arrays.
     _fields_ = [
         ("price", ctypes.c_double),
         ("paths", ctypes.c_uint32),
@@ -97,10 +100,10 @@ class FoLsmCallResult(ctypes.Structure):
         ("sample_standard_deviation", ctypes.c_double),
         ("has_standard_error", ctypes.c_int32),
         ("standard_error", ctypes.c_double),
-        ("observation_nodes", c_uint32_p), ("observation_capacity", ctypes.c_uint64),
-        ("exercise_counts", c_uint32_p),
+        ("observation_nodes", ctypes.c_void_p), ("observation_capacity", ctypes.c_uint64),
+        ("exercise_counts", ctypes.c_void_p),
         ("n_observations", ctypes.c_uint64),
-        ("diagnostics", ctypes.POINTER(FoLsmNodeDiagnostic)), ("diagnostics_capacity", ctypes.c_uint64),
+        ("diagnostics", ctypes.c_void_p), ("diagnostics_capacity", ctypes.c_uint64),
         ("n_diagnostics", ctypes.c_uint64),
     ]
 

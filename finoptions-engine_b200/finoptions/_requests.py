@@ -3,7 +3,9 @@
 from __future__ import annotations
 
 import ctypes
+from array import array
 from collections.abc import Sequence
+from itertools import chain
 from dataclasses import dataclass
 from typing import Any
 
@@ -31,8 +33,30 @@ class CallRequest:
     """A filled FoLsmCallRequest and the arrays its pointers borrow."""
 
     struct: _abi.FoLsmCallRequest
-    keepalive: tuple[np.ndarray, ...]
+    keepalive: tuple[Any, ...]
     exercise_rows: int
+
+
+def _spans(parts: tuple[Any, ...], typecode: str, convert: Any) -> tuple[tuple[Any, ...], list[tuple[int, int]]]:
+    """The buffers that hold `parts` and each part's (address, length) in them.
+
+    Plain lists and tuples of numbers go into one array.array, back to back (one C-level
+    conversion instead of a numpy conversion per part). Anything else, including elements that
+    array.array refuses, is converted part by part with `convert`, so its errors are unchanged.
+    """
+    if all(type(p) is list or type(p) is tuple for p in parts):
+        try:
+            flat = array(typecode, chain.from_iterable(parts))
+        except (TypeError, OverflowError, ValueError):
+            pass
+        else:
+            base, step, spans = flat.buffer_info()[0], flat.itemsize, []
+            for p in parts:
+                spans.append((base, len(p)))
+                base += step * len(p)
+            return (flat,), spans
+    arrays = tuple(convert(p) for p in parts)
+    return arrays, [(a.ctypes.data, a.size) for a in arrays]
 
 
 def lsm_call_request(
@@ -62,28 +86,21 @@ def lsm_call_request(
     tie_rule: int,
     insufficient_exercise_support: int,
 ) -> CallRequest:
-    arrays = (
-        _f64(schedule_times),
-        _f64(curve_times),
-        _f64(log_discounts),
-        _f64(dividend_yield_times),
-        _f64(cumulative_dividend_yields),
-        _u32(dividend_nodes),
-        _f64(dividend_amounts),
-        _u32(exercise_nodes),
-    )
-    st, ct, ld, yt, cy, dn, da, en = arrays
+    floats, (st, ct, ld, yt, cy, da) = _spans(
+        (schedule_times, curve_times, log_discounts, dividend_yield_times, cumulative_dividend_yields,
+         dividend_amounts), "d", _f64)
+    nodes, (dn, en) = _spans((dividend_nodes, exercise_nodes), "I", _u32)
     q = _abi.FoLsmCallRequest()
     q.initial_spot = initial_spot
     q.strike = strike
-    q.schedule_times, q.n_schedule_times = _ptr(st, ctypes.c_double), st.size
-    q.curve_times, q.n_curve_times = _ptr(ct, ctypes.c_double), ct.size
-    q.log_discounts, q.n_log_discounts = _ptr(ld, ctypes.c_double), ld.size
-    q.dividend_yield_times, q.n_dividend_yield_times = _ptr(yt, ctypes.c_double), yt.size
-    q.cumulative_dividend_yields, q.n_cumulative_dividend_yields = _ptr(cy, ctypes.c_double), cy.size
-    q.dividend_nodes, q.n_dividend_nodes = _ptr(dn, ctypes.c_uint32), dn.size
-    q.dividend_amounts, q.n_dividend_amounts = _ptr(da, ctypes.c_double), da.size
-    q.exercise_nodes, q.n_exercise_nodes = _ptr(en, ctypes.c_uint32), en.size
+    q.schedule_times, q.n_schedule_times = st
+    q.curve_times, q.n_curve_times = ct
+    q.log_discounts, q.n_log_discounts = ld
+    q.dividend_yield_times, q.n_dividend_yield_times = yt
+    q.cumulative_dividend_yields, q.n_cumulative_dividend_yields = cy
+    q.dividend_nodes, q.n_dividend_nodes = dn
+    q.dividend_amounts, q.n_dividend_amounts = da
+    q.exercise_nodes, q.n_exercise_nodes = en
     q.expiry_node = expiry_node
     q.annualized_volatility = annualized_volatility
     q.dividend_policy = dividend_policy
@@ -98,7 +115,13 @@ def lsm_call_request(
     q.condition_limit = condition_limit
     q.tie_rule = tie_rule
     q.insufficient_exercise_support = insufficient_exercise_support
-    return CallRequest(q, arrays, int(en.size))
+    return CallRequest(q, floats + nodes, en[1])
+
+
+_DIAGNOSTIC = np.dtype(_abi.FoLsmNodeDiagnostic)
+if array("d").itemsize != 8 or array("I").itemsize != 4:  # pragma: no cover - every supported platform
+    msg = "array.array('d'/'I') must be binary64 / 32-bit to back the C ABI's double / uint32_t arrays"
+    raise ImportError(msg)
 
 
 @dataclass
@@ -113,46 +136,47 @@ class CallResult:
     def as_tuple(self) -> tuple:
         """NativeLsmResult-shaped tuple (crates/finoptions-python/src/lib.rs:1074-1082)."""
         r = self.struct
-        rows = int(r.n_observations)
+        rows = r.n_observations
         diags = []
-        for i in range(int(r.n_diagnostics)):
-            d = self.diagnostics[i]
-            if d.kind == _abi.FO_DIAG_ORIGIN_DECISION:
-                diags.append((d.node, "origin_decision", bool(d.exercise), d.estimated_continuation,
-                              None, None, None, None, None, None, None))
-            elif d.kind == _abi.FO_DIAG_NO_IN_THE_MONEY_PATHS:
-                diags.append((d.node, "no_in_the_money_paths", None, None, None, None, None, None,
+        for (node, kind, exercise, continuation, itm, observations, columns, rank, condition, mean,
+             scale) in np.frombuffer(self.diagnostics, dtype=_DIAGNOSTIC, count=r.n_diagnostics).tolist():
+            if kind == _abi.FO_DIAG_REGRESSION:
+                diags.append((node, "regression", None, None, itm, observations, columns, rank, condition, mean,
+                              scale))
+            elif kind == _abi.FO_DIAG_ORIGIN_DECISION:
+                diags.append((node, "origin_decision", bool(exercise), continuation, None, None, None, None,
                               None, None, None))
-            elif d.kind == _abi.FO_DIAG_INSUFFICIENT_SUPPORT:
-                diags.append((d.node, "insufficient_exercise_support", None, None,
-                              d.in_the_money_paths, None, int(d.columns), None, None, None, None))
+            elif kind == _abi.FO_DIAG_NO_IN_THE_MONEY_PATHS:
+                diags.append((node, "no_in_the_money_paths", None, None, None, None, None, None, None, None,
+                              None))
+            elif kind == _abi.FO_DIAG_INSUFFICIENT_SUPPORT:
+                diags.append((node, "insufficient_exercise_support", None, None, itm, None, columns, None,
+                              None, None, None))
             else:
-                diags.append((d.node, "regression", None, None, d.in_the_money_paths,
-                              int(d.observations), int(d.columns), int(d.rank), d.condition_number,
-                              d.predictor_mean, d.predictor_scale))
+                diags.append((node, "regression", None, None, itm, observations, columns, rank, condition, mean,
+                              scale))
         return (
             r.price,
-            int(r.paths),
+            r.paths,
             r.sample_standard_deviation if r.has_sample_standard_deviation else None,
             r.standard_error if r.has_standard_error else None,
-            [int(v) for v in self.observation_nodes[:rows]],
-            [int(v) for v in self.exercise_counts[:rows]],
+            self.observation_nodes[:rows].tolist(),
+            self.exercise_counts[:rows].tolist(),
             diags,
         )
 
 
 def lsm_call_result(exercise_rows: int) -> CallResult:
     rows = exercise_rows + 1
-    nodes = np.zeros(rows, dtype=np.uint32)
-    counts = np.zeros(rows, dtype=np.uint32)
+    columns = np.zeros(2 * rows, dtype=np.uint32)
     diags = (_abi.FoLsmNodeDiagnostic * max(exercise_rows, 1))()
     r = _abi.FoLsmCallResult()
-    r.observation_nodes = _ptr(nodes, ctypes.c_uint32)
+    r.observation_nodes = columns.ctypes.data
     r.observation_capacity = rows
-    r.exercise_counts = _ptr(counts, ctypes.c_uint32)
-    r.diagnostics = ctypes.cast(diags, ctypes.POINTER(_abi.FoLsmNodeDiagnostic))
+    r.exercise_counts = r.observation_nodes + 4 * rows
+    r.diagnostics = ctypes.addressof(diags)
     r.diagnostics_capacity = exercise_rows
-    return CallResult(r, nodes, counts, diags)
+    return CallResult(r, columns[:rows], columns[rows:], diags)
 
 
 def lsm_call_greeks(nodes: int, dividends: int) -> tuple[_abi.FoLsmCallGreeks, np.ndarray, np.ndarray]:
