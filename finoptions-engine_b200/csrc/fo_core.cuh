@@ -773,6 +773,23 @@ FO_HD_NOINLINE void fit_continuation(const dd* sums, double pivot, uint64_t coun
     if (!done) fit_from_moments(sums, pivot, count, degree, rank_tolerance, m);
 }
 
+// The largest q >= 0 whose correctly rounded square root is at most `tol` (host side, for tol in
+// (0, 1)). The square root is monotone, so the solve's rank test fo_sqrt(norm / n) <= tol takes
+// the same decision as norm / n <= rank_limit(tol), without a square root on the device.
+inline double rank_limit(double tol) {
+    const auto step = [](double v, int64_t by) {
+        int64_t bits;
+        __builtin_memcpy(&bits, &v, sizeof bits);
+        bits += by;
+        __builtin_memcpy(&v, &bits, sizeof v);
+        return v;
+    };
+    double q = tol * tol;  // within an ulp or two of the limit
+    for (int i = 0; i < 64 && fo_sqrt(step(q, 1)) <= tol; ++i) q = step(q, 1);
+    for (int i = 0; i < 64 && q > 0.0 && fo_sqrt(q) > tol; ++i) q = step(q, -1);
+    return q;
+}
+
 // PolynomialModel::predict_for (regression.rs:197-224). Returns false for a non-finite result.
 // Model is FitModel or any type with the same mean / scale / alpha / beta / coef fields.
 template <typename Model>

@@ -96,6 +96,7 @@ struct DevicePlan {
     int32_t origin_row;        // 1 when row 0 is node 0 (common origin decision)
     double rank_tolerance;
     double condition_limit;
+    double rank_limit;         // rank_limit(rank_tolerance): the warp solve's rank test
     uint64_t train_paths, eval_paths;
     uint64_t train_seed, eval_seed;
     uint32_t train_domain, eval_domain;

@@ -873,6 +873,7 @@ DevicePlan device_plan(const HostPlan& hp, const InputOffsets& o, unsigned char*
     p.origin_row = hp.origin_row ? 1 : 0;
     p.rank_tolerance = hp.rank_tolerance;
     p.condition_limit = hp.condition_limit;
+    p.rank_limit = rank_limit(hp.rank_tolerance);
     p.train_paths = hp.train_paths;
     p.eval_paths = hp.eval_paths;
     p.train_seed = hp.train_seed;

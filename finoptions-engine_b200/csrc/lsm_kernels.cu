@@ -19,6 +19,7 @@
 
 #include "lsm_common.cuh"
 #include "lsm_device.cuh"
+#include "lsm_fit_warp.cuh"
 #include "lsm_kernels.h"
 #include "lsm_sync.cuh"
 
@@ -291,7 +292,8 @@ __global__ void __launch_bounds__(kBackwardThreads, 1) backward_kernel(BackwardA
         if (!stager) {
             combine_published<kSlots>(parts + size_t(parity) * a.partial_stride, seq, a.status, sm.total,
                                       &sm.wait_failed);
-            if (threadIdx.x == 0 && !sm.wait_failed) {
+            if (threadIdx.x < 32 && !sm.wait_failed) {
+                // Warp 0 decides the row (the same shared totals in every lane) and fits it.
                 const uint64_t itm = uint64_t(sm.total[0].hi);
                 const uint64_t bad = uint64_t(sm.total[kBadSlot].hi);
                 const uint64_t population = itm + bad;
@@ -304,11 +306,12 @@ __global__ void __launch_bounds__(kBackwardThreads, 1) backward_kernel(BackwardA
                 } else if (population < required || bad > 0) {
                     kind = kRuleFitFailed;  // InsufficientObservations / non-finite population
                 } else {
-                    fit_continuation(sm.total, fit_pivot, itm, degree, plan.rank_tolerance, &sm.model);
+                    fit_continuation_warp(sm.total, fit_pivot, itm, degree, plan.rank_tolerance, plan.rank_limit,
+                                          &sm.model);
                     kind = sm.model.status == kFitOk ? kRuleRegression : kRuleFitFailed;
                 }
-                sm.kind = kind;
-                if (blockIdx.x == 0) {
+                if (threadIdx.x == 0) sm.kind = kind;
+                if (threadIdx.x == 0 && blockIdx.x == 0) {
                     FitRecord& rec = a.records[row];
                     rec.kind = kind;
                     rec.itm = population;

@@ -54,3 +54,6 @@ extern "C" int harness_fit(const double* x, const double* y, uint64_t n, double 
     model_out[21] = condition;
     return m.status * 10 + (diag < 0 ? 9 : diag);
 }
+
+// rank_limit(tol): the largest q whose correctly rounded square root is at most tol.
+extern "C" double harness_rank_limit(double tol) { return rank_limit(tol); }

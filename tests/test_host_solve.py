@@ -4,6 +4,7 @@ Stieltjes fit (regression.rs:369-523) on in-the-money populations of realistic s
 from __future__ import annotations
 
 import ctypes
+import math
 import subprocess
 from pathlib import Path
 
@@ -62,3 +63,16 @@ def test_one_pass_moment_solve_matches_the_sequential_reference_fit(harness, deg
             predicted = _oracle.predict(ours, degree, x)
             worst = max(worst, float(np.max(np.abs(predicted - reference)) / np.max(np.abs(reference))))
     assert worst <= 1e-12
+
+
+def test_rank_limit_is_the_last_spread_the_rank_test_accepts(harness) -> None:
+    """norm / n <= rank_limit(tol) is the solve's rank test sqrt(norm / n) <= tol (correctly
+    rounded square root), so the warp solve needs no square root per step."""
+    harness.harness_rank_limit.argtypes = [ctypes.c_double]
+    harness.harness_rank_limit.restype = ctypes.c_double
+    rng = np.random.default_rng(5)
+    tolerances = [1e-12, 1e-8, 0.5, 0.3, math.nextafter(1.0, 0.0), 1e-300, 5e-324, *10.0 ** rng.uniform(-16, -0.01, 2000)]
+    for tol in tolerances:
+        q = harness.harness_rank_limit(float(tol))
+        assert q >= 0.0 and math.sqrt(q) <= tol, tol
+        assert math.sqrt(math.nextafter(q, math.inf)) > tol, tol
