@@ -121,7 +121,8 @@ __device__ __forceinline__ dd shfl_dd_down(dd v, int off);
 // Warp sums in double, then warp k combines slot k across the CTA's warps with a double-double
 // shuffle tree; lane 0 of warp k writes slot k of the CTA partial. Requires S <= warps per CTA.
 template <int S>
-__device__ __forceinline__ void cta_reduce_to(double (&acc)[S], double* smem /* [32 * S] */, double2* dst) {
+__device__ __forceinline__ void cta_reduce_to(double (&acc)[S], double* smem /* [32 * S] */, double2* dst,
+                                              size_t slot_stride = 1) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, warps = blockDim.x >> 5;
     const double total = warp_transpose_reduce<S>(acc);
     // lane l holds value l % S: lanes 0..S-1 publish
@@ -131,7 +132,7 @@ __device__ __forceinline__ void cta_reduce_to(double (&acc)[S], double* smem /* 
         dd v = dd_make(lane < warps ? smem[lane * S + warp] : 0.0);
 #pragma unroll
         for (int off = 16; off > 0; off >>= 1) v = dd_add(v, shfl_dd_down(v, off));
-        if (lane == 0) dst[warp] = make_double2(v.hi, v.lo);
+        if (lane == 0) dst[size_t(warp) * slot_stride] = make_double2(v.hi, v.lo);
     }
     __syncthreads();
 }

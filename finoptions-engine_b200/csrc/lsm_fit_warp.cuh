@@ -14,10 +14,9 @@
 //     rank_limit(rank_tolerance) (fo_core.cuh) instead of taking a square root: the same decision.
 //
 // Every value goes through the same binary64 operations in the same order as the one-thread
-// solve, so the fitted model is bit-identical to fit_continuation's. Lane 0 writes the model in
-// the order the one-thread solve writes it (partial writes before a failure included). The one-
-// thread solve is the latency floor of one serial chain of divisions per step; this one overlaps
-// them.
+// solve, so the fitted model is bit-identical to fit_continuation's, including what it has written
+// when it stops at a failure. The one-thread solve runs its divisions as one serial chain; this one
+// overlaps each step's four.
 #pragma once
 
 #include "fo_core.cuh"
@@ -28,13 +27,36 @@ namespace fo {
 
 constexpr unsigned kWarpLanes = 0xffffffffu;
 
+// Every lane stores its share of *m once, when the solve ends: the one-thread solve's final model
+// (arrays zeroed, then norm / coef of the first `columns` steps and alpha / beta of the first
+// `steps` taken from lane j = step j).
+__device__ __forceinline__ void store_fit(FitModel* m, int lane, double mean, double scale, double inv_scale,
+                                          int status, int aux, double aux_value, int columns, int steps,
+                                          double norm, double coef, double alpha, double beta) {
+    if (lane < kMaxColumns) {
+        m->norm[lane] = lane < columns ? norm : 0.0;
+        m->coef[lane] = lane < columns ? coef : 0.0;
+    }
+    if (lane < kMaxDegree) {
+        m->alpha[lane] = lane < steps ? alpha : 0.0;
+        m->beta[lane] = lane < steps ? beta : 0.0;
+    }
+    if (lane == 0) {
+        m->status = status;
+        m->aux = aux;
+        m->aux_value = aux_value;
+        m->mean = mean;
+        m->scale = scale;
+        m->inv_scale = (fo_fabs(scale) > 0x1p-960 && fo_fabs(scale) < 0x1p960) ? inv_scale : 0.0;
+    }
+}
+
 template <int D>
 __device__ __noinline__ bool fit_near_pivot_warp(const dd* sums, double pivot, uint64_t count, double spread_limit,
                                                  FitModel* m) {
     static_assert(D >= 1 && D <= kMaxDegree, "degree 0 is solved by one lane");
     constexpr int K = 2 * D + 2;  // moments 0..2D+1 (the last stays zero)
     const int lane = int(threadIdx.x & 31);
-    const bool writer = lane == 0;
     const double n = double(count);
     const double t1 = sums[1].hi + sums[1].lo;
     const double offset = t1 / n;
@@ -44,64 +66,52 @@ __device__ __noinline__ bool fit_near_pivot_warp(const dd* sums, double pivot, u
     const double mean = pivot + offset;
     const double scale = fo_sqrt(var);
     const double inv_scale = 1.0 / scale;  // make_divisor(scale).inv in its range; one division for both
-    if (writer) {
-#pragma unroll
-        for (int j = 0; j < kMaxDegree; ++j) {
-            m->alpha[j] = 0.0;
-            m->beta[j] = 0.0;
-        }
-#pragma unroll
-        for (int j = 0; j < kMaxColumns; ++j) {
-            m->coef[j] = 0.0;
-            m->norm[j] = 0.0;
-        }
-        m->status = kFitOk;
-        m->aux = 0;
-        m->aux_value = 0.0;
-        m->mean = mean;
-        m->scale = scale;
-        m->inv_scale = (fo_fabs(scale) > 0x1p-960 && fo_fabs(scale) < 0x1p960) ? inv_scale : 0.0;
-    }
     if (!fo_isfinite(mean) || !fo_isfinite(scale) || !(scale > 0.0)) {
-        if (writer) {
-            m->status = kFitDegeneratePredictor;
-            m->aux_value = scale;
-        }
+        store_fit(m, lane, mean, scale, inv_scale, kFitDegeneratePredictor, 0, scale, 0, 0, 0.0, 0.0, 0.0, 0.0);
         return true;
     }
 
-    // Binomial shift: term s of lane k is C(k, s) * delta^s * S_{k-s} (S = T for the power-sum
-    // lanes, with T_0 = n, and U for the response lanes), added in s = 0..k order, then scaled by
-    // scale^-k. C(k, s) is formed exactly in integers; delta^s and scale^-k by the same product
-    // chains as the one-thread solve.
+    // Binomial shift: lane k adds C(k, j) * delta^(k-j) * S_j for j = k..0 (S = T for the power-
+    // sum lanes, with T_0 = n, and U for the response lanes), the sequential order, then scales by
+    // scale^-k. The loop runs j from 2D down to 0 in every lane, so the sums are read uniformly;
+    // a lane adds from j = k on, carrying delta^(k-j) by the same product chain as the one-thread
+    // solve. C(k, j) is formed exactly in integers beforehand (constant divisors).
     const double delta = pivot - mean;
     const bool response = lane > 2 * D;
     const int k = response ? lane - (2 * D + 1) : lane;
     const bool shifting = !response || k <= D;
-    double acc = 0.0, dpow = 1.0, spow = 1.0;
-    int binomial = 1;
+    int binomial[2 * D + 1];
+    binomial[0] = 1;
 #pragma unroll
-    for (int s = 0; s <= 2 * D; ++s) {
-        if (s > 0) binomial = binomial * (k - s + 1) / s;
-        if (shifting && s <= k) {
-            const int j = k - s;
-            const double sj = response ? sums[kPowerSums + j].hi + sums[kPowerSums + j].lo
-                                       : (j == 0 ? n : sums[j].hi + sums[j].lo);
-            acc += double(binomial) * dpow * sj;
-            if (s > 0) spow *= inv_scale;
+    for (int j = 1; j <= 2 * D; ++j) binomial[j] = binomial[j - 1] * (k - j + 1) / j;  // 0 for j > k
+    double acc = 0.0, power = 1.0;
+#pragma unroll
+    for (int j = 2 * D; j >= 0; --j) {
+        const double tj = j == 0 ? n : sums[j].hi + sums[j].lo;
+        const double uj = j <= D ? sums[kPowerSums + j].hi + sums[kPowerSums + j].lo : 0.0;
+        if (shifting && j <= k) {
+            acc += double(binomial[j]) * power * (response ? uj : tj);
+            power *= delta;
         }
-        dpow *= delta;
     }
+    double spow = 1.0;
+#pragma unroll
+    for (int j = 1; j <= 2 * D; ++j)
+        if (j <= k) spow *= inv_scale;
     const double shifted = acc * spow;
     const double resp = __shfl_sync(kWarpLanes, shifted, lane + 2 * D + 1 < 32 ? lane + 2 * D + 1 : 31);
 
     // Stieltjes recurrence from the moments (lane l: sigma_l of p_j and p_{j-1}; lane i: a_i).
+    // Step j's norm, coefficient, alpha and beta stay in lane j until store_fit.
     double sig_cur = lane < K - 1 ? shifted : 0.0, sig_prev = 0.0;
     double a_cur = lane == 0 ? 1.0 : 0.0, a_prev = 0.0;
     double previous_norm = 1.0;
+    double out_norm = 0.0, out_coef = 0.0, out_alpha = 0.0, out_beta = 0.0;
+    int status = kFitOk, aux = 0, columns = 0, steps = 0;
 #pragma unroll
     for (int j = 0; j <= D; ++j) {
         const double sig_above = __shfl_down_sync(kWarpLanes, sig_cur, 1);
+        const double a_below = __shfl_up_sync(kWarpLanes, a_cur, 1);
         const double pn = a_cur * sig_cur, pw = a_cur * sig_above, pp = a_cur * resp;
         double norm = 0.0, proj = 0.0, wp = 0.0;
 #pragma unroll
@@ -119,43 +129,36 @@ __device__ __noinline__ bool fit_near_pivot_warp(const dd* sums, double pivot, u
         const double spread = __shfl_sync(kWarpLanes, quotient, 2);
         const double beta = j == 0 ? 0.0 : __shfl_sync(kWarpLanes, quotient, 3);
         if (!fo_isfinite(norm) || !fo_isfinite(proj) || !fo_isfinite(wp)) {
-            if (writer) {
-                m->status = kFitNonFinite;
-                m->aux = j;
-            }
-            return true;
+            status = kFitNonFinite;
+            aux = j;
+            break;
         }
         if (norm <= 0.0 || spread <= spread_limit) {
-            if (writer) {
-                m->status = kFitRankDeficient;
-                m->aux = j;
-            }
-            return true;
+            status = kFitRankDeficient;
+            aux = j;
+            break;
         }
-        if (writer) {
-            m->norm[j] = norm;
-            m->coef[j] = coef;
+        if (lane == j) {
+            out_norm = norm;
+            out_coef = coef;
         }
+        columns = j + 1;
         if (!fo_isfinite(coef)) {
-            if (writer) {
-                m->status = kFitNonFinite;
-                m->aux = j;
-            }
-            return true;
+            status = kFitNonFinite;
+            aux = j;
+            break;
         }
         if (j < D) {
             if (!fo_isfinite(alpha) || !fo_isfinite(beta)) {
-                if (writer) {
-                    m->status = kFitNonFinite;
-                    m->aux = j;
-                }
-                return true;
+                status = kFitNonFinite;
+                aux = j;
+                break;
             }
-            if (writer) {
-                m->alpha[j] = alpha;
-                m->beta[j] = beta;
+            if (lane == j) {
+                out_alpha = alpha;
+                out_beta = beta;
             }
-            const double a_below = __shfl_up_sync(kWarpLanes, a_cur, 1);
+            steps = j + 1;
             const double a_next = (lane > 0 ? a_below : 0.0) - alpha * a_cur - beta * a_prev;
             const double sig_next = (lane + 1 < K ? sig_above : 0.0) - alpha * sig_cur - beta * sig_prev;
             a_prev = a_cur;
@@ -165,6 +168,8 @@ __device__ __noinline__ bool fit_near_pivot_warp(const dd* sums, double pivot, u
             previous_norm = norm;
         }
     }
+    store_fit(m, lane, mean, scale, inv_scale, status, aux, 0.0, columns, steps, out_norm, out_coef, out_alpha,
+              out_beta);
     return true;
 }
 

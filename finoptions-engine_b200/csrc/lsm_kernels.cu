@@ -39,7 +39,9 @@ constexpr int kCombineThreads = kCombineWarps * 32;
 
 // Run by the combine warps only (they meet at named barrier 1). Warp 0 waits for every CTA's arrival;
 // then warp k < S sums slot k of the partials over the CTAs in block order (double-double, the
-// same fixed order in every CTA). *wait_failed is 1 when the wait timed out (out is not written).
+// same fixed order in every CTA). The partials are slot-major, [k][block], so a warp's loads are
+// contiguous: every CTA reads every CTA's partials, and the block-major layout made each lane's
+// load a separate sector. *wait_failed is 1 when the wait timed out (out is not written).
 template <int S>
 __device__ __forceinline__ void combine_published(const double2* partials, unsigned seq, DeviceStatus* st, dd* out,
                                                   int* wait_failed) {
@@ -57,14 +59,14 @@ __device__ __forceinline__ void combine_published(const double2* partials, unsig
 #pragma unroll
         for (int i = 0; i < kBatch; ++i) {
             const int b = lane + 32 * i;
-            v[i] = b < blocks ? __ldcg(&partials[b * S + warp]) : make_double2(0.0, 0.0);
+            v[i] = b < blocks ? __ldcg(&partials[warp * blocks + b]) : make_double2(0.0, 0.0);
         }
         dd acc = dd_make(0.0);
 #pragma unroll
         for (int i = 0; i < kBatch; ++i)
             if (lane + 32 * i < blocks) acc = dd_add(acc, dd{v[i].x, v[i].y});
         for (int b = lane + 32 * kBatch; b < blocks; b += 32) {
-            const double2 w = __ldcg(&partials[b * S + warp]);
+            const double2 w = __ldcg(&partials[warp * blocks + b]);
             acc = dd_add(acc, dd{w.x, w.y});
         }
 #pragma unroll
@@ -245,7 +247,7 @@ __global__ void __launch_bounds__(kBackwardThreads, 1) backward_kernel(BackwardA
             }
             spots[at] = sp;
         }
-        cta_reduce_to<2>(loc, sm.red, parts + size_t(parity) * a.partial_stride + size_t(blockIdx.x) * 2);
+        cta_reduce_to<2>(loc, sm.red, parts + size_t(parity) * a.partial_stride + blockIdx.x, gridDim.x);
         publish_partial(a.status);
         ++seq;
         if (!stager)
@@ -272,7 +274,7 @@ __global__ void __launch_bounds__(kBackwardThreads, 1) backward_kernel(BackwardA
     for (; row >= lowest; --row, ++order) {
         const bool stage_next = row - 1 >= lowest;
         const double stage_pivot = latest_mean;
-        cta_reduce_to<kSlots>(sums.acc, sm.red, parts + size_t(parity) * a.partial_stride + size_t(blockIdx.x) * kSlots);
+        cta_reduce_to<kSlots>(sums.acc, sm.red, parts + size_t(parity) * a.partial_stride + blockIdx.x, gridDim.x);
         publish_partial(a.status);
         ++seq;
 #pragma unroll
@@ -408,7 +410,7 @@ __global__ void __launch_bounds__(kBackwardThreads, 1) backward_kernel(BackwardA
                 acc[1] += w;
             }
         }
-        cta_reduce_to<2>(acc, sm.red, parts + size_t(parity) * a.partial_stride + size_t(blockIdx.x) * 2);
+        cta_reduce_to<2>(acc, sm.red, parts + size_t(parity) * a.partial_stride + blockIdx.x, gridDim.x);
         publish_partial(a.status);
         ++seq;
         if (!stager)

@@ -15,7 +15,7 @@ constexpr int kEvalThreads = 256;
 struct BackwardArgs {
     DevicePlan plan;
     const double* slab;          // stored training rows [rows - first_stored_row, paths]
-    double2* partials;           // [2][blocks][16] double-double CTA partials (ping-pong)
+    double2* partials;           // [2][16][blocks] double-double CTA partials (ping-pong), slot-major
     size_t partial_stride;       // doubles2 per ping-pong half
     FitRecord* records;          // [rows]
     DeviceStatus* status;
