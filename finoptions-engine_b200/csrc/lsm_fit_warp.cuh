@@ -87,17 +87,18 @@ __device__ __noinline__ bool fit_near_pivot_warp(const dd* sums, double pivot, u
     double acc = 0.0, power = 1.0;
 #pragma unroll
     for (int j = 2 * D; j >= 0; --j) {
+        // Branch-free: a lane adds +0.0 before its first term (its acc is still +0.0, so the sum
+        // is unchanged) and its own terms from j = k on.
         const double tj = j == 0 ? n : sums[j].hi + sums[j].lo;
         const double uj = j <= D ? sums[kPowerSums + j].hi + sums[kPowerSums + j].lo : 0.0;
-        if (shifting && j <= k) {
-            acc += double(binomial[j]) * power * (response ? uj : tj);
-            power *= delta;
-        }
+        const bool active = shifting && j <= k;
+        const double term = double(binomial[j]) * power * (response ? uj : tj);
+        acc += active ? term : 0.0;
+        power = active ? power * delta : power;
     }
     double spow = 1.0;
 #pragma unroll
-    for (int j = 1; j <= 2 * D; ++j)
-        if (j <= k) spow *= inv_scale;
+    for (int j = 1; j <= 2 * D; ++j) spow = j <= k ? spow * inv_scale : spow;
     const double shifted = acc * spow;
     const double resp = __shfl_sync(kWarpLanes, shifted, lane + 2 * D + 1 < 32 ? lane + 2 * D + 1 : 31);
 
@@ -128,45 +129,39 @@ __device__ __noinline__ bool fit_near_pivot_warp(const dd* sums, double pivot, u
         const double coef = __shfl_sync(kWarpLanes, quotient, 1);
         const double spread = __shfl_sync(kWarpLanes, quotient, 2);
         const double beta = j == 0 ? 0.0 : __shfl_sync(kWarpLanes, quotient, 3);
-        if (!fo_isfinite(norm) || !fo_isfinite(proj) || !fo_isfinite(wp)) {
-            status = kFitNonFinite;
-            aux = j;
-            break;
-        }
-        if (norm <= 0.0 || spread <= spread_limit) {
-            status = kFitRankDeficient;
-            aux = j;
-            break;
-        }
-        if (lane == j) {
+        // The one-thread solve's checks in its order, decided together (one branch per step).
+        const bool sums_finite = fo_isfinite(norm) && fo_isfinite(proj) && fo_isfinite(wp);
+        const bool deficient = norm <= 0.0 || spread <= spread_limit;
+        const bool kept = sums_finite && !deficient;  // norm and coef of step j are written
+        const bool coef_finite = fo_isfinite(coef);
+        const bool stepped = kept && coef_finite && j < D && fo_isfinite(alpha) && fo_isfinite(beta);
+        const int failed = !sums_finite ? kFitNonFinite
+                         : deficient    ? kFitRankDeficient
+                         : !coef_finite ? kFitNonFinite
+                         : (j < D && !stepped) ? kFitNonFinite
+                                               : kFitOk;
+        if (lane == j && kept) {
             out_norm = norm;
             out_coef = coef;
         }
-        columns = j + 1;
-        if (!fo_isfinite(coef)) {
-            status = kFitNonFinite;
+        if (lane == j && stepped) {
+            out_alpha = alpha;
+            out_beta = beta;
+        }
+        columns = kept ? j + 1 : columns;
+        steps = stepped ? j + 1 : steps;
+        const double a_next = (lane > 0 ? a_below : 0.0) - alpha * a_cur - beta * a_prev;
+        const double sig_next = (lane + 1 < K ? sig_above : 0.0) - alpha * sig_cur - beta * sig_prev;
+        if (failed != kFitOk) {
+            status = failed;
             aux = j;
             break;
         }
-        if (j < D) {
-            if (!fo_isfinite(alpha) || !fo_isfinite(beta)) {
-                status = kFitNonFinite;
-                aux = j;
-                break;
-            }
-            if (lane == j) {
-                out_alpha = alpha;
-                out_beta = beta;
-            }
-            steps = j + 1;
-            const double a_next = (lane > 0 ? a_below : 0.0) - alpha * a_cur - beta * a_prev;
-            const double sig_next = (lane + 1 < K ? sig_above : 0.0) - alpha * sig_cur - beta * sig_prev;
-            a_prev = a_cur;
-            a_cur = a_next;
-            sig_prev = sig_cur;
-            sig_cur = sig_next;
-            previous_norm = norm;
-        }
+        a_prev = a_cur;
+        a_cur = a_next;
+        sig_prev = sig_cur;
+        sig_cur = sig_next;
+        previous_norm = norm;
     }
     store_fit(m, lane, mean, scale, inv_scale, status, aux, 0.0, columns, steps, out_norm, out_coef, out_alpha,
               out_beta);
