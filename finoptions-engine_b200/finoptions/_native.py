@@ -203,7 +203,7 @@ def _executor_handle(executor: object) -> ctypes.c_void_p:
     return executor.raw
 
 
-def price_lsm_call_seeded_f64(  # noqa: PLR0913 - mirrors the reference's native signature
+def price_lsm_call_seeded_result_f64(  # noqa: PLR0913 - price_lsm_call_seeded_f64's signature
     initial_spot: float,
     strike: float,
     schedule_times: list[float],
@@ -230,7 +230,8 @@ def price_lsm_call_seeded_f64(  # noqa: PLR0913 - mirrors the reference's native
     tie_rule: str,
     insufficient_exercise_support: str,
 ) -> tuple:
-    """NativeLsmResult of one seeded single-contract LSM price (lib.rs:1169-1241)."""
+    """price_lsm_call_seeded_f64 returning the caller-owned result buffers (a CallResult) instead of
+    the NativeLsmResult tuple; the public pricing call builds its records straight from them."""
     handle = _executor_handle(executor)
     request = lsm_call_request(
         initial_spot=initial_spot,
@@ -271,7 +272,44 @@ def price_lsm_call_seeded_f64(  # noqa: PLR0913 - mirrors the reference's native
             if message.startswith(prefix):
                 raise InputError(f'{prefix} "{value}"')
     _check(status, err)
-    return result.as_tuple()
+    return result
+
+
+def price_lsm_call_seeded_f64(  # noqa: PLR0913 - mirrors the reference's native signature
+    initial_spot: float,
+    strike: float,
+    schedule_times: list[float],
+    curve_times: list[float],
+    log_discounts: list[float],
+    dividend_yield_times: list[float],
+    cumulative_dividend_yields: list[float],
+    dividend_nodes: list[int],
+    dividend_amounts: list[float],
+    exercise_nodes: list[int],
+    expiry_node: int,
+    annualized_volatility: float,
+    dividend_policy: str,
+    executor: CudaExecutor,
+    training_paths: int,
+    evaluation_paths: int,
+    training_seed: int,
+    training_domain: int,
+    evaluation_seed: int,
+    evaluation_domain: int,
+    polynomial_degree: int,
+    rank_tolerance: float,
+    condition_limit: float,
+    tie_rule: str,
+    insufficient_exercise_support: str,
+) -> tuple:
+    """NativeLsmResult of one seeded single-contract LSM price (lib.rs:1169-1241)."""
+    return price_lsm_call_seeded_result_f64(
+        initial_spot, strike, schedule_times, curve_times, log_discounts, dividend_yield_times,
+        cumulative_dividend_yields, dividend_nodes, dividend_amounts, exercise_nodes, expiry_node,
+        annualized_volatility, dividend_policy, executor, training_paths, evaluation_paths, training_seed,
+        training_domain, evaluation_seed, evaluation_domain, polynomial_degree, rank_tolerance, condition_limit,
+        tie_rule, insufficient_exercise_support,
+    ).as_tuple()
 
 
 def price_lsm_call_greeks_seeded_f64(  # noqa: PLR0913 - price_lsm_call_seeded_f64's signature

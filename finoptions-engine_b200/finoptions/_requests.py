@@ -133,17 +133,30 @@ class CallResult:
     exercise_counts: np.ndarray
     diagnostics: ctypes.Array
 
-    def as_tuple(self) -> tuple:
-        """NativeLsmResult-shaped tuple (crates/finoptions-python/src/lib.rs:1074-1082)."""
+    def head(self) -> tuple:
+        """(price, paths, sample SD or None, SE or None, observation nodes, exercise counts)."""
         r = self.struct
         rows = r.n_observations
+        return (
+            r.price,
+            r.paths,
+            r.sample_standard_deviation if r.has_sample_standard_deviation else None,
+            r.standard_error if r.has_standard_error else None,
+            self.observation_nodes[:rows].tolist(),
+            self.exercise_counts[:rows].tolist(),
+        )
+
+    def rows(self) -> list[tuple]:
+        """The diagnostics as plain tuples (node, kind code, exercise, estimated continuation,
+        in-the-money paths, observations, columns, rank, condition, predictor mean, scale)."""
+        return np.frombuffer(self.diagnostics, dtype=_DIAGNOSTIC, count=self.struct.n_diagnostics).tolist()
+
+    def as_tuple(self) -> tuple:
+        """NativeLsmResult-shaped tuple (crates/finoptions-python/src/lib.rs:1074-1082)."""
         diags = []
         for (node, kind, exercise, continuation, itm, observations, columns, rank, condition, mean,
-             scale) in np.frombuffer(self.diagnostics, dtype=_DIAGNOSTIC, count=r.n_diagnostics).tolist():
-            if kind == _abi.FO_DIAG_REGRESSION:
-                diags.append((node, "regression", None, None, itm, observations, columns, rank, condition, mean,
-                              scale))
-            elif kind == _abi.FO_DIAG_ORIGIN_DECISION:
+             scale) in self.rows():
+            if kind == _abi.FO_DIAG_ORIGIN_DECISION:
                 diags.append((node, "origin_decision", bool(exercise), continuation, None, None, None, None,
                               None, None, None))
             elif kind == _abi.FO_DIAG_NO_IN_THE_MONEY_PATHS:
@@ -155,15 +168,7 @@ class CallResult:
             else:
                 diags.append((node, "regression", None, None, itm, observations, columns, rank, condition, mean,
                               scale))
-        return (
-            r.price,
-            r.paths,
-            r.sample_standard_deviation if r.has_sample_standard_deviation else None,
-            r.standard_error if r.has_standard_error else None,
-            self.observation_nodes[:rows].tolist(),
-            self.exercise_counts[:rows].tolist(),
-            diags,
-        )
+        return (*self.head(), diags)
 
 
 def lsm_call_result(exercise_rows: int) -> CallResult:

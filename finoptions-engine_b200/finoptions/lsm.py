@@ -13,6 +13,12 @@ from math import isfinite
 from typing import Final
 
 from . import _native
+from ._abi import (
+    FO_DIAG_INSUFFICIENT_SUPPORT,
+    FO_DIAG_NO_IN_THE_MONEY_PATHS,
+    FO_DIAG_ORIGIN_DECISION,
+    FO_DIAG_REGRESSION,
+)
 from .model import (
     ConstantVolatility,
     CumulativeDividendYieldCurve,
@@ -182,6 +188,35 @@ _new_record = object.__new__
     "predictor_scale"))
 
 
+_OTHER_KINDS = frozenset((FO_DIAG_ORIGIN_DECISION, FO_DIAG_NO_IN_THE_MONEY_PATHS, FO_DIAG_INSUFFICIENT_SUPPORT))
+
+
+def _fit_records(rows: list[tuple]) -> tuple[ExerciseFitDiagnostics, ...]:
+    """The records of native diagnostic rows (CallResult.rows()): the records _fit_diagnostic makes
+    from the NativeLsmResult tuples of the same rows, in one pass."""
+    out = []
+    append = out.append
+    for node, kind, exercise, continuation, itm, observations, columns, rank, condition, mean, scale in rows:
+        if kind == FO_DIAG_REGRESSION or kind not in _OTHER_KINDS:  # unknown kinds read as regression rows
+            record = _new_record(RegressionFitDiagnostics)
+            _set_node(record, node)
+            _set_itm(record, itm)
+            _set_observations(record, observations)
+            _set_columns(record, columns)
+            _set_rank(record, rank)
+            _set_condition(record, condition)
+            _set_mean(record, mean)
+            _set_scale(record, scale)
+            append(record)
+        elif kind == FO_DIAG_ORIGIN_DECISION:
+            append(OriginDecisionDiagnostics(node=node, exercise=bool(exercise), estimated_continuation=continuation))
+        elif kind == FO_DIAG_NO_IN_THE_MONEY_PATHS:
+            append(NoInTheMoneyPathsDiagnostics(node=node))
+        else:
+            append(InsufficientExerciseSupportDiagnostics(node=node, in_the_money_paths=itm, required_paths=columns))
+    return tuple(out)
+
+
 def _fit_diagnostic(raw: tuple) -> ExerciseFitDiagnostics:
     (node, kind, exercise, continuation, itm, observations, columns, rank, condition, mean, scale) = raw
     if kind == "regression" and None not in (itm, observations, columns, rank, condition, mean, scale):
@@ -293,7 +328,7 @@ def price_lsm_call(  # noqa: PLR0913 - financial inputs remain independently typ
         method=method,
     )
     handle = native_executor(executor)
-    raw = _native.price_lsm_call_seeded_f64(
+    res = _native.price_lsm_call_seeded_result_f64(
         initial_spot,
         strike,
         list(schedule.times),
@@ -320,7 +355,7 @@ def price_lsm_call(  # noqa: PLR0913 - financial inputs remain independently typ
         method.tie_rule.value,
         method.insufficient_exercise_support.value,
     )
-    price, paths, sd, se, nodes, counts, diagnostics = raw
+    price, paths, sd, se, nodes, counts = res.head()
     return LsmResult(
         price=price,
         paths=paths,
@@ -328,7 +363,7 @@ def price_lsm_call(  # noqa: PLR0913 - financial inputs remain independently typ
         standard_error=se,
         observation_nodes=tuple(nodes),
         exercise_counts=tuple(counts),
-        fit_diagnostics=tuple(_fit_diagnostic(d) for d in diagnostics),
+        fit_diagnostics=_fit_records(res.rows()),
     )
 
 

@@ -117,3 +117,24 @@ def test_result_reader_builds_the_native_result_shape() -> None:
         (3, "regression", None, None, 40, 40, 3, 3, 12.5, 1.1, 0.2),
     ]
     assert all(type(v) is int for v in obs + cnt)
+
+
+def test_records_built_from_rows_equal_the_records_of_the_native_tuples() -> None:
+    from finoptions import lsm  # noqa: PLC0415 - the pricing module's private builders
+
+    res = lsm_call_result(5)
+    r = res.struct
+    r.n_observations, r.n_diagnostics = 6, 5
+    d = res.diagnostics
+    d[0].node, d[0].kind, d[0].exercise, d[0].estimated_continuation = 0, _abi.FO_DIAG_ORIGIN_DECISION, 0, 1.75
+    d[1].node, d[1].kind = 1, _abi.FO_DIAG_NO_IN_THE_MONEY_PATHS
+    d[2].node, d[2].kind, d[2].in_the_money_paths, d[2].columns = 2, _abi.FO_DIAG_INSUFFICIENT_SUPPORT, 1, 5
+    for i, kind in ((3, _abi.FO_DIAG_REGRESSION), (4, 7)):  # an unknown kind reads as a regression row
+        d[i].node, d[i].kind, d[i].in_the_money_paths, d[i].observations, d[i].columns = i, kind, 90 + i, 90 + i, 5
+        d[i].rank, d[i].condition_number, d[i].predictor_mean, d[i].predictor_scale = 5, 3.5 + i, 1.0 + i, 0.25
+    expected = tuple(lsm._fit_diagnostic(row) for row in res.as_tuple()[6])
+    got = lsm._fit_records(res.rows())
+    assert got == expected
+    assert [type(x).__name__ for x in got] == ["OriginDecisionDiagnostics", "NoInTheMoneyPathsDiagnostics",
+                                               "InsufficientExerciseSupportDiagnostics",
+                                               "RegressionFitDiagnostics", "RegressionFitDiagnostics"]
