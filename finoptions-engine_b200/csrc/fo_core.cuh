@@ -809,6 +809,27 @@ FO_HD bool predict_continuation(const Model& m, int degree, double predictor, do
     return true;
 }
 
+// predict_continuation for a degree fixed at compile time: the same operations in the same order,
+// with the basis recurrence unrolled (kernels that evaluate a fitted policy on every path are
+// instantiated per degree).
+template <int D, typename Model>
+FO_HD bool predict_continuation_d(const Model& m, double predictor, double* out) {
+    if (!fo_isfinite(predictor)) return false;
+    const double z = D == 0 ? 0.0 : divide(predictor - m.mean, Divisor{m.scale, m.inv_scale});
+    double prediction = m.coef[0];
+    double previous = 0.0, current = 1.0;
+#pragma unroll
+    for (int j = 0; j < D; ++j) {
+        const double next = fo_fma(z - m.alpha[j], current, -m.beta[j] * previous);
+        prediction = fo_fma(m.coef[j + 1], next, prediction);
+        previous = current;
+        current = next;
+    }
+    if (!fo_isfinite(prediction)) return false;
+    *out = prediction;
+    return true;
+}
+
 // ----------------------------------------------------------------------------------------------
 // Rank and two-norm condition diagnostic: one-sided Jacobi SVD of the <= 5x5 upper-triangular
 // transform from monomials to the orthonormal basis (regression.rs:540-577, 711-850).

@@ -458,6 +458,7 @@ struct EvalRow {
     double discount;
 };
 
+template <int D>
 __global__ void __launch_bounds__(kEvalThreads, 4) evaluate_kernel(EvalArgs a) {
     extern __shared__ __align__(16) unsigned char eval_smem_raw[];
     const DevicePlan& plan = a.plan;
@@ -486,7 +487,6 @@ __global__ void __launch_bounds__(kEvalThreads, 4) evaluate_kernel(EvalArgs a) {
     const double K = plan.strike;
     const Divisor Kd = make_divisor(K);
     const uint64_t P = plan.eval_paths;
-    const int degree = plan.degree;
     double sum = 0.0, sumsq = 0.0;
     for (uint64_t p = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; p < P; p += uint64_t(gridDim.x) * blockDim.x) {
         bool active = true;
@@ -509,7 +509,7 @@ __global__ void __launch_bounds__(kEvalThreads, 4) evaluate_kernel(EvalArgs a) {
             if (er.kind != kRuleRegression || !(spot > K)) return;
             const double intrinsic = spot - K;
             double continuation;
-            if (!predict_continuation(er.model, degree, divide(spot, Kd), &continuation)) {
+            if (!predict_continuation_d<D>(er.model, divide(spot, Kd), &continuation)) {
                 atomicMin(&a.status->eval_fail, ((unsigned long long)row << 33) | (p << 1));
                 return;
             }
@@ -636,14 +636,25 @@ size_t evaluate_smem_bytes(uint32_t rows) {
     return sizeof(double) * (257 * 2 + 64) + sizeof(EvalRow) * rows + sizeof(unsigned) * 2 * rows;
 }
 
-cudaError_t launch_evaluate(const EvalArgs& args, int blocks, cudaStream_t stream) {
-    const size_t smem = evaluate_smem_bytes(args.plan.rows);
+template <int D>
+static cudaError_t launch_evaluate_d(const EvalArgs& args, int blocks, size_t smem, cudaStream_t stream) {
     if (smem > 48 * 1024) {
-        cudaError_t e = cudaFuncSetAttribute(evaluate_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+        cudaError_t e = cudaFuncSetAttribute(evaluate_kernel<D>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
         if (e != cudaSuccess) return e;
     }
-    evaluate_kernel<<<blocks, kEvalThreads, smem, stream>>>(args);
+    evaluate_kernel<D><<<blocks, kEvalThreads, smem, stream>>>(args);
     return cudaGetLastError();
+}
+
+cudaError_t launch_evaluate(const EvalArgs& args, int blocks, cudaStream_t stream) {
+    const size_t smem = evaluate_smem_bytes(args.plan.rows);
+    switch (args.plan.degree) {  // validated to 0..4 on the host
+        case 0: return launch_evaluate_d<0>(args, blocks, smem, stream);
+        case 1: return launch_evaluate_d<1>(args, blocks, smem, stream);
+        case 2: return launch_evaluate_d<2>(args, blocks, smem, stream);
+        case 3: return launch_evaluate_d<3>(args, blocks, smem, stream);
+        default: return launch_evaluate_d<4>(args, blocks, smem, stream);
+    }
 }
 
 cudaError_t launch_finalize(const double2* partials, int blocks, uint64_t paths, double* out, cudaStream_t stream) {
