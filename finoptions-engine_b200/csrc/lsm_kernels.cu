@@ -170,6 +170,7 @@ struct BackwardSmem {
 // them to row k-1 (policy.rs:1049-1063) and adds the response sums U_0..U_4, which need the
 // decided values. Row k-1's sums are taken about the mean of the latest fitted row available when
 // its staging starts (two rows later than row k-1); any pivot near the in-the-money mean serves.
+template <int D>  // == plan.degree (launch_backward dispatches on it)
 __global__ void __launch_bounds__(kBackwardThreads, 1) backward_kernel(BackwardArgs a) {
     __shared__ BackwardSmem sm;
     extern __shared__ double backward_dyn[];
@@ -363,7 +364,7 @@ __global__ void __launch_bounds__(kBackwardThreads, 1) backward_kernel(BackwardA
                 if (sp > K) {
                     const double intrinsic = sp - K;
                     double continuation;
-                    if (!predict_continuation(model, degree, divide(sp, Kd), &continuation)) {
+                    if (!predict_continuation_d<D>(model, divide(sp, Kd), &continuation)) {
                         atomicMin(&a.status->fit_predict_fail, ((unsigned long long)order << 32) | p);
                     } else if (exercise_rule(plan.tie_rule, intrinsic, continuation)) {
                         v = intrinsic;
@@ -596,7 +597,7 @@ size_t backward_smem_bytes(int ppt) { return sizeof(double) * 3 * size_t(ppt) * 
 int backward_max_ppt() {
     // Dynamic shared memory available next to the kernel's static shared memory.
     cudaFuncAttributes attr{};
-    cudaFuncGetAttributes(&attr, backward_kernel);
+    cudaFuncGetAttributes(&attr, backward_kernel<kMaxDegree>);  // every degree has the same static shared memory
     int optin = 0, device = 0;
     cudaGetDevice(&device);
     cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device);
@@ -610,20 +611,31 @@ int backward_max_blocks(int device) {
     return sms;  // one 1024-thread CTA per SM; the dynamic shared memory keeps it at one
 }
 
-cudaError_t launch_backward(const BackwardArgs& args, int blocks, int ppt, cudaStream_t stream) {
+template <int D>
+static cudaError_t launch_backward_d(const BackwardArgs& args, int blocks, int ppt, cudaStream_t stream) {
     const size_t smem = backward_smem_bytes(ppt);
-    cudaError_t e = cudaFuncSetAttribute(backward_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+    cudaError_t e = cudaFuncSetAttribute(backward_kernel<D>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
     if (e != cudaSuccess) return e;
     int per_sm = 0;
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, backward_kernel, kBackwardThreads, smem);
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, backward_kernel<D>, kBackwardThreads, smem);
     if (e != cudaSuccess) return e;
     int device = 0, sms = 0;
     cudaGetDevice(&device);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
     if (per_sm < 1 || blocks > per_sm * sms) return cudaErrorCooperativeLaunchTooLarge;
     void* params[] = {const_cast<BackwardArgs*>(&args)};
-    return cudaLaunchCooperativeKernel((const void*)backward_kernel, dim3(blocks), dim3(kBackwardThreads), params, smem,
-                                       stream);
+    return cudaLaunchCooperativeKernel((const void*)backward_kernel<D>, dim3(blocks), dim3(kBackwardThreads), params,
+                                       smem, stream);
+}
+
+cudaError_t launch_backward(const BackwardArgs& args, int blocks, int ppt, cudaStream_t stream) {
+    switch (args.plan.degree) {  // validated to 0..4 on the host
+        case 0: return launch_backward_d<0>(args, blocks, ppt, stream);
+        case 1: return launch_backward_d<1>(args, blocks, ppt, stream);
+        case 2: return launch_backward_d<2>(args, blocks, ppt, stream);
+        case 3: return launch_backward_d<3>(args, blocks, ppt, stream);
+        default: return launch_backward_d<4>(args, blocks, ppt, stream);
+    }
 }
 
 cudaError_t launch_diagnose(const DevicePlan& plan, FitRecord* records, cudaStream_t stream) {
