@@ -91,7 +91,7 @@ __device__ __forceinline__ void cluster_combine(BatchBackwardSmem& sm) {
 // distributed shared memory. Problems of up to 64Ki paths run alone in a CTA with two loads at three
 // CTAs per SM; larger ones, whose single CTA would be a long tail, in clusters of four with four
 // loads at two CTAs per SM.
-template <int kLoads, int kMinBlocks, int kCluster>
+template <int kLoads, int kMinBlocks, int kCluster, int D>  // D == a.degree
 __global__ void __launch_bounds__(kBatchBackwardThreads, kMinBlocks) batch_backward_kernel(BatchArgs a) {
     constexpr int kBackwardBatch = kLoads;
     __shared__ BatchBackwardSmem sm;
@@ -255,7 +255,7 @@ __global__ void __launch_bounds__(kBatchBackwardThreads, kMinBlocks) batch_backw
                 if (regression && sc[u] > K) {
                     const double intrinsic = sc[u] - K;
                     double continuation;
-                    if (!predict_continuation(sm.model, degree, divide(sc[u], Kd), &continuation)) {
+                    if (!predict_continuation_d<D>(sm.model, divide(sc[u], Kd), &continuation)) {
                         atomicMin(&st->fit_predict_fail, ((unsigned long long)order << 32) | p);
                     } else if (exercise_rule(a.tie_rule, intrinsic, continuation)) {
                         v[u] = intrinsic;
@@ -343,7 +343,7 @@ __global__ void batch_diagnose_kernel(BatchArgs a, uint32_t n_records) {
 // group, so row and ragged batches run the one-strike body). kStaged: the group's fitted rules are
 // copied into shared memory ([strike][row]) before the paths run; otherwise each lookup reads the
 // FitRecord from HBM / L2.
-template <int S, bool kStaged>
+template <int S, bool kStaged, int D>  // D == a.degree
 __global__ void __launch_bounds__(kBatchEvalThreads, S <= 1 ? 4 : 3) batch_evaluate_kernel(BatchArgs a, uint32_t rule_rows) {
     __shared__ double sx[257], sf[257];
     __shared__ double red[32 * 2 * S];
@@ -395,7 +395,6 @@ __global__ void __launch_bounds__(kBatchEvalThreads, S <= 1 ? 4 : 3) batch_evalu
     const uint64_t P = plan.eval_paths;
     const uint64_t p = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x;
     const uint32_t last = rows - 1;
-    const int degree = a.degree;
     double payoff[S];
 #pragma unroll
     for (int k = 0; k < S; ++k) payoff[k] = 0.0;
@@ -429,8 +428,8 @@ __global__ void __launch_bounds__(kBatchEvalThreads, S <= 1 ? 4 : 3) batch_evalu
             if (kind != kRuleRegression || !(spot > K)) continue;
             const double intrinsic = spot - K;
             double continuation;
-            const bool ok = kStaged ? predict_continuation(staged[k * rule_rows + row], degree, divide(spot, Divisor{K, inv_strikes[k]}), &continuation)
-                                    : predict_continuation(a.records[rbase[k] + row].model, degree, divide(spot, Divisor{K, inv_strikes[k]}), &continuation);
+            const bool ok = kStaged ? predict_continuation_d<D>(staged[k * rule_rows + row], divide(spot, Divisor{K, inv_strikes[k]}), &continuation)
+                                    : predict_continuation_d<D>(a.records[rbase[k] + row].model, divide(spot, Divisor{K, inv_strikes[k]}), &continuation);
             if (!ok) {
                 atomicMin(&a.problem_status[first + k].eval_fail, ((unsigned long long)row << 33) | (p << 1));
                 continue;
@@ -730,8 +729,9 @@ cudaError_t launch_batch_simulate(const BatchArgs& a, cudaStream_t stream) {
     return cudaGetLastError();
 }
 
-cudaError_t launch_batch_backward(const BatchArgs& a, uint32_t n_large, cudaStream_t stream, cudaStream_t side,
-                                  cudaEvent_t fork, cudaEvent_t join) {
+template <int D>
+static cudaError_t launch_batch_backward_d(const BatchArgs& a, uint32_t n_large, cudaStream_t stream, cudaStream_t side,
+                                          cudaEvent_t fork, cudaEvent_t join) {
     // backward_order lists the problems above 64Ki paths first (clusters of four CTAs), then the
     // rest (one CTA each); the two launches run side by side when a second stream is given.
     constexpr int kCluster = 4;
@@ -754,13 +754,13 @@ cudaError_t launch_batch_backward(const BatchArgs& a, uint32_t n_large, cudaStre
         attr[0].val.clusterDim.z = 1;
         cfg.attrs = attr;
         cfg.numAttrs = 1;
-        cudaError_t e = cudaLaunchKernelEx(&cfg, batch_backward_kernel<4, 2, kCluster>, a);
+        cudaError_t e = cudaLaunchKernelEx(&cfg, batch_backward_kernel<4, 2, kCluster, D>, a);
         if (e != cudaSuccess) return e;
     }
     if (n_small > 0) {
         BatchArgs s = a;
         s.backward_order = a.backward_order + n_large;
-        batch_backward_kernel<2, 3, 1><<<n_small, kBatchBackwardThreads, 0, small_stream>>>(s);
+        batch_backward_kernel<2, 3, 1, D><<<n_small, kBatchBackwardThreads, 0, small_stream>>>(s);
         cudaError_t e = cudaGetLastError();
         if (e != cudaSuccess) return e;
         if (side) {
@@ -772,31 +772,54 @@ cudaError_t launch_batch_backward(const BatchArgs& a, uint32_t n_large, cudaStre
     return cudaSuccess;
 }
 
+cudaError_t launch_batch_backward(const BatchArgs& a, uint32_t n_large, cudaStream_t stream, cudaStream_t side,
+                                  cudaEvent_t fork, cudaEvent_t join) {
+    switch (a.degree) {  // validated to 0..4 on the host
+        case 0: return launch_batch_backward_d<0>(a, n_large, stream, side, fork, join);
+        case 1: return launch_batch_backward_d<1>(a, n_large, stream, side, fork, join);
+        case 2: return launch_batch_backward_d<2>(a, n_large, stream, side, fork, join);
+        case 3: return launch_batch_backward_d<3>(a, n_large, stream, side, fork, join);
+        default: return launch_batch_backward_d<4>(a, n_large, stream, side, fork, join);
+    }
+}
+
 cudaError_t launch_batch_diagnose(const BatchArgs& a, uint32_t n_records, cudaStream_t stream) {
     batch_diagnose_kernel<<<(n_records + 127) / 128, 128, 0, stream>>>(a, n_records);
     return cudaGetLastError();
 }
 
-template <int S>
+template <int S, int D>
 cudaError_t launch_batch_evaluate_width(const BatchArgs& a, uint32_t max_strikes, uint32_t max_rows, cudaStream_t stream) {
     const dim3 grid(a.eval_blocks, a.n_groups, (max_strikes + S - 1) / S);
     const size_t smem = sizeof(PolicyRule) * S * max_rows;
     if (smem <= kEvalRuleSmemBytes) {
-        cudaError_t e = cudaFuncSetAttribute(batch_evaluate_kernel<S, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        cudaError_t e = cudaFuncSetAttribute(batch_evaluate_kernel<S, true, D>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                              int(kEvalRuleSmemBytes));
         if (e != cudaSuccess) return e;
-        batch_evaluate_kernel<S, true><<<grid, kBatchEvalThreads, smem, stream>>>(a, max_rows);
+        batch_evaluate_kernel<S, true, D><<<grid, kBatchEvalThreads, smem, stream>>>(a, max_rows);
     } else {
-        batch_evaluate_kernel<S, false><<<grid, kBatchEvalThreads, 0, stream>>>(a, max_rows);
+        batch_evaluate_kernel<S, false, D><<<grid, kBatchEvalThreads, 0, stream>>>(a, max_rows);
     }
     return cudaGetLastError();
 }
 
+template <int D>
+static cudaError_t launch_batch_evaluate_d(const BatchArgs& a, uint32_t max_strikes, uint32_t max_rows,
+                                           cudaStream_t stream) {
+    if (max_strikes <= 1) return launch_batch_evaluate_width<1, D>(a, max_strikes, max_rows, stream);
+    if (max_strikes <= 2) return launch_batch_evaluate_width<2, D>(a, max_strikes, max_rows, stream);
+    if (max_strikes <= 4) return launch_batch_evaluate_width<4, D>(a, max_strikes, max_rows, stream);
+    return launch_batch_evaluate_width<kEvalStrikes, D>(a, max_strikes, max_rows, stream);
+}
+
 cudaError_t launch_batch_evaluate(const BatchArgs& a, uint32_t max_strikes, uint32_t max_rows, cudaStream_t stream) {
-    if (max_strikes <= 1) return launch_batch_evaluate_width<1>(a, max_strikes, max_rows, stream);
-    if (max_strikes <= 2) return launch_batch_evaluate_width<2>(a, max_strikes, max_rows, stream);
-    if (max_strikes <= 4) return launch_batch_evaluate_width<4>(a, max_strikes, max_rows, stream);
-    return launch_batch_evaluate_width<kEvalStrikes>(a, max_strikes, max_rows, stream);
+    switch (a.degree) {  // validated to 0..4 on the host
+        case 0: return launch_batch_evaluate_d<0>(a, max_strikes, max_rows, stream);
+        case 1: return launch_batch_evaluate_d<1>(a, max_strikes, max_rows, stream);
+        case 2: return launch_batch_evaluate_d<2>(a, max_strikes, max_rows, stream);
+        case 3: return launch_batch_evaluate_d<3>(a, max_strikes, max_rows, stream);
+        default: return launch_batch_evaluate_d<4>(a, max_strikes, max_rows, stream);
+    }
 }
 
 cudaError_t launch_batch_evaluate_greeks(const BatchArgs& a, uint32_t max_strikes, uint32_t max_rows,
