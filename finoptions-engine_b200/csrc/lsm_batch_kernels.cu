@@ -465,6 +465,7 @@ __global__ void __launch_bounds__(kBatchEvalThreads, S <= 1 ? 4 : 3) batch_evalu
 // Fused evaluation with pathwise adjoint Greeks: one strike per block (grid z = strike in group).
 // ---------------------------------------------------------------------------------------------
 
+template <int D>  // == a.degree
 __global__ void __launch_bounds__(kBatchEvalThreads, 4) batch_evaluate_greeks_kernel(BatchArgs a, uint32_t rule_rows) {
     __shared__ double sx[257], sf[257];
     __shared__ double red[32 * 2];
@@ -509,7 +510,6 @@ __global__ void __launch_bounds__(kBatchEvalThreads, 4) batch_evaluate_greeks_ke
     const uint64_t P = plan.eval_paths;
     const uint64_t p = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x;
     const uint32_t last = rows - 1;
-    const int degree = a.degree;
     const double sens_scale = 1.0 / g.sigma;  // (Z diffusion - diffusion^2) / sigma = Z sqrt(dt) - sigma dt
     double payoff = 0.0;
     bool active = p < P;
@@ -537,7 +537,7 @@ __global__ void __launch_bounds__(kBatchEvalThreads, 4) batch_evaluate_greeks_ke
         if (rule.kind != kRuleRegression || !(spot > K)) return;
         const double intrinsic = spot - K;
         double continuation;
-        if (!predict_continuation(rule, degree, divide(spot, Kd), &continuation)) {
+        if (!predict_continuation_d<D>(rule, divide(spot, Kd), &continuation)) {
             atomicMin(&a.problem_status[problem].eval_fail, ((unsigned long long)row << 33) | (p << 1));
             return;
         }
@@ -822,17 +822,29 @@ cudaError_t launch_batch_evaluate(const BatchArgs& a, uint32_t max_strikes, uint
     }
 }
 
-cudaError_t launch_batch_evaluate_greeks(const BatchArgs& a, uint32_t max_strikes, uint32_t max_rows,
-                                         cudaStream_t stream) {
+template <int D>
+static cudaError_t launch_batch_evaluate_greeks_d(const BatchArgs& a, uint32_t max_strikes, uint32_t max_rows,
+                                                  cudaStream_t stream) {
     const dim3 grid(a.eval_blocks, a.n_groups, max_strikes);
     const size_t smem = (sizeof(PolicyRule) + sizeof(unsigned)) * max_rows;
     if (smem > 48 * 1024) {
-        cudaError_t e = cudaFuncSetAttribute(batch_evaluate_greeks_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             int(smem));
+        cudaError_t e = cudaFuncSetAttribute(batch_evaluate_greeks_kernel<D>,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
         if (e != cudaSuccess) return e;
     }
-    batch_evaluate_greeks_kernel<<<grid, kBatchEvalThreads, smem, stream>>>(a, max_rows);
+    batch_evaluate_greeks_kernel<D><<<grid, kBatchEvalThreads, smem, stream>>>(a, max_rows);
     return cudaGetLastError();
+}
+
+cudaError_t launch_batch_evaluate_greeks(const BatchArgs& a, uint32_t max_strikes, uint32_t max_rows,
+                                         cudaStream_t stream) {
+    switch (a.degree) {  // validated to 0..4 on the host
+        case 0: return launch_batch_evaluate_greeks_d<0>(a, max_strikes, max_rows, stream);
+        case 1: return launch_batch_evaluate_greeks_d<1>(a, max_strikes, max_rows, stream);
+        case 2: return launch_batch_evaluate_greeks_d<2>(a, max_strikes, max_rows, stream);
+        case 3: return launch_batch_evaluate_greeks_d<3>(a, max_strikes, max_rows, stream);
+        default: return launch_batch_evaluate_greeks_d<4>(a, max_strikes, max_rows, stream);
+    }
 }
 
 cudaError_t launch_batch_summarize(const BatchArgs& a, cudaStream_t stream) {

@@ -34,6 +34,7 @@ struct GreeksEvalRow {
     double discount;
 };
 
+template <int D>  // == plan.degree
 __global__ void __launch_bounds__(kEvalThreads, 4) evaluate_greeks_kernel(EvalArgs a, GreeksArgs gk) {
     extern __shared__ __align__(16) unsigned char greeks_smem_raw[];
     __shared__ double gred[32 * kGreekSlots];
@@ -64,7 +65,6 @@ __global__ void __launch_bounds__(kEvalThreads, 4) evaluate_greeks_kernel(EvalAr
     const double K = plan.strike;
     const Divisor Kd = make_divisor(K);
     const uint64_t P = plan.eval_paths;
-    const int degree = plan.degree;
     const uint32_t last = rows - 1;
     double sum = 0.0, sumsq = 0.0;
     GreekSums gs;
@@ -93,7 +93,7 @@ __global__ void __launch_bounds__(kEvalThreads, 4) evaluate_greeks_kernel(EvalAr
             if (er.kind != kRuleRegression || !(spot > K)) return;
             const double intrinsic = spot - K;
             double continuation;
-            if (!predict_continuation(er.model, degree, divide(spot, Kd), &continuation)) {
+            if (!predict_continuation_d<D>(er.model, divide(spot, Kd), &continuation)) {
                 atomicMin(&a.status->eval_fail, ((unsigned long long)row << 33) | (p << 1));
                 return;
             }
@@ -177,15 +177,27 @@ size_t evaluate_greeks_smem_bytes(uint32_t rows) {
     return sizeof(double) * (257 * 2 + 64) + sizeof(GreeksEvalRow) * rows + sizeof(unsigned) * 2 * rows;
 }
 
-cudaError_t launch_evaluate_greeks(const EvalArgs& args, const GreeksArgs& greeks, int blocks, cudaStream_t stream) {
+template <int D>
+static cudaError_t launch_evaluate_greeks_d(const EvalArgs& args, const GreeksArgs& greeks, int blocks,
+                                            cudaStream_t stream) {
     const size_t smem = evaluate_greeks_smem_bytes(args.plan.rows);
     if (smem > 48 * 1024) {
         cudaError_t e =
-            cudaFuncSetAttribute(evaluate_greeks_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+            cudaFuncSetAttribute(evaluate_greeks_kernel<D>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
         if (e != cudaSuccess) return e;
     }
-    evaluate_greeks_kernel<<<blocks, kEvalThreads, smem, stream>>>(args, greeks);
+    evaluate_greeks_kernel<D><<<blocks, kEvalThreads, smem, stream>>>(args, greeks);
     return cudaGetLastError();
+}
+
+cudaError_t launch_evaluate_greeks(const EvalArgs& args, const GreeksArgs& greeks, int blocks, cudaStream_t stream) {
+    switch (args.plan.degree) {  // validated to 0..4 on the host
+        case 0: return launch_evaluate_greeks_d<0>(args, greeks, blocks, stream);
+        case 1: return launch_evaluate_greeks_d<1>(args, greeks, blocks, stream);
+        case 2: return launch_evaluate_greeks_d<2>(args, greeks, blocks, stream);
+        case 3: return launch_evaluate_greeks_d<3>(args, greeks, blocks, stream);
+        default: return launch_evaluate_greeks_d<4>(args, greeks, blocks, stream);
+    }
 }
 
 cudaError_t launch_finalize_greeks(const double2* partials, int blocks, double* out, cudaStream_t stream) {
