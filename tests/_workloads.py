@@ -190,7 +190,7 @@ def ragged_columns(contracts: int, seed: int = 41, min_paths: int = 8192, max_pa
 
 
 def ragged_request(c: RaggedColumns, *, seed: int = 41, support: int = 1, training_domain_start: int = 0,
-                   evaluation_domain_start: int = 1 << 20):
+                   evaluation_domain_start: int = 1 << 20, degree: int = 4):
     from finoptions._requests import lsm_ragged_request
 
     return lsm_ragged_request(
@@ -200,12 +200,12 @@ def ragged_request(c: RaggedColumns, *, seed: int = 41, support: int = 1, traini
         exercise_offsets=c.exercise_offsets, exercise_times=c.exercise_times, origin_exercise=0,
         training_paths=c.paths, evaluation_paths=c.paths, training_seed=seed,
         training_domain_start=training_domain_start, evaluation_seed=seed,
-        evaluation_domain_start=evaluation_domain_start, polynomial_degree=4, rank_tolerance=1e-12,
+        evaluation_domain_start=evaluation_domain_start, polynomial_degree=degree, rank_tolerance=1e-12,
         condition_limit=1e8, tie_rule=0, insufficient_exercise_support=support)
 
 
 def ragged_row_as_call(c: RaggedColumns, r: int, *, seed: int = 41, support: int = 1, training_domain: int = 0,
-                       evaluation_domain: int = 1 << 20) -> dict:
+                       evaluation_domain: int = 1 << 20, degree: int = 4) -> dict:
     """Row r of a ragged batch as single-contract arguments (the union mesh of its exercise and cash
     times, domains start + r)."""
     T, rate, q = float(c.maturities[r]), float(c.rates[r]), float(c.dividend_yields[r])
@@ -222,7 +222,7 @@ def ragged_row_as_call(c: RaggedColumns, r: int, *, seed: int = 41, support: int
         exercise_nodes=[node[t] for t in ex.tolist()], expiry_node=len(times) - 1,
         annualized_volatility=float(c.volatilities[r]), dividend_policy=0, training_paths=int(c.paths[r]),
         evaluation_paths=int(c.paths[r]), training_seed=seed, training_domain=training_domain + r,
-        evaluation_seed=seed, evaluation_domain=evaluation_domain + r, polynomial_degree=4, rank_tolerance=1e-12,
+        evaluation_seed=seed, evaluation_domain=evaluation_domain + r, polynomial_degree=degree, rank_tolerance=1e-12,
         condition_limit=1e8, tie_rule=0, insufficient_exercise_support=support)
 
 

@@ -99,6 +99,13 @@ def test_grouped_fail_policy_matches_the_oracle_or_fails_identically(native_exec
     check_against_oracle(native_executor, grouped_request(c, 1024, support=0))
 
 
+@pytest.mark.parametrize("degree", [0, 1, 3])
+def test_grouped_lower_degrees_match_the_oracle(native_executor, degree) -> None:
+    """Each regression degree runs its own instance of the batch backward and evaluation kernels."""
+    c = grouped_columns(8, strikes_per_group=5, seed=61 + degree, min_exercise=6, max_exercise=14)
+    assert check_against_oracle(native_executor, grouped_request(c, 2048, degree=degree)) is not None
+
+
 def test_grouped_tiny_populations_raise_the_oracle_error(native_executor) -> None:
     """With 8 training paths some strike has 1..4 in-the-money paths at a row: the fail policy
     raises InsufficientObservations for the lowest failing row."""

@@ -95,8 +95,9 @@ def fitted(native_executor):
     plan.close()
 
 
-def test_greeks_pass_prices_exactly_like_the_plain_entry(native_executor) -> None:
-    kwargs = contract(1 << 16)
+@pytest.mark.parametrize("degree", [4, 2])
+def test_greeks_pass_prices_exactly_like_the_plain_entry(native_executor, degree) -> None:
+    kwargs = {**contract(1 << 16), "polynomial_degree": degree}
     req = lsm_call_request(**kwargs)
     res = lsm_call_result(req.exercise_rows)
     g, d_l, d_d = lsm_call_greeks(NODES + 1, 2)

@@ -114,15 +114,16 @@ def gpu_ragged_greeks(native_executor, req, c):
     return cols.as_tuple(), delta, vega, d_l, offsets, d_d
 
 
-def test_ragged_greeks_match_the_single_contract_greeks(native_executor) -> None:
+@pytest.mark.parametrize("degree", [4, 1])
+def test_ragged_greeks_match_the_single_contract_greeks(native_executor, degree) -> None:
     from finoptions._requests import lsm_call_greeks, lsm_call_result
 
     c = ragged_columns(10, seed=53, min_paths=2048, max_paths=16384, min_exercise=4, max_exercise=24)
-    out, delta, vega, d_l, offsets, d_d = gpu_ragged_greeks(native_executor, ragged_request(c), c)
-    _, _, plain = gpu_ragged(native_executor, ragged_request(c))
+    out, delta, vega, d_l, offsets, d_d = gpu_ragged_greeks(native_executor, ragged_request(c, degree=degree), c)
+    _, _, plain = gpu_ragged(native_executor, ragged_request(c, degree=degree))
     np.testing.assert_allclose(out[0], plain[0], rtol=1e-13, atol=1e-14)
     for r in range(c.rows):
-        kw = ragged_row_as_call(c, r)
+        kw = ragged_row_as_call(c, r, degree=degree)
         req = lsm_call_request(**kw)
         res = lsm_call_result(req.exercise_rows)
         n_div = len(kw["dividend_nodes"])
