@@ -57,3 +57,34 @@ extern "C" int harness_fit(const double* x, const double* y, uint64_t n, double 
 
 // rank_limit(tol): the largest q whose correctly rounded square root is at most tol.
 extern "C" double harness_rank_limit(double tol) { return rank_limit(tol); }
+
+// predict_continuation_d<D> against predict_continuation(degree = D) on `n` predictors for a model
+// given as mean, scale, alpha[4], beta[4], coef[5]: the number of predictions whose bits or
+// success differ.
+extern "C" int harness_predict_mismatches(const double* model_in, int degree, const double* x, uint64_t n) {
+    FitModel m{};
+    m.mean = model_in[0];
+    m.scale = model_in[1];
+    m.inv_scale = make_divisor(m.scale).inv;
+    for (int i = 0; i < 4; ++i) m.alpha[i] = model_in[2 + i];
+    for (int i = 0; i < 4; ++i) m.beta[i] = model_in[6 + i];
+    for (int i = 0; i < 5; ++i) m.coef[i] = model_in[10 + i];
+    int bad = 0;
+    for (uint64_t i = 0; i < n; ++i) {
+        double a = -1.0, b = -2.0;
+        const bool ok_a = predict_continuation(m, degree, x[i], &a);
+        bool ok_b = false;
+        switch (degree) {
+            case 0: ok_b = predict_continuation_d<0>(m, x[i], &b); break;
+            case 1: ok_b = predict_continuation_d<1>(m, x[i], &b); break;
+            case 2: ok_b = predict_continuation_d<2>(m, x[i], &b); break;
+            case 3: ok_b = predict_continuation_d<3>(m, x[i], &b); break;
+            default: ok_b = predict_continuation_d<4>(m, x[i], &b); break;
+        }
+        uint64_t ba, bb;
+        __builtin_memcpy(&ba, &a, 8);
+        __builtin_memcpy(&bb, &b, 8);
+        if (ok_a != ok_b || (ok_a && ba != bb)) ++bad;
+    }
+    return bad;
+}

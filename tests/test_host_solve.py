@@ -76,3 +76,20 @@ def test_rank_limit_is_the_last_spread_the_rank_test_accepts(harness) -> None:
         q = harness.harness_rank_limit(float(tol))
         assert q >= 0.0 and math.sqrt(q) <= tol, tol
         assert math.sqrt(math.nextafter(q, math.inf)) > tol, tol
+
+
+@pytest.mark.parametrize("degree", [0, 1, 2, 3, 4])
+def test_per_degree_predictor_is_bit_identical_to_the_runtime_degree_predictor(harness, degree) -> None:
+    """The kernels that apply a fitted policy path by path are instantiated per degree
+    (predict_continuation_d<D>); each instance must predict exactly what the runtime-degree
+    predictor does, failures (non-finite predictor or prediction) included."""
+    harness.harness_predict_mismatches.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_uint64]
+    rng = np.random.default_rng(71 + degree)
+    for trial in range(20):
+        model = np.concatenate([[rng.uniform(0.8, 1.6), rng.uniform(0.02, 0.4)], rng.normal(0, 1.5, 4),
+                                rng.uniform(0.1, 2.0, 4), rng.normal(0, 5.0, 5)])
+        x = rng.uniform(0.5, 3.0, 4000)
+        x[:4] = [math.inf, -math.inf, math.nan, 1e308]
+        if trial == 0:
+            model[10] = math.inf  # non-finite prediction
+        assert harness.harness_predict_mismatches(model.ctypes.data, degree, x.ctypes.data, x.size) == 0
