@@ -162,8 +162,8 @@ struct BackwardSmem {
 // for the whole backward pass, so the only HBM traffic is one read of each stored row.
 //
 // Per exercise row k the CTA reduces its in-the-money power sums of row k and publishes them;
-// then the warps split. Warps 0..15 wait for every CTA's partial, combine them and thread 0 fits
-// row k's continuation. Meanwhile warps 16..31 take row k-1, whose spots were prefetched with
+// then the warps split. Warps 0..15 wait for every CTA's partial, combine them and warp 0 fits
+// row k's continuation (lsm_fit_warp.cuh). Meanwhile warps 16..31 take row k-1, whose spots were prefetched with
 // cp.async: its in-the-money test and the power sums T_0..T_8 of its moneyness do not depend on
 // row k's exercise decision, so they are accumulated while the grid synchronises and the fit
 // runs. After a CTA barrier every thread applies row k's exercise rule to its paths, discounts
@@ -314,16 +314,24 @@ __global__ void __launch_bounds__(kBackwardThreads, 1) backward_kernel(BackwardA
                     kind = sm.model.status == kFitOk ? kRuleRegression : kRuleFitFailed;
                 }
                 if (threadIdx.x == 0) sm.kind = kind;
-                if (threadIdx.x == 0 && blockIdx.x == 0) {
+                if (blockIdx.x == 0) {
+                    // CTA 0 writes the row's record; the model goes out as twelve 16-byte words from
+                    // as many lanes (a one-thread copy made CTA 0 the last to arrive at the next sync).
                     FitRecord& rec = a.records[row];
-                    rec.kind = kind;
-                    rec.itm = population;
-                    rec.pivot = fit_pivot;
-                    rec.model = sm.model;
-                    rec.origin_exercise = 0;
-                    rec.origin_continuation = 0.0;
-                    rec.diag_status = -1;
-                    if (kind == kRuleFitFailed) atomicMin(&a.status->fit_failed_order, order);
+                    constexpr int kModelWords = int(sizeof(FitModel) / sizeof(double2));
+                    static_assert(sizeof(FitModel) % sizeof(double2) == 0, "FitModel is 16-byte aligned");
+                    if (threadIdx.x < kModelWords)
+                        reinterpret_cast<double2*>(&rec.model)[threadIdx.x] =
+                            reinterpret_cast<const double2*>(&sm.model)[threadIdx.x];
+                    if (threadIdx.x == 0) {
+                        rec.kind = kind;
+                        rec.itm = population;
+                        rec.pivot = fit_pivot;
+                        rec.origin_exercise = 0;
+                        rec.origin_continuation = 0.0;
+                        rec.diag_status = -1;
+                        if (kind == kRuleFitFailed) atomicMin(&a.status->fit_failed_order, order);
+                    }
                 }
             }
         } else if (stage_next) {
