@@ -5,8 +5,8 @@ from __future__ import annotations
 import ctypes
 from array import array
 from collections.abc import Sequence
-from itertools import chain
 from dataclasses import dataclass
+from itertools import chain
 from typing import Any
 
 import numpy as np
