@@ -3,6 +3,7 @@
 from __future__ import annotations
 
 import ctypes
+import struct
 from array import array
 from collections.abc import Sequence
 from dataclasses import dataclass
@@ -118,7 +119,27 @@ def lsm_call_request(
     return CallRequest(q, floats + nodes, en[1])
 
 
-_DIAGNOSTIC = np.dtype(_abi.FoLsmNodeDiagnostic)
+def _record_format(structure: type) -> struct.Struct:
+    """A little-endian struct.Struct that reads `structure` (a ctypes.Structure of scalar fields)
+    field by field, with the padding its ctypes offsets imply."""
+    codes = {ctypes.c_uint32: "I", ctypes.c_int32: "i", ctypes.c_uint64: "Q", ctypes.c_int64: "q",
+             ctypes.c_double: "d"}
+    fmt, at = "<", 0
+    for name, ctype in structure._fields_:
+        offset = getattr(structure, name).offset
+        fmt += f"{offset - at}x" if offset > at else ""
+        fmt += codes[ctype]
+        at = offset + ctypes.sizeof(ctype)
+    size = ctypes.sizeof(structure)
+    fmt += f"{size - at}x" if size > at else ""
+    packed = struct.Struct(fmt)
+    if packed.size != size:  # pragma: no cover - the layout is fixed by the C header
+        msg = f"{structure.__name__}: format {fmt} reads {packed.size} bytes of {size}"
+        raise ImportError(msg)
+    return packed
+
+
+_DIAGNOSTIC = _record_format(_abi.FoLsmNodeDiagnostic)
 if array("d").itemsize != 8 or array("I").itemsize != 4:  # pragma: no cover - every supported platform
     msg = "array.array('d'/'I') must be binary64 / 32-bit to back the C ABI's double / uint32_t arrays"
     raise ImportError(msg)
@@ -149,7 +170,11 @@ class CallResult:
     def rows(self) -> list[tuple]:
         """The diagnostics as plain tuples (node, kind code, exercise, estimated continuation,
         in-the-money paths, observations, columns, rank, condition, predictor mean, scale)."""
-        return np.frombuffer(self.diagnostics, dtype=_DIAGNOSTIC, count=self.struct.n_diagnostics).tolist()
+        n = self.struct.n_diagnostics
+        if n > len(self.diagnostics):
+            msg = f"native result reports {n} diagnostics for a buffer of {len(self.diagnostics)}"
+            raise ValueError(msg)
+        return list(_DIAGNOSTIC.iter_unpack(memoryview(self.diagnostics).cast("B")[: n * _DIAGNOSTIC.size]))
 
     def as_tuple(self) -> tuple:
         """NativeLsmResult-shaped tuple (crates/finoptions-python/src/lib.rs:1074-1082)."""

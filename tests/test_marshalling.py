@@ -138,3 +138,19 @@ def test_records_built_from_rows_equal_the_records_of_the_native_tuples() -> Non
     assert [type(x).__name__ for x in got] == ["OriginDecisionDiagnostics", "NoInTheMoneyPathsDiagnostics",
                                                "InsufficientExerciseSupportDiagnostics",
                                                "RegressionFitDiagnostics", "RegressionFitDiagnostics"]
+
+
+def test_diagnostic_rows_read_the_ctypes_layout() -> None:
+    res = lsm_call_result(6)
+    r = res.struct
+    r.n_diagnostics = 6
+    for i in range(6):
+        d = res.diagnostics[i]
+        d.node, d.kind, d.exercise, d.estimated_continuation = i, i % 4, i & 1, 0.5 * i
+        d.in_the_money_paths, d.observations, d.columns, d.rank = 2**32 - 1 - i, 2**40 + i, 5, 4
+        d.condition_number, d.predictor_mean, d.predictor_scale = 1e8 - i, -1.5 * i, 2.0**-i
+    expected = np.frombuffer(res.diagnostics, dtype=np.dtype(_abi.FoLsmNodeDiagnostic), count=6).tolist()
+    assert res.rows() == expected
+    r.n_diagnostics = 7  # more than the buffer holds
+    with pytest.raises(ValueError, match="7 diagnostics"):
+        res.rows()
