@@ -42,17 +42,9 @@ KERNEL_NAMES = ("simulate_kernel", "backward_kernel", "diagnose_kernel", "evalua
 
 
 def workload_kwargs(paths: int = PATHS) -> dict:
-    t = [i / STEPS_IN_GRID for i in range(STEPS_IN_GRID + 1)]
-    return dict(
-        initial_spot=100.0, strike=100.0, schedule_times=t, curve_times=t,
-        log_discounts=[0.0 if i == 0 else -0.04 * t[i] for i in range(STEPS_IN_GRID + 1)],
-        dividend_yield_times=t,
-        cumulative_dividend_yields=[0.0 if i == 0 else 0.02 * t[i] for i in range(STEPS_IN_GRID + 1)],
-        dividend_nodes=[], dividend_amounts=[], exercise_nodes=list(range(STEPS_IN_GRID)),
-        expiry_node=STEPS_IN_GRID, annualized_volatility=0.25, dividend_policy=0, training_paths=paths,
-        evaluation_paths=paths, training_seed=11, training_domain=1, evaluation_seed=11, evaluation_domain=2,
-        polynomial_degree=4, rank_tolerance=1e-12, condition_limit=1e8, tie_rule=0, insufficient_exercise_support=0,
-    )
+    import _workloads
+
+    return _workloads.weekly_call_kwargs(paths)
 
 
 def path_steps(paths: int = PATHS) -> int:
@@ -165,6 +157,51 @@ def oracle_price(kwargs: dict, threads: int) -> tuple:
     from finoptions._requests import lsm_call_request
 
     return _oracle.price_lsm_call(lsm_call_request(**kwargs), threads)
+
+
+def public_call_arguments(kw: dict, executor) -> dict:
+    """finoptions.price_lsm_call's arguments for a contract given as single-contract kwargs."""
+    import finoptions as fo
+
+    times = tuple(kw["schedule_times"])
+    schedule = fo.EventSchedule(
+        times=times,
+        dividends=tuple(fo.CashDividend(node=int(n), amount=float(a))
+                        for n, a in zip(kw["dividend_nodes"], kw["dividend_amounts"], strict=True)),
+        exercise_nodes=tuple(int(n) for n in kw["exercise_nodes"]), expiry_node=int(kw["expiry_node"]))
+    support = (fo.InsufficientExerciseSupportPolicy.CONTINUE if kw["insufficient_exercise_support"]
+               else fo.InsufficientExerciseSupportPolicy.FAIL)
+    return dict(
+        initial_spot=float(kw["initial_spot"]), strike=float(kw["strike"]), schedule=schedule,
+        curve=fo.LogDiscountCurve(times=times, log_discounts=tuple(float(v) for v in kw["log_discounts"])),
+        dividend_yield_curve=fo.CumulativeDividendYieldCurve(
+            times=times, cumulative_yields=tuple(float(v) for v in kw["cumulative_dividend_yields"])),
+        volatility=fo.ConstantVolatility(float(kw["annualized_volatility"])),
+        dividend_policy=fo.DividendPolicy.LIQUIDATOR, executor=executor,
+        method=fo.Lsm(training_paths=int(kw["training_paths"]), evaluation_paths=int(kw["evaluation_paths"]),
+                      training_stream=fo.RandomStream(seed=int(kw["training_seed"]), domain=int(kw["training_domain"])),
+                      evaluation_stream=fo.RandomStream(seed=int(kw["evaluation_seed"]),
+                                                        domain=int(kw["evaluation_domain"])),
+                      insufficient_exercise_support=support))
+
+
+def one_by_one(calls: list[dict], batch_prices, batch_errors) -> dict:
+    """Prices the contracts one call at a time through finoptions.price_lsm_call (host inputs, host
+    results, every call synchronous) and checks each against its batch row: the same populations,
+    so the same price and standard error."""
+    import finoptions as fo
+    import numpy as np
+
+    fo.price_lsm_call(**calls[0])
+    t0 = time.perf_counter()
+    results = [fo.price_lsm_call(**a) for a in calls]
+    wall = time.perf_counter() - t0
+    prices = np.array([r.price for r in results])
+    errors = np.array([r.standard_error for r in results])
+    return {"contracts": len(calls), "seconds": wall, "contracts_per_s": len(calls) / wall,
+            "api": "finoptions.price_lsm_call(executor=CudaExecutor), one contract per call",
+            "max_rel_price_difference_vs_batch": float(np.max(np.abs(prices - batch_prices) / np.abs(batch_prices))),
+            "max_rel_se_difference_vs_batch": float(np.max(np.abs(errors - batch_errors) / np.abs(batch_errors)))}
 
 
 # ---- our arm -----------------------------------------------------------------------------------
@@ -408,6 +445,21 @@ def run_ragged(args: argparse.Namespace, executor) -> dict:
                      "kernels_ms": {n: round(v / calls, 3) for n, v in zip(names, kernel_ms, strict=True)},
                      "gpu_launches_per_call": int(launches.value)}
     out["greeks_overhead"] = out["price_and_greeks"]["device_ms_per_call"] / out["plain"]["device_ms_per_call"]
+    # The north-star comparison: the same contracts (same populations, so the same price and SE)
+    # priced one by one on the plain per-contract path, against the batched price + Greeks call.
+    import finoptions as fo
+
+    api_executor = fo.CudaExecutor(device=executor.device)
+    calls = [public_call_arguments(_workloads.ragged_row_as_call(c, r), api_executor) for r in range(c.rows)]
+    plain = one_by_one(calls, np.array(result.as_tuple()[0]), np.array(result.as_tuple()[2]))
+    out["plain_per_contract"] = plain
+    out["batched_vs_plain_same_contracts"] = {
+        "batched": "fo_price_lsm_ragged_f64 with the adjoint Greeks, host columns in and out",
+        "plain": plain["api"],
+        "batched_contracts_per_s": out["price_and_greeks"]["e2e_contracts_per_s"],
+        "plain_contracts_per_s": plain["contracts_per_s"],
+        "ratio": out["price_and_greeks"]["e2e_contracts_per_s"] / plain["contracts_per_s"],
+    }
     out["sample_greeks"] = {"delta_row0": float(arrays["delta"][0]), "vega_row0": float(arrays["vega"][0])}
     threads = cpu_threads()
     t0 = time.perf_counter()
@@ -502,6 +554,7 @@ GROUPED_STATES = 4096
 GROUPED_STRIKES = 8
 GROUPED_PATHS = 32768
 GROUPED_SAMPLE_STATES = 48
+GROUPED_PLAIN_SAMPLE = 1024
 
 
 def grouped_algorithmic_bytes(c, paths: int) -> dict:
@@ -582,6 +635,18 @@ def run_grouped(args: argparse.Namespace, executor) -> dict:
                          "algorithmic_bytes": b, "achieved_gbs": round(b / (per / 1e3) / 1e9, 1) if b else 0.0}
     dominant = max(algorithmic, key=lambda k: kernels[k]["ms_per_call"])
     achieved = algorithmic[dominant] / (kernels[dominant]["ms_per_call"] / 1e3) / 1e9
+    # The same contracts one by one on the plain per-contract path: the first GROUPED_PLAIN_SAMPLE
+    # rows (whole states), each repricing its state's populations (same price and SE as the batch).
+    import finoptions as fo
+    import numpy as np
+
+    api_executor = fo.CudaExecutor(device=executor.device)
+    sample_rows = min(contracts, GROUPED_PLAIN_SAMPLE)
+    calls = [public_call_arguments(_workloads.grouped_row_as_call(cols, r, GROUPED_PATHS), api_executor)
+             for r in range(sample_rows)]
+    plain = one_by_one(calls, np.array(result.as_tuple()[0][:sample_rows]), np.array(result.as_tuple()[2][:sample_rows]))
+    plain["sample"] = f"the first {sample_rows} of the {contracts} contracts ({sample_rows // GROUPED_STRIKES} states)"
+    e2e_contracts_per_s = contracts * steps / wall
     # CPU restatement of the reference's group-parallel CpuExecutor on a bounded sample of states.
     threads = cpu_threads()
     sample = _workloads.grouped_columns(GROUPED_SAMPLE_STATES, GROUPED_STRIKES, seed=23)
@@ -610,6 +675,11 @@ def run_grouped(args: argparse.Namespace, executor) -> dict:
                      "peak_source": peak_kind, "unit": "GB/s", "frac": round(achieved / hbm_peak, 4),
                      "traffic": batch_traffic(dominant, algorithmic[dominant])},
         "clocks": clocks.report(),
+        "plain_per_contract": plain,
+        "batched_vs_plain_same_contracts": {
+            "batched": "fo_price_lsm_grouped_f64, host columns in and out", "plain": plain["api"],
+            "batched_contracts_per_s": e2e_contracts_per_s, "plain_contracts_per_s": plain["contracts_per_s"],
+            "ratio": e2e_contracts_per_s / plain["contracts_per_s"]},
         "cpu_baseline": {"contracts_per_s": GROUPED_SAMPLE_STATES * GROUPED_STRIKES / cpu_s,
                          "path_steps_per_s": _workloads.path_steps(sample, GROUPED_PATHS) / cpu_s, "cores": threads,
                          "kind": "port", "sample": f"the first {GROUPED_SAMPLE_STATES} states of the workload "
@@ -634,25 +704,28 @@ def cpu_baseline(paths: int = PATHS) -> dict:
 
 
 def run_reference(args: argparse.Namespace) -> dict | None:
+    """The reference's CpuExecutor path (its CPU restatement; the Rust reference cannot be built
+    here) on every host thread: each step prices the full workload contract, 2^20 + 2^20 paths,
+    the configuration the line names."""
     rank, world, _ = dist_info()
     if rank != 0:
         return None
     threads = cpu_threads()
-    sample_paths = 1 << 18
-    kwargs = workload_kwargs(sample_paths)
+    paths = args.paths
+    kwargs = workload_kwargs(paths)
     for _ in range(args.warmup):
         oracle_price(kwargs, threads)
     t0 = time.perf_counter()
     for _ in range(args.steps):
         oracle_price(kwargs, threads)
     seconds = time.perf_counter() - t0
-    value = path_steps(sample_paths) * args.steps / seconds
-    sample = (f"each step prices the workload contract at 2^18 + 2^18 paths (1/4 of a full step) on {threads} "
-              "host threads with the CPU restatement of the reference engine (the Rust reference cannot be built here)")
+    value = path_steps(paths) * args.steps / seconds
+    sample = (f"each step prices the whole workload contract ({paths} + {paths} paths) on {threads} host threads "
+              "with the CPU restatement of the reference engine (path-parallel simulation, serial fit and evaluation)")
     return {
         "metric": METRIC, "value": value, "unit": UNIT, "impl": "reference", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": seconds / args.steps * 1e3, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": config(),
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": config(paths),
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
@@ -661,7 +734,8 @@ def run_reference(args: argparse.Namespace) -> dict | None:
 def main() -> None:
     parser = argparse.ArgumentParser(description=__doc__.splitlines()[0])
     parser.add_argument("--gpus", type=int, default=1)
-    parser.add_argument("--steps", type=int, default=200)
+    parser.add_argument("--steps", type=int, default=None,
+                        help="timed steps (default 200; 10 for --impl reference, whose steps take seconds each)")
     parser.add_argument("--warmup", type=int, default=5)
     parser.add_argument("--impl", choices=("ours", "reference"), default="ours")
     parser.add_argument("--paths", type=int, default=PATHS, help="paths per role (profiling captures shrink it)")
@@ -675,6 +749,8 @@ def main() -> None:
     args = parser.parse_args()
     if args.paths < 2:
         parser.error("--paths must be at least 2")
+    if args.steps is None:
+        args.steps = 10 if args.impl == "reference" else 200
     if args.warmup < 3:
         args.warmup = 3
     out = run_reference(args) if args.impl == "reference" else run_ours(args)

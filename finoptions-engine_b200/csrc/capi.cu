@@ -52,6 +52,7 @@ struct fo_lsm_call_plan {
     bool run_eval = true;
     int backward_blocks = 0;
     int ppt = 0;
+    bool backward_hbm = false;   // the backward pass keeps its values in HBM (after the slab)
     int eval_blocks = 0;
     uint32_t first_stored_row = 0;
     PlanLayout lay{};
@@ -91,7 +92,8 @@ Error open_device(int device, fo_executor* ex) {
                               " device(s) are visible");
     cudaDeviceProp prop{};
     FO_CUDA_TRY(cudaGetDeviceProperties(&prop, device), "cudaGetDeviceProperties");
-    if (prop.major != 10)
+    // The library holds sm_100a code only: another 10.x part would fail at its first launch.
+    if (prop.major != 10 || prop.minor != 0)
         return make_error(FO_ERR_EXECUTION, FO_CODE_UNSUPPORTED_DEVICE,
                           std::string("CudaExecutor requires an sm_100 (Blackwell B200) device; device ") +
                               std::to_string(device) + " is " + prop.name + " (sm_" + std::to_string(prop.major) +
@@ -113,19 +115,20 @@ Error open_device(int device, fo_executor* ex) {
     return Error{};
 }
 
-// Chooses the persistent grid (at most one CTA per SM) and the paths per thread whose values and
-// spots the backward kernel keeps in shared memory.
-Error choose_backward_shape(const fo_executor* ex, uint64_t paths, int* blocks, int* ppt) {
+// Chooses the persistent grid (at most one CTA per SM) and the paths per thread of the backward
+// pass. Populations up to the on-chip capacity (148 SMs x 1024 threads x the paths per thread
+// whose values and two spot rows fit in shared memory) keep them on chip; larger ones (*hbm) keep
+// the values in HBM and read the spots from the stored rows, on the whole grid.
+Error choose_backward_shape(const fo_executor* ex, uint64_t paths, int* blocks, int* ppt, bool* hbm) {
     const uint64_t threads = kBackwardThreads;
     const uint64_t max_blocks = uint64_t(ex->backward_blocks_max);
     const uint64_t max_ppt = uint64_t(ex->backward_max_ppt);
     uint64_t per_thread = (paths + max_blocks * threads - 1) / (max_blocks * threads);
     if (per_thread == 0) per_thread = 1;
-    if (per_thread > max_ppt)
+    *hbm = per_thread > max_ppt;
+    if (per_thread > uint64_t(INT32_MAX))
         return make_error(FO_ERR_EXECUTION, FO_CODE_CAPACITY_EXCEEDED,
-                          "training population of " + std::to_string(paths) +
-                              " paths exceeds the on-chip backward pass capacity of " +
-                              std::to_string(max_blocks * threads * max_ppt) + " paths on this device");
+                          "training population of " + std::to_string(paths) + " paths is too large for one device");
     *ppt = int(per_thread);
     *blocks = int(std::max<uint64_t>(1, (paths + threads * per_thread - 1) / (threads * per_thread)));
     return Error{};
@@ -253,7 +256,7 @@ Error plan_create(fo_executor* ex, const fo_lsm_call_request& q, bool own_memory
                                       "paths in one random domain; observed " + std::to_string(q.evaluation_paths));
     }
     plan->run_eval = plan->eval_error.ok();
-    e = choose_backward_shape(ex, hp.train_paths, &plan->backward_blocks, &plan->ppt);
+    e = choose_backward_shape(ex, hp.train_paths, &plan->backward_blocks, &plan->ppt, &plan->backward_hbm);
     if (!e.ok()) return e;
     const uint64_t eval_threads = kEvalThreads;
     const uint64_t eval_needed = plan->run_eval ? (hp.eval_paths + eval_threads - 1) / eval_threads : 1;
@@ -278,9 +281,17 @@ Error plan_create(fo_executor* ex, const fo_lsm_call_request& q, bool own_memory
         plan->h_out = ex->staging.ptr;
     }
     const uint64_t stored_rows = hp.rows() - plan->first_stored_row;
-    const size_t slab_bytes = sizeof(double) * stored_rows * hp.train_paths;
+    const size_t slab_bytes = sizeof(double) * stored_rows * hp.train_paths +
+                              (plan->backward_hbm ? sizeof(double) * hp.train_paths : 0);
     e = ex->slab.reserve(std::max<size_t>(slab_bytes, 8));
-    if (!e.ok()) return e;
+    if (!e.ok()) {
+        if (e.code == FO_CODE_CUDA_FAILURE)
+            return make_error(FO_ERR_EXECUTION, FO_CODE_CAPACITY_EXCEEDED,
+                              "training paths need " + std::to_string(slab_bytes) +
+                                  " bytes of device memory (paths x stored rows x 8 bytes), more than the device can "
+                                  "allocate: " + e.message);
+        return e;
+    }
     plan->d_slab = static_cast<double*>(ex->slab.ptr);
     unsigned char* dev = static_cast<unsigned char*>(plan->d_block);
     plan->dp = device_plan(hp, L, dev, plan->first_stored_row);
@@ -327,6 +338,9 @@ Error plan_launch(fo_lsm_call_plan* plan) {
     b.records = records;
     b.status = status;
     b.ppt = plan->ppt;
+    b.values = plan->backward_hbm
+                   ? plan->d_slab + uint64_t(plan->hp.rows() - plan->first_stored_row) * plan->hp.train_paths
+                   : nullptr;
     FO_CUDA_TRY(launch_backward(b, plan->backward_blocks, plan->ppt, s), "backward launch");
     FO_CUDA_TRY(mark(2), "event");
     // K3 diagnostics: nothing on the device reads them, so they run on the side stream next to
@@ -719,6 +733,56 @@ Error plan_revalue(fo_lsm_call_plan* plan, const fo_lsm_call_request& q, fo_lsm_
     return plan_collect(plan, result);
 }
 
+// Re-runs the evaluation of the plan's fitted policy on its current market with every path's
+// stopping row recorded, and copies those rows to the host: the per-path record that counts the
+// decisions in which two implementations differ.
+Error plan_stopping_rows(fo_lsm_call_plan* plan, uint32_t* rows_out, uint64_t capacity) {
+    if (!plan->fitted)
+        return make_error(FO_ERR_EXECUTION, FO_CODE_INVALID_ARGUMENT, "the plan has no fitted policy; launch it first");
+    if (!plan->run_eval) return plan->eval_error;
+    const uint64_t n = plan->hp.eval_paths;
+    if (!rows_out || capacity < n)
+        return make_error(FO_ERR_EXECUTION, FO_CODE_INVALID_ARGUMENT,
+                          "stopping rows need " + std::to_string(n) + " entries; capacity is " + std::to_string(capacity));
+    fo_executor* ex = plan->ex;
+    cudaStream_t s = ex->stream;
+    const PlanLayout& L = plan->lay;
+    unsigned char* dev = static_cast<unsigned char*>(plan->d_block);
+    FitRecord origin{};
+    FO_CUDA_TRY(cudaMemcpyAsync(&origin, dev + L.records, sizeof(FitRecord), cudaMemcpyDeviceToHost, s), "record copy");
+    FO_CUDA_TRY(cudaStreamSynchronize(s), "record copy");
+    if (plan->hp.origin_row && origin.kind == kRuleOrigin && origin.origin_exercise) {
+        // LsmEvaluation::deterministic (policy.rs:657-669): every path stops at the origin row.
+        std::fill(rows_out, rows_out + n, 0u);
+        return Error{};
+    }
+    DeviceBuffer stops;
+    Error e = stops.reserve(sizeof(uint32_t) * n);
+    if (!e.ok()) return e;
+    auto* status = reinterpret_cast<DeviceStatus*>(dev + L.status);
+    FO_CUDA_TRY(cudaMemsetAsync(&status->eval_sim_fail, 0xff, sizeof(unsigned long long), s), "reset");
+    FO_CUDA_TRY(cudaMemsetAsync(&status->eval_fail, 0xff, 2 * sizeof(unsigned long long), s), "reset");
+    FO_CUDA_TRY(cudaMemsetAsync(dev + L.counts, 0, sizeof(unsigned) * plan->hp.rows(), s), "reset");
+    FO_CUDA_TRY(cudaMemsetAsync(dev + L.itm_counts, 0, sizeof(unsigned) * plan->hp.rows(), s), "reset");
+    EvalArgs a{};
+    a.plan = plan->dp;
+    a.records = reinterpret_cast<const FitRecord*>(dev + L.records);
+    a.partials = reinterpret_cast<double2*>(dev + L.eval_partials);
+    a.counts = reinterpret_cast<unsigned*>(dev + L.counts);
+    a.itm_counts = reinterpret_cast<unsigned*>(dev + L.itm_counts);
+    a.status = status;
+    a.stops = static_cast<uint32_t*>(stops.ptr);
+    FO_CUDA_TRY(launch_evaluate(a, plan->eval_blocks, s), "stopping-row evaluation launch");
+    DeviceStatus st{};
+    FO_CUDA_TRY(cudaMemcpyAsync(rows_out, stops.ptr, sizeof(uint32_t) * n, cudaMemcpyDeviceToHost, s), "stops copy");
+    FO_CUDA_TRY(cudaMemcpyAsync(&st, status, sizeof(DeviceStatus), cudaMemcpyDeviceToHost, s), "status copy");
+    FO_CUDA_TRY(cudaStreamSynchronize(s), "stopping-row evaluation");
+    if (st.eval_sim_fail != kNone || st.eval_fail != kNone || st.eval_terminal_fail != kNone)
+        return make_error(FO_ERR_LSM, FO_CODE_INVALID_ARGUMENT,
+                          "the plan's evaluation fails on its current market; price it for the typed error");
+    return Error{};
+}
+
 Error enable_greeks(fo_lsm_call_plan* plan, bool enabled) {
     if (enabled && plan->gk.dividends > uint32_t(kMaxGreekDividends))
         return make_error(FO_ERR_EXECUTION, FO_CODE_CAPACITY_EXCEEDED,
@@ -895,6 +959,14 @@ int fo_lsm_call_plan_greeks(fo_lsm_call_plan* plan, fo_lsm_call_greeks* greeks, 
     if (!e.ok()) return finish(err, e);
     std::lock_guard<std::mutex> lock(plan->ex->mu);
     return finish(err, plan_greeks(plan, greeks));
+}
+
+int fo_lsm_call_plan_stopping_rows(fo_lsm_call_plan* plan, uint32_t* rows, uint64_t capacity, fo_error* err) {
+    Error e = require(plan, "plan");
+    if (!e.ok()) return finish(err, e);
+    std::lock_guard<std::mutex> lock(plan->ex->mu);
+    cudaSetDevice(plan->ex->device);
+    return finish(err, plan_stopping_rows(plan, rows, capacity));
 }
 
 int fo_lsm_call_plan_revalue_f64(fo_lsm_call_plan* plan, const fo_lsm_call_request* market, fo_lsm_call_result* result,
@@ -1085,44 +1157,63 @@ namespace {
 static __device__ __align__(256) unsigned char g_noalloc_scratch[FO_NOALLOC_SCRATCH_BYTES];
 
 std::mutex g_noalloc_mu;
-void* g_noalloc_address[256] = {};
 
-// The array's device address on the current device, looked up once per device. In host code the
-// symbol is only a host-side stand-in, never a device address.
-Error noalloc_scratch(int device, unsigned char** out) {
+// What the allocation-free entry needs to know about a device, looked up on its first call there
+// (with the device current) and kept: the array's device address - in host code the symbol is only
+// a host-side stand-in, never a device address - and the launch shapes.
+struct NoallocDevice {
+    bool ready = false;
+    unsigned char* scratch = nullptr;
+    int sms = 0;
+    int backward_blocks_max = 0;
+    int backward_max_ppt = 0;
+};
+NoallocDevice g_noalloc_devices[256];
+
+Error noalloc_device(int device, NoallocDevice* out) {
     if (device < 0 || device >= 256)
         return make_error(FO_ERR_EXECUTION, FO_CODE_NO_DEVICE, "device ordinal outside the supported range");
     std::lock_guard<std::mutex> lock(g_noalloc_mu);
-    if (!g_noalloc_address[device]) {
+    NoallocDevice& d = g_noalloc_devices[device];
+    if (!d.ready) {
+        int major = 0, minor = 0, cooperative = 0;
+        FO_CUDA_TRY(cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, device), "cudaDeviceGetAttribute");
+        FO_CUDA_TRY(cudaDeviceGetAttribute(&minor, cudaDevAttrComputeCapabilityMinor, device), "cudaDeviceGetAttribute");
+        FO_CUDA_TRY(cudaDeviceGetAttribute(&cooperative, cudaDevAttrCooperativeLaunch, device), "cudaDeviceGetAttribute");
+        if (major != 10 || minor != 0)
+            return make_error(FO_ERR_EXECUTION, FO_CODE_UNSUPPORTED_DEVICE,
+                              "allocation-free pricing requires an sm_100 (Blackwell B200) device; device " +
+                                  std::to_string(device) + " is sm_" + std::to_string(major) + std::to_string(minor));
+        if (!cooperative)
+            return make_error(FO_ERR_EXECUTION, FO_CODE_UNSUPPORTED_DEVICE, "device does not support cooperative launches");
         void* p = nullptr;
         const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
         if (e != cudaSuccess) return cuda_error(e, "cudaGetSymbolAddress of the allocation-free scratch");
-        g_noalloc_address[device] = p;
+        FO_CUDA_TRY(cudaDeviceGetAttribute(&d.sms, cudaDevAttrMultiProcessorCount, device), "cudaDeviceGetAttribute");
+        d.scratch = static_cast<unsigned char*>(p);
+        d.backward_blocks_max = backward_max_blocks(device);
+        d.backward_max_ppt = backward_max_ppt();
+        d.ready = true;
     }
-    *out = static_cast<unsigned char*>(g_noalloc_address[device]);
+    *out = d;
     return Error{};
 }
 
 Error price_noalloc(const fo_lsm_call_request& q, cudaStream_t stream, fo_lsm_call_result* result) {
     int device = 0;
     FO_CUDA_TRY(cudaGetDevice(&device), "cudaGetDevice");
-    cudaDeviceProp prop{};
-    FO_CUDA_TRY(cudaGetDeviceProperties(&prop, device), "cudaGetDeviceProperties");
-    if (prop.major != 10)
-        return make_error(FO_ERR_EXECUTION, FO_CODE_UNSUPPORTED_DEVICE,
-                          std::string("allocation-free pricing requires an sm_100 (Blackwell B200) device; device ") +
-                              std::to_string(device) + " is " + prop.name);
-    unsigned char* scratch = nullptr;
-    Error e = noalloc_scratch(device, &scratch);
+    NoallocDevice dev_info;
+    Error e = noalloc_device(device, &dev_info);
     if (!e.ok()) return e;
+    unsigned char* scratch = dev_info.scratch;
     // A stack executor carries the caller's stream and the device's launch shapes; it owns no
     // memory and creates nothing.
     fo_executor shadow;
     shadow.device = device;
-    shadow.sms = prop.multiProcessorCount;
+    shadow.sms = dev_info.sms;
     shadow.stream = stream;
-    shadow.backward_blocks_max = backward_max_blocks(device);
-    shadow.backward_max_ppt = backward_max_ppt();
+    shadow.backward_blocks_max = dev_info.backward_blocks_max;
+    shadow.backward_max_ppt = dev_info.backward_max_ppt;
     shadow.eval_blocks_per_sm = 8;
     fo_lsm_call_plan plan;
     plan.ex = &shadow;
@@ -1138,7 +1229,7 @@ Error price_noalloc(const fo_lsm_call_request& q, cudaStream_t stream, fo_lsm_ca
                                      "paths in one random domain; observed " + std::to_string(q.evaluation_paths));
     }
     plan.run_eval = plan.eval_error.ok();
-    e = choose_backward_shape(&shadow, hp.train_paths, &plan.backward_blocks, &plan.ppt);
+    e = choose_backward_shape(&shadow, hp.train_paths, &plan.backward_blocks, &plan.ppt, &plan.backward_hbm);
     if (!e.ok()) return e;
     const uint64_t eval_needed = plan.run_eval ? (hp.eval_paths + kEvalThreads - 1) / kEvalThreads : 1;
     plan.eval_blocks = int(std::max<uint64_t>(1, std::min<uint64_t>(eval_needed, uint64_t(shadow.sms) * 8)));
@@ -1146,7 +1237,8 @@ Error price_noalloc(const fo_lsm_call_request& q, cudaStream_t stream, fo_lsm_ca
     plan.lay = layout_for(hp, plan.backward_blocks, plan.eval_blocks);
     const PlanLayout& L = plan.lay;
     const uint64_t stored_rows = hp.rows() - plan.first_stored_row;
-    const uint64_t slab_bytes = uint64_t(sizeof(double)) * stored_rows * hp.train_paths;
+    const uint64_t slab_bytes = uint64_t(sizeof(double)) * stored_rows * hp.train_paths +
+                                (plan.backward_hbm ? uint64_t(sizeof(double)) * hp.train_paths : 0);
     const uint64_t needed = uint64_t(L.total) + slab_bytes;
     if (needed > FO_NOALLOC_SCRATCH_BYTES)
         return make_error(FO_ERR_EXECUTION, FO_CODE_CAPACITY_EXCEEDED,

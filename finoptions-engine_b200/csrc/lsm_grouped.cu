@@ -1054,7 +1054,7 @@ Error validate_request(const BatchView& v, const fo_batch_result_columns* out) {
     if (!e.ok()) return e;
     e = validate_mesh_domain(v);
     if (!e.ok()) return e;
-    if (out->rows != v.rows())
+    if (out && out->rows != v.rows())
         return make_error(FO_ERR_EXECUTION, FO_CODE_INVALID_ARGUMENT,
                           "result columns hold " + u(out->rows) + " rows; the batch has " + u(v.rows()));
     return Error{};
@@ -1529,7 +1529,7 @@ Error validate_ragged(const fo_lsm_ragged_request& q, const fo_batch_result_colu
     streams.evaluation_domain_start = q.evaluation_domain_start;
     e = validate_streams(streams, rows);
     if (!e.ok()) return e;
-    if (out->rows != rows)
+    if (out && out->rows != rows)
         return make_error(FO_ERR_EXECUTION, FO_CODE_INVALID_ARGUMENT,
                           "result columns hold " + u(out->rows) + " rows; the batch has " + u(rows));
     return Error{};
@@ -1657,6 +1657,31 @@ int fo_price_lsm_ragged_f64(fo_executor* executor, const fo_lsm_ragged_request* 
     if (ce != cudaSuccess) return finish(err, cuda_error(ce, "cudaSetDevice"));
     try {
         return finish(err, price_ragged(executor, *request, out, greeks));
+    } catch (const std::bad_alloc&) {
+        return finish(err, make_error(FO_ERR_EXECUTION, FO_CODE_CAPACITY_EXCEEDED, "host memory exhausted"));
+    }
+}
+
+int fo_validate_lsm_grouped_f64(const fo_lsm_grouped_request* request, int32_t grouped, fo_error* err) {
+    if (!request)
+        return finish(err, make_error(FO_ERR_EXECUTION, FO_CODE_INVALID_ARGUMENT, "request must not be NULL"));
+    if (grouped && !request->group_offsets && request->n_group_offsets)
+        return finish(err, make_error(FO_ERR_EXECUTION, FO_CODE_INVALID_ARGUMENT, "group offsets must not be NULL"));
+    if (!grouped && request->group_offsets)
+        return finish(err, make_error(FO_ERR_EXECUTION, FO_CODE_INVALID_ARGUMENT,
+                                      "a row-addressed batch takes no group offsets"));
+    try {
+        return finish(err, validate_request(BatchView{request, grouped != 0}, nullptr));
+    } catch (const std::bad_alloc&) {
+        return finish(err, make_error(FO_ERR_EXECUTION, FO_CODE_CAPACITY_EXCEEDED, "host memory exhausted"));
+    }
+}
+
+int fo_validate_lsm_ragged_f64(const fo_lsm_ragged_request* request, fo_error* err) {
+    if (!request)
+        return finish(err, make_error(FO_ERR_EXECUTION, FO_CODE_INVALID_ARGUMENT, "request must not be NULL"));
+    try {
+        return finish(err, validate_ragged(*request, nullptr));
     } catch (const std::bad_alloc&) {
         return finish(err, make_error(FO_ERR_EXECUTION, FO_CODE_CAPACITY_EXCEEDED, "host memory exhausted"));
     }

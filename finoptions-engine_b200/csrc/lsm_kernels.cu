@@ -157,9 +157,12 @@ struct BackwardSmem {
     int wait_failed;
 };
 
-// Each thread owns paths gtid + j * nthreads (j < ppt). Their discounted values, the current
-// row's spots and the staged row's spots live in this CTA's shared memory ([j * blockDim + tid])
-// for the whole backward pass, so the only HBM traffic is one read of each stored row.
+// Each thread owns paths gtid + j * nthreads (j < ppt). When the population fits on chip
+// (kHbm false), their discounted values, the current row's spots and the staged row's spots live
+// in this CTA's shared memory ([j * blockDim + tid]) for the whole backward pass, so the only HBM
+// traffic is one read of each stored row. Larger populations (kHbm true) keep each path's value in
+// HBM at a.values[p] and read the spots straight from the stored rows; the arithmetic and its order
+// are the same, so a path's decisions do not depend on where its value lives.
 //
 // Per exercise row k the CTA reduces its in-the-money power sums of row k and publishes them;
 // then the warps split. Warps 0..15 wait for every CTA's partial, combine them and warp 0 fits
@@ -170,7 +173,7 @@ struct BackwardSmem {
 // them to row k-1 (policy.rs:1049-1063) and adds the response sums U_0..U_4, which need the
 // decided values. Row k-1's sums are taken about the mean of the latest fitted row available when
 // its staging starts (two rows later than row k-1); any pivot near the in-the-money mean serves.
-template <int D>  // == plan.degree (launch_backward dispatches on it)
+template <int D, bool kHbm>  // D == plan.degree (launch_backward dispatches on it)
 __global__ void __launch_bounds__(kBackwardThreads, 1) backward_kernel(BackwardArgs a) {
     __shared__ BackwardSmem sm;
     extern __shared__ double backward_dyn[];
@@ -183,8 +186,9 @@ __global__ void __launch_bounds__(kBackwardThreads, 1) backward_kernel(BackwardA
     const bool stager = warp >= kCombineWarps;
     const int stage_threads = T - kCombineThreads;
     const int stage_tid = int(threadIdx.x) - kCombineThreads;
-    // values, the spots of the row being decided, and the spots of the row being staged (filled
-    // by cp.async while the current row is reduced and solved); the two spot buffers alternate.
+    // On chip: values, the spots of the row being decided, and the spots of the row being staged
+    // (filled by cp.async while the current row is reduced and solved); the two spot buffers
+    // alternate.
     double* values = backward_dyn;
     double* spots = backward_dyn + size_t(ppt) * T;
     double* spots_next = backward_dyn + 2 * size_t(ppt) * T;
@@ -200,6 +204,11 @@ __global__ void __launch_bounds__(kBackwardThreads, 1) backward_kernel(BackwardA
     const uint32_t fsr = plan.first_stored_row;
     const int lowest = plan.origin_row ? 1 : 0;
     auto row_ptr = [&](uint32_t row) { return a.slab + uint64_t(row - fsr) * P; };
+    // Value of this thread's j-th path (p = gtid + j * nthreads < P): shared memory or HBM.
+    auto value = [&](int j) -> double& {
+        if constexpr (kHbm) return a.values[gtid + uint64_t(j) * nthreads];
+        else return values[j * T + threadIdx.x];
+    };
     {
         const double* terminal = row_ptr(E);
 #pragma unroll 4
@@ -210,7 +219,7 @@ __global__ void __launch_bounds__(kBackwardThreads, 1) backward_kernel(BackwardA
                 const double d = __ldcs(&terminal[p]) - K;
                 v = d > 0.0 ? d : 0.0;
             }
-            values[j * T + threadIdx.x] = v;
+            if (!kHbm || p < P) value(j) = v;
         }
     }
     double2* parts = a.partials;
@@ -231,12 +240,11 @@ __global__ void __launch_bounds__(kBackwardThreads, 1) backward_kernel(BackwardA
 #pragma unroll 4
         for (int j = 0; j < ppt; ++j) {
             const uint64_t p = gtid + uint64_t(j) * nthreads;
-            const int at = j * T + threadIdx.x;
             double sp = 0.0, x = 0.0;
             if (p < P) {
                 sp = __ldcs(&srow[p]);
-                const double v = values[at] * disc;
-                values[at] = v;
+                const double v = value(j) * disc;
+                value(j) = v;
                 if (!fo_isfinite(v)) atomicMin(&a.status->fit_payoff_fail, ((unsigned long long)order << 32) | p);
                 if (sp > K) {
                     x = divide(sp, Kd);
@@ -246,7 +254,7 @@ __global__ void __launch_bounds__(kBackwardThreads, 1) backward_kernel(BackwardA
                     }
                 }
             }
-            spots[at] = sp;
+            if constexpr (!kHbm) spots[j * T + threadIdx.x] = sp;
         }
         cta_reduce_to<2>(loc, sm.red, parts + size_t(parity) * a.partial_stride + blockIdx.x, gridDim.x);
         publish_partial(a.status);
@@ -260,12 +268,14 @@ __global__ void __launch_bounds__(kBackwardThreads, 1) backward_kernel(BackwardA
         if (sm.total[0].hi > 0.0) fit_pivot = dd_round(dd_div(sm.total[1], sm.total[0]));
         latest_mean = fit_pivot;
         for (int j = 0; j < ppt; ++j) {
-            const int at = j * T + threadIdx.x;
-            if (spots[at] > K) {
-                const double x = divide(spots[at], Kd), y = values[at];
+            const uint64_t p = gtid + uint64_t(j) * nthreads;
+            if (kHbm && p >= P) break;
+            const double sp = kHbm ? __ldcg(&srow[p]) : spots[j * T + threadIdx.x];
+            if (sp > K) {
+                const double x = divide(sp, Kd), y = value(j);
                 if (!fo_isfinite(x) || !fo_isfinite(y)) {
                     sums.acc[kBadSlot] += 1.0;
-                    atomicMin(&a.status->fit_nonfinite, ((unsigned long long)order << 32) | (gtid + uint64_t(j) * nthreads));
+                    atomicMin(&a.status->fit_nonfinite, ((unsigned long long)order << 32) | p);
                 } else {
                     accumulate_itm(sums, x, y, fit_pivot);
                 }
@@ -280,7 +290,7 @@ __global__ void __launch_bounds__(kBackwardThreads, 1) backward_kernel(BackwardA
         ++seq;
 #pragma unroll
         for (int k = 0; k < kSlots; ++k) sums.acc[k] = 0.0;
-        if (stage_next && stager) {
+        if (!kHbm && stage_next && stager) {
             // Load the next row's spots for the positions this thread stages (after the release
             // above, which would otherwise wait for these loads).
             const double* srow = row_ptr(uint32_t(row - 1));
@@ -336,12 +346,13 @@ __global__ void __launch_bounds__(kBackwardThreads, 1) backward_kernel(BackwardA
             }
         } else if (stage_next) {
             // Row k-1: in-the-money test and power sums, independent of row k's decision.
-            cp_async_wait_all();
+            const double* srow = row_ptr(uint32_t(row - 1));
+            if constexpr (!kHbm) cp_async_wait_all();
             for (int j = 0; j < ppt; ++j) {
                 for (int t = stage_tid; t < T; t += stage_threads) {
                     const uint64_t p = block_first + uint64_t(t) + uint64_t(j) * nthreads;
                     if (p >= P) continue;
-                    const double sp = spots_next[j * T + t];
+                    const double sp = kHbm ? __ldcg(&srow[p]) : spots_next[j * T + t];
                     if (sp > K) {
                         const double x = divide(sp, Kd);
                         if (!fo_isfinite(x)) {
@@ -361,14 +372,16 @@ __global__ void __launch_bounds__(kBackwardThreads, 1) backward_kernel(BackwardA
         const bool regression = kind == kRuleRegression;
         const FitModel& model = sm.model;  // read from shared memory
         const double disc = stage_next ? plan.disc_from_later[row - 1] : 1.0;
+        const double* cur_row = row_ptr(uint32_t(row));
+        const double* next_row = stage_next ? row_ptr(uint32_t(row - 1)) : cur_row;
 #pragma unroll 2
         for (int j = 0; j < ppt; ++j) {
             const uint64_t p = gtid + uint64_t(j) * nthreads;
             const int at = j * T + threadIdx.x;
             if (p >= P) continue;
-            double v = values[at];
+            double v = value(j);
             if (regression) {
-                const double sp = spots[at];
+                const double sp = kHbm ? __ldcg(&cur_row[p]) : spots[at];
                 if (sp > K) {
                     const double intrinsic = sp - K;
                     double continuation;
@@ -380,7 +393,7 @@ __global__ void __launch_bounds__(kBackwardThreads, 1) backward_kernel(BackwardA
                 }
             }
             if (stage_next) {
-                const double sp = spots_next[at];
+                const double sp = kHbm ? __ldcg(&next_row[p]) : spots_next[at];
                 v *= disc;
                 if (!fo_isfinite(v))
                     atomicMin(&a.status->fit_payoff_fail, ((unsigned long long)(order + 1) << 32) | p);
@@ -398,7 +411,7 @@ __global__ void __launch_bounds__(kBackwardThreads, 1) backward_kernel(BackwardA
                     }
                 }
             }
-            values[at] = v;
+            value(j) = v;
         }
         double* swap = spots;
         spots = spots_next;
@@ -412,7 +425,7 @@ __global__ void __launch_bounds__(kBackwardThreads, 1) backward_kernel(BackwardA
         for (int j = 0; j < ppt; ++j) {
             const uint64_t p = gtid + uint64_t(j) * nthreads;
             if (p < P) {
-                const double w = values[j * T + threadIdx.x] * plan.origin_discount;
+                const double w = value(j) * plan.origin_discount;
                 if (!fo_isfinite(w))
                     atomicMin(&a.status->fit_payoff_fail, ((unsigned long long)order << 32) | p);
                 acc[0] += 1.0;
@@ -509,6 +522,7 @@ __global__ void __launch_bounds__(kEvalThreads, 4) evaluate_kernel(EvalArgs a) {
                 if (!fo_isfinite(payoff)) atomicMin(&a.status->eval_terminal_fail, (unsigned long long)p);
                 active = false;
                 atomicAdd(&counts[row], 1u);
+                if (a.stops) a.stops[p] = uint32_t(row);
                 return;
             }
             if (er.kind == kRuleNoSupport) {
@@ -528,6 +542,7 @@ __global__ void __launch_bounds__(kEvalThreads, 4) evaluate_kernel(EvalArgs a) {
                     atomicMin(&a.status->eval_fail, ((unsigned long long)row << 33) | (p << 1) | 1ull);
                 active = false;
                 atomicAdd(&counts[row], 1u);
+                if (a.stops) a.stops[p] = uint32_t(row);
             }
         };
         const SimResult r = simulate_path(plan, zig, plan.eval_seed, plan.eval_domain, uint32_t(p), observe);
@@ -605,7 +620,7 @@ size_t backward_smem_bytes(int ppt) { return sizeof(double) * 3 * size_t(ppt) * 
 int backward_max_ppt() {
     // Dynamic shared memory available next to the kernel's static shared memory.
     cudaFuncAttributes attr{};
-    cudaFuncGetAttributes(&attr, backward_kernel<kMaxDegree>);  // every degree has the same static shared memory
+    cudaFuncGetAttributes(&attr, backward_kernel<kMaxDegree, false>);  // every degree has the same static shared memory
     int optin = 0, device = 0;
     cudaGetDevice(&device);
     cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device);
@@ -619,31 +634,38 @@ int backward_max_blocks(int device) {
     return sms;  // one 1024-thread CTA per SM; the dynamic shared memory keeps it at one
 }
 
-template <int D>
+template <int D, bool kHbm>
 static cudaError_t launch_backward_d(const BackwardArgs& args, int blocks, int ppt, cudaStream_t stream) {
-    const size_t smem = backward_smem_bytes(ppt);
-    cudaError_t e = cudaFuncSetAttribute(backward_kernel<D>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+    const size_t smem = kHbm ? 0 : backward_smem_bytes(ppt);
+    cudaError_t e = cudaFuncSetAttribute(backward_kernel<D, kHbm>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         int(smem));
     if (e != cudaSuccess) return e;
     int per_sm = 0;
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, backward_kernel<D>, kBackwardThreads, smem);
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, backward_kernel<D, kHbm>, kBackwardThreads, smem);
     if (e != cudaSuccess) return e;
     int device = 0, sms = 0;
     cudaGetDevice(&device);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
     if (per_sm < 1 || blocks > per_sm * sms) return cudaErrorCooperativeLaunchTooLarge;
     void* params[] = {const_cast<BackwardArgs*>(&args)};
-    return cudaLaunchCooperativeKernel((const void*)backward_kernel<D>, dim3(blocks), dim3(kBackwardThreads), params,
-                                       smem, stream);
+    return cudaLaunchCooperativeKernel((const void*)backward_kernel<D, kHbm>, dim3(blocks), dim3(kBackwardThreads),
+                                       params, smem, stream);
+}
+
+template <bool kHbm>
+static cudaError_t launch_backward_storage(const BackwardArgs& args, int blocks, int ppt, cudaStream_t stream) {
+    switch (args.plan.degree) {  // validated to 0..4 on the host
+        case 0: return launch_backward_d<0, kHbm>(args, blocks, ppt, stream);
+        case 1: return launch_backward_d<1, kHbm>(args, blocks, ppt, stream);
+        case 2: return launch_backward_d<2, kHbm>(args, blocks, ppt, stream);
+        case 3: return launch_backward_d<3, kHbm>(args, blocks, ppt, stream);
+        default: return launch_backward_d<4, kHbm>(args, blocks, ppt, stream);
+    }
 }
 
 cudaError_t launch_backward(const BackwardArgs& args, int blocks, int ppt, cudaStream_t stream) {
-    switch (args.plan.degree) {  // validated to 0..4 on the host
-        case 0: return launch_backward_d<0>(args, blocks, ppt, stream);
-        case 1: return launch_backward_d<1>(args, blocks, ppt, stream);
-        case 2: return launch_backward_d<2>(args, blocks, ppt, stream);
-        case 3: return launch_backward_d<3>(args, blocks, ppt, stream);
-        default: return launch_backward_d<4>(args, blocks, ppt, stream);
-    }
+    return args.values ? launch_backward_storage<true>(args, blocks, ppt, stream)
+                       : launch_backward_storage<false>(args, blocks, ppt, stream);
 }
 
 cudaError_t launch_diagnose(const DevicePlan& plan, FitRecord* records, cudaStream_t stream) {

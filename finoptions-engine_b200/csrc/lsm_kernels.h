@@ -19,7 +19,10 @@ struct BackwardArgs {
     size_t partial_stride;       // doubles2 per ping-pong half
     FitRecord* records;          // [rows]
     DeviceStatus* status;
-    int ppt;                     // paths per thread (values and spots staged in shared memory)
+    int ppt;                     // paths per thread
+    double* values;              // NULL: values and spots on chip (shared memory); else [train paths]
+                                 // values in HBM, spots read from the slab (populations beyond the
+                                 // on-chip capacity)
 };
 
 struct EvalArgs {
@@ -29,6 +32,7 @@ struct EvalArgs {
     unsigned* counts;            // [rows] stopping counts
     unsigned* itm_counts;        // [rows] active in-the-money paths at unsupported rows
     DeviceStatus* status;
+    uint32_t* stops;             // optional [evaluation paths]: the row at which each path stopped
 };
 
 // Pathwise adjoint Greeks of the fused evaluation (lsm_greeks.cu).

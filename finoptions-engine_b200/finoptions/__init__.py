@@ -30,6 +30,8 @@ from .batch_lsm import (
     price_lsm_call_grouped_batch,
     price_lsm_call_ragged,
     price_lsm_call_ragged_greeks,
+    validate_lsm_call_grouped_batch,
+    validate_lsm_call_ragged,
 )
 from .dividends import BatchError, MaturityBoundary, RaggedCashDividends
 from .greeks import LsmCallContract, LsmGreeks, lsm_call_price, price_lsm_call_greeks
@@ -136,4 +138,6 @@ __all__ = [
     "price_lsm_call_ragged",
     "price_lsm_call_ragged_greeks",
     "simulate_gbm_seeded",
+    "validate_lsm_call_grouped_batch",
+    "validate_lsm_call_ragged",
 ]

@@ -252,6 +252,7 @@ EXPORTED_SYMBOLS: Final = (
     "fo_lsm_call_plan_set_greeks",
     "fo_lsm_call_plan_greeks",
     "fo_lsm_call_plan_revalue_f64",
+    "fo_lsm_call_plan_stopping_rows",
     "fo_price_lsm_grouped_f64",
     "fo_price_lsm_batch_f64",
     "fo_price_lsm_ragged_f64",
@@ -260,6 +261,8 @@ EXPORTED_SYMBOLS: Final = (
     "fo_simulate_gbm_seeded_f64",
     "fo_sample_standard_normals_f64",
     "fo_build_info",
+    "fo_validate_lsm_grouped_f64",
+    "fo_validate_lsm_ragged_f64",
 )
 
 _library: ctypes.CDLL | None = None
@@ -302,6 +305,8 @@ def _declare(lib: ctypes.CDLL) -> None:
     lib.fo_lsm_call_plan_greeks.restype = ctypes.c_int
     lib.fo_lsm_call_plan_revalue_f64.argtypes = [vp, ctypes.POINTER(FoLsmCallRequest), ctypes.POINTER(FoLsmCallResult), err]
     lib.fo_lsm_call_plan_revalue_f64.restype = ctypes.c_int
+    lib.fo_lsm_call_plan_stopping_rows.argtypes = [vp, ctypes.c_void_p, ctypes.c_uint64, err]
+    lib.fo_lsm_call_plan_stopping_rows.restype = ctypes.c_int
     lib.fo_lsm_call_plan_destroy.argtypes = [vp]
     lib.fo_lsm_call_plan_destroy.restype = None
     for name in ("fo_price_lsm_grouped_f64", "fo_price_lsm_batch_f64"):
@@ -323,6 +328,10 @@ def _declare(lib: ctypes.CDLL) -> None:
         c_double_p, ctypes.c_uint64, err,
     ]
     lib.fo_sample_standard_normals_f64.restype = ctypes.c_int
+    lib.fo_validate_lsm_grouped_f64.argtypes = [ctypes.POINTER(FoLsmGroupedRequest), ctypes.c_int32, err]
+    lib.fo_validate_lsm_grouped_f64.restype = ctypes.c_int
+    lib.fo_validate_lsm_ragged_f64.argtypes = [ctypes.POINTER(FoLsmRaggedRequest), err]
+    lib.fo_validate_lsm_ragged_f64.restype = ctypes.c_int
     lib.fo_build_info.argtypes = [ctypes.c_char_p, ctypes.c_uint64]
     lib.fo_build_info.restype = ctypes.c_int
 

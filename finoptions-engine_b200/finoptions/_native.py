@@ -470,8 +470,9 @@ def _grouped(  # noqa: PLR0913
     condition_limit: float,
     tie_rule: str,
     insufficient_exercise_support: str,
-) -> tuple:
-    handle = _executor_handle(executor)
+) -> tuple | None:
+    # executor None: run the whole-request validation only (no device is touched).
+    handle = None if executor is None else _executor_handle(executor)
     tie = _parse(_TIE_RULES, tie_rule, "exercise tie rule")
     support = _parse(_SUPPORT, insufficient_exercise_support, "insufficient exercise support policy")
     request = lsm_grouped_request(
@@ -495,8 +496,12 @@ def _grouped(  # noqa: PLR0913
         **dividends,
         **mesh,
     )
-    columns = batch_columns(request.rows)
     err = _abi.FoError()
+    if handle is None:
+        grouped = 1 if entry == "fo_price_lsm_grouped_f64" else 0
+        _check(_lib().fo_validate_lsm_grouped_f64(ctypes.byref(request.struct), grouped, ctypes.byref(err)), err)
+        return None
+    columns = batch_columns(request.rows)
     status = getattr(_lib(), entry)(handle, ctypes.byref(request.struct), ctypes.byref(columns.struct),
                                     ctypes.byref(err))
     _check(status, err)
@@ -617,8 +622,9 @@ def price_lsm_call_ragged_f64(  # noqa: PLR0913 - one argument per ragged column
     insufficient_exercise_support, log_discount_nodes=None,
 ) -> tuple:
     """Ragged batch (per-contract path counts; no reference counterpart): NativeBatchLsmResult, and
-    with log_discount_nodes (mesh nodes per row) also (delta, vega, dP/dL, offsets, dP/dD)."""
-    handle = _executor_handle(executor)
+    with log_discount_nodes (mesh nodes per row) also (delta, vega, dP/dL, offsets, dP/dD). With
+    executor None the request is only validated (nothing is priced; returns None)."""
+    handle = None if executor is None else _executor_handle(executor)
     request = lsm_ragged_request(
         initial_spots=initial_spots, strikes=strikes, maturities=maturities, rates=rates, volatilities=volatilities,
         dividend_yields=dividend_yields, dividend_offsets=dividend_offsets, dividend_times=dividend_times,
@@ -634,8 +640,11 @@ def price_lsm_call_ragged_f64(  # noqa: PLR0913 - one argument per ragged column
         insufficient_exercise_support=_parse(_SUPPORT, insufficient_exercise_support,
                                              "insufficient exercise support policy"),
     )
-    columns = batch_columns(request.rows)
     err = _abi.FoError()
+    if handle is None:
+        _check(_lib().fo_validate_lsm_ragged_f64(ctypes.byref(request.struct), ctypes.byref(err)), err)
+        return None
+    columns = batch_columns(request.rows)
     greeks = None
     if log_discount_nodes is not None:
         rows = request.rows

@@ -316,7 +316,7 @@ def _check_partition(result: LsmBatchResult, evaluation_paths: int, what: str) -
 def _method_arguments(mesh: ExerciseMesh, executor: object, method: Lsm) -> tuple:
     return (
         *_mesh_arguments(mesh),
-        native_executor(executor),
+        None if executor is None else native_executor(executor),
         method.training_paths,
         method.evaluation_paths,
         method.training_stream.seed,
@@ -347,6 +347,25 @@ def price_lsm_call_grouped_batch(
     if type(groups) is not LsmStrikeGroups:
         raise InputError("groups must be LsmStrikeGroups")
     _validate_executor_method(executor, method, "grouped batched LSM")
+    return _grouped_call(groups, mesh, executor, method)
+
+
+def validate_lsm_call_grouped_batch(*, groups: LsmStrikeGroups, mesh: ExerciseMesh, method: Lsm) -> None:
+    """Every check price_lsm_call_grouped_batch makes on the whole request before it plans any
+    group (method, columns, the stream domain ranges over every group, mesh domain), with the same
+    typed errors, and without touching a device. A caller that prices a batch in shards runs it on
+    the whole request first: each shard sees fewer groups and shifted domains, so the shards alone
+    cannot see, e.g., training and evaluation domain ranges that overlap."""
+    if type(groups) is not LsmStrikeGroups:
+        raise InputError("groups must be LsmStrikeGroups")
+    if type(method) is not Lsm:
+        raise InputError("method must be Lsm")
+    if method.evaluation_paths < _MIN_EVALUATION_PATHS:
+        raise InputError("grouped batched LSM requires at least two independent evaluation paths")
+    _grouped_call(groups, mesh, None, method)
+
+
+def _grouped_call(groups: LsmStrikeGroups, mesh: ExerciseMesh, executor: object, method: Lsm) -> LsmBatchResult | None:
     _validate_mesh(mesh, groups.dividends, int(groups.initial_spots.size))
     common = (groups.group_offsets, groups.initial_spots, groups.strikes, groups.maturities, groups.rates,
               groups.volatilities)
@@ -364,6 +383,8 @@ def price_lsm_call_grouped_batch(
             d.maturity_boundary.value, *tail)
     else:
         raise LsmError("group dividends changed type after request validation")
+    if executor is None:
+        return None
     return _check_partition(_freeze(raw), method.evaluation_paths, "grouped LSM")
 
 
@@ -493,7 +514,8 @@ def _ragged_arguments(contracts: LsmRaggedContracts, origin_exercise: OriginExer
         contracts.dividend_yields, None if cash is None else cash.offsets, None if cash is None else cash.times,
         None if cash is None else cash.amounts, dividend_policy.value, maturity_boundary.value,
         contracts.exercise.offsets, contracts.exercise.times, origin_exercise.value, contracts.training_paths,
-        contracts.evaluation_paths, native_executor(executor), training_stream.seed, training_stream.domain,
+        contracts.evaluation_paths, None if executor is None else native_executor(executor), training_stream.seed,
+        training_stream.domain,
         evaluation_stream.seed, evaluation_stream.domain, polynomial_degree, rank_tolerance, condition_limit,
         tie_rule.value, insufficient_exercise_support.value,
     )
@@ -519,6 +541,26 @@ def price_lsm_call_ragged(  # noqa: PLR0913 - method settings stay explicit keyw
         contracts, origin_exercise, dividend_policy, maturity_boundary, executor, training_stream, evaluation_stream,
         insufficient_exercise_support, polynomial_degree, rank_tolerance, condition_limit, tie_rule))
     return _freeze(raw)
+
+
+def validate_lsm_call_ragged(  # noqa: PLR0913 - method settings stay explicit keywords
+    *,
+    contracts: LsmRaggedContracts,
+    origin_exercise: OriginExercise,
+    training_stream: RandomStream,
+    evaluation_stream: RandomStream,
+    insufficient_exercise_support: InsufficientExerciseSupportPolicy,
+    dividend_policy: DividendPolicy = DividendPolicy.LIQUIDATOR,
+    maturity_boundary: MaturityBoundary = MaturityBoundary.STRICTLY_BEFORE,
+    polynomial_degree: int = 4,
+    rank_tolerance: float = 1.0e-12,
+    condition_limit: float = 1.0e8,
+    tie_rule: ExerciseTieRule = ExerciseTieRule.STRICTLY_GREATER,
+) -> None:
+    """Every check price_lsm_call_ragged makes on the whole request, without touching a device."""
+    _native.price_lsm_call_ragged_f64(*_ragged_arguments(
+        contracts, origin_exercise, dividend_policy, maturity_boundary, None, training_stream, evaluation_stream,
+        insufficient_exercise_support, polynomial_degree, rank_tolerance, condition_limit, tie_rule))
 
 
 def price_lsm_call_ragged_greeks(  # noqa: PLR0913 - method settings stay explicit keywords
@@ -568,4 +610,6 @@ __all__ = [
     "price_lsm_call_grouped_batch",
     "price_lsm_call_ragged",
     "price_lsm_call_ragged_greeks",
+    "validate_lsm_call_grouped_batch",
+    "validate_lsm_call_ragged",
 ]

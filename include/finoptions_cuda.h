@@ -348,6 +348,12 @@ int fo_lsm_call_plan_greeks(fo_lsm_call_plan* plan, fo_lsm_call_greeks* greeks, 
 int fo_lsm_call_plan_revalue_f64(fo_lsm_call_plan* plan, const fo_lsm_call_request* market,
                                  fo_lsm_call_result* result, fo_error* err);
 
+/* Every evaluation path's stopping observation row under the plan's fitted policy on its current
+ * market (rows[p] for evaluation path p; capacity >= evaluation paths). No counterpart in the
+ * reference: a diagnostic that counts, path by path, the exercise decisions in which this engine
+ * and another implementation of the same contract differ. It re-runs the evaluation pass. */
+int fo_lsm_call_plan_stopping_rows(fo_lsm_call_plan* plan, uint32_t* rows, uint64_t capacity, fo_error* err);
+
 /* Allocation-free variant of fo_price_lsm_call_f64. It has no counterpart in the reference.
  *
  * For callers that cannot allocate device memory: code whose device memory belongs to another
@@ -359,8 +365,8 @@ int fo_lsm_call_plan_revalue_f64(fo_lsm_call_plan* plan, const fo_lsm_call_reque
  * training_paths x stored rows x 8 bytes, partials, status, results) in one file-scope device
  * array of FO_NOALLOC_SCRATCH_BYTES (64 MiB) that every GPU loading this library holds until the
  * process exits. Requests that need more return FO_ERR_EXECUTION / FO_CODE_CAPACITY_EXCEEDED.
- * The first call on a device looks up the array's device address; make that first call before
- * any stream capture. Every call shares the one array and clears what must start at zero itself;
+ * The first call on a device looks up the array's device address and the device's launch shapes
+ * (kept for later calls); make that first call before any stream capture. Every call shares the one array and clears what must start at zero itself;
  * calls that overlap on the GPU (two streams, or two threads) race on it and must be serialised
  * by the caller. The call synchronises `cuda_stream` before returning. */
 #define FO_NOALLOC_SCRATCH_BYTES (64ull << 20)
@@ -547,6 +553,14 @@ int fo_validate_ragged_exercise_times(const int64_t* offsets, uint64_t n_offsets
                                       uint64_t n_times, fo_error* err);
 /* Runs every host-side check fo_price_lsm_call_f64 performs before touching a device. */
 int fo_validate_lsm_call_request(const fo_lsm_call_request* request, fo_error* err);
+/* Every check fo_price_lsm_grouped_f64 (grouped != 0) or fo_price_lsm_batch_f64 (grouped == 0)
+ * makes on the whole request before planning any group, in the reference's order (the method,
+ * lib.rs:1302-1415; the columns, input.rs:502-706; the stream domain ranges over every group,
+ * input.rs:201-255; the mesh domain, pricing.rs:356-400, 622-664), with the same errors. A caller
+ * that prices a batch in shards runs it on the whole request first. */
+int fo_validate_lsm_grouped_f64(const fo_lsm_grouped_request* request, int32_t grouped, fo_error* err);
+/* The same for fo_price_lsm_ragged_f64. */
+int fo_validate_lsm_ragged_f64(const fo_lsm_ragged_request* request, fo_error* err);
 
 /* ---- build identity ------------------------------------------------------------------------- */
 

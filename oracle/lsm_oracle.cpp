@@ -953,9 +953,12 @@ struct Evaluation {
     std::vector<uint32_t> counts;
 };
 
+// payoffs_out / stops_out (optional, `paths` entries each) receive every path's discounted payoff
+// and the observation row at which it stopped: the per-path record finite-difference checks use to
+// find the paths whose stopping row a bump moved.
 Failure evaluate(const Estimator& est, const Plan& plan, const Fitted& fitted,
                  const std::vector<double>& evaluation, uint64_t paths, double initial_spot,
-                 Evaluation* out) {
+                 Evaluation* out, double* payoffs_out = nullptr, uint32_t* stops_out = nullptr) {
     const size_t rows = plan.rows();
     out->paths = uint32_t(paths);
     out->counts.assign(rows, 0);
@@ -965,6 +968,10 @@ Failure evaluate(const Estimator& est, const Plan& plan, const Fitted& fitted,
         out->has_sd = true;
         out->sd = 0.0;
         out->se = 0.0;
+        for (uint64_t p = 0; p < paths; ++p) {
+            if (payoffs_out) payoffs_out[p] = out->price;
+            if (stops_out) stops_out[p] = 0;
+        }
         return Failure{};
     }
     std::vector<uint8_t> active(paths, 1);
@@ -1003,6 +1010,7 @@ Failure evaluate(const Estimator& est, const Plan& plan, const Fitted& fitted,
                     }
                     payoffs[p] = payoff;
                     active[p] = 0;
+                    if (stops_out) stops_out[p] = uint32_t(row);
                     count += 1;
                 }
             }
@@ -1023,9 +1031,11 @@ Failure evaluate(const Estimator& est, const Plan& plan, const Fitted& fitted,
         }
         payoffs[p] = payoff;
         active[p] = 0;
+        if (stops_out) stops_out[p] = uint32_t(terminal_row);
         terminal_count += 1;
     }
     out->counts[terminal_row] = terminal_count;
+    if (payoffs_out) std::copy(payoffs.begin(), payoffs.end(), payoffs_out);
     // LsmEvaluation::from_path_payoffs (policy.rs:891-926)
     uint32_t count = 0;
     double mean = 0.0, m2 = 0.0;
@@ -1048,6 +1058,42 @@ Failure evaluate(const Estimator& est, const Plan& plan, const Fitted& fitted,
         out->sd = sd;
         out->se = se;
     }
+    return Failure{};
+}
+
+// The payoffs of evaluation paths whose stopping rows are given (frozen_stops[p], e.g. the rows a
+// base market's policy chose): (S_row - K) exp(L_row) at an early row, max(S_T - K, 0) exp(L_T) at
+// expiry. With every decision frozen, a central difference of this price over a bumped market is
+// the pathwise derivative that a fixed-policy adjoint forms (the exercise indicators held fixed).
+Failure evaluate_frozen(const Estimator& est, const Plan& plan, const Fitted& fitted,
+                        const std::vector<double>& evaluation, uint64_t paths, const uint32_t* frozen_stops,
+                        Evaluation* out, double* payoffs_out, uint32_t* stops_out) {
+    const size_t rows = plan.rows();
+    out->paths = uint32_t(paths);
+    out->counts.assign(rows, 0);
+    std::vector<double> payoffs(paths, 0.0);
+    for (uint64_t p = 0; p < paths; ++p) {
+        const uint32_t row = frozen_stops[p];
+        if (row >= rows) return fail(ORC_INVALID_INPUT);
+        const double spot = evaluation[row * paths + p];
+        const double intrinsic = row + 1 == rows ? call_intrinsic(spot, est.strike) : spot - est.strike;
+        payoffs[p] = intrinsic * fitted.discount_to_origin[row];
+        out->counts[row] += 1;
+        if (stops_out) stops_out[p] = row;
+    }
+    uint32_t count = 0;
+    double mean = 0.0, m2 = 0.0;
+    for (uint64_t p = 0; p < paths; ++p) {
+        count += 1;
+        const double delta = payoffs[p] - mean;
+        mean += delta / double(count);
+        m2 = std::fma(delta, payoffs[p] - mean, m2);
+    }
+    out->price = mean;
+    out->has_sd = paths > 1;
+    out->sd = paths > 1 ? std::sqrt(m2 / double(uint32_t(paths - 1))) : 0.0;
+    out->se = paths > 1 ? out->sd / std::sqrt(double(uint32_t(paths))) : 0.0;
+    if (payoffs_out) std::copy(payoffs.begin(), payoffs.end(), payoffs_out);
     return Failure{};
 }
 
@@ -1483,6 +1529,96 @@ int orc_price_lsm_call(const fo_lsm_call_request* q, int32_t threads, fo_lsm_cal
     result->n_diagnostics = fitted.diagnostics.size();
     for (size_t i = 0; i < fitted.diagnostics.size() && i < result->diagnostics_capacity; ++i)
         result->diagnostics[i] = fitted.diagnostics[i];
+    return FO_OK;
+}
+
+// One contract on a list of markets with common random numbers: the reference's
+// bump-and-reprice (two price_lsm_call calls on identical streams, policy.rs:306-336) when
+// refit != 0, and the fixed-policy revaluation of FittedLsmCallPolicy::evaluate (policy.rs:642-834)
+// when refit == 0 - the policy is fitted once on `base` (training simulation and fit with the base
+// market) and every market's evaluation paths are stopped by it, discounted with the market's own
+// curve. Every market keeps the base's schedule, nodes, strike, path counts, streams and method;
+// its spot, log discounts, cumulative yields, cash amounts and volatility may differ.
+// frozen_stops (optional, refit == 0 only, [evaluation_paths]) fixes every path's stopping row
+// instead of applying the policy (evaluate_frozen).
+// prices[m] receives market m's price; payoffs / stops (optional, [n_markets][evaluation_paths])
+// every path's discounted payoff and stopping row. Markets run in parallel over `threads` workers,
+// each market's simulations on threads / workers threads; the lowest failing market's failure is
+// reported.
+int orc_price_lsm_call_markets(const fo_lsm_call_request* base, const fo_lsm_call_request* markets,
+                               uint64_t n_markets, int32_t refit, const uint32_t* frozen_stops, int32_t threads,
+                               double* prices, double* payoffs, uint32_t* stops, fo_error* err) {
+    auto plan_of = [](const fo_lsm_call_request* q) {
+        return plan_from_gbm(q->schedule_times, q->n_schedule_times, q->log_discounts, q->cumulative_dividend_yields,
+                             q->dividend_nodes, q->dividend_amounts, q->n_dividend_nodes, q->exercise_nodes,
+                             q->n_exercise_nodes, q->expiry_node, q->annualized_volatility, q->dividend_policy);
+    };
+    const Estimator est{base->strike, Spec{int(base->polynomial_degree), base->rank_tolerance, base->condition_limit},
+                        base->tie_rule, base->insufficient_exercise_support};
+    const uint64_t paths = base->evaluation_paths;
+    Fitted base_fit;
+    if (!refit) {
+        const Plan plan = plan_of(base);
+        std::vector<double> training;
+        Failure f = simulate(plan, base->initial_spot, base->training_paths, base->training_seed,
+                             base->training_domain, threads, &training);
+        if (f.ok()) f = fit_policy(est, plan, training, base->training_paths, base->initial_spot, &base_fit);
+        if (!f.ok()) {
+            write_error(err, f, FO_ERR_LSM);
+            return FO_ERR_LSM;
+        }
+    }
+    const int workers = std::max(1, std::min<int>(threads, int(std::min<uint64_t>(n_markets, 256))));
+    const int sim_threads = std::max(1, threads / workers);
+    std::vector<Failure> failures(n_markets);
+    std::atomic<uint64_t> next{0};
+    auto worker = [&]() {
+        for (uint64_t m = next.fetch_add(1); m < n_markets; m = next.fetch_add(1)) {
+            const fo_lsm_call_request* q = markets + m;
+            const Plan plan = plan_of(q);
+            Fitted fitted;
+            Evaluation ev;
+            Failure f;
+            if (refit) {
+                std::vector<double> training;
+                f = simulate(plan, q->initial_spot, q->training_paths, q->training_seed, q->training_domain,
+                             sim_threads, &training);
+                if (f.ok()) f = fit_policy(est, plan, training, q->training_paths, q->initial_spot, &fitted);
+            } else {
+                fitted.rules = base_fit.rules;
+                fitted.diagnostics = base_fit.diagnostics;
+                fitted.discount_to_origin.resize(plan.rows());
+                for (size_t r = 0; r < plan.rows() && f.ok(); ++r) {
+                    if (!checked_discount(plan.log_discounts[plan.observation_nodes[r]], &fitted.discount_to_origin[r])) {
+                        f = fail(ORC_UNREPRESENTABLE_DISCOUNT);
+                        f.node = plan.observation_nodes[r];
+                    }
+                }
+            }
+            std::vector<double> evaluation;
+            if (f.ok())
+                f = simulate(plan, q->initial_spot, q->evaluation_paths, q->evaluation_seed, q->evaluation_domain,
+                             sim_threads, &evaluation);
+            double* pay_m = payoffs ? payoffs + m * paths : nullptr;
+            uint32_t* stop_m = stops ? stops + m * paths : nullptr;
+            if (f.ok() && frozen_stops && !refit)
+                f = evaluate_frozen(est, plan, fitted, evaluation, paths, frozen_stops, &ev, pay_m, stop_m);
+            else if (f.ok())
+                f = evaluate(est, plan, fitted, evaluation, paths, q->initial_spot, &ev, pay_m, stop_m);
+            failures[m] = f;
+            prices[m] = f.ok() ? ev.price : std::nan("");
+        }
+    };
+    std::vector<std::thread> pool;
+    for (int w = 1; w < workers; ++w) pool.emplace_back(worker);
+    worker();
+    for (auto& t : pool) t.join();
+    for (uint64_t m = 0; m < n_markets; ++m) {
+        if (!failures[m].ok()) {
+            write_error(err, failures[m], FO_ERR_LSM);
+            return FO_ERR_LSM;
+        }
+    }
     return FO_OK;
 }
 

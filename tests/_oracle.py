@@ -56,6 +56,10 @@ def load() -> ctypes.CDLL:
             ctypes.POINTER(_abi.FoLsmCallRequest), ctypes.c_int32, ctypes.POINTER(_abi.FoLsmCallResult), err,
             ctypes.POINTER(ctypes.c_int32),
         ]
+        lib.orc_price_lsm_call_markets.argtypes = [
+            ctypes.POINTER(_abi.FoLsmCallRequest), ctypes.POINTER(_abi.FoLsmCallRequest), ctypes.c_uint64,
+            ctypes.c_int32, ctypes.c_void_p, ctypes.c_int32, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, err,
+        ]
         lib.orc_price_lsm_grouped.argtypes = [
             ctypes.POINTER(_abi.FoLsmGroupedRequest), ctypes.c_int32, ctypes.POINTER(_abi.FoBatchResultColumns), err,
         ]
@@ -114,6 +118,34 @@ def price_lsm_call(request: CallRequest, threads: int = 8) -> tuple:
     if status:
         raise OracleFailure(status, err, stage.value)
     return result.as_tuple()
+
+
+def price_markets(base: CallRequest, markets: list[CallRequest], *, refit: bool, threads: int = 8,
+                  paths: bool = True, frozen_stops: np.ndarray | None = None
+                  ) -> tuple[np.ndarray, np.ndarray | None, np.ndarray | None]:
+    """One contract on several markets with common random numbers: refit=True prices each market
+    from scratch (the reference's bump-and-reprice), refit=False evaluates every market with the
+    policy fitted once on `base`, or, given frozen_stops, stops path p at row frozen_stops[p] in
+    every market. Returns prices [markets] and, with paths=True, every path's discounted payoff and
+    stopping row [markets, evaluation paths]."""
+    n = len(markets)
+    table = (_abi.FoLsmCallRequest * n)(*[m.struct for m in markets])
+    prices = np.zeros(n)
+    n_paths = int(base.struct.evaluation_paths)
+    payoffs = np.zeros((n, n_paths)) if paths else None
+    stops = np.zeros((n, n_paths), dtype=np.uint32) if paths else None
+    err = _abi.FoError()
+    frozen = None
+    if frozen_stops is not None:
+        frozen = np.ascontiguousarray(frozen_stops, dtype=np.uint32)
+        assert frozen.size == n_paths
+    status = load().orc_price_lsm_call_markets(
+        ctypes.byref(base.struct), table, n, 1 if refit else 0, None if frozen is None else frozen.ctypes.data,
+        threads, prices.ctypes.data,
+        payoffs.ctypes.data if paths else None, stops.ctypes.data if paths else None, ctypes.byref(err))
+    if status:
+        raise OracleFailure(status, err)
+    return prices, payoffs, stops
 
 
 def price_lsm_grouped(request: GroupedRequest, threads: int = 8) -> tuple:

@@ -16,6 +16,26 @@ from finoptions._requests import GroupedRequest, lsm_grouped_request
 
 TRAINING_DOMAIN_START = 0
 EVALUATION_DOMAIN_START = 1 << 20
+WEEKLY_INTERVALS = 52
+
+
+def weekly_call_kwargs(paths: int = 1 << 20, *, dividends: bool = False) -> dict:
+    """The weekly single-contract workload: S0 = K = 100, T = 1, grid t_i = i/52, exercise at nodes
+    0..51 (the origin a common decision) plus expiry 52, log discounts -0.04 t, cumulative yield
+    0.02 t, sigma = 0.25, Philox seed 11 with domains 1 / 2, degree 4, fail on insufficient support.
+    dividends=True adds two cash dividends of 1.5 at weeks 13 and 39 (liquidator)."""
+    n = WEEKLY_INTERVALS
+    t = [i / n for i in range(n + 1)]
+    return dict(
+        initial_spot=100.0, strike=100.0, schedule_times=t, curve_times=t,
+        log_discounts=[0.0 if i == 0 else -0.04 * t[i] for i in range(n + 1)], dividend_yield_times=t,
+        cumulative_dividend_yields=[0.0 if i == 0 else 0.02 * t[i] for i in range(n + 1)],
+        dividend_nodes=[13, 39] if dividends else [], dividend_amounts=[1.5, 1.5] if dividends else [],
+        exercise_nodes=list(range(n)), expiry_node=n, annualized_volatility=0.25, dividend_policy=0,
+        training_paths=paths, evaluation_paths=paths, training_seed=11, training_domain=1, evaluation_seed=11,
+        evaluation_domain=2, polynomial_degree=4, rank_tolerance=1e-12, condition_limit=1e8, tie_rule=0,
+        insufficient_exercise_support=0,
+    )
 
 
 @dataclass
@@ -204,26 +224,52 @@ def ragged_request(c: RaggedColumns, *, seed: int = 41, support: int = 1, traini
         condition_limit=1e8, tie_rule=0, insufficient_exercise_support=support)
 
 
+def explicit_call_kwargs(*, s0: float, strike: float, maturity: float, rate: float, dividend_yield: float,
+                         volatility: float, exercise_times: np.ndarray, cash_times: np.ndarray,
+                         cash_amounts: np.ndarray, paths: int, seed: int, training_domain: int,
+                         evaluation_domain: int, support: int = 1, degree: int = 4) -> dict:
+    """A contract of an explicit-mesh batch as single-contract arguments: the grid is the union of its
+    exercise and cash times plus the origin and maturity, L = -r t, cumulative yield q t."""
+    times = [0.0, *np.union1d(exercise_times, cash_times[cash_times < maturity]).tolist(), maturity]
+    node = {t: i for i, t in enumerate(times)}
+    return dict(
+        initial_spot=s0, strike=strike, schedule_times=times, curve_times=times,
+        log_discounts=[0.0 if i == 0 else -rate * t for i, t in enumerate(times)], dividend_yield_times=times,
+        cumulative_dividend_yields=[0.0 if i == 0 else dividend_yield * t for i, t in enumerate(times)],
+        dividend_nodes=[node[t] for t in cash_times.tolist()], dividend_amounts=cash_amounts.tolist(),
+        exercise_nodes=[node[t] for t in exercise_times.tolist()], expiry_node=len(times) - 1,
+        annualized_volatility=volatility, dividend_policy=0, training_paths=paths, evaluation_paths=paths,
+        training_seed=seed, training_domain=training_domain, evaluation_seed=seed,
+        evaluation_domain=evaluation_domain, polynomial_degree=degree, rank_tolerance=1e-12, condition_limit=1e8,
+        tie_rule=0, insufficient_exercise_support=support)
+
+
 def ragged_row_as_call(c: RaggedColumns, r: int, *, seed: int = 41, support: int = 1, training_domain: int = 0,
                        evaluation_domain: int = 1 << 20, degree: int = 4) -> dict:
     """Row r of a ragged batch as single-contract arguments (the union mesh of its exercise and cash
     times, domains start + r)."""
-    T, rate, q = float(c.maturities[r]), float(c.rates[r]), float(c.dividend_yields[r])
-    ex = c.exercise_times[c.exercise_offsets[r]:c.exercise_offsets[r + 1]]
-    cash = c.dividend_times[c.dividend_offsets[r]:c.dividend_offsets[r + 1]]
-    amounts = c.dividend_amounts[c.dividend_offsets[r]:c.dividend_offsets[r + 1]]
-    times = [0.0, *np.union1d(ex, cash[cash < T]).tolist(), T]
-    node = {t: i for i, t in enumerate(times)}
-    return dict(
-        initial_spot=float(c.initial_spots[r]), strike=float(c.strikes[r]), schedule_times=times, curve_times=times,
-        log_discounts=[0.0 if i == 0 else -rate * t for i, t in enumerate(times)], dividend_yield_times=times,
-        cumulative_dividend_yields=[0.0 if i == 0 else q * t for i, t in enumerate(times)],
-        dividend_nodes=[node[t] for t in cash.tolist()], dividend_amounts=amounts.tolist(),
-        exercise_nodes=[node[t] for t in ex.tolist()], expiry_node=len(times) - 1,
-        annualized_volatility=float(c.volatilities[r]), dividend_policy=0, training_paths=int(c.paths[r]),
-        evaluation_paths=int(c.paths[r]), training_seed=seed, training_domain=training_domain + r,
-        evaluation_seed=seed, evaluation_domain=evaluation_domain + r, polynomial_degree=degree, rank_tolerance=1e-12,
-        condition_limit=1e8, tie_rule=0, insufficient_exercise_support=support)
+    cash = slice(c.dividend_offsets[r], c.dividend_offsets[r + 1])
+    return explicit_call_kwargs(
+        s0=float(c.initial_spots[r]), strike=float(c.strikes[r]), maturity=float(c.maturities[r]),
+        rate=float(c.rates[r]), dividend_yield=float(c.dividend_yields[r]), volatility=float(c.volatilities[r]),
+        exercise_times=c.exercise_times[c.exercise_offsets[r]:c.exercise_offsets[r + 1]],
+        cash_times=c.dividend_times[cash], cash_amounts=c.dividend_amounts[cash], paths=int(c.paths[r]), seed=seed,
+        training_domain=training_domain + r, evaluation_domain=evaluation_domain + r, support=support, degree=degree)
+
+
+def grouped_row_as_call(c: GroupedColumns, row: int, paths: int, *, seed: int = 23, support: int = 1,
+                        degree: int = 4) -> dict:
+    """Strike row `row` of a grouped explicit-mesh workload as single-contract arguments: its state's
+    mesh, market and populations (domains start + group)."""
+    g = int(np.searchsorted(c.group_offsets, row, side="right")) - 1
+    cash = slice(c.dividend_offsets[g], c.dividend_offsets[g + 1])
+    return explicit_call_kwargs(
+        s0=float(c.initial_spots[g]), strike=float(c.strikes[row]), maturity=float(c.maturities[g]),
+        rate=float(c.rates[g]), dividend_yield=0.0, volatility=float(c.volatilities[g]),
+        exercise_times=c.exercise_times[c.exercise_offsets[g]:c.exercise_offsets[g + 1]],
+        cash_times=c.dividend_times[cash], cash_amounts=c.dividend_amounts[cash], paths=paths, seed=seed,
+        training_domain=TRAINING_DOMAIN_START + g, evaluation_domain=EVALUATION_DOMAIN_START + g, support=support,
+        degree=degree)
 
 
 def ragged_path_steps(c: RaggedColumns) -> int:

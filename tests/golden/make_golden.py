@@ -1,7 +1,8 @@
 """Extract the reference's known-answer vectors for the LSM hot path into golden.json.
 
-Run in a checkout where the reference source tree is mounted (default /root/reference, or pass
-the path). Every value is read from the reference's own test sources, as text, at the cited
+    python tests/golden/make_golden.py <path of the reference source tree>
+
+Every value is read from the reference's own test sources, as text, at the cited
 lines; nothing is computed here. The committed golden.json is what the test suite reads, so the
 tests never need the reference tree at run time.
 
@@ -65,7 +66,9 @@ def zignor(root: Path) -> dict:
 
 
 def main() -> None:
-    root = Path(sys.argv[1]) if len(sys.argv) > 1 else Path("/root/reference")
+    if len(sys.argv) != 2:
+        sys.exit("usage: make_golden.py <path of the reference source tree>")
+    root = Path(sys.argv[1])
     out = Path(__file__).with_name("golden.json")
     golden = {
         "philox": philox(root),

@@ -16,7 +16,7 @@ import pytest
 pytestmark = pytest.mark.gpu
 
 HERE = Path(__file__).resolve().parent
-BUILD = HERE.parent / "oracle" / "_build"
+BUILD = HERE / "native" / "_build"
 
 
 def harness() -> ctypes.CDLL:

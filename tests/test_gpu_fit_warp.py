@@ -21,7 +21,7 @@ import pytest
 pytestmark = pytest.mark.gpu
 
 HERE = Path(__file__).resolve().parent
-BUILD = HERE.parent / "oracle" / "_build"
+BUILD = HERE / "native" / "_build"
 CSRC = HERE.parent / "finoptions-engine_b200" / "csrc"
 POWER_SUMS, SLOTS = 9, 14
 STATUS_OFFSET = 168  # FitModel: mean, scale, inv_scale, alpha[4], beta[4], coef[5], norm[5], status

@@ -18,7 +18,7 @@ import pytest
 pytestmark = pytest.mark.gpu
 
 HERE = Path(__file__).resolve().parent
-BUILD = HERE.parent / "oracle" / "_build"
+BUILD = HERE / "native" / "_build"
 CSRC = HERE.parent / "finoptions-engine_b200" / "csrc"
 BLOCKS = 4
 

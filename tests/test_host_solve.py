@@ -14,7 +14,7 @@ import pytest
 import _oracle
 
 HERE = Path(__file__).resolve().parent
-BUILD = HERE.parent / "oracle" / "_build"
+BUILD = HERE / "native" / "_build"
 
 
 @pytest.fixture(scope="module")

@@ -3,7 +3,8 @@
 fo_price_lsm_call_f64_noalloc serves callers that cannot allocate device memory (their device
 memory belongs to another allocator, or cudaMalloc's implicit synchronisation is not acceptable on
 their path). It must produce the same result as fo_price_lsm_call_f64 on consecutive calls, which
-share its one device scratch array, and must reject requests larger than that array.
+share its one device scratch array, must leave the device's free memory unchanged, and must reject
+requests larger than that array.
 """
 
 from __future__ import annotations
@@ -69,3 +70,22 @@ def test_no_alloc_entry_rejects_requests_beyond_its_scratch() -> None:
     assert status == _abi.FO_ERR_EXECUTION
     message = err.message.decode()
     assert "allocation-free entry point holds at most 67108864 bytes" in message
+
+
+def test_no_alloc_calls_leave_the_device_free_memory_unchanged() -> None:
+    """After a first call (which loads the kernels it launches), further calls whose scratch needs
+    (about 28 MB here) are well above the driver's allocation granularity move no device memory."""
+    import torch
+
+    torch.cuda.mem_get_info(0)  # the runtime's own set-up happens before anything is measured
+    request = weekly_request(65536)
+    status, err, _ = price_no_alloc(request)
+    assert status == 0, err.message
+    torch.cuda.synchronize()
+    free_before, _ = torch.cuda.mem_get_info(0)
+    for _ in range(3):
+        status, err, _ = price_no_alloc(request)
+        assert status == 0, err.message
+    torch.cuda.synchronize()
+    free_after, _ = torch.cuda.mem_get_info(0)
+    assert free_after == free_before
