@@ -200,8 +200,17 @@ def one_by_one(calls: list[dict], batch_prices, batch_errors) -> dict:
     errors = np.array([r.standard_error for r in results])
     return {"contracts": len(calls), "seconds": wall, "contracts_per_s": len(calls) / wall,
             "api": "finoptions.price_lsm_call(executor=CudaExecutor), one contract per call",
-            "max_rel_price_difference_vs_batch": float(np.max(np.abs(prices - batch_prices) / np.abs(batch_prices))),
-            "max_rel_se_difference_vs_batch": float(np.max(np.abs(errors - batch_errors) / np.abs(batch_errors)))}
+            "max_rel_price_difference_vs_batch": relative_difference(prices, batch_prices),
+            "max_rel_se_difference_vs_batch": relative_difference(errors, batch_errors)}
+
+
+def relative_difference(a, b) -> float:
+    """Largest |a - b| / |b| over the entries, with 0 where both are 0 (worthless contracts)."""
+    import numpy as np
+
+    diff = np.abs(np.asarray(a) - np.asarray(b))
+    scale = np.abs(np.asarray(b))
+    return float(np.max(np.where(diff == 0.0, 0.0, diff / np.where(scale == 0.0, 1.0, scale))))
 
 
 # ---- our arm -----------------------------------------------------------------------------------
@@ -417,8 +426,6 @@ def run_ragged(args: argparse.Namespace, executor) -> dict:
     steps = _workloads.ragged_path_steps(c)
     ms = (ctypes.c_double * 5)()
     launches = ctypes.c_uint64()
-    names = ("batch_simulate_kernel", "batch_backward_kernel", "batch_diagnose_kernel", "batch_evaluate_kernel",
-             "batch_summarize_kernel")
     out = {"workload": (f"ragged batch: {c.rows} contracts, paths per role log-uniform in [8192, 262144] "
                         f"(mean {float(c.paths.mean()):.0f}), 4-104 exercise dates, S0~U[20,500], K/S0~U[0.7,1.3], "
                         "sigma~U[0.05,0.8], T~U[0.1,3], r~U[0,0.08], even rows yield q~U[0,0.05], odd rows 1-6 cash "
@@ -442,8 +449,8 @@ def run_ragged(args: argparse.Namespace, executor) -> dict:
         out[name] = {"device_ms_per_call": device_ms, "device_contracts_per_s": c.rows / (device_ms / 1e3),
                      "device_path_steps_per_s": steps / (device_ms / 1e3),
                      "e2e_contracts_per_s": c.rows * calls / wall, "e2e_ms_per_call": wall / calls * 1e3,
-                     "kernels_ms": {n: round(v / calls, 3) for n, v in zip(names, kernel_ms, strict=True)},
-                     "gpu_launches_per_call": int(launches.value)}
+                     "kernels_ms": {"batch_persistent_kernel": round(kernel_ms[0] / calls, 3)},
+                     "gpu_launches_per_call": int(launches.value), "launch_shape": batch_launch(lib, executor)}
     out["greeks_overhead"] = out["price_and_greeks"]["device_ms_per_call"] / out["plain"]["device_ms_per_call"]
     # The north-star comparison: the same contracts (same populations, so the same price and SE)
     # priced one by one on the plain per-contract path, against the batched price + Greeks call.
@@ -570,16 +577,16 @@ def grouped_algorithmic_bytes(c, paths: int) -> dict:
     }
 
 
-def batch_traffic(kernel: str, algorithmic_bytes: int) -> int | None:
-    """DRAM bytes per call of a batch kernel: the ncu-measured ratio of DRAM to algorithmic bytes
-    (profiles/traffic.json) times this call's algorithmic bytes."""
-    path = ROOT / "profiles" / "traffic.json"
-    if not path.is_file():
-        return None
-    entry = json.loads(path.read_text()).get(kernel)
-    if entry is None or "dram_bytes_per_algorithmic_byte" not in entry:
-        return None
-    return int(entry["dram_bytes_per_algorithmic_byte"] * algorithmic_bytes)
+def batch_launch(lib, executor) -> dict:
+    """The launch shape the executor used for its last batch call (autotuned per shape class)."""
+    from finoptions import _abi
+
+    info = _abi.FoBatchLaunchInfo()
+    lib.fo_executor_batch_launch(executor.raw, ctypes.byref(info))
+    t = info.tuning
+    return {"sim_blocks_per_item": t.sim_blocks, "eval_blocks_per_item": t.eval_blocks,
+            "strikes_per_eval_item": t.strikes, "ctas_per_sm": t.ctas_per_sm or "max", "ctas": info.grid,
+            "work_items": int(info.items), "chosen_by": ("caller", "autotuner (cached)", "autotuner")[info.source]}
 
 
 def run_grouped(args: argparse.Namespace, executor) -> dict:
@@ -620,21 +627,19 @@ def run_grouped(args: argparse.Namespace, executor) -> dict:
         wall = time.perf_counter() - t0
     h2d, d2h = ctypes.c_uint64(), ctypes.c_uint64()
     lib.fo_executor_batch_transfer_bytes(executor.raw, ctypes.byref(h2d), ctypes.byref(d2h))
-    names = ("batch_simulate_kernel", "batch_backward_kernel", "batch_diagnose_kernel", "batch_evaluate_kernel",
-             "batch_summarize_kernel")
     device_ms = sum(kernel_ms) / steps
     contracts = req.rows
     steps_per_call = _workloads.path_steps(cols, GROUPED_PATHS)
     algorithmic = grouped_algorithmic_bytes(cols, GROUPED_PATHS)
     hbm_peak, peak_kind = measured_peaks()
-    kernels = {}
-    for name, total in zip(names, kernel_ms, strict=True):
-        per = total / steps
-        b = algorithmic.get(name, 0)
-        kernels[name] = {"ms_per_call": round(per, 4), "share": round(total / sum(kernel_ms), 4),
-                         "algorithmic_bytes": b, "achieved_gbs": round(b / (per / 1e3) / 1e9, 1) if b else 0.0}
-    dominant = max(algorithmic, key=lambda k: kernels[k]["ms_per_call"])
-    achieved = algorithmic[dominant] / (kernels[dominant]["ms_per_call"] / 1e3) / 1e9
+    # One persistent launch per call: its algorithmic bytes are the training rows' store and the
+    # fits' reads and value round trips; its time also holds the (issue-bound) evaluation.
+    launch_bytes = sum(algorithmic.values())
+    kernels = {"batch_persistent_kernel": {"ms_per_call": round(device_ms, 4), "share": 1.0,
+                                           "algorithmic_bytes": launch_bytes,
+                                           "achieved_gbs": round(launch_bytes / (device_ms / 1e3) / 1e9, 1)}}
+    dominant = "batch_persistent_kernel"
+    achieved = launch_bytes / (device_ms / 1e3) / 1e9
     # The same contracts one by one on the plain per-contract path: the first GROUPED_PLAIN_SAMPLE
     # rows (whole states), each repricing its state's populations (same price and SE as the batch).
     import finoptions as fo
@@ -670,10 +675,11 @@ def run_grouped(args: argparse.Namespace, executor) -> dict:
                 "ms_per_call": wall / steps * 1e3, "h2d_bytes_per_step": int(h2d.value),
                 "d2h_bytes_per_step": int(d2h.value), "api": "fo_price_lsm_grouped_f64 (host columns in and out)"},
         "gpu_launches": launches,
+        "launch_shape": batch_launch(lib, executor),
         "kernels": kernels,
-        "roofline": {"kernel": dominant, "bound": "hbm", "achieved": round(achieved, 1), "peak": hbm_peak,
-                     "peak_source": peak_kind, "unit": "GB/s", "frac": round(achieved / hbm_peak, 4),
-                     "traffic": batch_traffic(dominant, algorithmic[dominant])},
+        "roofline": {"kernel": dominant, "bound": "hbm (fits) + issue (simulation, evaluation)",
+                     "achieved": round(achieved, 1), "peak": hbm_peak, "peak_source": peak_kind, "unit": "GB/s",
+                     "frac": round(achieved / hbm_peak, 4), "traffic": None},
         "clocks": clocks.report(),
         "plain_per_contract": plain,
         "batched_vs_plain_same_contracts": {

@@ -15,6 +15,7 @@ import os
 import shutil
 import subprocess
 import sys
+from concurrent.futures import ThreadPoolExecutor
 from pathlib import Path
 
 HERE = Path(__file__).resolve().parent
@@ -22,7 +23,7 @@ CSRC = HERE / "csrc"
 OUT_DIR = HERE / "finoptions" / "_lib"
 OUT = OUT_DIR / "libfinoptions_cuda.so"
 BUILD_DIR = HERE / "_build"
-SOURCES = ("host.cpp", "capi.cu", "lsm_kernels.cu", "lsm_greeks.cu", "lsm_batch_kernels.cu", "lsm_grouped.cu")
+SOURCES = ("host.cpp", "capi.cu", "lsm_kernels.cu", "lsm_greeks.cu", "lsm_persistent.cu", "lsm_grouped.cu")
 NVCC_FLAGS = (
     "-gencode", "arch=compute_100a,code=sm_100a",
     "-lineinfo", "-O3", "--fmad=false", "-std=c++17",
@@ -58,19 +59,24 @@ def build(verbose: bool = False, force: bool = False) -> Path:
         return OUT
     OUT_DIR.mkdir(parents=True, exist_ok=True)
     BUILD_DIR.mkdir(parents=True, exist_ok=True)
-    objects = []
-    for src in SOURCES:
+    def compile_one(src: str) -> tuple[str, subprocess.CompletedProcess]:
         obj = BUILD_DIR / (Path(src).stem + ".o")
         cmd = [nvcc(), *NVCC_FLAGS, "-x", "cu", "-c", str(CSRC / src), "-o", str(obj)]
         if verbose:
             cmd += ["-Xptxas", "-v"]
-        result = subprocess.run(cmd, capture_output=True, text=True, check=False)
+        return str(obj), subprocess.run(cmd, capture_output=True, text=True, check=False)
+
+    # The translation units are independent: compile them side by side.
+    with ThreadPoolExecutor(max_workers=max(1, min(len(SOURCES), os.cpu_count() or 1))) as pool:
+        compiled = list(pool.map(compile_one, SOURCES))
+    objects = []
+    for src, (obj, result) in zip(SOURCES, compiled, strict=True):
         if verbose or result.returncode:
             sys.stderr.write(result.stdout + result.stderr)
         if result.returncode:
             msg = f"nvcc failed for {src}"
             raise RuntimeError(msg)
-        objects.append(str(obj))
+        objects.append(obj)
     tmp = OUT.with_suffix(".so.tmp")
     link = [nvcc(), "-gencode", "arch=compute_100a,code=sm_100a", "-shared", "-o", str(tmp), *objects,
             "-Xcompiler", "-fPIC"]

@@ -792,6 +792,137 @@ Error enable_greeks(fo_lsm_call_plan* plan, bool enabled) {
     return Error{};
 }
 
+// simulate_gbm_seeded_f64 (normals == NULL: the path's Philox stream from (seed, domain)) and
+// simulate_gbm_f64 (normals: a caller matrix [intervals, paths], time-major) over K1; checks in the
+// reference's order (GbmPathPlan::simulate / simulate_seeded, path.rs:139-175, 533-615,
+// seeded.rs:384-397) with its messages. Buffers live on the device when *_on_device, else on the
+// host. Returns with the states written and the executor's stream idle.
+Error simulate_gbm(fo_executor* executor, const fo_gbm_seeded_request& q, const double* normals, uint64_t normal_rows,
+                   bool normals_on_device, double* states, uint64_t out_len, bool states_on_device) {
+    const bool external = normals != nullptr;
+    HostPlan hp;
+    Error e = build_gbm_plan(q.schedule_times, q.n_schedule_times, q.curve_times, q.n_curve_times, q.log_discounts,
+                             q.n_log_discounts, q.dividend_yield_times, q.n_dividend_yield_times,
+                             q.cumulative_dividend_yields, q.n_cumulative_dividend_yields, q.dividend_nodes,
+                             q.n_dividend_nodes, q.dividend_amounts, q.n_dividend_amounts, q.exercise_nodes,
+                             q.n_exercise_nodes, q.expiry_node, q.annualized_volatility, q.dividend_policy, &hp);
+    if (!e.ok()) return e;
+    const uint64_t paths = q.paths;
+    const uint64_t intervals = hp.intervals();
+    const double s0 = q.initial_spot;
+    auto bad_spot = [&] {
+        return make_error(FO_ERR_SIMULATION, FO_CODE_INVALID_INITIAL_SPOT,
+                          "initial spot must be finite, nonnegative, and canonical; observed " + fmt_f64(s0));
+    };
+    const bool spot_ok = std::isfinite(s0) && s0 >= 0.0 && !(s0 == 0.0 && std::signbit(s0));
+    if (external) {
+        // simulate_gbm_f64 (lib.rs:1000-1008) checks the matrix's interval rows after the plan;
+        // GbmPathPlan::validate_execution (path.rs:558-603) then the spot, the path count and the
+        // finiteness of every variate.
+        if (normal_rows != intervals)
+            return make_error(FO_ERR_SIMULATION, FO_CODE_BUFFER_LENGTH_MISMATCH,
+                              "normal interval-row buffer length mismatch: expected " + std::to_string(intervals) +
+                                  ", observed " + std::to_string(normal_rows));
+        if (!spot_ok) return bad_spot();
+        if (paths == 0)
+            return make_error(FO_ERR_SIMULATION, FO_CODE_EMPTY_PATH_SET, "simulation path count must be positive");
+    } else {
+        if (paths == 0)
+            return make_error(FO_ERR_SIMULATION, FO_CODE_EMPTY_PATH_SET, "simulation path count must be positive");
+        if (!spot_ok) return bad_spot();
+        if (paths > 0xffffffffull)
+            return make_error(FO_ERR_SIMULATION, FO_CODE_RANDOM_PATH_NAMESPACE_OVERFLOW,
+                              "seeded simulation supports at most 4294967295 paths in one random domain; observed " +
+                                  std::to_string(paths));
+    }
+    const uint64_t n_normals = external ? intervals * paths : 0;
+    const uint64_t rows = hp.rows();
+    if (!states || out_len != rows * paths)
+        return make_error(FO_ERR_EXECUTION, FO_CODE_INVALID_ARGUMENT,
+                          "states buffer must hold exactly " + std::to_string(rows * paths) + " values");
+    hp.sim_start = s0;
+    hp.initial_spot = s0;
+    hp.disc_from_later.assign(rows, 1.0);
+    hp.disc_to_origin.assign(rows, 1.0);
+    PlanLayout L = layout_for(hp, 1, 1);
+    e = executor->scratch.reserve(L.total);
+    if (e.ok()) e = executor->staging.reserve(std::max(L.inputs_bytes, L.out_bytes));
+    if (e.ok() && !states_on_device) e = executor->slab.reserve(sizeof(double) * rows * paths);
+    if (e.ok() && external && !normals_on_device) e = executor->normals.reserve(sizeof(double) * n_normals);
+    if (!e.ok()) return e;
+    unsigned char* dev = static_cast<unsigned char*>(executor->scratch.ptr);
+    pack_inputs(hp, L, static_cast<unsigned char*>(executor->staging.ptr));
+    cudaStream_t s = executor->stream;
+    DevicePlan dp = device_plan(hp, L, dev, 0);
+    auto* status = reinterpret_cast<DeviceStatus*>(dev + L.status);
+    double* out = states_on_device ? states : static_cast<double*>(executor->slab.ptr);
+    const double* d_normals = normals;
+    FO_CUDA_TRY(cudaMemcpyAsync(dev, executor->staging.ptr, L.inputs_bytes, cudaMemcpyHostToDevice, s), "upload");
+    FO_CUDA_TRY(cudaMemsetAsync(status, 0xff, kStatusNoneBytes, s), "reset");
+    if (external) {
+        if (!normals_on_device) {
+            FO_CUDA_TRY(cudaMemcpyAsync(executor->normals.ptr, normals, sizeof(double) * n_normals,
+                                        cudaMemcpyHostToDevice, s),
+                        "normals upload");
+            d_normals = static_cast<const double*>(executor->normals.ptr);
+        }
+        // Every variate is checked before any path is computed (path.rs:596-603).
+        unsigned long long first = 0;
+        FO_CUDA_TRY(launch_first_nonfinite(d_normals, n_normals, &status->eval_sim_fail, s), "normals check");
+        FO_CUDA_TRY(cudaMemcpyAsync(&first, &status->eval_sim_fail, sizeof(first), cudaMemcpyDeviceToHost, s), "status");
+        FO_CUDA_TRY(cudaStreamSynchronize(s), "normals check");
+        if (first != kNone) {
+            double observed = 0.0;
+            FO_CUDA_TRY(cudaMemcpyAsync(&observed, d_normals + first, sizeof(double), cudaMemcpyDeviceToHost, s),
+                        "normal copy");
+            FO_CUDA_TRY(cudaStreamSynchronize(s), "normal copy");
+            Error ne = make_error(FO_ERR_SIMULATION, FO_CODE_NON_FINITE_NORMAL_BUFFER,
+                                  "standard-normal buffer contains a non-finite value at interval " +
+                                      std::to_string(first / paths) + ", path " + std::to_string(first % paths) + ": " +
+                                      fmt_f64(observed));
+            ne.path = int64_t(first % paths);
+            return ne;
+        }
+        FO_CUDA_TRY(launch_simulate_external(dp, paths, d_normals, out, &status->train_sim_fail, s), "simulation launch");
+    } else {
+        FO_CUDA_TRY(launch_simulate(dp, paths, q.seed, q.domain, out, 0, 0, &status->train_sim_fail, s),
+                    "simulation launch");
+    }
+    unsigned long long fail = 0;
+    FO_CUDA_TRY(cudaMemcpyAsync(&fail, &status->train_sim_fail, sizeof(fail), cudaMemcpyDeviceToHost, s), "status");
+    FO_CUDA_TRY(cudaStreamSynchronize(s), "simulation");
+    if (fail != kNone) {
+        auto* d_replay = reinterpret_cast<SimFailure*>(dev + L.replay);
+        SimFailure f{};
+        if (external)
+            FO_CUDA_TRY(launch_replay_external(dp, paths, d_normals, fail, d_replay, s), "replay");
+        else
+            FO_CUDA_TRY(launch_replay(dp, q.seed, q.domain, uint32_t(fail), -1, d_replay, s), "replay");
+        FO_CUDA_TRY(cudaMemcpyAsync(&f, d_replay, sizeof(f), cudaMemcpyDeviceToHost, s), "replay copy");
+        FO_CUDA_TRY(cudaStreamSynchronize(s), "replay");
+        Error se = make_error(FO_ERR_SIMULATION, simulation_failure_code(f.code),
+                              simulation_failure_message(f.code, uint32_t(f.interval), fail, f.spot, f.normal));
+        se.path = int64_t(fail);
+        return se;
+    }
+    if (!states_on_device) {
+        FO_CUDA_TRY(cudaMemcpyAsync(states, out, sizeof(double) * rows * paths, cudaMemcpyDeviceToHost, s), "states copy");
+        FO_CUDA_TRY(cudaStreamSynchronize(s), "states copy");
+    }
+    return Error{};
+}
+
+// The standalone simulation exports classify failures as the reference's Python boundary does
+// (IntoPySimulationError, crates/finoptions-python/src/lib.rs:277-292): non-finite transitions and
+// exhausted or rejected random draws stay SimulationErrors, every other simulation failure (spot,
+// path count, buffer lengths, non-finite normals, escrowed forwards) is an InputError.
+Error simulation_entry_error(Error e) {
+    if (e.kind == FO_ERR_SIMULATION && e.code != FO_CODE_NON_FINITE_PATH_TRANSITION &&
+        e.code != FO_CODE_RANDOM_NORMAL_BUDGET_EXHAUSTED && e.code != FO_CODE_RANDOM_NORMAL_REJECTION_LIMIT)
+        e.kind = FO_ERR_INPUT;
+    return e;
+}
+
 int finish(fo_error* err, const Error& e) {
     if (!e.ok()) write_error(err, e);
     return e.kind;
@@ -987,67 +1118,28 @@ int fo_simulate_gbm_seeded_f64(fo_executor* executor, const fo_gbm_seeded_reques
     if (!e.ok()) return finish(err, e);
     std::lock_guard<std::mutex> lock(executor->mu);
     cudaSetDevice(executor->device);
-    HostPlan hp;
-    e = build_gbm_plan(q->schedule_times, q->n_schedule_times, q->curve_times, q->n_curve_times, q->log_discounts,
-                       q->n_log_discounts, q->dividend_yield_times, q->n_dividend_yield_times, q->cumulative_dividend_yields,
-                       q->n_cumulative_dividend_yields, q->dividend_nodes, q->n_dividend_nodes, q->dividend_amounts,
-                       q->n_dividend_amounts, q->exercise_nodes, q->n_exercise_nodes, q->expiry_node,
-                       q->annualized_volatility, q->dividend_policy, &hp);
+    return finish(err, simulation_entry_error(simulate_gbm(executor, *q, nullptr, 0, false, states, out_len, false)));
+}
+
+int fo_simulate_gbm_f64(fo_executor* executor, const fo_gbm_seeded_request* q, const double* normals,
+                        uint64_t normal_rows, double* states, uint64_t out_len, fo_error* err) {
+    Error e = require(executor, "executor");
+    if (e.ok()) e = require(q, "request");
+    if (e.ok()) e = require(normals, "normals");
     if (!e.ok()) return finish(err, e);
-    // validate_seeded (seeded.rs:384-397)
-    const double s0 = q->initial_spot;
-    if (!std::isfinite(s0) || s0 < 0.0 || (s0 == 0.0 && std::signbit(s0)))
-        return finish(err, make_error(FO_ERR_SIMULATION, FO_CODE_INVALID_INITIAL_SPOT,
-                                      "initial spot must be finite, nonnegative, and canonical; observed " + fmt_f64(s0)));
-    if (q->paths == 0)
-        return finish(err, make_error(FO_ERR_SIMULATION, FO_CODE_EMPTY_PATH_SET, "simulation path count must be positive"));
-    if (q->paths > 0xffffffffull)
-        return finish(err, make_error(FO_ERR_SIMULATION, FO_CODE_RANDOM_PATH_NAMESPACE_OVERFLOW,
-                                      "seeded simulation supports at most 4294967295 paths in one random domain; observed " +
-                                          std::to_string(q->paths)));
-    const uint64_t rows = hp.rows();
-    if (!states || out_len != rows * q->paths)
-        return finish(err, make_error(FO_ERR_EXECUTION, FO_CODE_INVALID_ARGUMENT,
-                                      "states buffer must hold exactly " + std::to_string(rows * q->paths) + " values"));
-    hp.sim_start = s0;
-    hp.initial_spot = s0;
-    hp.disc_from_later.assign(rows, 1.0);
-    hp.disc_to_origin.assign(rows, 1.0);
-    PlanLayout L = layout_for(hp, 1, 1);
-    e = executor->scratch.reserve(L.total);
-    if (e.ok()) e = executor->staging.reserve(std::max(L.inputs_bytes, L.out_bytes));
-    if (e.ok()) e = executor->slab.reserve(sizeof(double) * rows * q->paths);
+    std::lock_guard<std::mutex> lock(executor->mu);
+    cudaSetDevice(executor->device);
+    return finish(err, simulation_entry_error(simulate_gbm(executor, *q, normals, normal_rows, false, states, out_len, false)));
+}
+
+int fo_simulate_gbm_device_f64(fo_executor* executor, const fo_gbm_seeded_request* q, const double* device_normals,
+                               uint64_t normal_rows, double* device_states, uint64_t out_len, fo_error* err) {
+    Error e = require(executor, "executor");
+    if (e.ok()) e = require(q, "request");
     if (!e.ok()) return finish(err, e);
-    unsigned char* dev = static_cast<unsigned char*>(executor->scratch.ptr);
-    pack_inputs(hp, L, static_cast<unsigned char*>(executor->staging.ptr));
-    cudaStream_t s = executor->stream;
-    DevicePlan dp = device_plan(hp, L, dev, 0);
-    auto* status = reinterpret_cast<DeviceStatus*>(dev + L.status);
-    auto run = [&]() -> Error {
-        FO_CUDA_TRY(cudaMemcpyAsync(dev, executor->staging.ptr, L.inputs_bytes, cudaMemcpyHostToDevice, s), "upload");
-        FO_CUDA_TRY(cudaMemsetAsync(status, 0xff, kStatusNoneBytes, s), "reset");
-        FO_CUDA_TRY(launch_simulate(dp, q->paths, q->seed, q->domain, static_cast<double*>(executor->slab.ptr), 0, 0,
-                                    &status->train_sim_fail, s),
-                    "simulation launch");
-        unsigned long long fail = 0;
-        FO_CUDA_TRY(cudaMemcpyAsync(&fail, &status->train_sim_fail, sizeof(fail), cudaMemcpyDeviceToHost, s), "status");
-        FO_CUDA_TRY(cudaStreamSynchronize(s), "simulation");
-        if (fail != kNone) {
-            auto* d_replay = reinterpret_cast<SimFailure*>(dev + L.replay);
-            SimFailure f{};
-            FO_CUDA_TRY(launch_replay(dp, q->seed, q->domain, uint32_t(fail), -1, d_replay, s), "replay");
-            FO_CUDA_TRY(cudaMemcpyAsync(&f, d_replay, sizeof(f), cudaMemcpyDeviceToHost, s), "replay copy");
-            FO_CUDA_TRY(cudaStreamSynchronize(s), "replay");
-            Error se = make_error(FO_ERR_SIMULATION, simulation_failure_code(f.code),
-                                  simulation_failure_message(f.code, uint32_t(f.interval), fail, f.spot, f.normal));
-            se.path = int64_t(fail);
-            return se;
-        }
-        FO_CUDA_TRY(cudaMemcpy(states, executor->slab.ptr, sizeof(double) * rows * q->paths, cudaMemcpyDeviceToHost),
-                    "states copy");
-        return Error{};
-    };
-    return finish(err, run());
+    std::lock_guard<std::mutex> lock(executor->mu);
+    cudaSetDevice(executor->device);
+    return finish(err, simulation_entry_error(simulate_gbm(executor, *q, device_normals, normal_rows, true, device_states, out_len, true)));
 }
 
 int fo_sample_standard_normals_f64(fo_executor* executor, uint64_t seed, uint32_t domain, uint32_t path_start,

@@ -5,11 +5,13 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <map>
 #include <mutex>
 #include <string>
 
 #include "../../include/finoptions_cuda.h"
 #include "host.h"
+#include "lsm_batch_kernels.h"
 
 namespace fo {
 
@@ -83,6 +85,7 @@ struct fo_executor {
     std::mutex mu;
     fo::DeviceBuffer slab;        // training path storage shared by this executor's plans (stream-ordered)
     fo::DeviceBuffer scratch;     // per-call block for one-shot calls
+    fo::DeviceBuffer normals;     // caller standard normals of a host-buffer external-normal simulation
     fo::PinnedBuffer staging;     // one-shot upload / download staging
     fo::DeviceBuffer batch;       // batch arena (plans, records, values, outputs)
     fo::PinnedBuffer batch_host;  // batch upload / download staging
@@ -90,6 +93,15 @@ struct fo_executor {
     double batch_ms[FO_BATCH_KERNELS] = {};              // last batch call, summed over waves
     uint64_t batch_launches = 0;
     uint64_t batch_h2d = 0, batch_d2h = 0;                // bytes copied by the last batch call
+    fo::BatchTuning batch_tuning;                         // launch shape when the autotuner is off
+    bool batch_autotune = true;                           // pick shapes per class (else batch_tuning)
+    std::map<std::string, fo::BatchTuning> batch_tuned;   // autotuned shape per wave class
+    fo::BatchTuning batch_tuning_used;                    // shape of the last batch launch
+    int batch_tuning_source = 0;                          // 0 set by the caller, 1 cached, 2 tuned now
+    uint64_t batch_tuning_runs = 0;                       // launches the last tuning timed
+    int batch_grid = 0;                                   // CTAs of the last batch launch
+    int batch_strikes = 0;                                // strikes per evaluation item of the last launch
+    uint64_t batch_items = 0;                             // work items of the last launch
     ~fo_executor() {
         for (cudaEvent_t& e : batch_marks)
             if (e) cudaEventDestroy(e);

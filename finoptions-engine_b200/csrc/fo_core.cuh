@@ -760,6 +760,21 @@ FO_HD bool fit_near_pivot(const dd* sums, double pivot, uint64_t count, double r
     return true;
 }
 
+// Whether a row's power sums about `pivot` must be taken again about the row's own mean. Each
+// term t^k = (x - pivot)^k is rounded on its own, and the binomial shift to the mean multiplies
+// those roundings by about ((|mean - pivot| + sd) / sd)^(2d): a pivot more than one standard
+// deviation from the mean (a small in-the-money population whose mean moved far from the previous
+// row's) loses the digits the fit needs. *mean_out receives the mean rounded to binary64, the new
+// pivot; about it the offset is a rounding error and the near-pivot solve applies.
+FO_HD bool pivot_too_far(const dd* sums, double pivot, uint64_t count, double* mean_out) {
+    const double n = double(count);
+    const double t1 = sums[1].hi + sums[1].lo;
+    const double offset = t1 / n;
+    const double var = (sums[2].hi + sums[2].lo - t1 * offset) / n;
+    *mean_out = pivot + offset;
+    return var > 0.0 && offset * offset > var && fo_isfinite(*mean_out);
+}
+
 FO_HD_NOINLINE void fit_continuation(const dd* sums, double pivot, uint64_t count, int degree,
                                      double rank_tolerance, FitModel* m) {
     bool done = false;

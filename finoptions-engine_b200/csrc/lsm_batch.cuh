@@ -94,10 +94,43 @@ struct PolicyRule {
 // Shared memory the evaluation may spend on staged rules; larger groups read them from HBM.
 constexpr size_t kEvalRuleSmemBytes = 96 * 1024;
 
+// ---- persistent launch ------------------------------------------------------------------------
+// One launch prices a whole wave: its CTAs take work items from a queue in order until it is empty.
+// The queue is topologically ordered (every item depends only on items before it), so every item a
+// CTA waits on has already been taken by a running CTA, and the waits end.
+enum BatchItemKind : uint32_t {
+    kItemNone = 0,
+    kItemSimulate = 1,  // training paths of blocks [first, first + count) of group `index`
+    kItemBackward = 2,  // backward fit (and row diagnostics) of problem `index`
+    kItemEvaluate = 3,  // evaluation blocks [first, first + count) of group `index`, strike chunk `chunk`
+};
+
+struct BatchItem {
+    uint32_t kind;
+    uint32_t index;
+    uint32_t first;
+    uint32_t count;
+    uint32_t chunk;
+    uint32_t pad[3];
+};
+
+// Dependency counters of one launch, all zeroed before it: a group's backward items wait until
+// sim_done[g] reaches its training blocks, its evaluation items until bwd_done[g] reaches its
+// problems; the item that brings eval_done[g] to the group's evaluation units writes the group's
+// summaries. A wait gives up after a time limit and raises *timeout (no item ever waits forever).
+struct BatchQueue {
+    const BatchItem* items;
+    uint32_t n_items;
+    unsigned* next;
+    unsigned* sim_done;
+    unsigned* bwd_done;
+    unsigned* eval_done;
+    unsigned* timeout;
+};
+
 struct BatchArgs {
     const BatchGroup* groups;
     const BatchProblem* problems;
-    const uint32_t* backward_order;  // [problems]: problem of backward CTA i, largest work first
     uint32_t n_groups;
     uint32_t n_problems;
     double* slab;

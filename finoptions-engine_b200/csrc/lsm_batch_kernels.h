@@ -1,4 +1,4 @@
-// lsm_batch_kernels.h - host launchers of the batch LSM kernels (lsm_batch_kernels.cu).
+// lsm_batch_kernels.h - host interface of the persistent batch LSM kernel (lsm_persistent.cu).
 #pragma once
 
 #include <cuda_runtime.h>
@@ -11,18 +11,20 @@ constexpr int kBatchSimThreads = 256;
 constexpr int kBatchBackwardThreads = 256;
 constexpr int kBatchEvalThreads = 256;
 
-cudaError_t launch_batch_simulate(const BatchArgs& a, cudaStream_t stream);
-// backward_order holds the n_large problems above 64Ki paths first (clusters of four CTAs on
-// `stream`), then the rest (one CTA each, on `side` between fork and join when side is not null).
-cudaError_t launch_batch_backward(const BatchArgs& a, uint32_t n_large, cudaStream_t stream, cudaStream_t side,
-                                  cudaEvent_t fork, cudaEvent_t join);
-cudaError_t launch_batch_diagnose(const BatchArgs& a, uint32_t n_records, cudaStream_t stream);
-// max_strikes: strikes of the widest group; max_rows: the largest observation-row count of the
-// wave's groups (sizes the staged rules).
-cudaError_t launch_batch_evaluate(const BatchArgs& a, uint32_t max_strikes, uint32_t max_rows, cudaStream_t stream);
-// One block per (path block, group, strike): the adjoint Greeks variant of the evaluation.
-cudaError_t launch_batch_evaluate_greeks(const BatchArgs& a, uint32_t max_strikes, uint32_t max_rows,
-                                         cudaStream_t stream);
-cudaError_t launch_batch_summarize(const BatchArgs& a, cudaStream_t stream);
+// Launch shape of a persistent batch launch (lsm_persistent.cu). The autotuner picks it per shape
+// class; the results do not depend on it.
+struct BatchTuning {
+    int sim_blocks = 2;   // training-simulation blocks of 256 paths per work item
+    int eval_blocks = 1;  // evaluation blocks of 256 paths per work item
+    int strikes = 8;      // strikes an evaluation item applies together (1, 2, 4 or 8)
+    int ctas_per_sm = 0;  // resident CTAs per SM (0: as many as fit)
+};
+
+// Shared memory of the staged fitted rules: `strikes` x rule_rows PolicyRules, or with the Greeks
+// one strike's rules and its per-row stopping counts.
+size_t persistent_rule_bytes(int strikes, bool greeks, uint32_t rule_rows);
+// One persistent launch over the queue q; *grid_out receives the CTAs launched.
+cudaError_t launch_batch_persistent(const BatchArgs& a, const BatchQueue& q, int strikes, uint32_t rule_rows,
+                                    bool stage, int ctas_per_sm, cudaStream_t stream, int* grid_out);
 
 }  // namespace fo

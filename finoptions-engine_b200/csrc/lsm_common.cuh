@@ -80,6 +80,37 @@ __device__ __forceinline__ SimResult simulate_path(const DevicePlan& plan, const
     return r;
 }
 
+// simulate_path for caller-supplied standard normals: normals[i * paths + path] drives interval i
+// (GbmPathPlan::simulate with an external shock matrix, path.rs:139-175). The buffer was checked for
+// non-finite values before the launch; only a non-finite transition fails here.
+template <typename Store>
+__device__ __forceinline__ SimResult simulate_path_external(const DevicePlan& plan, const double* normals,
+                                                            uint64_t paths, uint64_t path, Store&& store) {
+    double spot = plan.sim_start;
+    SimResult r{0, 0, 0.0, 0.0};
+    if (plan.row_node[0] == 0) store(0, spot);
+    for (uint32_t i = 0; i < plan.intervals; ++i) {
+        const double z = normals[uint64_t(i) * paths + path];
+        const StepCoef c = plan.steps[i];
+        const double next = gbm_advance(spot, c.diffusion, c.log_drift, z);
+        if (!fo_isfinite(next)) {
+            r.code = 3;
+            r.interval = int(i);
+            r.spot = spot;
+            r.normal = z;
+            return r;
+        }
+        spot = next;
+        const NodeEvent ev = plan.events[i + 1];
+        const bool dividend = (ev.flags & kEventDividend) != 0;
+        const bool terminal = (ev.flags & kEventTerminal) != 0;
+        if (dividend && terminal) spot = apply_cash_dividend(plan.policy, ev.dividend_amount, spot);
+        if (ev.row >= 0) store(ev.row, spot);
+        if (dividend && !terminal) spot = apply_cash_dividend(plan.policy, ev.dividend_amount, spot);
+    }
+    return r;
+}
+
 // ---------------------------------------------------------------------------------------------
 // Reductions
 // ---------------------------------------------------------------------------------------------

@@ -172,7 +172,7 @@ __device__ __noinline__ bool fit_near_pivot_warp(const dd* sums, double pivot, u
 // = rank_limit(rank_tolerance)); on return *m is complete and visible to the whole warp. Degree 0
 // and the double-double fallback (pivot more than one standard deviation from the mean) run on
 // lane 0 as in fit_continuation.
-__device__ __noinline__ void fit_continuation_warp(const dd* sums, double pivot, uint64_t count, int degree,
+static __device__ __noinline__ void fit_continuation_warp(const dd* sums, double pivot, uint64_t count, int degree,
                                                    double rank_tolerance, double spread_limit, FitModel* m) {
     const bool writer = (threadIdx.x & 31) == 0;
     bool done;

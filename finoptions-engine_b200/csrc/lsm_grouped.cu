@@ -5,12 +5,14 @@
 // Host side: request validation in the reference's order (lib.rs:1302-1415 parse_batch_lsm_method,
 // input.rs try_new, BatchRandomStreams::validate, validate_exercise_mesh_domain), then per group
 // the exact union mesh, curves, event schedule and simulation plan (build_path_plan). Groups are
-// priced in waves sized to the device memory budget; each wave is five kernels
-// (lsm_batch_kernels.cu). The lowest failing group is reported with the typed error its serial
-// replay in the reference would raise (pricing.rs:452-503); no partial result is returned.
+// priced in waves sized to the device memory budget; each wave is one persistent launch that
+// drains a queue of simulation, fit and evaluation items (lsm_persistent.cu). The lowest failing
+// group is reported with the typed error its serial replay in the reference would raise
+// (pricing.rs:452-503); no partial result is returned.
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <numeric>
 #include <thread>
 #include <utility>
 #include <cmath>
@@ -30,6 +32,10 @@ using namespace fo;
 namespace {
 
 constexpr unsigned long long kNone = ~0ull;
+// Shared memory the persistent launch may spend on staged fitted rules (with three 80-register
+// CTAs per SM, about 57 KB each leaves every CTA resident; more lowers the CTAs per SM).
+constexpr size_t kPersistentRuleSmemBytes = 200 * 1024;
+constexpr int kPersistentMaxCtasPerSm = 3;  // the persistent kernel's launch bounds
 constexpr uint64_t kU32Max = 0xffffffffull;
 
 std::string u(uint64_t v) { return std::to_string(v); }
@@ -793,7 +799,8 @@ Error build_group(const BatchMethod& m, const GroupSpec& gs, GroupWork* w) {
 // ---- device layout of one wave ------------------------------------------------------------------
 
 struct WaveLayout {
-    size_t groups, problems, order, group_status, problem_status, summaries;  // read-back region: group_status..summaries
+    size_t groups, problems, items, group_status, problem_status, summaries;  // read-back region: group_status..summaries
+    size_t counters;
     size_t greek_sums;                                                  // (read back, Greeks only)
     size_t counts, itm_counts, stop_counts, eval_partials, greek_partials, records, values, slab, replay;
     size_t out_begin, out_bytes, clear_begin, clear_bytes, total;
@@ -808,6 +815,7 @@ struct Wave {
     uint32_t eval_blocks = 0;    // largest evaluation grid of a group
     uint32_t train_blocks = 0;   // largest training grid of a group
     uint64_t partial_slots = 0;  // evaluation blocks summed over the problems (one partial slot each)
+    uint64_t item_bound = 0;     // work items of the persistent launch, at most (one block per item)
     bool greeks = false;         // adjoint Greeks buffers
 };
 
@@ -827,7 +835,7 @@ WaveLayout layout_for(const Wave& w, size_t base) {
     const uint64_t G = w.g1 - w.g0, P = w.problems;
     L.groups = take(sizeof(BatchGroup) * G);
     L.problems = take(sizeof(BatchProblem) * P);
-    L.order = take(sizeof(uint32_t) * P);
+    L.items = take(sizeof(BatchItem) * std::max<uint64_t>(w.item_bound, 1));
     off = align_up(off, 256);
     L.out_begin = off;
     L.group_status = take(sizeof(GroupStatus) * G);
@@ -841,6 +849,7 @@ WaveLayout layout_for(const Wave& w, size_t base) {
     L.itm_counts = take(sizeof(unsigned) * w.records);
     L.stop_counts = take(w.greeks ? sizeof(unsigned) * w.records : 0);
     L.records = take(sizeof(FitRecord) * w.records);
+    L.counters = take(sizeof(unsigned) * (3 * G + 2));  // next item, timeout, sim / bwd / eval done per group
     off = align_up(off, 256);
     L.clear_bytes = off - L.clear_begin;
     L.eval_partials = take(sizeof(double2) * 2 * std::max<uint64_t>(w.partial_slots, 1));
@@ -1102,6 +1111,69 @@ void write_greeks(const GreeksSink& sink, uint64_t row, const GroupWork& gw, dou
     dl[hp.row_node[rows - 1]] += sums[kGreekTerminal] / n;
 }
 
+// Shape class of a wave for the autotuner: launches of one class share their best launch shape.
+template <typename Work, typename WaveT>
+std::string tuning_key(const Work& work, const WaveT& w, bool greeks, int degree, uint32_t max_rows,
+                       uint32_t max_strikes) {
+    uint64_t max_paths = 1;
+    for (uint64_t g = w.g0; g < w.g1; ++g) max_paths = std::max<uint64_t>(max_paths, work[g].hp.train_paths);
+    auto log2_ceil = [](uint64_t v) {
+        int k = 0;
+        while ((uint64_t(1) << k) < v && k < 63) ++k;
+        return k;
+    };
+    return std::to_string(greeks) + "/" + std::to_string(degree) + "/" + std::to_string(log2_ceil(max_paths)) + "/" +
+           std::to_string((max_rows + 15) / 16) + "/" + std::to_string(max_strikes) + "/" +
+           std::to_string(log2_ceil(w.g1 - w.g0));
+}
+
+// The autotuner: a coordinate search from the default launch shape over the evaluation blocks per
+// item, the simulation blocks per item, the strikes per evaluation item and the CTAs per SM, each
+// candidate timed by one launch of the wave; a change is kept when it is at least 2% faster.
+template <typename Run>
+Error autotune_wave(Run& run, bool greeks, int max_strikes, BatchTuning* best, uint64_t* runs) {
+    BatchTuning cur;
+    float cur_ms = 0.f;
+    Error e = run(cur, &cur_ms);
+    if (!e.ok()) return e;
+    *runs = 1;
+    auto attempt = [&](BatchTuning cand) -> Error {
+        float ms = 0.f;
+        Error te = run(cand, &ms);
+        if (!te.ok()) return te;
+        *runs += 1;
+        if (ms < 0.98f * cur_ms) {
+            cur = cand;
+            cur_ms = ms;
+        }
+        return Error{};
+    };
+    for (const int eval_blocks : {2, 4}) {
+        BatchTuning c = cur;
+        c.eval_blocks = eval_blocks;
+        if (!(e = attempt(c)).ok()) return e;
+    }
+    {
+        BatchTuning c = cur;
+        c.sim_blocks = 8;
+        if (!(e = attempt(c)).ok()) return e;
+    }
+    int widest = 1;
+    while (widest < kEvalStrikes && widest < max_strikes) widest *= 2;
+    if (!greeks && widest > 1) {
+        BatchTuning c = cur;
+        c.strikes = widest / 2;
+        if (!(e = attempt(c)).ok()) return e;
+    }
+    {
+        BatchTuning c = cur;
+        c.ctas_per_sm = 2;
+        if (!(e = attempt(c)).ok()) return e;
+    }
+    *best = cur;
+    return Error{};
+}
+
 // Prices validated groups: host plans, waves within the memory budget, five kernels per wave,
 // the lowest failing group's typed error or the row-aligned result columns (and, with a sink,
 // the adjoint Greeks of every row).
@@ -1208,6 +1280,7 @@ Error price_groups(fo_executor* ex, const BatchMethod& m, const std::vector<Grou
             cur.eval_blocks = std::max(cur.eval_blocks, eval_blocks);
             cur.train_blocks = std::max(cur.train_blocks, train_blocks);
             cur.partial_slots += strikes_g * eval_blocks;
+            cur.item_bound += train_blocks + strikes_g + strikes_g * eval_blocks;
             cur.greeks = greeks;
             bytes += cost;
         }
@@ -1221,11 +1294,13 @@ Error price_groups(fo_executor* ex, const BatchMethod& m, const std::vector<Grou
     std::vector<DevicePlan> plans(launchable);
     for (uint64_t g = 0; g < launchable; ++g) plans[g] = device_plan(work[g].hp, offsets[g], dev);
 
-    // Host staging: inputs, then per wave the group / problem tables and the read-back region.
+    // Host staging: inputs, then per wave the group / problem / item tables followed by the
+    // read-back region. The two never overlap: the autotuner launches a wave several times from the
+    // same tables, reading results back between the launches.
     size_t stage = in_bytes;
     for (const Wave& w : waves) {
         const WaveLayout L = layout_for(w, 0);
-        stage = std::max(stage, std::max(L.out_begin, L.out_bytes));
+        stage = std::max(stage, L.out_begin + L.out_bytes);
     }
     e = ex->batch_host.reserve(stage);
     if (!e.ok()) return e;
@@ -1259,6 +1334,7 @@ Error price_groups(fo_executor* ex, const BatchMethod& m, const std::vector<Grou
         // Group and problem tables.
         auto* hg = reinterpret_cast<BatchGroup*>(host + (L.groups - in_bytes));
         auto* hpb = reinterpret_cast<BatchProblem*>(host + (L.problems - in_bytes));
+        unsigned char* back = host + (L.out_begin - in_bytes);  // the read-back region, after the tables
         uint64_t slab = 0, record = 0, problem = 0, values = 0, partial = 0;
         slab_of.assign(w.g1 - w.g0, 0);
         uint32_t max_rows = 1, max_strikes = 1;
@@ -1288,87 +1364,178 @@ Error price_groups(fo_executor* ex, const BatchMethod& m, const std::vector<Grou
             slab += uint64_t(hp.rows() - (hp.origin_row ? 1 : 0)) * hp.train_paths;
             max_rows = std::max<uint32_t>(max_rows, hp.rows());
         }
-        // Backward dispatch order: the problems above 64Ki training paths (run by clusters of CTAs)
-        // first, then the rest; within each, largest training work (paths x rows) first, ties in
-        // problem order.
-        uint32_t n_large = 0;
-        {
-            auto* order = reinterpret_cast<uint32_t*>(host + (L.order - in_bytes));
-            std::vector<std::pair<uint64_t, uint32_t>> work_of;
-            work_of.reserve(w.problems);
-            for (uint64_t i = 0; i < w.problems; ++i) {
-                const HostPlan& hp = work[w.g0 + hpb[i].group].hp;
-                const bool large = hp.train_paths > 65536;
-                n_large += large ? 1u : 0u;
-                work_of.emplace_back(uint64_t(hp.train_paths) * hp.rows(), uint32_t(i));
+        // One persistent launch of the wave with launch shape `tune`. Every launch recomputes the
+        // whole wave from its inputs (the state it writes is cleared first), so the result does not
+        // depend on the shape or on launches before it.
+        auto run_wave = [&](const BatchTuning& tune, float* launch_ms) -> Error {
+            // The persistent launch's work queue (lsm_persistent.cu), topologically ordered: every
+            // group's training simulation (largest training work first, long fits right after their
+            // group's), the other fits (largest paths x rows first, ties in problem order), then the
+            // groups' evaluations in the order their last fit was queued. Items cover tune.sim_blocks / tune.eval_blocks blocks of 256
+            // paths; an evaluation item applies `eval_strikes` strikes together (all of a group's strikes
+            // when they fit, with the Greeks one).
+            const uint64_t G = w.g1 - w.g0;
+            int eval_strikes = 1;
+            if (!greeks)
+                while (eval_strikes < kEvalStrikes && eval_strikes < int(max_strikes) && eval_strikes < tune.strikes)
+                    eval_strikes *= 2;
+            const size_t rule_bytes = persistent_rule_bytes(eval_strikes, greeks, max_rows);
+            const bool stage = rule_bytes <= kPersistentRuleSmemBytes;
+            if (greeks && !stage)
+                return make_error(FO_ERR_EXECUTION, FO_CODE_CAPACITY_EXCEEDED,
+                                  "adjoint Greeks of a batch hold at most " +
+                                      u(kPersistentRuleSmemBytes / (sizeof(PolicyRule) + 4)) +
+                                      " observation rows per contract; observed " + u(max_rows));
+            std::vector<BatchItem> items;
+            items.reserve(w.item_bound);
+            {
+                const uint32_t sim_step = uint32_t(std::max(1, tune.sim_blocks));
+                const uint32_t eval_step = uint32_t(std::max(1, tune.eval_blocks));
+                std::vector<uint32_t> gorder(G);
+                std::iota(gorder.begin(), gorder.end(), 0u);
+                auto train_work = [&](uint32_t gl) {
+                    const HostPlan& hp = work[w.g0 + gl].hp;
+                    return uint64_t(hp.train_paths) * hp.rows() * (1 + uint64_t(hg[gl].problems));
+                };
+                std::stable_sort(gorder.begin(), gorder.end(),
+                                 [&](uint32_t x, uint32_t y) { return train_work(x) > train_work(y); });
+                // Fits by work (training paths x rows), largest first. A fit that alone is long next to
+                // a CTA's share of all fitting work (at least half of it on the largest grid) is queued
+                // right after its group's simulation, so it starts early instead of after every
+                // group's simulation.
+                std::vector<std::pair<uint64_t, uint32_t>> fits;
+                fits.reserve(w.problems);
+                uint64_t fit_work = 0;
+                for (uint64_t i = 0; i < w.problems; ++i) {
+                    const HostPlan& hp = work[w.g0 + hpb[i].group].hp;
+                    fits.emplace_back(uint64_t(hp.train_paths) * hp.rows(), uint32_t(i));
+                    fit_work += fits.back().first;
+                }
+                std::stable_sort(fits.begin(), fits.end(), [](const auto& x, const auto& y) { return x.first > y.first; });
+                const uint64_t long_fit = fit_work / (2 * uint64_t(std::max(1, ex->sms)) * kPersistentMaxCtasPerSm);
+                std::vector<std::vector<uint32_t>> early(G);
+                std::vector<uint32_t> late;
+                for (const auto& f : fits) {
+                    if (f.first >= long_fit) early[hpb[f.second].group].push_back(f.second);
+                    else late.push_back(f.second);
+                }
+                std::vector<uint64_t> last_fit(G, 0);
+                uint64_t queued_fits = 0;
+                auto queue_fit = [&](uint32_t i) {
+                    items.push_back(BatchItem{kItemBackward, i, 0, 0, 0, {0, 0, 0}});
+                    last_fit[hpb[i].group] = queued_fits++;
+                };
+                for (const uint32_t gl : gorder) {
+                    const uint32_t blocks = eval_blocks_for(work[w.g0 + gl].hp.train_paths);
+                    for (uint32_t b = 0; b < blocks; b += sim_step)
+                        items.push_back(BatchItem{kItemSimulate, gl, b, std::min(sim_step, blocks - b), 0, {0, 0, 0}});
+                    for (const uint32_t i : early[gl]) queue_fit(i);
+                }
+                for (const uint32_t i : late) queue_fit(i);
+                std::vector<uint32_t> eorder(G);
+                std::iota(eorder.begin(), eorder.end(), 0u);
+                std::stable_sort(eorder.begin(), eorder.end(),
+                                 [&](uint32_t x, uint32_t y) { return last_fit[x] < last_fit[y]; });
+                for (const uint32_t gl : eorder) {
+                    const uint32_t blocks = eval_blocks_for(work[w.g0 + gl].hp.eval_paths);
+                    const uint32_t chunks = greeks ? hg[gl].problems : (hg[gl].problems + eval_strikes - 1) / eval_strikes;
+                    for (uint32_t z = 0; z < chunks; ++z)
+                        for (uint32_t b = 0; b < blocks; b += eval_step)
+                            items.push_back(BatchItem{kItemEvaluate, gl, b, std::min(eval_step, blocks - b), z, {0, 0, 0}});
+                }
+                std::memcpy(host + (L.items - in_bytes), items.data(), sizeof(BatchItem) * items.size());
             }
-            std::stable_sort(work_of.begin(), work_of.end(), [&](const auto& x, const auto& y) {
-                const bool lx = work[w.g0 + hpb[x.second].group].hp.train_paths > 65536;
-                const bool ly = work[w.g0 + hpb[y.second].group].hp.train_paths > 65536;
-                if (lx != ly) return lx;
-                return x.first > y.first;
-            });
-            for (uint64_t i = 0; i < w.problems; ++i) order[i] = work_of[i].second;
+            // The group and problem tables and the queue's items (the item region is sized for the
+            // finest cut; only the items of this launch shape travel).
+            const size_t table_bytes = (L.items - L.groups) + sizeof(BatchItem) * items.size();
+            FO_CUDA_TRY(cudaMemcpyAsync(dev + L.groups, host + (L.groups - in_bytes), table_bytes,
+                                        cudaMemcpyHostToDevice, s),
+                        "batch table upload");
+            ex->batch_h2d += table_bytes;
+            FO_CUDA_TRY(cudaMemsetAsync(dev + L.out_begin, 0xff, L.summaries - L.out_begin, s), "batch status reset");
+            FO_CUDA_TRY(cudaMemsetAsync(dev + L.clear_begin, 0, L.clear_bytes, s), "batch reset");
+            BatchArgs a{};
+            a.groups = reinterpret_cast<const BatchGroup*>(dev + L.groups);
+            a.problems = reinterpret_cast<const BatchProblem*>(dev + L.problems);
+            a.n_groups = uint32_t(G);
+            a.n_problems = uint32_t(w.problems);
+            a.slab = reinterpret_cast<double*>(dev + L.slab);
+            a.values = reinterpret_cast<double*>(dev + L.values);
+            a.records = reinterpret_cast<FitRecord*>(dev + L.records);
+            a.group_status = reinterpret_cast<GroupStatus*>(dev + L.group_status);
+            a.problem_status = reinterpret_cast<ProblemStatus*>(dev + L.problem_status);
+            a.counts = reinterpret_cast<unsigned*>(dev + L.counts);
+            a.itm_counts = reinterpret_cast<unsigned*>(dev + L.itm_counts);
+            a.eval_partials = reinterpret_cast<double2*>(dev + L.eval_partials);
+            a.summaries = reinterpret_cast<ProblemSummary*>(dev + L.summaries);
+            a.greek_partials = greeks ? reinterpret_cast<double2*>(dev + L.greek_partials) : nullptr;
+            a.greek_sums = greeks ? reinterpret_cast<double*>(dev + L.greek_sums) : nullptr;
+            a.stop_counts = greeks ? reinterpret_cast<unsigned*>(dev + L.stop_counts) : nullptr;
+            a.train_blocks = w.train_blocks;
+            a.eval_blocks = w.eval_blocks;
+            a.degree = m.degree;
+            a.rank_tolerance = m.rank_tolerance;
+            a.condition_limit = m.condition_limit;
+            a.tie_rule = m.tie_rule;
+            a.support = m.support;
+            unsigned* counters = reinterpret_cast<unsigned*>(dev + L.counters);
+            BatchQueue q{};
+            q.items = reinterpret_cast<const BatchItem*>(dev + L.items);
+            q.n_items = uint32_t(items.size());
+            q.next = counters;
+            q.timeout = counters + 1;
+            q.sim_done = counters + 2;
+            q.bwd_done = counters + 2 + G;
+            q.eval_done = counters + 2 + 2 * G;
+            cudaEvent_t* mark = ex->batch_marks;
+            FO_CUDA_TRY(cudaEventRecord(mark[0], s), "event");
+            int grid = 0;
+            FO_CUDA_TRY(launch_batch_persistent(a, q, eval_strikes, max_rows, stage, tune.ctas_per_sm, s, &grid),
+                        "batch launch");
+            FO_CUDA_TRY(cudaEventRecord(mark[1], s), "event");
+            ex->batch_launches += 1;
+            ex->batch_grid = grid;
+            ex->batch_strikes = eval_strikes;
+            ex->batch_items = items.size();
+            unsigned timed_out = 0;
+            FO_CUDA_TRY(cudaMemcpyAsync(back, dev + L.out_begin, L.out_bytes, cudaMemcpyDeviceToHost, s), "batch result copy");
+            FO_CUDA_TRY(cudaMemcpyAsync(&timed_out, q.timeout, sizeof(unsigned), cudaMemcpyDeviceToHost, s),
+                        "batch status copy");
+            ex->batch_d2h += L.out_bytes + sizeof(unsigned);
+            FO_CUDA_TRY(cudaStreamSynchronize(s), "batch pricing");
+            FO_CUDA_TRY(cudaEventElapsedTime(launch_ms, mark[0], mark[1]), "event");
+            if (timed_out)
+                return make_error(FO_ERR_EXECUTION, FO_CODE_BARRIER_TIMEOUT,
+                                  "a batch work item waited too long for the items it depends on; the device result was "
+                                  "discarded");
+            return Error{};
+        };
+        BatchTuning tune = ex->batch_tuning;
+        ex->batch_tuning_source = 0;
+        if (ex->batch_autotune) {
+            const std::string key = tuning_key(work, w, greeks, m.degree, max_rows, max_strikes);
+            const auto found = ex->batch_tuned.find(key);
+            if (found != ex->batch_tuned.end()) {
+                tune = found->second;
+                ex->batch_tuning_source = 1;
+            } else {
+                Error te = autotune_wave(run_wave, greeks, int(max_strikes), &tune, &ex->batch_tuning_runs);
+                if (!te.ok()) return te;
+                ex->batch_tuned.emplace(key, tune);
+                ex->batch_tuning_source = 2;
+            }
         }
-        FO_CUDA_TRY(cudaMemcpyAsync(dev + L.groups, host + (L.groups - in_bytes), L.out_begin - L.groups,
-                                    cudaMemcpyHostToDevice, s),
-                    "batch table upload");
-        ex->batch_h2d += L.out_begin - L.groups;
-        FO_CUDA_TRY(cudaMemsetAsync(dev + L.out_begin, 0xff, L.summaries - L.out_begin, s), "batch status reset");
-        FO_CUDA_TRY(cudaMemsetAsync(dev + L.clear_begin, 0, L.clear_bytes, s), "batch reset");
-        BatchArgs a{};
-        a.groups = reinterpret_cast<const BatchGroup*>(dev + L.groups);
-        a.problems = reinterpret_cast<const BatchProblem*>(dev + L.problems);
-        a.backward_order = reinterpret_cast<const uint32_t*>(dev + L.order);
-        a.n_groups = uint32_t(w.g1 - w.g0);
-        a.n_problems = uint32_t(w.problems);
-        a.slab = reinterpret_cast<double*>(dev + L.slab);
-        a.values = reinterpret_cast<double*>(dev + L.values);
-        a.records = reinterpret_cast<FitRecord*>(dev + L.records);
-        a.group_status = reinterpret_cast<GroupStatus*>(dev + L.group_status);
-        a.problem_status = reinterpret_cast<ProblemStatus*>(dev + L.problem_status);
-        a.counts = reinterpret_cast<unsigned*>(dev + L.counts);
-        a.itm_counts = reinterpret_cast<unsigned*>(dev + L.itm_counts);
-        a.eval_partials = reinterpret_cast<double2*>(dev + L.eval_partials);
-        a.summaries = reinterpret_cast<ProblemSummary*>(dev + L.summaries);
-        a.greek_partials = greeks ? reinterpret_cast<double2*>(dev + L.greek_partials) : nullptr;
-        a.greek_sums = greeks ? reinterpret_cast<double*>(dev + L.greek_sums) : nullptr;
-        a.stop_counts = greeks ? reinterpret_cast<unsigned*>(dev + L.stop_counts) : nullptr;
-        a.train_blocks = w.train_blocks;
-        a.eval_blocks = w.eval_blocks;
-        a.degree = m.degree;
-        a.rank_tolerance = m.rank_tolerance;
-        a.condition_limit = m.condition_limit;
-        a.tie_rule = m.tie_rule;
-        a.support = m.support;
-        cudaEvent_t* mark = ex->batch_marks;
-        FO_CUDA_TRY(cudaEventRecord(mark[0], s), "event");
-        FO_CUDA_TRY(launch_batch_simulate(a, s), "batch training simulation launch");
-        FO_CUDA_TRY(cudaEventRecord(mark[1], s), "event");
-        FO_CUDA_TRY(launch_batch_backward(a, n_large, s, ex->side, ex->fork, ex->join), "batch backward launch");
-        FO_CUDA_TRY(cudaEventRecord(mark[2], s), "event");
-        FO_CUDA_TRY(launch_batch_diagnose(a, uint32_t(w.records), s), "batch diagnose launch");
-        FO_CUDA_TRY(cudaEventRecord(mark[3], s), "event");
-        if (greeks)
-            FO_CUDA_TRY(launch_batch_evaluate_greeks(a, max_strikes, max_rows, s), "batch Greeks evaluation launch");
-        else
-            FO_CUDA_TRY(launch_batch_evaluate(a, max_strikes, max_rows, s), "batch evaluation launch");
-        FO_CUDA_TRY(cudaEventRecord(mark[4], s), "event");
-        FO_CUDA_TRY(launch_batch_summarize(a, s), "batch summary launch");
-        FO_CUDA_TRY(cudaEventRecord(mark[5], s), "event");
-        ex->batch_launches += FO_BATCH_KERNELS;
-        FO_CUDA_TRY(cudaMemcpyAsync(host, dev + L.out_begin, L.out_bytes, cudaMemcpyDeviceToHost, s), "batch result copy");
-        ex->batch_d2h += L.out_bytes;
-        FO_CUDA_TRY(cudaStreamSynchronize(s), "batch pricing");
-        for (int k = 0; k < FO_BATCH_KERNELS; ++k) {
+        ex->batch_tuning_used = tune;
+        {
             float ms = 0.f;
-            FO_CUDA_TRY(cudaEventElapsedTime(&ms, mark[k], mark[k + 1]), "event");
-            ex->batch_ms[k] += ms;
+            Error re = run_wave(tune, &ms);
+            if (!re.ok()) return re;
+            ex->batch_ms[0] += ms;
         }
-        const auto* gst = reinterpret_cast<const GroupStatus*>(host + (L.group_status - L.out_begin));
-        const auto* pst = reinterpret_cast<const ProblemStatus*>(host + (L.problem_status - L.out_begin));
-        const auto* sum = reinterpret_cast<const ProblemSummary*>(host + (L.summaries - L.out_begin));
-        const auto* greek_sums = reinterpret_cast<const double*>(host + (L.greek_sums - L.out_begin));
+        const auto* gst = reinterpret_cast<const GroupStatus*>(back + (L.group_status - L.out_begin));
+        const auto* pst = reinterpret_cast<const ProblemStatus*>(back + (L.problem_status - L.out_begin));
+        const auto* sum = reinterpret_cast<const ProblemSummary*>(back + (L.summaries - L.out_begin));
+        const auto* greek_sums = reinterpret_cast<const double*>(back + (L.greek_sums - L.out_begin));
         std::vector<unsigned> stops;
         if (greeks) {
             stops.resize(w.records);
@@ -1685,6 +1852,48 @@ int fo_validate_lsm_ragged_f64(const fo_lsm_ragged_request* request, fo_error* e
     } catch (const std::bad_alloc&) {
         return finish(err, make_error(FO_ERR_EXECUTION, FO_CODE_CAPACITY_EXCEEDED, "host memory exhausted"));
     }
+}
+
+int fo_executor_set_batch_tuning(fo_executor* executor, int32_t autotune, const fo_batch_tuning* fixed, fo_error* err) {
+    if (!executor)
+        return finish(err, make_error(FO_ERR_EXECUTION, FO_CODE_INVALID_ARGUMENT, "executor must not be NULL"));
+    std::lock_guard<std::mutex> lock(executor->mu);
+    if (autotune) {
+        executor->batch_autotune = true;
+        return FO_OK;
+    }
+    if (!fixed)
+        return finish(err, make_error(FO_ERR_EXECUTION, FO_CODE_INVALID_ARGUMENT,
+                                      "a fixed batch launch shape must be given when the autotuner is off"));
+    const bool valid = fixed->sim_blocks >= 1 && fixed->sim_blocks <= 64 && fixed->eval_blocks >= 1 &&
+                       fixed->eval_blocks <= 64 && (fixed->strikes == 1 || fixed->strikes == 2 ||
+                                                    fixed->strikes == 4 || fixed->strikes == 8) &&
+                       fixed->ctas_per_sm >= 0 && fixed->ctas_per_sm <= 8;
+    if (!valid)
+        return finish(err, make_error(FO_ERR_EXECUTION, FO_CODE_INVALID_ARGUMENT,
+                                      "batch launch shape outside its range: blocks per item 1..64, strikes per "
+                                      "evaluation item 1, 2, 4 or 8, CTAs per SM 0..8"));
+    executor->batch_autotune = false;
+    executor->batch_tuning.sim_blocks = fixed->sim_blocks;
+    executor->batch_tuning.eval_blocks = fixed->eval_blocks;
+    executor->batch_tuning.strikes = fixed->strikes;
+    executor->batch_tuning.ctas_per_sm = fixed->ctas_per_sm;
+    return FO_OK;
+}
+
+int fo_executor_batch_launch(fo_executor* executor, fo_batch_launch_info* out) {
+    if (!executor || !out) return FO_ERR_EXECUTION;
+    std::lock_guard<std::mutex> lock(executor->mu);
+    const BatchTuning& t = executor->batch_tuning_used;
+    out->tuning.sim_blocks = t.sim_blocks;
+    out->tuning.eval_blocks = t.eval_blocks;
+    out->tuning.strikes = executor->batch_strikes;
+    out->tuning.ctas_per_sm = t.ctas_per_sm;
+    out->source = executor->batch_tuning_source;
+    out->grid = executor->batch_grid;
+    out->items = executor->batch_items;
+    out->tuning_launches = executor->batch_tuning_source == 2 ? executor->batch_tuning_runs : 0;
+    return FO_OK;
 }
 
 int fo_executor_batch_kernel_ms(fo_executor* executor, double* kernel_ms, uint64_t capacity, uint64_t* launches) {

@@ -17,6 +17,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <algorithm>
+
 #include "lsm_common.cuh"
 #include "lsm_device.cuh"
 #include "lsm_fit_warp.cuh"
@@ -127,6 +129,35 @@ __global__ void __launch_bounds__(256) simulate_kernel(DevicePlan plan, uint64_t
     }
 }
 
+// External normals: the lowest index of a non-finite value in the [intervals, paths] buffer.
+__global__ void __launch_bounds__(256) first_nonfinite_kernel(const double* values, uint64_t n,
+                                                              unsigned long long* first) {
+    for (uint64_t i = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; i < n; i += uint64_t(gridDim.x) * blockDim.x)
+        if (!fo_isfinite(values[i])) atomicMin(first, (unsigned long long)i);
+}
+
+// K1 driven by caller normals: one thread per path, time-major [rows, paths] stores.
+__global__ void __launch_bounds__(256) simulate_external_kernel(DevicePlan plan, uint64_t paths, const double* normals,
+                                                                double* out, unsigned long long* fail) {
+    for (uint64_t p = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; p < paths;
+         p += uint64_t(gridDim.x) * blockDim.x) {
+        const SimResult r = simulate_path_external(plan, normals, paths, p,
+                                                   [&](int row, double value) { out[uint64_t(row) * paths + p] = value; });
+        if (r.code != 0) atomicMin(fail, (unsigned long long)p);
+    }
+}
+
+__global__ void replay_external_kernel(DevicePlan plan, uint64_t paths, const double* normals, uint64_t path,
+                                       SimFailure* out) {
+    if (threadIdx.x != 0) return;
+    const SimResult r = simulate_path_external(plan, normals, paths, path, [](int, double) {});
+    out->code = r.code;
+    out->interval = r.interval;
+    out->spot = r.spot;
+    out->normal = r.normal;
+    out->observed = 0.0;
+}
+
 // Re-runs one path serially to recover the typed failure details and the state at `want_row`.
 __global__ void replay_kernel(DevicePlan plan, uint64_t seed, uint32_t domain, uint32_t path, int want_row,
                               SimFailure* out) {
@@ -153,9 +184,38 @@ struct BackwardSmem {
     double red[32 * kSlots];
     dd total[kSlots];
     FitModel model;
+    double new_pivot;  // the row's own mean, when its sums are taken again about it
     int kind;
     int wait_failed;
 };
+
+// Decision of warp 0 that the row's sums must be taken again about its own mean (pivot_too_far)
+// before it is fitted; not a rule kind of any record.
+constexpr int kRecenterRow = -1;
+
+// This thread's in-the-money paths of the row being decided, summed about `pivot` and reduced over
+// the CTA into dst (the classification of each path is the main pass's). Out of line: it runs only
+// when the pivot lies far from the row's mean, and keeps the backward loop's registers untouched.
+template <bool kHbm>
+__device__ __noinline__ void recenter_partial(const double* values_smem, const double* values_hbm,
+                                              const double* spots_smem, const double* row_spots, uint64_t P,
+                                              uint64_t gtid, uint64_t nthreads, int ppt, double K, Divisor Kd,
+                                              double pivot, double* red, double2* dst, unsigned blocks) {
+    RowSums s;
+#pragma unroll
+    for (int k = 0; k < kSlots; ++k) s.acc[k] = 0.0;
+    for (int j = 0; j < ppt; ++j) {
+        const uint64_t p = gtid + uint64_t(j) * nthreads;
+        if (p >= P) break;
+        const double sp = kHbm ? __ldcg(&row_spots[p]) : spots_smem[j * blockDim.x + threadIdx.x];
+        if (!(sp > K)) continue;
+        const double x = divide(sp, Kd);
+        const double y = kHbm ? values_hbm[p] : values_smem[j * blockDim.x + threadIdx.x];
+        if (!fo_isfinite(x) || !fo_isfinite(y)) s.acc[kBadSlot] += 1.0;
+        else accumulate_itm(s, x, y, pivot);
+    }
+    cta_reduce_to<kSlots>(s.acc, red, dst, blocks);
+}
 
 // Each thread owns paths gtid + j * nthreads (j < ppt). When the population fits on chip
 // (kHbm false), their discounted values, the current row's spots and the staged row's spots live
@@ -302,48 +362,54 @@ __global__ void __launch_bounds__(kBackwardThreads, 1) backward_kernel(BackwardA
             }
             cp_async_commit();
         }
+        // Warp 0 decides the row from the combined totals (the same in every lane and every CTA) and
+        // fits it, or first asks for the row's sums about its own mean (once per row).
+        auto decide_row = [&](bool allow_recenter) {
+            const uint64_t itm = uint64_t(sm.total[0].hi);
+            const uint64_t bad = uint64_t(sm.total[kBadSlot].hi);
+            const uint64_t population = itm + bad;
+            const uint32_t required = uint32_t(degree + 1);
+            int kind;
+            double mean = fit_pivot;
+            if (population == 0) {
+                kind = plan.support == 1 ? kRuleContinue : kRuleNoSupport;
+            } else if (population < required && plan.support == 1) {
+                kind = kRuleContinue;
+            } else if (population < required || bad > 0) {
+                kind = kRuleFitFailed;  // InsufficientObservations / non-finite population
+            } else if (allow_recenter && degree > 0 && pivot_too_far(sm.total, fit_pivot, itm, &mean)) {
+                kind = kRecenterRow;
+                if (threadIdx.x == 0) sm.new_pivot = mean;
+            } else {
+                fit_continuation_warp(sm.total, fit_pivot, itm, degree, plan.rank_tolerance, plan.rank_limit,
+                                      &sm.model);
+                kind = sm.model.status == kFitOk ? kRuleRegression : kRuleFitFailed;
+            }
+            if (threadIdx.x == 0) sm.kind = kind;
+            if (blockIdx.x == 0 && kind != kRecenterRow) {
+                // CTA 0 writes the row's record; the model goes out as twelve 16-byte words from
+                // as many lanes (a one-thread copy made CTA 0 the last to arrive at the next sync).
+                FitRecord& rec = a.records[row];
+                constexpr int kModelWords = int(sizeof(FitModel) / sizeof(double2));
+                static_assert(sizeof(FitModel) % sizeof(double2) == 0, "FitModel is 16-byte aligned");
+                if (threadIdx.x < kModelWords)
+                    reinterpret_cast<double2*>(&rec.model)[threadIdx.x] =
+                        reinterpret_cast<const double2*>(&sm.model)[threadIdx.x];
+                if (threadIdx.x == 0) {
+                    rec.kind = kind;
+                    rec.itm = population;
+                    rec.pivot = fit_pivot;
+                    rec.origin_exercise = 0;
+                    rec.origin_continuation = 0.0;
+                    rec.diag_status = -1;
+                    if (kind == kRuleFitFailed) atomicMin(&a.status->fit_failed_order, order);
+                }
+            }
+        };
         if (!stager) {
             combine_published<kSlots>(parts + size_t(parity) * a.partial_stride, seq, a.status, sm.total,
                                       &sm.wait_failed);
-            if (threadIdx.x < 32 && !sm.wait_failed) {
-                // Warp 0 decides the row (the same shared totals in every lane) and fits it.
-                const uint64_t itm = uint64_t(sm.total[0].hi);
-                const uint64_t bad = uint64_t(sm.total[kBadSlot].hi);
-                const uint64_t population = itm + bad;
-                const uint32_t required = uint32_t(degree + 1);
-                int kind;
-                if (population == 0) {
-                    kind = plan.support == 1 ? kRuleContinue : kRuleNoSupport;
-                } else if (population < required && plan.support == 1) {
-                    kind = kRuleContinue;
-                } else if (population < required || bad > 0) {
-                    kind = kRuleFitFailed;  // InsufficientObservations / non-finite population
-                } else {
-                    fit_continuation_warp(sm.total, fit_pivot, itm, degree, plan.rank_tolerance, plan.rank_limit,
-                                          &sm.model);
-                    kind = sm.model.status == kFitOk ? kRuleRegression : kRuleFitFailed;
-                }
-                if (threadIdx.x == 0) sm.kind = kind;
-                if (blockIdx.x == 0) {
-                    // CTA 0 writes the row's record; the model goes out as twelve 16-byte words from
-                    // as many lanes (a one-thread copy made CTA 0 the last to arrive at the next sync).
-                    FitRecord& rec = a.records[row];
-                    constexpr int kModelWords = int(sizeof(FitModel) / sizeof(double2));
-                    static_assert(sizeof(FitModel) % sizeof(double2) == 0, "FitModel is 16-byte aligned");
-                    if (threadIdx.x < kModelWords)
-                        reinterpret_cast<double2*>(&rec.model)[threadIdx.x] =
-                            reinterpret_cast<const double2*>(&sm.model)[threadIdx.x];
-                    if (threadIdx.x == 0) {
-                        rec.kind = kind;
-                        rec.itm = population;
-                        rec.pivot = fit_pivot;
-                        rec.origin_exercise = 0;
-                        rec.origin_continuation = 0.0;
-                        rec.diag_status = -1;
-                        if (kind == kRuleFitFailed) atomicMin(&a.status->fit_failed_order, order);
-                    }
-                }
-            }
+            if (threadIdx.x < 32 && !sm.wait_failed) decide_row(true);
         } else if (stage_next) {
             // Row k-1: in-the-money test and power sums, independent of row k's decision.
             const double* srow = row_ptr(uint32_t(row - 1));
@@ -367,6 +433,23 @@ __global__ void __launch_bounds__(kBackwardThreads, 1) backward_kernel(BackwardA
         }
         __syncthreads();
         if (sm.wait_failed) return;
+        if (sm.kind == kRecenterRow) {
+            // One more grid exchange: every CTA sums the row about its mean and warp 0 fits it.
+            fit_pivot = sm.new_pivot;
+            parity ^= 1;
+            recenter_partial<kHbm>(values, a.values, spots, row_ptr(uint32_t(row)), P, gtid, nthreads, ppt, K, Kd,
+                                   fit_pivot, sm.red, parts + size_t(parity) * a.partial_stride + blockIdx.x,
+                                   gridDim.x);
+            publish_partial(a.status);
+            ++seq;
+            if (!stager) {
+                combine_published<kSlots>(parts + size_t(parity) * a.partial_stride, seq, a.status, sm.total,
+                                          &sm.wait_failed);
+                if (threadIdx.x < 32 && !sm.wait_failed) decide_row(false);
+            }
+            __syncthreads();
+            if (sm.wait_failed) return;
+        }
         const int kind = sm.kind;
         if (kind == kRuleFitFailed) return;  // identical decision in every CTA
         const bool regression = kind == kRuleRegression;
@@ -418,6 +501,9 @@ __global__ void __launch_bounds__(kBackwardThreads, 1) backward_kernel(BackwardA
         spots_next = swap;
         fit_pivot = stage_pivot;
         if (regression) latest_mean = model.mean;
+        // Consecutive exchanges use alternate partial buffers: a CTA overwrites a buffer only after
+        // every CTA has arrived at the exchange in between, that is, has finished reading it.
+        parity ^= 1;
     }
     // Common origin decision (policy.rs:265-281): mean of values discounted to the origin.
     if (plan.origin_row) {
@@ -606,6 +692,26 @@ cudaError_t launch_simulate(const DevicePlan& plan, uint64_t paths, uint64_t see
     if (blocks > (1u << 20)) blocks = 1u << 20;
     simulate_kernel<<<unsigned(blocks), threads, 0, stream>>>(plan, paths, seed, domain, out, store_first_row,
                                                                reconstruct_escrowed, fail);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_first_nonfinite(const double* values, uint64_t n, unsigned long long* first, cudaStream_t stream) {
+    const uint64_t blocks = std::min<uint64_t>((n + 255) / 256, 148u * 16u);
+    first_nonfinite_kernel<<<unsigned(std::max<uint64_t>(blocks, 1)), 256, 0, stream>>>(values, n, first);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_simulate_external(const DevicePlan& plan, uint64_t paths, const double* normals, double* out,
+                                     unsigned long long* fail, cudaStream_t stream) {
+    uint64_t blocks = (paths + 255) / 256;
+    if (blocks > (1u << 20)) blocks = 1u << 20;
+    simulate_external_kernel<<<unsigned(blocks), 256, 0, stream>>>(plan, paths, normals, out, fail);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_replay_external(const DevicePlan& plan, uint64_t paths, const double* normals, uint64_t path,
+                                   SimFailure* out, cudaStream_t stream) {
+    replay_external_kernel<<<1, 32, 0, stream>>>(plan, paths, normals, path, out);
     return cudaGetLastError();
 }
 

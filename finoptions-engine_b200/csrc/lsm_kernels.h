@@ -64,6 +64,13 @@ cudaError_t launch_simulate(const DevicePlan& plan, uint64_t paths, uint64_t see
                             cudaStream_t stream);
 cudaError_t launch_replay(const DevicePlan& plan, uint64_t seed, uint32_t domain, uint32_t path, int want_row,
                           SimFailure* out, cudaStream_t stream);
+// External normals ([intervals, paths], time-major): the first non-finite value's index, the
+// simulation, and the replay of one failing path.
+cudaError_t launch_first_nonfinite(const double* values, uint64_t n, unsigned long long* first, cudaStream_t stream);
+cudaError_t launch_simulate_external(const DevicePlan& plan, uint64_t paths, const double* normals, double* out,
+                                     unsigned long long* fail, cudaStream_t stream);
+cudaError_t launch_replay_external(const DevicePlan& plan, uint64_t paths, const double* normals, uint64_t path,
+                                   SimFailure* out, cudaStream_t stream);
 int backward_max_blocks(int device);
 int backward_max_ppt();
 size_t backward_smem_bytes(int ppt);

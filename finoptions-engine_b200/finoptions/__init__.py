@@ -61,10 +61,13 @@ from .simulation import (
     CpuExecutor,
     CpuMathBackend,
     CudaExecutor,
+    DeviceGbmPaths,
     ExecutionError,
     GbmPaths,
     RandomStream,
     SimulationError,
+    simulate_gbm,
+    simulate_gbm_on_device,
     simulate_gbm_seeded,
 )
 
@@ -95,6 +98,7 @@ __all__ = [
     "CpuMathBackend",
     "CudaExecutor",
     "CumulativeDividendYieldCurve",
+    "DeviceGbmPaths",
     "DividendPolicy",
     "EscrowedCashDividendBatch",
     "EscrowedVolatilityConvention",
@@ -137,6 +141,8 @@ __all__ = [
     "price_lsm_call_grouped_batch",
     "price_lsm_call_ragged",
     "price_lsm_call_ragged_greeks",
+    "simulate_gbm",
+    "simulate_gbm_on_device",
     "simulate_gbm_seeded",
     "validate_lsm_call_grouped_batch",
     "validate_lsm_call_ragged",

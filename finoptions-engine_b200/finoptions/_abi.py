@@ -230,6 +230,16 @@ class FoGbmSeededRequest(ctypes.Structure):
     ]
 
 
+class FoBatchTuning(ctypes.Structure):
+    _fields_ = [("sim_blocks", ctypes.c_int32), ("eval_blocks", ctypes.c_int32), ("strikes", ctypes.c_int32),
+                ("ctas_per_sm", ctypes.c_int32)]
+
+
+class FoBatchLaunchInfo(ctypes.Structure):
+    _fields_ = [("tuning", FoBatchTuning), ("source", ctypes.c_int32), ("grid", ctypes.c_int32),
+                ("items", ctypes.c_uint64), ("tuning_launches", ctypes.c_uint64)]
+
+
 PACKAGE_ROOT: Final = Path(__file__).resolve().parent
 LIBRARY_PATH: Final = PACKAGE_ROOT / "_lib" / "libfinoptions_cuda.so"
 
@@ -258,7 +268,11 @@ EXPORTED_SYMBOLS: Final = (
     "fo_price_lsm_ragged_f64",
     "fo_executor_batch_kernel_ms",
     "fo_executor_batch_transfer_bytes",
+    "fo_executor_set_batch_tuning",
+    "fo_executor_batch_launch",
     "fo_simulate_gbm_seeded_f64",
+    "fo_simulate_gbm_f64",
+    "fo_simulate_gbm_device_f64",
     "fo_sample_standard_normals_f64",
     "fo_build_info",
     "fo_validate_lsm_grouped_f64",
@@ -321,8 +335,18 @@ def _declare(lib: ctypes.CDLL) -> None:
     u64p = ctypes.POINTER(ctypes.c_uint64)
     lib.fo_executor_batch_transfer_bytes.argtypes = [vp, u64p, u64p]
     lib.fo_executor_batch_transfer_bytes.restype = ctypes.c_int
+    lib.fo_executor_set_batch_tuning.argtypes = [vp, ctypes.c_int32, ctypes.POINTER(FoBatchTuning), err]
+    lib.fo_executor_set_batch_tuning.restype = ctypes.c_int
+    lib.fo_executor_batch_launch.argtypes = [vp, ctypes.POINTER(FoBatchLaunchInfo)]
+    lib.fo_executor_batch_launch.restype = ctypes.c_int
     lib.fo_simulate_gbm_seeded_f64.argtypes = [vp, ctypes.POINTER(FoGbmSeededRequest), c_double_p, ctypes.c_uint64, err]
     lib.fo_simulate_gbm_seeded_f64.restype = ctypes.c_int
+    lib.fo_simulate_gbm_f64.argtypes = [vp, ctypes.POINTER(FoGbmSeededRequest), c_double_p, ctypes.c_uint64,
+                                        c_double_p, ctypes.c_uint64, err]
+    lib.fo_simulate_gbm_f64.restype = ctypes.c_int
+    lib.fo_simulate_gbm_device_f64.argtypes = [vp, ctypes.POINTER(FoGbmSeededRequest), vp, ctypes.c_uint64, vp,
+                                               ctypes.c_uint64, err]
+    lib.fo_simulate_gbm_device_f64.restype = ctypes.c_int
     lib.fo_sample_standard_normals_f64.argtypes = [
         vp, ctypes.c_uint64, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint64, ctypes.c_uint32,
         c_double_p, ctypes.c_uint64, err,

@@ -409,6 +409,100 @@ def simulate_gbm_seeded_f64(  # noqa: PLR0913 - mirrors the reference's native s
     return out
 
 
+
+def _gbm_request(initial_spot, schedule_times, curve_times, log_discounts, dividend_yield_times,
+                 cumulative_dividend_yields, dividend_nodes, dividend_amounts, exercise_nodes, expiry_node,
+                 annualized_volatility, dividend_policy, paths, seed=0, domain=0):
+    return gbm_seeded_request(
+        initial_spot=initial_spot, schedule_times=schedule_times, curve_times=curve_times,
+        log_discounts=log_discounts, dividend_yield_times=dividend_yield_times,
+        cumulative_dividend_yields=cumulative_dividend_yields, dividend_nodes=dividend_nodes,
+        dividend_amounts=dividend_amounts, exercise_nodes=exercise_nodes, expiry_node=expiry_node,
+        annualized_volatility=annualized_volatility,
+        dividend_policy=_parse(_DIVIDEND_POLICIES, dividend_policy, "dividend policy"), paths=paths, seed=seed,
+        domain=domain)
+
+
+def simulate_gbm_f64(  # noqa: PLR0913 - mirrors the reference's native signature
+    initial_spot: float,
+    schedule_times: list[float],
+    curve_times: list[float],
+    log_discounts: list[float],
+    dividend_yield_times: list[float],
+    cumulative_dividend_yields: list[float],
+    dividend_nodes: list[int],
+    dividend_amounts: list[float],
+    exercise_nodes: list[int],
+    expiry_node: int,
+    annualized_volatility: float,
+    dividend_policy: str,
+    executor: CudaExecutor,
+    normals: np.ndarray,
+) -> np.ndarray:
+    """Time-major [observations, paths] GBM states driven by caller normals [intervals, paths]
+    (simulate_gbm_f64, lib.rs:969-1018)."""
+    handle = _executor_handle(executor)
+    rows, paths = (int(n) for n in normals.shape)
+    request = _gbm_request(initial_spot, schedule_times, curve_times, log_discounts, dividend_yield_times,
+                           cumulative_dividend_yields, dividend_nodes, dividend_amounts, exercise_nodes, expiry_node,
+                           annualized_volatility, dividend_policy, paths)
+    out = np.empty((request.rows, paths), dtype=np.float64)
+    err = _abi.FoError()
+    # A one-element stand-in keeps the pointer valid for an empty matrix (the engine rejects it first).
+    source = normals if normals.size else np.zeros(1)
+    status = _lib().fo_simulate_gbm_f64(handle, ctypes.byref(request.struct), _dp(source), ctypes.c_uint64(rows),
+                                        _dp(out) if out.size else None, ctypes.c_uint64(out.size), ctypes.byref(err))
+    _check(status, err)
+    return out
+
+
+def simulate_gbm_device_f64(  # noqa: PLR0913 - the simulation arguments plus the device buffers
+    initial_spot: float,
+    schedule_times: list[float],
+    curve_times: list[float],
+    log_discounts: list[float],
+    dividend_yield_times: list[float],
+    cumulative_dividend_yields: list[float],
+    dividend_nodes: list[int],
+    dividend_amounts: list[float],
+    exercise_nodes: list[int],
+    expiry_node: int,
+    annualized_volatility: float,
+    dividend_policy: str,
+    executor: CudaExecutor,
+    paths: int,
+    seed: int = 0,
+    domain: int = 0,
+    normals: Any = None,
+) -> Any:
+    """The states as a torch.float64 tensor [observations, paths] on the executor's device, written
+    there by the kernel (no host copy): from the Philox streams (seed, domain), or from `normals`,
+    a C-contiguous torch.float64 tensor [intervals, paths] on the same device."""
+    import torch  # noqa: PLC0415 - only device-tensor callers need torch
+
+    handle = _executor_handle(executor)
+    device = torch.device("cuda", executor.device)
+    if normals is not None:
+        if (not isinstance(normals, torch.Tensor) or normals.dtype != torch.float64 or normals.device != device
+                or normals.dim() != 2 or not normals.is_contiguous()):
+            raise InputError(f"normals must be a C-contiguous torch.float64 [intervals, paths] tensor on {device}")
+        paths = int(normals.shape[1])
+    request = _gbm_request(initial_spot, schedule_times, curve_times, log_discounts, dividend_yield_times,
+                           cumulative_dividend_yields, dividend_nodes, dividend_amounts, exercise_nodes, expiry_node,
+                           annualized_volatility, dividend_policy, paths, seed, domain)
+    out = torch.empty((request.rows, paths), dtype=torch.float64, device=device)
+    # Work queued on torch's stream (the normals, the output's allocation) finishes before the
+    # executor's stream reads or writes them; the call returns once the states are written.
+    torch.cuda.current_stream(device).synchronize()
+    err = _abi.FoError()
+    status = _lib().fo_simulate_gbm_device_f64(
+        handle, ctypes.byref(request.struct), None if normals is None else ctypes.c_void_p(normals.data_ptr()),
+        ctypes.c_uint64(0 if normals is None else normals.shape[0]), ctypes.c_void_p(out.data_ptr()),
+        ctypes.c_uint64(out.numel()), ctypes.byref(err))
+    _check(status, err)
+    return out
+
+
 def _method(
     exercise_mesh: str,
     base_intervals: int | None,

@@ -11,7 +11,7 @@ from __future__ import annotations
 from dataclasses import dataclass, field
 from enum import StrEnum
 from itertools import pairwise
-from typing import Final
+from typing import Any, Final
 
 import numpy as np
 import numpy.typing as npt
@@ -171,6 +171,160 @@ def _validate_specs(schedule: object, curve: object, dividend_yield_curve: objec
             raise InputError(msg)
 
 
+def _plan_arguments(initial_spot: float, schedule: EventSchedule, curve: LogDiscountCurve,
+                    dividend_yield_curve: CumulativeDividendYieldCurve, volatility: ConstantVolatility,
+                    dividend_policy: DividendPolicy) -> tuple:
+    return (
+        initial_spot,
+        list(schedule.times),
+        list(curve.times),
+        list(curve.log_discounts),
+        list(dividend_yield_curve.times),
+        list(dividend_yield_curve.cumulative_yields),
+        [d.node for d in schedule.dividends],
+        [d.amount for d in schedule.dividends],
+        list(schedule.exercise_nodes),
+        schedule.expiry_node,
+        volatility.annualized_decimal,
+        dividend_policy.value,
+    )
+
+
+def _validate_normal_matrix(normals: object) -> None:
+    # _validate_normal_matrix (python/finoptions/simulation.py:181-193): borrowed, never cast or copied.
+    if type(normals) is not np.ndarray:
+        msg = f"normals must be a plain numpy.ndarray; observed {type(normals).__name__}"
+        raise InputError(msg)
+    if normals.dtype != np.dtype(np.float64):
+        msg = f"normals must have dtype float64; observed {normals.dtype}"
+        raise InputError(msg)
+    if normals.ndim != 2:  # noqa: PLR2004 - [intervals, paths]
+        msg = f"normals must have shape [intervals, paths]; observed {normals.shape!r}"
+        raise InputError(msg)
+    if not normals.flags.c_contiguous:
+        msg = "normals must be C-contiguous; implicit copies are forbidden"
+        raise InputError(msg)
+
+
+def simulate_gbm(  # noqa: PLR0913 - each financial input is independently typed
+    *,
+    initial_spot: float,
+    schedule: EventSchedule,
+    curve: LogDiscountCurve,
+    dividend_yield_curve: CumulativeDividendYieldCurve,
+    volatility: ConstantVolatility,
+    dividend_policy: DividendPolicy,
+    executor: CudaExecutor,
+    normals: Float64Matrix,
+) -> GbmPaths:
+    """Simulate exact adjacent-node GBM paths on the device from explicit standard normals
+    (simulate_gbm, python/finoptions/simulation.py:210-259).
+
+    ``normals`` is a C-contiguous float64 matrix [intervals, paths], read without casting or
+    copying on the host. Every variate is checked for finiteness before any path is computed.
+
+    Raises:
+        InputError: If a runtime type, grid, shape, value, or financial input is invalid.
+        SimulationError: For a wrong interval-row count, an empty path set, a non-finite variate or
+            a non-finite path transition.
+
+    """
+    if type(initial_spot) is not float:
+        msg = f"initial_spot must be a plain float; observed {type(initial_spot).__name__}"
+        raise InputError(msg)
+    _validate_specs(schedule, curve, dividend_yield_curve, volatility, dividend_policy)
+    handle = native_executor(executor)
+    _validate_normal_matrix(normals)
+    states = _native.simulate_gbm_f64(
+        *_plan_arguments(initial_spot, schedule, curve, dividend_yield_curve, volatility, dividend_policy),
+        handle,
+        normals,
+    )
+    states.flags.writeable = False
+    return GbmPaths(observation_nodes=(*schedule.exercise_nodes, schedule.expiry_node), states=states)
+
+
+@dataclass(frozen=True, slots=True)
+class DeviceGbmPaths:
+    """GbmPaths whose states stay in device memory: a torch.float64 tensor [observations, paths] on
+    the executor's device, time-major like GbmPaths.states. ``to_host()`` copies it to GbmPaths."""
+
+    observation_nodes: tuple[int, ...]
+    states: Any
+
+    @property
+    def path_count(self) -> int:
+        """Number of simulated paths."""
+        return int(self.states.shape[1])
+
+    def values_at(self, node: int) -> Any:
+        """The device row of an observed node (a view, no copy)."""
+        if type(node) is not int:
+            msg = f"observation node must be a plain int; observed {type(node).__name__}"
+            raise InputError(msg)
+        try:
+            row = self.observation_nodes.index(node)
+        except ValueError as error:
+            raise KeyError(node) from error
+        return self.states[row]
+
+    def to_host(self) -> GbmPaths:
+        """Copy the states to host memory as read-only GbmPaths."""
+        states = self.states.cpu().numpy()
+        states.flags.writeable = False
+        return GbmPaths(observation_nodes=self.observation_nodes, states=states)
+
+
+def simulate_gbm_on_device(  # noqa: PLR0913 - each financial input is independently typed
+    *,
+    initial_spot: float,
+    schedule: EventSchedule,
+    curve: LogDiscountCurve,
+    dividend_yield_curve: CumulativeDividendYieldCurve,
+    volatility: ConstantVolatility,
+    dividend_policy: DividendPolicy,
+    executor: CudaExecutor,
+    paths: int | None = None,
+    random_stream: RandomStream | None = None,
+    normals: Any = None,
+) -> DeviceGbmPaths:
+    """simulate_gbm_seeded or simulate_gbm with the states left on the device.
+
+    Give either ``paths`` and ``random_stream`` (Philox streams, the same values as
+    simulate_gbm_seeded) or ``normals``, a C-contiguous torch.float64 tensor [intervals, paths] on
+    the executor's device (the same values as simulate_gbm on those normals). The returned tensor
+    is written by the kernel in place; nothing passes through host memory. For further device work
+    (a caller's own regression, a DLPack consumer) without a host round trip.
+    """
+    if type(initial_spot) is not float:
+        msg = f"initial_spot must be a plain float; observed {type(initial_spot).__name__}"
+        raise InputError(msg)
+    _validate_specs(schedule, curve, dividend_yield_curve, volatility, dividend_policy)
+    handle = native_executor(executor)
+    if normals is None:
+        if type(paths) is not int or not 1 <= paths <= _MAX_PATHS:
+            msg = f"paths must be a plain int in [1, {_MAX_PATHS}]; observed {paths!r}"
+            raise InputError(msg)
+        if type(random_stream) is not RandomStream:
+            msg = f"random_stream must be RandomStream; observed {type(random_stream).__name__}"
+            raise InputError(msg)
+        seed, domain = random_stream.seed, random_stream.domain
+    else:
+        if paths is not None or random_stream is not None:
+            msg = "give either normals or paths with a random_stream, not both"
+            raise InputError(msg)
+        seed, domain, paths = 0, 0, 0
+    states = _native.simulate_gbm_device_f64(
+        *_plan_arguments(initial_spot, schedule, curve, dividend_yield_curve, volatility, dividend_policy),
+        handle,
+        paths,
+        seed,
+        domain,
+        normals,
+    )
+    return DeviceGbmPaths(observation_nodes=(*schedule.exercise_nodes, schedule.expiry_node), states=states)
+
+
 def simulate_gbm_seeded(  # noqa: PLR0913 - each financial input is independently typed
     *,
     initial_spot: float,
@@ -200,18 +354,7 @@ def simulate_gbm_seeded(  # noqa: PLR0913 - each financial input is independentl
         msg = f"random_stream must be RandomStream; observed {type(random_stream).__name__}"
         raise InputError(msg)
     states = _native.simulate_gbm_seeded_f64(
-        initial_spot,
-        list(schedule.times),
-        list(curve.times),
-        list(curve.log_discounts),
-        list(dividend_yield_curve.times),
-        list(dividend_yield_curve.cumulative_yields),
-        [d.node for d in schedule.dividends],
-        [d.amount for d in schedule.dividends],
-        list(schedule.exercise_nodes),
-        schedule.expiry_node,
-        volatility.annualized_decimal,
-        dividend_policy.value,
+        *_plan_arguments(initial_spot, schedule, curve, dividend_yield_curve, volatility, dividend_policy),
         handle,
         paths,
         random_stream.seed,
@@ -225,10 +368,13 @@ __all__ = [
     "CpuExecutor",
     "CpuMathBackend",
     "CudaExecutor",
+    "DeviceGbmPaths",
     "ExecutionError",
     "GbmPaths",
     "RandomStream",
     "SimulationError",
     "native_executor",
+    "simulate_gbm",
+    "simulate_gbm_on_device",
     "simulate_gbm_seeded",
 ]

@@ -99,6 +99,8 @@ typedef enum fo_error_code {
     FO_CODE_RANDOM_NORMAL_REJECTION_LIMIT,
     FO_CODE_NON_FINITE_PATH_TRANSITION,
     FO_CODE_SHAPE_OVERFLOW,
+    FO_CODE_BUFFER_LENGTH_MISMATCH,
+    FO_CODE_NON_FINITE_NORMAL_BUFFER,
     /* RegressionError (crates/finoptions-lsm/src/error.rs:1-160) */
     FO_CODE_UNSUPPORTED_DEGREE = 300,
     FO_CODE_INVALID_RANK_TOLERANCE,
@@ -488,15 +490,41 @@ typedef struct fo_ragged_greeks_columns {
 int fo_price_lsm_ragged_f64(fo_executor* executor, const fo_lsm_ragged_request* request,
                             fo_batch_result_columns* out, fo_ragged_greeks_columns* greeks, fo_error* err);
 
-/* Device time of the executor's last grouped / row batch call (no counterpart in the reference; a
- * measurement hook). kernel_ms[k] receives the milliseconds of batch kernel k summed over the
- * call's waves, k = 0 training simulation, 1 backward fits, 2 diagnostics, 3 evaluation,
- * 4 summaries; *launches receives the number of kernel launches. Timed with CUDA events on the
- * executor's stream. */
+/* Device time of the executor's last grouped / row / ragged batch call (no counterpart in the
+ * reference; a measurement hook). A batch runs as one persistent launch per wave (a wave: the groups
+ * that fit the device memory budget together): kernel_ms[0] receives the milliseconds of those
+ * launches summed over the call's waves and kernel_ms[1..] zero; *launches receives the number of
+ * launches. Timed with CUDA events on the executor's stream. */
 #define FO_BATCH_KERNELS 5
 int fo_executor_batch_kernel_ms(fo_executor* executor, double* kernel_ms, uint64_t capacity, uint64_t* launches);
 /* Host->device and device->host bytes the executor's last batch call copied. */
 int fo_executor_batch_transfer_bytes(fo_executor* executor, uint64_t* h2d_bytes, uint64_t* d2h_bytes);
+
+/* ---- batch launch shape (no counterpart in the reference) ------------------------------------
+ * A batch wave is one persistent launch whose CTAs take work items from a queue: the training
+ * simulation of a block range of one group, the backward fit of one (group, strike) problem, the
+ * evaluation of a block range of one group for a chunk of its strikes. Its shape: */
+typedef struct fo_batch_tuning {
+    int32_t sim_blocks;   /* training-simulation blocks (256 paths each) per work item, 1..64     */
+    int32_t eval_blocks;  /* evaluation blocks (256 paths each) per work item, 1..64              */
+    int32_t strikes;      /* strikes an evaluation item applies together: 1, 2, 4 or 8            */
+    int32_t ctas_per_sm;  /* resident CTAs per SM, 0..8 (0: as many as the registers allow)       */
+} fo_batch_tuning;
+
+/* autotune != 0 (the default): the executor picks the shape per class of wave (path counts, rows,
+ * strikes per group, group count, degree, Greeks) by timing a few candidates on the first wave of
+ * the class, and keeps the fastest for later waves of the class. autotune == 0: every launch takes
+ * *fixed. Every shape gives the same results, bit for bit. */
+int fo_executor_set_batch_tuning(fo_executor* executor, int32_t autotune, const fo_batch_tuning* fixed, fo_error* err);
+
+typedef struct fo_batch_launch_info {
+    fo_batch_tuning tuning;    /* shape of the last launch (strikes: as launched)          */
+    int32_t source;            /* 0: fixed by the caller, 1: tuned earlier, 2: tuned now   */
+    int32_t grid;              /* CTAs launched                                            */
+    uint64_t items;            /* work items of the last launch                            */
+    uint64_t tuning_launches;  /* launches the tuner timed (source 2)                      */
+} fo_batch_launch_info;
+int fo_executor_batch_launch(fo_executor* executor, fo_batch_launch_info* out);
 
 /* ---- simulation exports --------------------------------------------------------------------- */
 
@@ -520,9 +548,30 @@ typedef struct fo_gbm_seeded_request {
 
 /* Time-major [n_exercise_nodes + 1, paths] pre-event states at every exercise node followed by
  * the post-event expiry state (path.rs:948-1024). `states` holds out_len doubles, exactly
- * (n_exercise_nodes + 1) * paths. */
+ * (n_exercise_nodes + 1) * paths. The three simulation exports return FO_ERR_SIMULATION only for
+ * a non-finite path transition or an exhausted / rejected random draw; every other simulation
+ * failure (spot, path count, buffer lengths, non-finite normals, escrowed forwards) is
+ * FO_ERR_INPUT, as the reference's Python boundary classifies them (lib.rs:277-292). */
 int fo_simulate_gbm_seeded_f64(fo_executor* executor, const fo_gbm_seeded_request* request,
                                double* states, uint64_t out_len, fo_error* err);
+
+/* simulate_gbm_f64 (crates/finoptions-python/src/lib.rs:969-1018): the same paths driven by the
+ * caller's standard normals instead of Philox streams. normals holds normal_rows x request->paths
+ * values, time-major ([interval][path]), and normal_rows must equal the schedule's intervals; the
+ * request's seed and domain are not read. Checks run in the reference's order: the plan, the
+ * interval rows, the initial spot, the path count, then every normal for finiteness before any path
+ * is computed (SimulationError with the interval and path of the first bad value, as
+ * GbmPathPlan::validate_execution, path.rs:558-603). */
+int fo_simulate_gbm_f64(fo_executor* executor, const fo_gbm_seeded_request* request, const double* normals,
+                        uint64_t normal_rows, double* states, uint64_t out_len, fo_error* err);
+/* Device-resident form of both simulation exports (no counterpart in the reference): states and
+ * normals are device pointers on the executor's device (e.g. a torch tensor's storage); normals ==
+ * NULL simulates the request's Philox streams (fo_simulate_gbm_seeded_f64), otherwise the caller's
+ * normals (fo_simulate_gbm_f64). Nothing is copied to the host; the call returns once the states
+ * are written. */
+int fo_simulate_gbm_device_f64(fo_executor* executor, const fo_gbm_seeded_request* request,
+                               const double* device_normals, uint64_t normal_rows, double* device_states,
+                               uint64_t out_len, fo_error* err);
 
 /* Path-local standard normals: out[p * normals_per_path + k] is the k-th ZIGNOR normal of path
  * path_start + p in namespace (seed, domain), with a normal budget of normals_per_path. */

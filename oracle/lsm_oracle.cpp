@@ -46,6 +46,7 @@ enum OracleCode : int32_t {
     ORC_BUDGET_EXHAUSTED = 1,
     ORC_REJECTION_LIMIT = 2,
     ORC_NON_FINITE_PATH_TRANSITION = 3,
+    ORC_NON_FINITE_NORMAL_BUFFER = 4,
     ORC_INSUFFICIENT_OBSERVATIONS = 10,
     ORC_NON_FINITE_PREDICTOR = 11,
     ORC_NON_FINITE_RESPONSE = 12,
@@ -359,8 +360,10 @@ Failure build_escrowed_plan(const std::vector<double>& times, const std::vector<
 // ---------------------------------------------------------------------------------------------
 
 // One path; `obs` receives rows() pre-event states (path-major slice).
+// `normals`, when given, replaces the Philox stream: the variate of interval i is
+// normals[i * stride + path] (GbmPathPlan::simulate_with, path.rs:139-175).
 Failure simulate_one(const Plan& plan, double initial_spot, uint32_t path, uint64_t seed,
-                     uint32_t domain, double* obs) {
+                     uint32_t domain, double* obs, const double* normals = nullptr, uint64_t stride = 0) {
     const uint32_t budget = uint32_t(plan.times.size() - 1);
     PathStream stream(seed, domain, path, budget);
     double spot = initial_spot;
@@ -371,7 +374,8 @@ Failure simulate_one(const Plan& plan, double initial_spot, uint32_t path, uint6
     }
     for (size_t interval = 0; interval < plan.steps.size(); ++interval) {
         double normal = 0.0;
-        const int status = sample_standard_normal(stream, &normal);
+        const int status = normals ? ORC_OK : sample_standard_normal(stream, &normal);
+        if (normals) normal = normals[interval * stride + path];
         if (status != ORC_OK) {
             Failure f = fail(status);
             f.interval = int64_t(interval);
@@ -429,7 +433,7 @@ Failure reconstruct_escrowed(const Plan& plan, double initial_spot, uint32_t pat
 // Time-major [rows, paths] simulation, path-parallel over `threads` workers with the lowest
 // failing path reported (seeded.rs:147-196). Escrowed plans start at S0 - prepaid[0].
 Failure simulate(const Plan& plan, double initial_spot, uint64_t paths, uint64_t seed,
-                 uint32_t domain, int threads, std::vector<double>* time_major) {
+                 uint32_t domain, int threads, std::vector<double>* time_major, const double* normals = nullptr) {
     const size_t rows = plan.rows();
     double start = initial_spot;
     if (plan.escrowed) {
@@ -442,7 +446,7 @@ Failure simulate(const Plan& plan, double initial_spot, uint64_t paths, uint64_t
         std::vector<double> obs(rows);
         for (uint64_t p = begin; p < end; ++p) {
             if (p > first_failure.load(std::memory_order_relaxed)) return;
-            Failure f = simulate_one(plan, start, uint32_t(p), seed, domain, obs.data());
+            Failure f = simulate_one(plan, start, uint32_t(p), seed, domain, obs.data(), normals, paths);
             if (f.ok() && plan.escrowed) f = reconstruct_escrowed(plan, initial_spot, uint32_t(p), obs.data());
             if (!f.ok()) {
                 uint64_t cur = first_failure.load();
@@ -467,7 +471,7 @@ Failure simulate(const Plan& plan, double initial_spot, uint64_t paths, uint64_t
     const uint64_t failed = first_failure.load();
     if (failed != UINT64_MAX) {
         std::vector<double> obs(rows);
-        Failure f = simulate_one(plan, start, uint32_t(failed), seed, domain, obs.data());
+        Failure f = simulate_one(plan, start, uint32_t(failed), seed, domain, obs.data(), normals, paths);
         if (f.ok() && plan.escrowed) f = reconstruct_escrowed(plan, initial_spot, uint32_t(failed), obs.data());
         return f;
     }
@@ -1486,6 +1490,40 @@ int orc_simulate_gbm_seeded(const fo_gbm_seeded_request* q, int32_t threads, dou
     }
     std::vector<double> tm;
     Failure f = simulate(plan, q->initial_spot, q->paths, q->seed, q->domain, threads, &tm);
+    if (!f.ok()) {
+        write_error(err, f, FO_ERR_SIMULATION);
+        return FO_ERR_SIMULATION;
+    }
+    std::memcpy(states, tm.data(), tm.size() * sizeof(double));
+    return FO_OK;
+}
+
+// simulate_gbm_f64 over the oracle: `normals` is [intervals][paths]. Every variate is checked
+// before any path is stepped (GbmPathPlan::validate_execution, path.rs:558-603); the first
+// non-finite one fails with its interval and path.
+int orc_simulate_gbm(const fo_gbm_seeded_request* q, const double* normals, int32_t threads, double* states,
+                     uint64_t out_len, fo_error* err) {
+    Plan plan = plan_from_gbm(q->schedule_times, q->n_schedule_times, q->log_discounts,
+                              q->cumulative_dividend_yields, q->dividend_nodes, q->dividend_amounts,
+                              q->n_dividend_nodes, q->exercise_nodes, q->n_exercise_nodes, q->expiry_node,
+                              q->annualized_volatility, q->dividend_policy);
+    const uint64_t paths = q->paths;
+    if (paths == 0 || out_len != plan.rows() * paths) {
+        write_error(err, fail(ORC_INVALID_INPUT), FO_ERR_INPUT);
+        return FO_ERR_INPUT;
+    }
+    const uint64_t n = plan.steps.size() * paths;
+    for (uint64_t i = 0; i < n; ++i)
+        if (!std::isfinite(normals[i])) {
+            Failure f = fail(ORC_NON_FINITE_NORMAL_BUFFER);
+            f.interval = int64_t(i / paths);
+            f.path = int64_t(i % paths);
+            f.x = normals[i];
+            write_error(err, f, FO_ERR_SIMULATION);
+            return FO_ERR_SIMULATION;
+        }
+    std::vector<double> tm;
+    Failure f = simulate(plan, q->initial_spot, paths, 0, 0, threads, &tm, normals);
     if (!f.ok()) {
         write_error(err, f, FO_ERR_SIMULATION);
         return FO_ERR_SIMULATION;

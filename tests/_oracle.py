@@ -52,6 +52,10 @@ def load() -> ctypes.CDLL:
         lib.orc_simulate_gbm_seeded.argtypes = [
             ctypes.POINTER(_abi.FoGbmSeededRequest), ctypes.c_int32, ctypes.c_void_p, ctypes.c_uint64, err,
         ]
+        lib.orc_simulate_gbm.argtypes = [
+            ctypes.POINTER(_abi.FoGbmSeededRequest), ctypes.c_void_p, ctypes.c_int32, ctypes.c_void_p, ctypes.c_uint64,
+            err,
+        ]
         lib.orc_price_lsm_call.argtypes = [
             ctypes.POINTER(_abi.FoLsmCallRequest), ctypes.c_int32, ctypes.POINTER(_abi.FoLsmCallResult), err,
             ctypes.POINTER(ctypes.c_int32),
@@ -103,6 +107,19 @@ def simulate(request: GbmRequest, threads: int = 8) -> np.ndarray:
     out = np.zeros((request.rows, int(q.paths)))
     err = _abi.FoError()
     status = load().orc_simulate_gbm_seeded(ctypes.byref(q), threads, out.ctypes.data, out.size, ctypes.byref(err))
+    if status:
+        raise OracleFailure(status, err)
+    return out
+
+
+def simulate_from(request: GbmRequest, normals: np.ndarray, threads: int = 8) -> np.ndarray:
+    """States [rows, paths] stepped by the caller's normals [intervals, paths] (simulate_gbm_f64)."""
+    q = request.struct
+    normals = np.ascontiguousarray(normals, dtype=np.float64)
+    out = np.zeros((request.rows, int(q.paths)))
+    err = _abi.FoError()
+    status = load().orc_simulate_gbm(ctypes.byref(q), normals.ctypes.data, threads, out.ctypes.data, out.size,
+                                     ctypes.byref(err))
     if status:
         raise OracleFailure(status, err)
     return out

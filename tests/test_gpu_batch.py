@@ -255,3 +255,43 @@ def test_overlapping_domain_ranges_are_rejected(native_executor) -> None:
     status, err, _ = gpu_batch(native_executor, req)
     assert status == _abi.FO_ERR_INPUT
     assert err.message.decode() == "batched LSM training domains [0, 3) overlap evaluation domains [2, 5)"
+
+
+def test_arrow_tables_price_like_the_numpy_columns(executor) -> None:
+    """The same grouped request from pyarrow tables (finoptions.arrow) and from NumPy columns."""
+    import finoptions as fo
+    import pyarrow as pa
+    from finoptions import arrow
+
+    c = grouped_columns(6, strikes_per_group=4, seed=47, min_exercise=5, max_exercise=12)
+    mesh = fo.ExplicitExerciseMesh(schedules=fo.RaggedExerciseTimes(offsets=c.exercise_offsets, times=c.exercise_times),
+                                   origin_exercise=fo.OriginExercise.EXCLUDED)
+    method = fo.Lsm(training_paths=4096, evaluation_paths=4096, training_stream=fo.RandomStream(seed=23, domain=0),
+                    evaluation_stream=fo.RandomStream(seed=23, domain=1 << 20),
+                    insufficient_exercise_support=fo.InsufficientExerciseSupportPolicy.CONTINUE)
+    div = [c.dividend_times[c.dividend_offsets[g]:c.dividend_offsets[g + 1]].tolist() for g in range(c.groups)]
+    amt = [c.dividend_amounts[c.dividend_offsets[g]:c.dividend_offsets[g + 1]].tolist() for g in range(c.groups)]
+    states = pa.table({"spot": c.initial_spots, "maturity": c.maturities, "rate": c.rates, "vol": c.volatilities,
+                       "div_times": pa.array(div, type=pa.large_list(pa.float64())),
+                       "div_amounts": pa.array(amt, type=pa.large_list(pa.float64()))})
+    strikes = pa.table({"strike": c.strikes})
+    table = arrow.price_lsm_strike_group_tables(
+        states, strikes, group_offsets=pa.array(c.group_offsets, type=pa.uint32()),
+        state_columns=arrow.LsmStrikeGroupColumns(initial_spot="spot", maturity="maturity", rate="rate",
+                                                  volatility="vol"),
+        strike_column="strike",
+        dividends=arrow.CashDividendColumns(times="div_times", amounts="div_amounts",
+                                            policy=fo.DividendPolicy.LIQUIDATOR,
+                                            maturity_boundary=fo.MaturityBoundary.STRICTLY_BEFORE),
+        mesh=mesh, executor=executor, method=method)
+    groups = fo.LsmStrikeGroups(
+        group_offsets=c.group_offsets, initial_spots=c.initial_spots, strikes=c.strikes, maturities=c.maturities,
+        rates=c.rates, volatilities=c.volatilities,
+        dividends=fo.CashDividendBatch(
+            schedules=fo.RaggedCashDividends(offsets=c.dividend_offsets, times=c.dividend_times,
+                                             amounts=c.dividend_amounts),
+            policy=fo.DividendPolicy.LIQUIDATOR, maturity_boundary=fo.MaturityBoundary.STRICTLY_BEFORE))
+    direct = fo.price_lsm_call_grouped_batch(groups=groups, mesh=mesh, executor=executor, method=method)
+    assert table.num_rows == c.strikes.size
+    for name in ("prices", "standard_errors", "early_exercise_paths", "maximum_regression_condition_numbers"):
+        np.testing.assert_array_equal(table.column(name).to_numpy(), getattr(direct, name), err_msg=name)

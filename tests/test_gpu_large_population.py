@@ -38,7 +38,12 @@ def assert_matches_oracle(gpu: tuple, want: tuple) -> None:
     assert gpu[2] == pytest.approx(sd, rel=1e-9)
     assert gpu[3] == pytest.approx(se, rel=1e-9)
     assert (gpu[1], gpu[4], gpu[5]) == (paths, nodes, counts)
-    assert [d[:5] for d in gpu[6]] == [d[:5] for d in diags]  # node, kind, ITM counts, columns
+    for d, o in zip(gpu[6], diags, strict=True):
+        assert d[:2] == o[:2]
+        if d[1] == "origin_decision":  # (node, kind, exercised, continuation value, None)
+            assert d[2] == o[2] and d[3] == pytest.approx(o[3], rel=1e-9)
+        else:  # node, kind, in-the-money counts, columns
+            assert d[:5] == o[:5]
 
 
 def test_weekly_contract_at_2p21_paths_matches_the_oracle(native_executor) -> None:

@@ -21,6 +21,7 @@ from finoptions import _abi
 from finoptions._requests import gbm_seeded_request, lsm_call_request, lsm_call_result
 
 import _oracle
+from _workloads import grouped_columns, grouped_row_as_call
 
 pytestmark = pytest.mark.gpu
 GOLDEN = json.loads((Path(__file__).parent / "golden" / "golden.json").read_text())
@@ -169,6 +170,22 @@ ORACLE_CODES = {
     20: "FO_CODE_NON_FINITE_DISCOUNTED_PAYOFF",
     21: "FO_CODE_EVALUATION_OUTSIDE_TRAINING_SUPPORT",
 }
+
+
+def test_a_row_far_from_the_previous_rows_mean_is_fitted_about_its_own(native_executor) -> None:
+    """Strike 1.2 S0 of a 17-date state (row 55 of the seed-71 grouped columns): its first exercise
+    row has 6 in-the-money paths whose mean moneyness (1.0023, sd 0.0026) lies nine standard
+    deviations from the next row's (1.026), the pivot its power sums are staged about. The engine
+    takes that row's sums again about its own mean; its condition number and the price match the
+    oracle."""
+    c = grouped_columns(12, 8, seed=71, min_exercise=6, max_exercise=20)
+    req = lsm_call_request(**grouped_row_as_call(c, 55, 4096))
+    status, err, gpu = gpu_price(native_executor, req)
+    assert status == 0, err.message
+    oracle = _oracle.price_lsm_call(req, 16)
+    assert_parity(gpu, oracle)
+    assert gpu[6][0][4] == 6
+    assert math.isclose(gpu[6][0][8], oracle[6][0][8], rel_tol=1e-10)
 
 
 def test_full_size_weekly_contract_matches_the_oracle(native_executor) -> None:

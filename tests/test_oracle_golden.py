@@ -176,3 +176,45 @@ def test_continuous_yield_european_slice_covers_black_scholes_merton() -> None:
     expected = spot * math.exp(-q_yield * maturity) * cdf(d1) - strike * math.exp(-rate * maturity) * cdf(d1 - srt)
     assert abs(price - expected) <= 5.0 * se
     assert diags == []
+
+
+def _explicit_normals_request(paths: int, dividend: tuple[int, float] | None = None, exercises=(1, 2)):
+    from finoptions._requests import gbm_seeded_request
+
+    times = [0.0, 0.25, 0.5, 1.0]
+    return gbm_seeded_request(
+        initial_spot=100.0, schedule_times=times, curve_times=times, log_discounts=[0.0, -0.01, -0.02, -0.05],
+        dividend_yield_times=times, cumulative_dividend_yields=[0.0] * 4,
+        dividend_nodes=[] if dividend is None else [dividend[0]], dividend_amounts=[] if dividend is None else [dividend[1]],
+        exercise_nodes=list(exercises), expiry_node=3, annualized_volatility=0.20, dividend_policy=0, paths=paths,
+        seed=0, domain=0,
+    )
+
+
+def test_explicit_normal_paths_follow_the_adjacent_transition() -> None:
+    """The reference's tests/test_simulation.py:59-96 closed form: S *= exp(-(dL) - v/2 + sqrt(v) z)."""
+    normals = np.array([[0.0, 1.0], [0.5, -0.5], [-1.0, 0.25]])
+    states = _oracle.simulate_from(_explicit_normals_request(2), normals)
+    times, logs = (0.0, 0.25, 0.5, 1.0), (0.0, -0.01, -0.02, -0.05)
+    current, want = np.full(2, 100.0), []
+    for i in range(3):
+        variance = 0.2**2 * (times[i + 1] - times[i])
+        current = current * np.exp(-(logs[i + 1] - logs[i]) - 0.5 * variance + np.sqrt(variance) * normals[i])
+        want.append(current.copy())
+    np.testing.assert_allclose(states, np.array(want), rtol=2e-15, atol=0.0)
+
+
+def test_explicit_normal_paths_store_the_pre_dividend_exercise_state() -> None:
+    """tests/test_simulation.py:99-116: a same-node dividend is applied after the exercise observation."""
+    states = _oracle.simulate_from(_explicit_normals_request(1, dividend=(1, 200.0), exercises=(1,)), np.zeros((3, 1)))
+    assert states[0, 0] > 0.0 and states[1, 0] == 0.0
+
+
+def test_explicit_normal_paths_reject_the_first_non_finite_variate() -> None:
+    """tests/test_simulation.py:136-139: the first bad variate in [interval][path] order is reported."""
+    normals = np.zeros((3, 2))
+    normals[2, 1] = np.nan
+    normals[2, 0] = np.inf
+    with pytest.raises(_oracle.OracleFailure) as failure:
+        _oracle.simulate_from(_explicit_normals_request(2), normals)
+    assert failure.value.path == 0 and "interval=2" in str(failure.value)

@@ -167,3 +167,21 @@ def test_cpu_executor_is_not_a_fallback() -> None:
             executor=CpuExecutor(threads=2), method=method(),
         )
     assert CudaExecutor is not CpuExecutor
+
+
+def test_simulation_entries_do_not_fall_back_to_the_cpu() -> None:
+    from finoptions import ExecutionError, simulate_gbm, simulate_gbm_on_device
+    from finoptions.model import DividendPolicy
+
+    schedule = EventSchedule(times=(0.0, 0.5, 1.0), dividends=(), exercise_nodes=(1,), expiry_node=2)
+    common = dict(initial_spot=100.0, schedule=schedule,
+                  curve=LogDiscountCurve(times=schedule.times, log_discounts=(0.0, -0.02, -0.05)),
+                  dividend_yield_curve=CumulativeDividendYieldCurve.zero(times=schedule.times),
+                  volatility=ConstantVolatility(0.2), dividend_policy=DividendPolicy.LIQUIDATOR,
+                  executor=CpuExecutor(threads=2))
+    with pytest.raises(ExecutionError, match="prices only on CudaExecutor"):
+        simulate_gbm(**common, normals=np.zeros((2, 4)))
+    with pytest.raises(ExecutionError, match="prices only on CudaExecutor"):
+        simulate_gbm_on_device(**common, paths=4, random_stream=RandomStream(seed=1, domain=1))
+    with pytest.raises(InputError, match="initial_spot must be a plain float"):
+        simulate_gbm(**{**common, "initial_spot": 100}, normals=np.zeros((2, 4)))
