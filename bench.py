@@ -148,6 +148,29 @@ def profiled_traffic(kernel: str) -> float | None:
     return None if entry is None else float(entry["dram_bytes_per_path_row"])
 
 
+def profiled_instructions(kernel: str) -> float | None:
+    """Warp instructions per path-step of `kernel` from the committed ncu summary, if present."""
+    path = ROOT / "profiles" / "issue.json"
+    if not path.is_file():
+        return None
+    data = json.loads(path.read_text())
+    entry = data.get(kernel)
+    return None if entry is None else float(entry["warp_instructions"]) / float(data["path_steps_profiled"])
+
+
+def issue_rate(kernel: str, ms: float, path_steps_per_launch: int, sm_mhz: float, sms: int) -> dict | None:
+    """Issue-rate roofline of an instruction-bound kernel: warp instructions per launch (the profiled
+    count per path-step times the launch's path-steps) over its measured time, against the issue
+    peak of one warp instruction per scheduler per cycle (4 per SM) at the SM clock seen under load."""
+    per_step = profiled_instructions(kernel)
+    if per_step is None or ms <= 0 or sm_mhz <= 0:
+        return None
+    achieved = per_step * path_steps_per_launch / (ms / 1e3)
+    peak = 4.0 * sms * sm_mhz * 1e6
+    return {"warp_instructions_per_path_step": round(per_step, 2), "achieved_winst_per_s": achieved,
+            "peak_winst_per_s": peak, "frac": round(achieved / peak, 4)}
+
+
 def cpu_threads() -> int:
     return len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else (os.cpu_count() or 1)
 
@@ -346,6 +369,13 @@ def run_ours(args: argparse.Namespace) -> dict | None:
     dom_ms = per_kernel[dominant] / per_kernel_launches
     achieved = algorithmic / (dom_ms / 1e3) / 1e9
     traffic_unit = profiled_traffic(dominant)
+    clock_report = clocks.report()
+    sm_mhz = float(clock_report.get("sm_mhz") or 0.0)
+    sms = torch.cuda.get_device_properties(0).multi_processor_count
+    for name in ("simulate_kernel", "evaluate_kernel"):
+        rate = issue_rate(name, roofline_all[name]["ms_per_launch"], path_steps(paths) // 2, sm_mhz, sms)
+        if rate is not None:
+            roofline_all[name]["issue"] = rate
     out = {
         "metric": METRIC,
         "value": value,
@@ -370,16 +400,21 @@ def run_ours(args: argparse.Namespace) -> dict | None:
         "gpu_launches": int(kernels.value) * args.steps,
         "roofline": {
             "kernel": dominant,
-            "bound": "hbm",
+            # The backward pass is bound by the latency of its 52 dependent row exchanges (each row
+            # a grid-wide reduction and a regression solve), not by HBM: achieved / peak below is its
+            # HBM fraction, us_per_row the figure that bounds it.
+            "bound": "latency" if dominant == "backward_kernel" else "hbm",
             "achieved": round(achieved, 1),
             "peak": hbm_peak,
             "peak_source": peak_kind,
             "unit": "GB/s",
             "frac": round(achieved / hbm_peak, 4),
             "traffic": None if traffic_unit is None else int(traffic_unit * stored_rows * paths),
+            "rows": stored_rows,
+            "us_per_row": round(dom_ms * 1e3 / stored_rows, 2),
         },
         "kernels": roofline_all,
-        "clocks": clocks.report(),
+        "clocks": clock_report,
         "result": {"price": price, "standard_error": se},
     }
     if world == 1:
@@ -445,11 +480,11 @@ def run_ragged(args: argparse.Namespace, executor) -> dict:
             lib.fo_executor_batch_kernel_ms(executor.raw, ms, 5, ctypes.byref(launches))
             kernel_ms = [a + b for a, b in zip(kernel_ms, ms, strict=True)]
         wall = time.perf_counter() - t0
-        device_ms = sum(kernel_ms) / calls
+        device_ms = kernel_ms[0] / calls
         out[name] = {"device_ms_per_call": device_ms, "device_contracts_per_s": c.rows / (device_ms / 1e3),
                      "device_path_steps_per_s": steps / (device_ms / 1e3),
                      "e2e_contracts_per_s": c.rows * calls / wall, "e2e_ms_per_call": wall / calls * 1e3,
-                     "kernels_ms": {"batch_persistent_kernel": round(kernel_ms[0] / calls, 3)},
+                     "kernels_ms": batch_kernel_ms(kernel_ms, calls),
                      "gpu_launches_per_call": int(launches.value), "launch_shape": batch_launch(lib, executor)}
     out["greeks_overhead"] = out["price_and_greeks"]["device_ms_per_call"] / out["plain"]["device_ms_per_call"]
     # The north-star comparison: the same contracts (same populations, so the same price and SE)
@@ -577,6 +612,16 @@ def grouped_algorithmic_bytes(c, paths: int) -> dict:
     }
 
 
+def batch_kernel_ms(kernel_ms: list, calls: int) -> dict:
+    """Per-call device milliseconds of a batch call's graph, split into the phase kernels when the
+    executor ran them (fo_executor_batch_kernel_ms slots 1..3)."""
+    out = {"graph": round(kernel_ms[0] / calls, 3)}
+    if any(kernel_ms[1:4]):
+        out.update(simulate=round(kernel_ms[1] / calls, 3), fit=round(kernel_ms[2] / calls, 3),
+                   evaluate=round(kernel_ms[3] / calls, 3))
+    return out
+
+
 def batch_launch(lib, executor) -> dict:
     """The launch shape the executor used for its last batch call (autotuned per shape class)."""
     from finoptions import _abi
@@ -586,7 +631,9 @@ def batch_launch(lib, executor) -> dict:
     t = info.tuning
     return {"sim_blocks_per_item": t.sim_blocks, "eval_blocks_per_item": t.eval_blocks,
             "strikes_per_eval_item": t.strikes, "ctas_per_sm": t.ctas_per_sm or "max", "ctas": info.grid,
-            "work_items": int(info.items), "chosen_by": ("caller", "autotuner (cached)", "autotuner")[info.source]}
+            "work_items": int(info.items), "chosen_by": ("caller", "autotuner (cached)", "autotuner")[info.source],
+            "executor": "phase kernels (simulation, fit, evaluation, summary)" if t.phases else "one persistent launch",
+            "graph_replays_last_call": int(info.graph_replays), "graph_captures_last_call": int(info.graph_captures)}
 
 
 def run_grouped(args: argparse.Namespace, executor) -> dict:
@@ -627,7 +674,7 @@ def run_grouped(args: argparse.Namespace, executor) -> dict:
         wall = time.perf_counter() - t0
     h2d, d2h = ctypes.c_uint64(), ctypes.c_uint64()
     lib.fo_executor_batch_transfer_bytes(executor.raw, ctypes.byref(h2d), ctypes.byref(d2h))
-    device_ms = sum(kernel_ms) / steps
+    device_ms = kernel_ms[0] / steps
     contracts = req.rows
     steps_per_call = _workloads.path_steps(cols, GROUPED_PATHS)
     algorithmic = grouped_algorithmic_bytes(cols, GROUPED_PATHS)
@@ -640,6 +687,19 @@ def run_grouped(args: argparse.Namespace, executor) -> dict:
                                            "achieved_gbs": round(launch_bytes / (device_ms / 1e3) / 1e9, 1)}}
     dominant = "batch_persistent_kernel"
     achieved = launch_bytes / (device_ms / 1e3) / 1e9
+    bound = "hbm (fits) + issue (simulation, evaluation)"
+    phases = batch_kernel_ms(kernel_ms, steps)
+    if len(phases) > 1:  # the phase executor: one kernel per item kind, inside the same graph
+        kernels = {"batch_" + name + "_kernel": {"ms_per_call": ms, "share": round(ms / device_ms, 4)}
+                   for name, ms in phases.items() if name != "graph"}
+        for name, key in (("simulate", "batch_simulate_kernel"), ("fit", "batch_backward_kernel")):
+            k = kernels["batch_" + name + "_kernel"]
+            k.update(algorithmic_bytes=algorithmic[key],
+                     achieved_gbs=round(algorithmic[key] / (k["ms_per_call"] / 1e3) / 1e9, 1))
+        dominant = "batch_fit_kernel"
+        achieved = kernels[dominant]["achieved_gbs"]
+        bound = "latency (one CTA per problem, row by row; values and spots from L2 / HBM)"
+
     # The same contracts one by one on the plain per-contract path: the first GROUPED_PLAIN_SAMPLE
     # rows (whole states), each repricing its state's populations (same price and SE as the batch).
     import finoptions as fo
@@ -677,7 +737,7 @@ def run_grouped(args: argparse.Namespace, executor) -> dict:
         "gpu_launches": launches,
         "launch_shape": batch_launch(lib, executor),
         "kernels": kernels,
-        "roofline": {"kernel": dominant, "bound": "hbm (fits) + issue (simulation, evaluation)",
+        "roofline": {"kernel": dominant, "bound": bound,
                      "achieved": round(achieved, 1), "peak": hbm_peak, "peak_source": peak_kind, "unit": "GB/s",
                      "frac": round(achieved / hbm_peak, 4), "traffic": None},
         "clocks": clocks.report(),

@@ -6,6 +6,7 @@
 
 #include <algorithm>
 #include <map>
+#include <vector>
 #include <mutex>
 #include <string>
 
@@ -102,7 +103,14 @@ struct fo_executor {
     int batch_grid = 0;                                   // CTAs of the last batch launch
     int batch_strikes = 0;                                // strikes per evaluation item of the last launch
     uint64_t batch_items = 0;                             // work items of the last launch
+    // The last batch wave as a captured CUDA graph (table upload, resets, the persistent launch and
+    // the read-back), replayed while a wave's launch key (addresses, sizes, launch arguments)
+    // repeats; any other key captures again.
+    cudaGraphExec_t batch_graph = nullptr;
+    std::vector<unsigned char> batch_graph_key;
+    uint64_t batch_graph_replays = 0, batch_graph_captures = 0;  // last batch call
     ~fo_executor() {
+        if (batch_graph) cudaGraphExecDestroy(batch_graph);
         for (cudaEvent_t& e : batch_marks)
             if (e) cudaEventDestroy(e);
         if (fork) cudaEventDestroy(fork);

@@ -22,6 +22,8 @@ struct BatchGroup {
     uint32_t first_problem;  // wave-local index of the group's first strike problem
     uint32_t problems;       // strike rows in the group
     double sigma;            // the plan's constant volatility (adjoint vega)
+    uint32_t fit_items;      // backward work items of the group (team members summed over its problems)
+    uint32_t pad;
 };
 
 // One (group, strike) problem of the launched wave.
@@ -32,7 +34,15 @@ struct BatchProblem {
     uint64_t values;         // first element of its training values (train_paths doubles)
     int32_t skip_fit;        // 1: the host already failed this problem's fit (no backward pass)
     uint32_t partial_base;   // first of its evaluation blocks' partial slots (one per block)
+    uint32_t members;        // CTAs that fit it together (1: one CTA)
+    uint32_t team_base;      // first of its team's exchange slots (2 x members x kTeamSlots double2)
 };
+
+// Training paths one member of a team fits: problems with more are split over several CTAs, whose
+// CTA sums are exchanged once per row (at most kMaxTeam members; the queue holds them in a row).
+constexpr uint64_t kTeamPaths = 32768;
+constexpr uint32_t kMaxTeam = 64;
+constexpr int kTeamSlots = 16;  // double2 slots of one member's exchange (the row reduction's sums)
 
 // Failure keys; every word starts as all-ones ("none") and keeps the lowest key with atomicMin.
 struct GroupStatus {
@@ -101,7 +111,7 @@ constexpr size_t kEvalRuleSmemBytes = 96 * 1024;
 enum BatchItemKind : uint32_t {
     kItemNone = 0,
     kItemSimulate = 1,  // training paths of blocks [first, first + count) of group `index`
-    kItemBackward = 2,  // backward fit (and row diagnostics) of problem `index`
+    kItemBackward = 2,  // backward fit of problem `index` by team member `first` of `count`
     kItemEvaluate = 3,  // evaluation blocks [first, first + count) of group `index`, strike chunk `chunk`
 };
 
@@ -116,8 +126,10 @@ struct BatchItem {
 
 // Dependency counters of one launch, all zeroed before it: a group's backward items wait until
 // sim_done[g] reaches its training blocks, its evaluation items until bwd_done[g] reaches its
-// problems; the item that brings eval_done[g] to the group's evaluation units writes the group's
+// fit items; the item that brings eval_done[g] to the group's evaluation units writes the group's
 // summaries. A wait gives up after a time limit and raises *timeout (no item ever waits forever).
+// The members of a team are consecutive items and wait only on each other and on earlier items,
+// and a team has at most kMaxTeam members (fewer than the launch's CTAs), so its waits end too.
 struct BatchQueue {
     const BatchItem* items;
     uint32_t n_items;
@@ -147,6 +159,8 @@ struct BatchArgs {
     double2* greek_partials;   // [evaluation blocks of all problems][kGreekSlots]
     double* greek_sums;        // [problems][kGreekSlots]
     unsigned* stop_counts;     // [records]
+    double2* team_slots;       // exchange slots of the teams (BatchProblem::team_base)
+    unsigned* team_arrive;     // [problems]: arrivals at the team's exchanges
     uint32_t train_blocks;     // training-simulation blocks of the largest group (grid x)
     uint32_t eval_blocks;      // evaluation blocks of the largest group (grid x, partials stride)
     int32_t degree;

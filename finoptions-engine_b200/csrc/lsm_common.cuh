@@ -238,7 +238,7 @@ __device__ __forceinline__ void accumulate_itm(RowSums& r, double x, double y, d
 #pragma unroll
     for (int k = 1; k < kPowerSums; ++k) {
         r.acc[k] += pw;
-        if (k < kResponseSums) r.acc[kPowerSums + k] += y * pw;
+        if (k < kResponseSums) r.acc[kPowerSums + k] = fo_fma(y, pw, r.acc[kPowerSums + k]);
         pw *= t;
     }
 }
@@ -260,7 +260,7 @@ __device__ __forceinline__ void accumulate_responses(RowSums& r, double t, doubl
     double pw = t;
 #pragma unroll
     for (int k = 1; k < kResponseSums; ++k) {
-        r.acc[kPowerSums + k] += y * pw;
+        r.acc[kPowerSums + k] = fo_fma(y, pw, r.acc[kPowerSums + k]);
         pw *= t;
     }
 }

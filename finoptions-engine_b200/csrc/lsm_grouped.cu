@@ -803,6 +803,7 @@ struct WaveLayout {
     size_t counters;
     size_t greek_sums;                                                  // (read back, Greeks only)
     size_t counts, itm_counts, stop_counts, eval_partials, greek_partials, records, values, slab, replay;
+    size_t team_arrive, team_slots;
     size_t out_begin, out_bytes, clear_begin, clear_bytes, total;
 };
 
@@ -816,11 +817,18 @@ struct Wave {
     uint32_t train_blocks = 0;   // largest training grid of a group
     uint64_t partial_slots = 0;  // evaluation blocks summed over the problems (one partial slot each)
     uint64_t item_bound = 0;     // work items of the persistent launch, at most (one block per item)
+    uint64_t team_slots = 0;     // exchange slots (double2) of the teams of large problems
     bool greeks = false;         // adjoint Greeks buffers
 };
 
 uint32_t eval_blocks_for(uint64_t eval_paths) {
     return uint32_t((eval_paths + kBatchEvalThreads - 1) / kBatchEvalThreads);
+}
+
+// CTAs that fit a problem of `train_paths` paths together (one up to kTeamPaths).
+uint32_t team_members(uint64_t train_paths) {
+    const uint64_t m = (train_paths + kTeamPaths - 1) / kTeamPaths;
+    return uint32_t(std::max<uint64_t>(1, std::min<uint64_t>(m, kMaxTeam)));
 }
 
 WaveLayout layout_for(const Wave& w, size_t base) {
@@ -849,12 +857,15 @@ WaveLayout layout_for(const Wave& w, size_t base) {
     L.itm_counts = take(sizeof(unsigned) * w.records);
     L.stop_counts = take(w.greeks ? sizeof(unsigned) * w.records : 0);
     L.records = take(sizeof(FitRecord) * w.records);
-    L.counters = take(sizeof(unsigned) * (3 * G + 2));  // next item, timeout, sim / bwd / eval done per group
+    // next item (one launch), timeout, next item of each phase kernel, sim / bwd / eval done per group
+    L.counters = take(sizeof(unsigned) * (3 * G + 5));
+    L.team_arrive = take(sizeof(unsigned) * P);
     off = align_up(off, 256);
     L.clear_bytes = off - L.clear_begin;
     L.eval_partials = take(sizeof(double2) * 2 * std::max<uint64_t>(w.partial_slots, 1));
     L.greek_partials = take(w.greeks ? sizeof(double2) * kGreekSlots * w.partial_slots : 0);
     L.replay = take(sizeof(SimFailure));
+    L.team_slots = take(sizeof(double2) * std::max<uint64_t>(w.team_slots, 1));
     L.values = take(sizeof(double) * std::max<uint64_t>(w.value_elems, 1));
     L.slab = take(sizeof(double) * std::max<uint64_t>(w.slab_elems, 1));
     L.total = align_up(off, 256);
@@ -1127,9 +1138,10 @@ std::string tuning_key(const Work& work, const WaveT& w, bool greeks, int degree
            std::to_string(log2_ceil(w.g1 - w.g0));
 }
 
-// The autotuner: a coordinate search from the default launch shape over the evaluation blocks per
-// item, the simulation blocks per item, the strikes per evaluation item and the CTAs per SM, each
-// candidate timed by one launch of the wave; a change is kept when it is at least 2% faster.
+// The autotuner: a coordinate search from the default launch shape over the executor (one persistent
+// launch or three phase kernels), the evaluation blocks per item, the simulation blocks per item,
+// the strikes per evaluation item and the CTAs per SM, each candidate timed by one launch of the
+// wave; a change is kept when it is at least 1% faster.
 template <typename Run>
 Error autotune_wave(Run& run, bool greeks, int max_strikes, BatchTuning* best, uint64_t* runs) {
     BatchTuning cur;
@@ -1142,12 +1154,17 @@ Error autotune_wave(Run& run, bool greeks, int max_strikes, BatchTuning* best, u
         Error te = run(cand, &ms);
         if (!te.ok()) return te;
         *runs += 1;
-        if (ms < 0.98f * cur_ms) {
+        if (ms < 0.99f * cur_ms) {
             cur = cand;
             cur_ms = ms;
         }
         return Error{};
     };
+    {
+        BatchTuning c = cur;  // the three phase kernels instead of one persistent launch
+        c.phases = 1;
+        if (!(e = attempt(c)).ok()) return e;
+    }
     for (const int eval_blocks : {2, 4}) {
         BatchTuning c = cur;
         c.eval_blocks = eval_blocks;
@@ -1165,7 +1182,7 @@ Error autotune_wave(Run& run, bool greeks, int max_strikes, BatchTuning* best, u
         c.strikes = widest / 2;
         if (!(e = attempt(c)).ok()) return e;
     }
-    {
+    if (!cur.phases) {  // CTAs per SM only shape the persistent launch
         BatchTuning c = cur;
         c.ctas_per_sm = 2;
         if (!(e = attempt(c)).ok()) return e;
@@ -1280,7 +1297,9 @@ Error price_groups(fo_executor* ex, const BatchMethod& m, const std::vector<Grou
             cur.eval_blocks = std::max(cur.eval_blocks, eval_blocks);
             cur.train_blocks = std::max(cur.train_blocks, train_blocks);
             cur.partial_slots += strikes_g * eval_blocks;
-            cur.item_bound += train_blocks + strikes_g + strikes_g * eval_blocks;
+            const uint32_t members = team_members(hp.train_paths);
+            cur.item_bound += train_blocks + strikes_g * members + strikes_g * eval_blocks;
+            if (members > 1) cur.team_slots += strikes_g * 2ull * members * kTeamSlots;
             cur.greeks = greeks;
             bytes += cost;
         }
@@ -1300,7 +1319,7 @@ Error price_groups(fo_executor* ex, const BatchMethod& m, const std::vector<Grou
     size_t stage = in_bytes;
     for (const Wave& w : waves) {
         const WaveLayout L = layout_for(w, 0);
-        stage = std::max(stage, L.out_begin + L.out_bytes);
+        stage = std::max(stage, L.out_begin + L.out_bytes + 16);
     }
     e = ex->batch_host.reserve(stage);
     if (!e.ok()) return e;
@@ -1310,6 +1329,7 @@ Error price_groups(fo_executor* ex, const BatchMethod& m, const std::vector<Grou
         if (!mk) FO_CUDA_TRY(cudaEventCreate(&mk), "cudaEventCreate");
     for (double& ms : ex->batch_ms) ms = 0.0;
     ex->batch_launches = 0;
+    ex->batch_graph_replays = ex->batch_graph_captures = 0;
     ex->batch_h2d = ex->batch_d2h = 0;
     if (launchable > 0) {
         std::memset(host, 0, in_bytes);
@@ -1335,7 +1355,7 @@ Error price_groups(fo_executor* ex, const BatchMethod& m, const std::vector<Grou
         auto* hg = reinterpret_cast<BatchGroup*>(host + (L.groups - in_bytes));
         auto* hpb = reinterpret_cast<BatchProblem*>(host + (L.problems - in_bytes));
         unsigned char* back = host + (L.out_begin - in_bytes);  // the read-back region, after the tables
-        uint64_t slab = 0, record = 0, problem = 0, values = 0, partial = 0;
+        uint64_t slab = 0, record = 0, problem = 0, values = 0, partial = 0, team = 0;
         slab_of.assign(w.g1 - w.g0, 0);
         uint32_t max_rows = 1, max_strikes = 1;
         for (uint64_t g = w.g0; g < w.g1; ++g) {
@@ -1347,6 +1367,8 @@ Error price_groups(fo_executor* ex, const BatchMethod& m, const std::vector<Grou
             bg.first_problem = uint32_t(problem);
             bg.problems = uint32_t(work[g].end_row - work[g].first_row);
             bg.sigma = work[g].sigma;
+            const uint32_t members = team_members(hp.train_paths);
+            bg.fit_items = bg.problems * members;
             max_strikes = std::max(max_strikes, bg.problems);
             for (uint64_t r = work[g].first_row; r < work[g].end_row; ++r) {
                 BatchProblem& pb = hpb[problem];
@@ -1356,6 +1378,9 @@ Error price_groups(fo_executor* ex, const BatchMethod& m, const std::vector<Grou
                 pb.values = values;
                 pb.skip_fit = work[g].fit.ok() ? 0 : 1;
                 pb.partial_base = uint32_t(partial);
+                pb.members = members;
+                pb.team_base = uint32_t(team);
+                if (members > 1) team += 2ull * members * kTeamSlots;
                 partial += eval_blocks_for(hp.eval_paths);
                 record += hp.rows();
                 values += hp.train_paths;
@@ -1367,6 +1392,7 @@ Error price_groups(fo_executor* ex, const BatchMethod& m, const std::vector<Grou
         // One persistent launch of the wave with launch shape `tune`. Every launch recomputes the
         // whole wave from its inputs (the state it writes is cleared first), so the result does not
         // depend on the shape or on launches before it.
+        float phase_ms[3] = {0.f, 0.f, 0.f};  // the phase kernels of the last launch (phase executor)
         auto run_wave = [&](const BatchTuning& tune, float* launch_ms) -> Error {
             // The persistent launch's work queue (lsm_persistent.cu), topologically ordered: every
             // group's training simulation (largest training work first, long fits right after their
@@ -1388,6 +1414,7 @@ Error price_groups(fo_executor* ex, const BatchMethod& m, const std::vector<Grou
                                       " observation rows per contract; observed " + u(max_rows));
             std::vector<BatchItem> items;
             items.reserve(w.item_bound);
+            uint32_t phase_items[3] = {0, 0, 0};  // simulation, fit, evaluation items (phase order only)
             {
                 const uint32_t sim_step = uint32_t(std::max(1, tune.sim_blocks));
                 const uint32_t eval_step = uint32_t(std::max(1, tune.eval_blocks));
@@ -1399,17 +1426,18 @@ Error price_groups(fo_executor* ex, const BatchMethod& m, const std::vector<Grou
                 };
                 std::stable_sort(gorder.begin(), gorder.end(),
                                  [&](uint32_t x, uint32_t y) { return train_work(x) > train_work(y); });
-                // Fits by work (training paths x rows), largest first. A fit that alone is long next to
-                // a CTA's share of all fitting work (at least half of it on the largest grid) is queued
-                // right after its group's simulation, so it starts early instead of after every
-                // group's simulation.
+                // Fits by one member's work (its training paths x rows), largest first. A fit that alone
+                // is long next to a CTA's share of all fitting work (at least half of it on the largest
+                // grid) is queued right after its group's simulation, so it starts early instead of
+                // after every group's simulation. A team's members are queued in a row.
                 std::vector<std::pair<uint64_t, uint32_t>> fits;
                 fits.reserve(w.problems);
                 uint64_t fit_work = 0;
                 for (uint64_t i = 0; i < w.problems; ++i) {
                     const HostPlan& hp = work[w.g0 + hpb[i].group].hp;
-                    fits.emplace_back(uint64_t(hp.train_paths) * hp.rows(), uint32_t(i));
-                    fit_work += fits.back().first;
+                    const uint64_t member_paths = (hp.train_paths + hpb[i].members - 1) / hpb[i].members;
+                    fits.emplace_back(member_paths * hp.rows(), uint32_t(i));
+                    fit_work += fits.back().first * hpb[i].members;
                 }
                 std::stable_sort(fits.begin(), fits.end(), [](const auto& x, const auto& y) { return x.first > y.first; });
                 const uint64_t long_fit = fit_work / (2 * uint64_t(std::max(1, ex->sms)) * kPersistentMaxCtasPerSm);
@@ -1422,16 +1450,26 @@ Error price_groups(fo_executor* ex, const BatchMethod& m, const std::vector<Grou
                 std::vector<uint64_t> last_fit(G, 0);
                 uint64_t queued_fits = 0;
                 auto queue_fit = [&](uint32_t i) {
-                    items.push_back(BatchItem{kItemBackward, i, 0, 0, 0, {0, 0, 0}});
+                    for (uint32_t m = 0; m < hpb[i].members; ++m)
+                        items.push_back(BatchItem{kItemBackward, i, m, hpb[i].members, 0, {0, 0, 0}});
                     last_fit[hpb[i].group] = queued_fits++;
                 };
+                // The phase kernels take the items kind by kind: every simulation, then every fit
+                // (largest first), then every evaluation.
                 for (const uint32_t gl : gorder) {
                     const uint32_t blocks = eval_blocks_for(work[w.g0 + gl].hp.train_paths);
                     for (uint32_t b = 0; b < blocks; b += sim_step)
                         items.push_back(BatchItem{kItemSimulate, gl, b, std::min(sim_step, blocks - b), 0, {0, 0, 0}});
-                    for (const uint32_t i : early[gl]) queue_fit(i);
+                    if (!tune.phases)
+                        for (const uint32_t i : early[gl]) queue_fit(i);
                 }
-                for (const uint32_t i : late) queue_fit(i);
+                phase_items[0] = uint32_t(items.size());
+                if (tune.phases) {
+                    for (const auto& f : fits) queue_fit(f.second);
+                } else {
+                    for (const uint32_t i : late) queue_fit(i);
+                }
+                phase_items[1] = uint32_t(items.size()) - phase_items[0];
                 std::vector<uint32_t> eorder(G);
                 std::iota(eorder.begin(), eorder.end(), 0u);
                 std::stable_sort(eorder.begin(), eorder.end(),
@@ -1443,17 +1481,12 @@ Error price_groups(fo_executor* ex, const BatchMethod& m, const std::vector<Grou
                         for (uint32_t b = 0; b < blocks; b += eval_step)
                             items.push_back(BatchItem{kItemEvaluate, gl, b, std::min(eval_step, blocks - b), z, {0, 0, 0}});
                 }
+                phase_items[2] = uint32_t(items.size()) - phase_items[0] - phase_items[1];
                 std::memcpy(host + (L.items - in_bytes), items.data(), sizeof(BatchItem) * items.size());
             }
             // The group and problem tables and the queue's items (the item region is sized for the
             // finest cut; only the items of this launch shape travel).
             const size_t table_bytes = (L.items - L.groups) + sizeof(BatchItem) * items.size();
-            FO_CUDA_TRY(cudaMemcpyAsync(dev + L.groups, host + (L.groups - in_bytes), table_bytes,
-                                        cudaMemcpyHostToDevice, s),
-                        "batch table upload");
-            ex->batch_h2d += table_bytes;
-            FO_CUDA_TRY(cudaMemsetAsync(dev + L.out_begin, 0xff, L.summaries - L.out_begin, s), "batch status reset");
-            FO_CUDA_TRY(cudaMemsetAsync(dev + L.clear_begin, 0, L.clear_bytes, s), "batch reset");
             BatchArgs a{};
             a.groups = reinterpret_cast<const BatchGroup*>(dev + L.groups);
             a.problems = reinterpret_cast<const BatchProblem*>(dev + L.problems);
@@ -1471,6 +1504,8 @@ Error price_groups(fo_executor* ex, const BatchMethod& m, const std::vector<Grou
             a.greek_partials = greeks ? reinterpret_cast<double2*>(dev + L.greek_partials) : nullptr;
             a.greek_sums = greeks ? reinterpret_cast<double*>(dev + L.greek_sums) : nullptr;
             a.stop_counts = greeks ? reinterpret_cast<unsigned*>(dev + L.stop_counts) : nullptr;
+            a.team_slots = reinterpret_cast<double2*>(dev + L.team_slots);
+            a.team_arrive = reinterpret_cast<unsigned*>(dev + L.team_arrive);
             a.train_blocks = w.train_blocks;
             a.eval_blocks = w.eval_blocks;
             a.degree = m.degree;
@@ -1484,27 +1519,104 @@ Error price_groups(fo_executor* ex, const BatchMethod& m, const std::vector<Grou
             q.n_items = uint32_t(items.size());
             q.next = counters;
             q.timeout = counters + 1;
-            q.sim_done = counters + 2;
-            q.bwd_done = counters + 2 + G;
-            q.eval_done = counters + 2 + 2 * G;
+            q.sim_done = counters + 5;
+            q.bwd_done = counters + 5 + G;
+            q.eval_done = counters + 5 + 2 * G;
+            // The phase kernels' parts of the queue (the items are in phase order then).
+            BatchQueue qs[3] = {q, q, q};
+            {
+                uint32_t at = 0;
+                for (int k = 0; k < 3; ++k) {
+                    qs[k].items = q.items + at;
+                    qs[k].n_items = phase_items[k];
+                    qs[k].next = counters + 2 + k;
+                    at += phase_items[k];
+                }
+            }
             cudaEvent_t* mark = ex->batch_marks;
-            FO_CUDA_TRY(cudaEventRecord(mark[0], s), "event");
             int grid = 0;
-            FO_CUDA_TRY(launch_batch_persistent(a, q, eval_strikes, max_rows, stage, tune.ctas_per_sm, s, &grid),
-                        "batch launch");
-            FO_CUDA_TRY(cudaEventRecord(mark[1], s), "event");
+            PersistentLaunch launch[4] = {};
+            const int n_launches = tune.phases ? 4 : 1;
+            if (tune.phases) {
+                FO_CUDA_TRY(prepare_batch_phases(a, qs, eval_strikes, max_rows, stage, launch), "batch launch");
+                grid = launch[1].grid;
+            } else {
+                FO_CUDA_TRY(prepare_batch_persistent(a, q, eval_strikes, max_rows, stage, tune.ctas_per_sm, &launch[0]),
+                            "batch launch");
+                grid = launch[0].grid;
+            }
+            // The wave's stream work, in order: table upload, status / state resets, the persistent
+            // launch between two timing marks, the read-back (results, then the timeout flag into
+            // the pinned tail of the read-back region).
+            unsigned* timed_out = reinterpret_cast<unsigned*>(back + L.out_bytes);
+            auto enqueue = [&]() -> cudaError_t {
+                cudaError_t ce = cudaMemcpyAsync(dev + L.groups, host + (L.groups - in_bytes), table_bytes,
+                                                 cudaMemcpyHostToDevice, s);
+                if (ce == cudaSuccess) ce = cudaMemsetAsync(dev + L.out_begin, 0xff, L.summaries - L.out_begin, s);
+                if (ce == cudaSuccess) ce = cudaMemsetAsync(dev + L.clear_begin, 0, L.clear_bytes, s);
+                // External record nodes: the marks are recorded when the graph runs (a plain record
+                // during capture would only order the captured work).
+                if (ce == cudaSuccess) ce = cudaEventRecordWithFlags(mark[0], s, cudaEventRecordExternal);
+                for (int k = 0; k < n_launches && ce == cudaSuccess; ++k) {
+                    ce = enqueue_batch_persistent(launch[k], a, tune.phases ? qs[k < 3 ? k : 2] : q, max_rows, stage, s);
+                    if (ce == cudaSuccess) ce = cudaEventRecordWithFlags(mark[k + 1], s, cudaEventRecordExternal);
+                }
+                if (ce == cudaSuccess) ce = cudaMemcpyAsync(back, dev + L.out_begin, L.out_bytes, cudaMemcpyDeviceToHost, s);
+                if (ce == cudaSuccess)
+                    ce = cudaMemcpyAsync(timed_out, q.timeout, sizeof(unsigned), cudaMemcpyDeviceToHost, s);
+                return ce;
+            };
+            // Launch key: everything the captured work depends on.
+            std::vector<unsigned char> key;
+            auto put = [&](const void* p, size_t n) {
+                const auto* c = static_cast<const unsigned char*>(p);
+                key.insert(key.end(), c, c + n);
+            };
+            const void* bases[2] = {dev, host};
+            const size_t sizes[8] = {L.groups, L.out_begin, L.out_bytes, L.summaries, L.clear_begin, L.clear_bytes,
+                                     table_bytes, in_bytes};
+            put(bases, sizeof bases);
+            put(sizes, sizeof sizes);
+            put(&a, sizeof a);
+            put(&q, sizeof q);
+            put(qs, sizeof qs);
+            put(launch, sizeof launch);
+            put(&n_launches, sizeof n_launches);
+            const uint32_t extra[2] = {max_rows, stage ? 1u : 0u};
+            put(extra, sizeof extra);
+            if (!ex->batch_graph || key != ex->batch_graph_key) {
+                if (ex->batch_graph) {
+                    cudaGraphExecDestroy(ex->batch_graph);
+                    ex->batch_graph = nullptr;
+                }
+                cudaGraph_t graph = nullptr;
+                FO_CUDA_TRY(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal), "batch capture");
+                const cudaError_t ce = enqueue();
+                const cudaError_t ee = cudaStreamEndCapture(s, &graph);
+                FO_CUDA_TRY(ce, "batch capture");
+                FO_CUDA_TRY(ee, "batch capture");
+                const cudaError_t ie = cudaGraphInstantiate(&ex->batch_graph, graph, 0);
+                cudaGraphDestroy(graph);
+                FO_CUDA_TRY(ie, "batch graph instantiation");
+                ex->batch_graph_key = std::move(key);
+                ex->batch_graph_captures += 1;
+            } else {
+                ex->batch_graph_replays += 1;
+            }
+            FO_CUDA_TRY(cudaGraphLaunch(ex->batch_graph, s), "batch graph launch");
+            ex->batch_h2d += table_bytes;
             ex->batch_launches += 1;
             ex->batch_grid = grid;
             ex->batch_strikes = eval_strikes;
             ex->batch_items = items.size();
-            unsigned timed_out = 0;
-            FO_CUDA_TRY(cudaMemcpyAsync(back, dev + L.out_begin, L.out_bytes, cudaMemcpyDeviceToHost, s), "batch result copy");
-            FO_CUDA_TRY(cudaMemcpyAsync(&timed_out, q.timeout, sizeof(unsigned), cudaMemcpyDeviceToHost, s),
-                        "batch status copy");
             ex->batch_d2h += L.out_bytes + sizeof(unsigned);
             FO_CUDA_TRY(cudaStreamSynchronize(s), "batch pricing");
-            FO_CUDA_TRY(cudaEventElapsedTime(launch_ms, mark[0], mark[1]), "event");
-            if (timed_out)
+            FO_CUDA_TRY(cudaEventElapsedTime(launch_ms, mark[0], mark[n_launches]), "event");
+            for (int k = 0; k < 3; ++k) phase_ms[k] = 0.f;
+            if (tune.phases)  // the summary kernel is counted with the evaluation
+                for (int k = 0; k < 3; ++k)
+                    FO_CUDA_TRY(cudaEventElapsedTime(&phase_ms[k], mark[k], mark[k == 2 ? 4 : k + 1]), "event");
+            if (*timed_out)
                 return make_error(FO_ERR_EXECUTION, FO_CODE_BARRIER_TIMEOUT,
                                   "a batch work item waited too long for the items it depends on; the device result was "
                                   "discarded");
@@ -1531,6 +1643,7 @@ Error price_groups(fo_executor* ex, const BatchMethod& m, const std::vector<Grou
             Error re = run_wave(tune, &ms);
             if (!re.ok()) return re;
             ex->batch_ms[0] += ms;
+            for (int k = 0; k < 3; ++k) ex->batch_ms[1 + k] += phase_ms[k];
         }
         const auto* gst = reinterpret_cast<const GroupStatus*>(back + (L.group_status - L.out_begin));
         const auto* pst = reinterpret_cast<const ProblemStatus*>(back + (L.problem_status - L.out_begin));
@@ -1868,16 +1981,17 @@ int fo_executor_set_batch_tuning(fo_executor* executor, int32_t autotune, const 
     const bool valid = fixed->sim_blocks >= 1 && fixed->sim_blocks <= 64 && fixed->eval_blocks >= 1 &&
                        fixed->eval_blocks <= 64 && (fixed->strikes == 1 || fixed->strikes == 2 ||
                                                     fixed->strikes == 4 || fixed->strikes == 8) &&
-                       fixed->ctas_per_sm >= 0 && fixed->ctas_per_sm <= 8;
+                       fixed->ctas_per_sm >= 0 && fixed->ctas_per_sm <= 8 && (fixed->phases == 0 || fixed->phases == 1);
     if (!valid)
         return finish(err, make_error(FO_ERR_EXECUTION, FO_CODE_INVALID_ARGUMENT,
                                       "batch launch shape outside its range: blocks per item 1..64, strikes per "
-                                      "evaluation item 1, 2, 4 or 8, CTAs per SM 0..8"));
+                                      "evaluation item 1, 2, 4 or 8, CTAs per SM 0..8, phases 0 or 1"));
     executor->batch_autotune = false;
     executor->batch_tuning.sim_blocks = fixed->sim_blocks;
     executor->batch_tuning.eval_blocks = fixed->eval_blocks;
     executor->batch_tuning.strikes = fixed->strikes;
     executor->batch_tuning.ctas_per_sm = fixed->ctas_per_sm;
+    executor->batch_tuning.phases = fixed->phases;
     return FO_OK;
 }
 
@@ -1889,10 +2003,13 @@ int fo_executor_batch_launch(fo_executor* executor, fo_batch_launch_info* out) {
     out->tuning.eval_blocks = t.eval_blocks;
     out->tuning.strikes = executor->batch_strikes;
     out->tuning.ctas_per_sm = t.ctas_per_sm;
+    out->tuning.phases = t.phases;
     out->source = executor->batch_tuning_source;
     out->grid = executor->batch_grid;
     out->items = executor->batch_items;
     out->tuning_launches = executor->batch_tuning_source == 2 ? executor->batch_tuning_runs : 0;
+    out->graph_replays = executor->batch_graph_replays;
+    out->graph_captures = executor->batch_graph_captures;
     return FO_OK;
 }
 

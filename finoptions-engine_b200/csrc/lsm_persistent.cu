@@ -43,10 +43,13 @@ __device__ __forceinline__ unsigned long long ld_l2_u64(const unsigned long long
 __device__ __forceinline__ bool status_failed(const unsigned long long* word) { return ld_l2_u64(word) != kNone; }
 
 // Thread 0 waits (time-bounded) until *counter reaches target; every thread returns whether it did.
-__device__ bool wait_for(const unsigned* counter, unsigned target, unsigned* timeout, int* flag) {
+// The pause between polls doubles from 64 ns up to max_pause: dependency waits keep their polls of
+// L2 rare, a team's per-row exchange polls often.
+__device__ bool wait_for(const unsigned* counter, unsigned target, unsigned* timeout, int* flag,
+                         unsigned max_pause = 4096) {
     if (threadIdx.x == 0) {
         int ok = 1;
-        unsigned pause = 64;  // ns, doubled up to 4 us: waiting CTAs keep their polls of L2 rare
+        unsigned pause = 64;
         unsigned long long start = 0;
         while (ld_relaxed_gpu(counter) < target) {
             if (ld_volatile_u32(timeout) != 0) {
@@ -62,7 +65,7 @@ __device__ bool wait_for(const unsigned* counter, unsigned target, unsigned* tim
                 break;
             }
             __nanosleep(pause);
-            pause = pause < 4096 ? 2 * pause : pause;
+            pause = pause < max_pause ? 2 * pause : pause;
         }
         __threadfence();  // acquire: the items counted are visible to this CTA's reads below
         *flag = ok;
@@ -81,9 +84,11 @@ __device__ __forceinline__ unsigned signal_done(unsigned* counter, unsigned n) {
     return before;
 }
 
-// The part of a fitted record the evaluation reads, loaded from L2: the model's first sixteen
-// doubles are mean, scale, inv_scale, alpha[4], beta[4], coef[5] - PolicyRule's layout. The record
-// is 16-byte aligned (16-byte loads); a staged PolicyRule only 8-byte aligned (8-byte stores).
+// The part of a fitted record the evaluation reads: the model's first sixteen doubles are mean,
+// scale, inv_scale, alpha[4], beta[4], coef[5] - PolicyRule's layout. The record is 16-byte aligned
+// (16-byte loads); a staged PolicyRule only 8-byte aligned (8-byte stores). Records written by other
+// CTAs of the same launch are read through L2; kReadOnly (a later kernel) may use the read-only path.
+template <bool kReadOnly = false>
 __device__ __forceinline__ void load_rule(const FitRecord& rec, PolicyRule* out) {
     static_assert(offsetof(FitModel, mean) == 0 && offsetof(FitModel, coef) + sizeof(double) * kMaxColumns == 128,
                   "FitModel starts with the sixteen doubles of a PolicyRule");
@@ -93,11 +98,11 @@ __device__ __forceinline__ void load_rule(const FitRecord& rec, PolicyRule* out)
     double* dst = reinterpret_cast<double*>(out);
 #pragma unroll
     for (int i = 0; i < 8; ++i) {
-        const double2 v = __ldcg(src + i);
+        const double2 v = kReadOnly ? __ldg(src + i) : __ldcg(src + i);
         dst[2 * i] = v.x;
         dst[2 * i + 1] = v.y;
     }
-    out->kind = __ldcg(&rec.kind);
+    out->kind = kReadOnly ? __ldg(&rec.kind) : __ldcg(&rec.kind);
 }
 
 __device__ __forceinline__ uint32_t blocks_of(uint64_t paths) {
@@ -108,7 +113,7 @@ __device__ __forceinline__ uint32_t blocks_of(uint64_t paths) {
 
 __device__ void simulate_item(const BatchArgs& a, uint32_t gi, uint32_t first, uint32_t count, const SmemZig& zig) {
     const BatchGroup& g = a.groups[gi];
-    const DevicePlan& plan = g.plan;
+    const DevicePlan plan = g.plan;  // a local copy: its fields stay in registers (no reloads across stores)
     const uint64_t P = plan.train_paths;
     const uint32_t fsr = plan.first_stored_row;
     double* out = a.slab + g.slab_offset;
@@ -129,6 +134,48 @@ __device__ void simulate_item(const BatchArgs& a, uint32_t gi, uint32_t first, u
 
 // ---- backward fit of one problem ----------------------------------------------------------------
 
+// The CTAs that fit one problem together. Member m owns the contiguous paths [lo, hi).
+struct Team {
+    uint32_t member, members;
+    double2* slots;    // [2][members][kSlots]
+    unsigned* arrive;  // arrivals at this problem's exchanges
+    unsigned round;    // exchanges this member has made
+    unsigned* timeout;
+    int* flag;
+};
+
+// Every member publishes its CTA totals of a reduction (S double-double slots) and sums all members'
+// in member order, so each member ends with the same totals. Consecutive exchanges alternate between
+// two buffers: a member overwrites one only after every member has arrived at the exchange in
+// between, that is, has finished reading it. False when a wait gave up (the timeout flag is set).
+static_assert(kTeamSlots == kSlots, "a member's exchange holds one row reduction");
+
+template <int S, bool kTeam>
+__device__ bool team_exchange(Team& t, dd* total /* shared [S] */) {
+    if constexpr (!kTeam) return true;
+    if (t.members == 1) return true;
+    const unsigned parity = t.round & 1u;
+    if (threadIdx.x < S)
+        t.slots[(size_t(parity) * t.members + t.member) * kSlots + threadIdx.x] =
+            make_double2(total[threadIdx.x].hi, total[threadIdx.x].lo);
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) atomicAdd(t.arrive, 1u);
+    t.round += 1;
+    if (!wait_for(t.arrive, t.members * t.round, t.timeout, t.flag, 256)) return false;
+    if (threadIdx.x < S) {
+        const double2* column = t.slots + size_t(parity) * t.members * kSlots + threadIdx.x;
+        dd acc = dd_make(0.0);
+        for (uint32_t m = 0; m < t.members; ++m) {
+            const double2 v = __ldcg(column + size_t(m) * kSlots);
+            acc = dd_add(acc, dd{v.x, v.y});
+        }
+        total[threadIdx.x] = acc;
+    }
+    __syncthreads();
+    return true;
+}
+
 struct BackwardItemSmem {
     double red[32 * kSlots];
     dd total[kSlots];
@@ -138,26 +185,47 @@ struct BackwardItemSmem {
     int recenter;
 };
 
-// One CTA per problem: backward induction over the group's stored rows with the problem's values in
-// HBM, one CTA-wide deterministic reduction of in-the-money power sums per row and the regression
-// solve by one warp (policy.rs:215-296, 471-601). Thread t owns paths t + m * 256 (m = 0, 1, ...),
-// loading kPersistentLoads of them together.
-template <int D>
-__device__ void backward_item(const BatchArgs& a, uint32_t pi, BackwardItemSmem& sm) {
+// Backward induction of one problem over the group's stored rows with the problem's values in HBM
+// (policy.rs:215-296, 471-601): per row one deterministic reduction of in-the-money power sums and
+// the regression solve by one warp. A problem of up to kTeamPaths paths is one CTA's; a larger one
+// is split over a team of CTAs (this one is member `member` of `members`), each owning a contiguous
+// range of paths, whose CTA sums are exchanged in member order before every decision, so that every
+// member fits the same model; member 0 writes the records. Thread t owns paths lo + t + m * 256
+// (m = 0, 1, ...), loading kPersistentLoads of them together. False when a team exchange gave up.
+// A stored training state. The persistent launch reads rows that other CTAs of the same launch wrote,
+// so through L2 (the SM's L1 is not coherent with other SMs' writes); the fit kernel of the phase
+// executor runs after the simulation kernel has finished, so its reads may use the read-only path.
+template <bool kReadOnly>
+__device__ __forceinline__ double load_slab(const double* p) {
+    if constexpr (kReadOnly) return __ldg(p);
+    else return __ldcg(p);
+}
+
+template <int D, bool kReadOnlySlab, bool kTeam>
+__device__ bool backward_item(const BatchArgs& a, uint32_t pi, uint32_t member, uint32_t members, unsigned* timeout,
+                              int* flag, BackwardItemSmem& sm) {
     constexpr int kL = kPersistentLoads;
     const BatchProblem pr = a.problems[pi];
-    if (pr.skip_fit) return;
-    if (status_failed(&a.group_status[pr.group].train_sim_fail)) return;
+    if (pr.skip_fit) return true;
+    if (status_failed(&a.group_status[pr.group].train_sim_fail)) return true;
     const BatchGroup& g = a.groups[pr.group];
-    const DevicePlan& plan = g.plan;
+    const DevicePlan plan = g.plan;  // a local copy: its fields stay in registers (no reloads across stores)
     ProblemStatus* st = a.problem_status + pi;
     FitRecord* records = a.records + pr.records;
-    double* values = a.values + pr.values;
-    const double* slab = a.slab + g.slab_offset;
+    // Restrict-qualified: this problem's values are its own, and the slab is only read here, so the
+    // loads of several paths may be issued together, ahead of the stores.
+    double* __restrict__ values = a.values + pr.values;
+    const double* __restrict__ slab = a.slab + g.slab_offset;
     const uint64_t P = plan.train_paths;
     const unsigned T = blockDim.x;
     const uint64_t step = uint64_t(T) * kL;
-    const uint64_t first = threadIdx.x;
+    // This member's paths [lo, hi): contiguous ranges of a multiple of 256 paths, in member order.
+    const uint64_t span = members == 1 ? P : ((P + members - 1) / members + 255) / 256 * 256;
+    const uint64_t lo = members == 1 ? 0 : (uint64_t(member) * span < P ? uint64_t(member) * span : P);
+    const uint64_t hi = members == 1 ? P : (lo + span < P ? lo + span : P);
+    const uint64_t first = lo + threadIdx.x;
+    Team team{member, members, a.team_slots + pr.team_base, a.team_arrive + pi, 0u, timeout, flag};
+    const bool writer = member == 0;
     const double K = pr.strike;
     const Divisor Kd = make_divisor(K);
     const int degree = a.degree;
@@ -167,18 +235,18 @@ __device__ void backward_item(const BatchArgs& a, uint32_t pi, BackwardItemSmem&
     auto row_ptr = [&](uint32_t row) { return slab + uint64_t(row - fsr) * P; };
     {
         const double* terminal = row_ptr(E);
-        for (uint64_t base = first; base < P; base += step) {
+        for (uint64_t base = first; base < hi; base += step) {
             double s[kL];
 #pragma unroll
             for (int u = 0; u < kL; ++u) {
                 const uint64_t p = base + uint64_t(u) * T;
-                s[u] = p < P ? __ldcg(&terminal[p]) : 0.0;
+                s[u] = p < hi ? load_slab<kReadOnlySlab>(&terminal[p]) : 0.0;
             }
 #pragma unroll
             for (int u = 0; u < kL; ++u) {
                 const uint64_t p = base + uint64_t(u) * T;
                 const double d = s[u] - K;
-                if (p < P) values[p] = d > 0.0 ? d : 0.0;
+                if (p < hi) values[p] = d > 0.0 ? d : 0.0;
             }
         }
     }
@@ -193,18 +261,18 @@ __device__ void backward_item(const BatchArgs& a, uint32_t pi, BackwardItemSmem&
         const double disc = plan.disc_from_later[row];
         const double* srow = row_ptr(uint32_t(row));
         double loc[2] = {0.0, 0.0};
-        for (uint64_t base = first; base < P; base += step) {
+        for (uint64_t base = first; base < hi; base += step) {
             double v[kL], s[kL];
 #pragma unroll
             for (int u = 0; u < kL; ++u) {
                 const uint64_t p = base + uint64_t(u) * T;
-                v[u] = p < P ? values[p] : 0.0;
-                s[u] = p < P ? __ldcg(&srow[p]) : 0.0;
+                v[u] = p < hi ? values[p] : 0.0;
+                s[u] = p < hi ? load_slab<kReadOnlySlab>(&srow[p]) : 0.0;
             }
 #pragma unroll
             for (int u = 0; u < kL; ++u) {
                 const uint64_t p = base + uint64_t(u) * T;
-                if (p >= P) continue;
+                if (p >= hi) continue;
                 v[u] *= disc;
                 values[p] = v[u];
                 if (!fo_isfinite(v[u])) atomicMin(&st->fit_payoff_fail, ((unsigned long long)order << 32) | p);
@@ -218,19 +286,20 @@ __device__ void backward_item(const BatchArgs& a, uint32_t pi, BackwardItemSmem&
             }
         }
         cta_reduce_dd<2>(loc, sm.red, sm.total);
+        if (!team_exchange<2, kTeam>(team, sm.total)) return false;
         if (sm.total[0].hi > 0.0) pivot = dd_round(dd_div(sm.total[1], sm.total[0]));
-        for (uint64_t base = first; base < P; base += step) {
+        for (uint64_t base = first; base < hi; base += step) {
             double v[kL], s[kL];
 #pragma unroll
             for (int u = 0; u < kL; ++u) {
                 const uint64_t p = base + uint64_t(u) * T;
-                v[u] = p < P ? values[p] : 0.0;
-                s[u] = p < P ? __ldcg(&srow[p]) : 0.0;
+                v[u] = p < hi ? values[p] : 0.0;
+                s[u] = p < hi ? load_slab<kReadOnlySlab>(&srow[p]) : 0.0;
             }
 #pragma unroll
             for (int u = 0; u < kL; ++u) {
                 const uint64_t p = base + uint64_t(u) * T;
-                if (p >= P || !(s[u] > K)) continue;
+                if (p >= hi || !(s[u] > K)) continue;
                 const double x = divide(s[u], Kd);
                 if (!fo_isfinite(x) || !fo_isfinite(v[u])) {
                     sums.acc[kBadSlot] += 1.0;
@@ -243,6 +312,7 @@ __device__ void backward_item(const BatchArgs& a, uint32_t pi, BackwardItemSmem&
     }
     for (; row >= lowest; --row, ++order) {
         cta_reduce_dd<kSlots>(sums.acc, sm.red, sm.total);
+        if (!team_exchange<kSlots, kTeam>(team, sm.total)) return false;
         if (threadIdx.x == 0) {
             const uint64_t itm = uint64_t(sm.total[0].hi);
             double mean = pivot;
@@ -260,24 +330,25 @@ __device__ void backward_item(const BatchArgs& a, uint32_t pi, BackwardItemSmem&
             const double* cur = row_ptr(uint32_t(row));
 #pragma unroll
             for (int k = 0; k < kSlots; ++k) sums.acc[k] = 0.0;
-            for (uint64_t base = first; base < P; base += step) {
+            for (uint64_t base = first; base < hi; base += step) {
                 double v[kL], s[kL];
 #pragma unroll
                 for (int u = 0; u < kL; ++u) {
                     const uint64_t p = base + uint64_t(u) * T;
-                    v[u] = p < P ? values[p] : 0.0;
-                    s[u] = p < P ? __ldcg(&cur[p]) : 0.0;
+                    v[u] = p < hi ? values[p] : 0.0;
+                    s[u] = p < hi ? load_slab<kReadOnlySlab>(&cur[p]) : 0.0;
                 }
 #pragma unroll
                 for (int u = 0; u < kL; ++u) {
                     const uint64_t p = base + uint64_t(u) * T;
-                    if (p >= P || !(s[u] > K)) continue;
+                    if (p >= hi || !(s[u] > K)) continue;
                     const double x = divide(s[u], Kd);
                     if (!fo_isfinite(x) || !fo_isfinite(v[u])) sums.acc[kBadSlot] += 1.0;
                     else accumulate_itm(sums, x, v[u], pivot);
                 }
             }
             cta_reduce_dd<kSlots>(sums.acc, sm.red, sm.total);
+            if (!team_exchange<kSlots, kTeam>(team, sm.total)) return false;
         }
         if (threadIdx.x < 32) {
             // Warp 0 decides the row and fits it (the lane-parallel solve, bit-identical to the
@@ -300,11 +371,11 @@ __device__ void backward_item(const BatchArgs& a, uint32_t pi, BackwardItemSmem&
             FitRecord& rec = records[row];
             constexpr int kModelWords = int(sizeof(FitModel) / sizeof(double2));
             static_assert(sizeof(FitModel) % sizeof(double2) == 0, "FitModel is 16-byte aligned");
-            if (threadIdx.x < kModelWords)
+            if (writer && threadIdx.x < kModelWords)
                 reinterpret_cast<double2*>(&rec.model)[threadIdx.x] =
                     reinterpret_cast<const double2*>(&sm.model)[threadIdx.x];
-            if (threadIdx.x == 0) {
-                sm.kind = kind;
+            if (threadIdx.x == 0) sm.kind = kind;
+            if (writer && threadIdx.x == 0) {
                 rec.kind = kind;
                 rec.itm = population;
                 rec.pivot = pivot;
@@ -315,7 +386,7 @@ __device__ void backward_item(const BatchArgs& a, uint32_t pi, BackwardItemSmem&
         }
         __syncthreads();
         const int kind = sm.kind;
-        if (kind == kRuleFitFailed) return;  // the problem's fit raised; the host reports it
+        if (kind == kRuleFitFailed) return true;  // the problem's fit raised; the host reports it
         const bool regression = kind == kRuleRegression;
         if (regression) pivot = sm.model.mean;
         const bool stage_next = row - 1 >= lowest;
@@ -324,20 +395,20 @@ __device__ void backward_item(const BatchArgs& a, uint32_t pi, BackwardItemSmem&
         const double* nxt = stage_next ? row_ptr(uint32_t(row - 1)) : cur;
 #pragma unroll
         for (int k = 0; k < kSlots; ++k) sums.acc[k] = 0.0;
-        for (uint64_t base = first; base < P; base += step) {
+        for (uint64_t base = first; base < hi; base += step) {
             double v[kL], sc[kL], sn[kL];
 #pragma unroll
             for (int u = 0; u < kL; ++u) {
                 const uint64_t p = base + uint64_t(u) * T;
-                const bool in = p < P;
+                const bool in = p < hi;
                 v[u] = in ? values[p] : 0.0;
-                sc[u] = in && regression ? __ldcg(&cur[p]) : 0.0;
-                sn[u] = in && stage_next ? __ldcg(&nxt[p]) : 0.0;
+                sc[u] = in && regression ? load_slab<kReadOnlySlab>(&cur[p]) : 0.0;
+                sn[u] = in && stage_next ? load_slab<kReadOnlySlab>(&nxt[p]) : 0.0;
             }
 #pragma unroll
             for (int u = 0; u < kL; ++u) {
                 const uint64_t p = base + uint64_t(u) * T;
-                if (p >= P) continue;
+                if (p >= hi) continue;
                 if (regression && sc[u] > K) {
                     const double intrinsic = sc[u] - K;
                     double continuation;
@@ -365,24 +436,24 @@ __device__ void backward_item(const BatchArgs& a, uint32_t pi, BackwardItemSmem&
 #pragma unroll
             for (int u = 0; u < kL; ++u) {
                 const uint64_t p = base + uint64_t(u) * T;
-                if (p < P) values[p] = v[u];
+                if (p < hi) values[p] = v[u];
             }
         }
     }
     // Common origin decision (policy.rs:265-281): mean of the values discounted to the origin.
     if (plan.origin_row) {
         double acc[2] = {0.0, 0.0};
-        for (uint64_t base = first; base < P; base += step) {
+        for (uint64_t base = first; base < hi; base += step) {
             double v[kL];
 #pragma unroll
             for (int u = 0; u < kL; ++u) {
                 const uint64_t p = base + uint64_t(u) * T;
-                v[u] = p < P ? values[p] : 0.0;
+                v[u] = p < hi ? values[p] : 0.0;
             }
 #pragma unroll
             for (int u = 0; u < kL; ++u) {
                 const uint64_t p = base + uint64_t(u) * T;
-                if (p >= P) continue;
+                if (p >= hi) continue;
                 const double w = v[u] * plan.origin_discount;
                 if (!fo_isfinite(w)) atomicMin(&st->fit_payoff_fail, ((unsigned long long)order << 32) | p);
                 acc[0] += 1.0;
@@ -390,7 +461,8 @@ __device__ void backward_item(const BatchArgs& a, uint32_t pi, BackwardItemSmem&
             }
         }
         cta_reduce_dd<2>(acc, sm.red, sm.total);
-        if (threadIdx.x == 0) {
+        if (!team_exchange<2, kTeam>(team, sm.total)) return false;
+        if (writer && threadIdx.x == 0) {
             const double mean = dd_round(dd_div(sm.total[1], sm.total[0]));
             const double intrinsic = plan.initial_spot - K > 0.0 ? plan.initial_spot - K : 0.0;
             FitRecord& rec = records[0];
@@ -401,6 +473,7 @@ __device__ void backward_item(const BatchArgs& a, uint32_t pi, BackwardItemSmem&
             rec.diag_status = -1;
         }
     }
+    return true;
 }
 
 // Rank / condition diagnostic of every regression row of problem pi (regression.rs:540-577); the
@@ -461,15 +534,16 @@ struct EvalSmem {
 // Evaluation blocks [first, first + count) of group gi for strike chunk z: each thread
 // re-simulates one evaluation path per block and applies up to S fitted policies on the fly
 // (policy.rs:642-834); per (problem, block) double-double partials and stopping counts.
-template <int S, int D>
+// kStaged: the rules were staged in shared memory (read there with shared-memory loads); otherwise
+// each lookup reads the FitRecord through L2.
+template <int S, int D, bool kStaged, bool kReadOnly>
 __device__ void evaluate_item(const BatchArgs& a, uint32_t gi, uint32_t first, uint32_t count, uint32_t z,
-                              const SmemZig& zig, EvalSmem<S>& sm, PolicyRule* staged, bool stage_rules,
-                              uint32_t rule_rows) {
+                              const SmemZig& zig, EvalSmem<S>& sm, PolicyRule* staged, uint32_t rule_rows) {
     const BatchGroup& g = a.groups[gi];
     const uint32_t p0 = g.first_problem + z * S;
     const int ns = min(S, int(g.problems) - int(z) * S);
     if (ns <= 0 || status_failed(&a.group_status[gi].train_sim_fail)) return;  // uniform over the CTA
-    const DevicePlan& plan = g.plan;
+    const DevicePlan plan = g.plan;  // a local copy: its fields stay in registers (no reloads across stores)
     const uint32_t rows = plan.rows;
     if (threadIdx.x < S) {
         const bool live = int(threadIdx.x) < ns;
@@ -481,10 +555,10 @@ __device__ void evaluate_item(const BatchArgs& a, uint32_t gi, uint32_t first, u
         sm.problem[threadIdx.x] = live ? p0 + threadIdx.x : p0;
     }
     __syncthreads();
-    if (stage_rules) {
+    if constexpr (kStaged) {
         for (uint32_t i = threadIdx.x; i < uint32_t(ns) * rows; i += blockDim.x) {
             const uint32_t k = i / rows, r = i % rows;
-            load_rule(a.records[sm.rbase[k] + r], &staged[k * rule_rows + r]);
+            load_rule<kReadOnly>(a.records[sm.rbase[k] + r], &staged[k * rule_rows + r]);
         }
         __syncthreads();
     }
@@ -520,19 +594,16 @@ __device__ void evaluate_item(const BatchArgs& a, uint32_t gi, uint32_t first, u
                 if (!((active >> k) & 1u)) continue;
                 const double K = sm.strikes[k];
                 PolicyRule loaded;
-                const PolicyRule* rule = &staged[k * rule_rows + row];
-                if (!stage_rules) {
-                    load_rule(a.records[sm.rbase[k] + row], &loaded);
-                    rule = &loaded;
-                }
-                if (rule->kind == kRuleNoSupport) {
+                if constexpr (!kStaged) load_rule<kReadOnly>(a.records[sm.rbase[k] + row], &loaded);
+                const PolicyRule& rule = kStaged ? staged[k * rule_rows + row] : loaded;
+                if (rule.kind == kRuleNoSupport) {
                     if (spot > K) atomicAdd(&a.itm_counts[sm.rbase[k] + row], 1u);
                     continue;
                 }
-                if (rule->kind != kRuleRegression || !(spot > K)) continue;
+                if (rule.kind != kRuleRegression || !(spot > K)) continue;
                 const double intrinsic = spot - K;
                 double continuation;
-                if (!predict_continuation_d<D>(*rule, divide(spot, Divisor{K, sm.inv_strikes[k]}), &continuation)) {
+                if (!predict_continuation_d<D>(rule, divide(spot, Divisor{K, sm.inv_strikes[k]}), &continuation)) {
                     atomicMin(&a.problem_status[sm.problem[k]].eval_fail, ((unsigned long long)row << 33) | (p << 1));
                     continue;
                 }
@@ -576,16 +647,16 @@ struct GreeksEvalSmem {
 
 // The adjoint variant: evaluation blocks [first, first + count) of group gi for its strike k alone,
 // with the pathwise Greeks (lsm_adjoint.cuh) summed per block in double-double.
-template <int D>
+template <int D, bool kReadOnly>
 __device__ void evaluate_greeks_item(const BatchArgs& a, uint32_t gi, uint32_t first, uint32_t count, uint32_t k,
                                      const SmemZig& zig, GreeksEvalSmem& sm, PolicyRule* rules, unsigned* stops) {
     const BatchGroup& g = a.groups[gi];
     if (k >= g.problems || status_failed(&a.group_status[gi].train_sim_fail)) return;  // uniform over the CTA
     const uint32_t problem = g.first_problem + k;
     const BatchProblem pr = a.problems[problem];
-    const DevicePlan& plan = g.plan;
+    const DevicePlan plan = g.plan;  // a local copy: its fields stay in registers (no reloads across stores)
     const uint32_t rows = plan.rows;
-    for (uint32_t r = threadIdx.x; r < rows; r += blockDim.x) load_rule(a.records[pr.records + r], &rules[r]);
+    for (uint32_t r = threadIdx.x; r < rows; r += blockDim.x) load_rule<kReadOnly>(a.records[pr.records + r], &rules[r]);
     const double K = pr.strike;
     const Divisor Kd = make_divisor(K);
     const uint64_t P = plan.eval_paths;
@@ -826,23 +897,77 @@ __device__ void summarize_problem(const BatchArgs& a, uint32_t i, int lane) {
 
 // ---- the persistent kernel ------------------------------------------------------------------------
 
+// Executors of the work items. kPhaseAll is the persistent launch: one kernel drains the whole queue,
+// items of every kind waiting on the counters. The other phases run the items of one kind as a
+// queue-draining kernel of their own, launched in stream order (simulation, fits, evaluation), so
+// that each kind gets the register budget and CTAs per SM that suit it; their dependency waits are
+// then already met. Both run the same item functions, so they give the same results, bit for bit.
+enum BatchPhase : int { kPhaseAll = 0, kPhaseSimulate = 1, kPhaseFit = 2, kPhaseEvaluate = 3 };
+
+// Shared memory of the items a kernel runs: all kinds for the persistent launch, one kind each for
+// the phase kernels (less static shared memory leaves more of the SM's L1).
+template <int S>
+union AllItemsSmem {
+    BackwardItemSmem bwd;
+    EvalSmem<S> eval;
+    GreeksEvalSmem greeks;
+};
+struct NoItemSmem {};
+struct FitItemSmem {
+    BackwardItemSmem bwd;
+};
+template <int S>
+struct EvalItemSmem {
+    EvalSmem<S> eval;
+};
+struct GreeksItemSmem {
+    GreeksEvalSmem greeks;
+};
+template <int kPhase, int S, bool kGreeks>
+struct PhaseSmem {
+    using type = AllItemsSmem<S>;
+};
+template <int S, bool kGreeks>
+struct PhaseSmem<1, S, kGreeks> {
+    using type = NoItemSmem;
+};
+template <int S, bool kGreeks>
+struct PhaseSmem<2, S, kGreeks> {
+    using type = FitItemSmem;
+};
+template <int S>
+struct PhaseSmem<3, S, false> {
+    using type = EvalItemSmem<S>;
+};
+template <int S>
+struct PhaseSmem<3, S, true> {
+    using type = GreeksItemSmem;
+};
+
+template <int kPhase, int S, bool kGreeks>
+struct PhaseOccupancy {
+    // Resident CTAs per SM the register budget is cut for.
+    static constexpr int value = kPhase == kPhaseSimulate ? 6
+                                 : kPhase == kPhaseEvaluate && (S == 1 || kGreeks) ? 4
+                                                                                   : 3;
+};
+
 // S: strikes an evaluation item applies together (kGreeks: one, with the adjoint). The dynamic
 // shared memory holds the staged rules (S x rule_rows PolicyRules, plus per-row stopping counts with
 // the Greeks) when stage_rules is set.
-template <int S, bool kGreeks, int D>
-__global__ void __launch_bounds__(kPersistentThreads, 3)
+template <int kPhase, int S, bool kGreeks, int D>
+__global__ void __launch_bounds__(kPersistentThreads, (PhaseOccupancy<kPhase, S, kGreeks>::value))
     batch_persistent_kernel(BatchArgs a, BatchQueue q, uint32_t rule_rows, int stage_rules) {
+    constexpr bool kSim = kPhase == kPhaseAll || kPhase == kPhaseSimulate;
+    constexpr bool kFit = kPhase == kPhaseAll || kPhase == kPhaseFit;
+    constexpr bool kEval = kPhase == kPhaseAll || kPhase == kPhaseEvaluate;
     __shared__ double sx[257], sf[257];
     __shared__ BatchItem item;
     __shared__ int flag;
-    __shared__ union {
-        BackwardItemSmem bwd;
-        EvalSmem<S> eval;
-        GreeksEvalSmem greeks;
-    } sm;
+    __shared__ typename PhaseSmem<kPhase, S, kGreeks>::type sm;
     extern __shared__ __align__(16) unsigned char persistent_dyn[];
     PolicyRule* staged = reinterpret_cast<PolicyRule*>(persistent_dyn);
-    load_zig_tables(sx, sf);
+    if constexpr (kSim || kEval) load_zig_tables(sx, sf);
     const SmemZig zig = make_zig(sx, sf);
     for (;;) {
         __syncthreads();  // the previous item is done with the shared memory
@@ -858,30 +983,48 @@ __global__ void __launch_bounds__(kPersistentThreads, 3)
         const BatchItem it = item;
         if (it.kind == kItemNone) return;
         if (it.kind == kItemSimulate) {
-            simulate_item(a, it.index, it.first, it.count, zig);
-            signal_done(&q.sim_done[it.index], it.count);
-        } else if (it.kind == kItemBackward) {
-            const uint32_t gi = a.problems[it.index].group;
-            const uint32_t sim_blocks = blocks_of(a.groups[gi].plan.train_paths);
-            if (wait_for(&q.sim_done[gi], sim_blocks, q.timeout, &flag)) {
-                backward_item<D>(a, it.index, sm.bwd);
-                __syncthreads();
-                diagnose_problem(a, it.index);
+            if constexpr (kSim) {
+                simulate_item(a, it.index, it.first, it.count, zig);
+                signal_done(&q.sim_done[it.index], it.count);
             }
-            signal_done(&q.bwd_done[gi], 1u);
-        } else {
+        } else if (it.kind == kItemBackward) {
+            if constexpr (kFit) {
+                const uint32_t gi = a.problems[it.index].group;
+                const uint32_t sim_blocks = blocks_of(a.groups[gi].plan.train_paths);
+                // The fit kernel runs after the simulation kernel: its dependencies are met.
+                if (kPhase == kPhaseFit || wait_for(&q.sim_done[gi], sim_blocks, q.timeout, &flag)) {
+                    // Lone CTAs run a copy of the fit without the team exchanges (fewer live registers).
+                    const bool done =
+                        it.count == 1
+                            ? backward_item<D, kPhase == kPhaseFit, false>(a, it.index, 0, 1, q.timeout, &flag, sm.bwd)
+                            : backward_item<D, kPhase == kPhaseFit, true>(a, it.index, it.first, it.count, q.timeout,
+                                                                          &flag, sm.bwd);
+                    __syncthreads();
+                    if (done && it.first == 0) diagnose_problem(a, it.index);  // member 0 wrote the records
+                }
+                signal_done(&q.bwd_done[gi], 1u);
+            }
+        } else if constexpr (kEval) {
             const uint32_t gi = it.index;
             const BatchGroup& g = a.groups[gi];
-            if (wait_for(&q.bwd_done[gi], g.problems, q.timeout, &flag)) {
+            if (kPhase == kPhaseEvaluate || wait_for(&q.bwd_done[gi], g.fit_items, q.timeout, &flag)) {
                 if constexpr (kGreeks) {
                     unsigned* stops = reinterpret_cast<unsigned*>(staged + rule_rows);
-                    evaluate_greeks_item<D>(a, gi, it.first, it.count, it.chunk, zig, sm.greeks, staged, stops);
+                    evaluate_greeks_item<D, kPhase == kPhaseEvaluate>(a, gi, it.first, it.count, it.chunk, zig,
+                                                                      sm.greeks, staged, stops);
                 } else {
-                    evaluate_item<S, D>(a, gi, it.first, it.count, it.chunk, zig, sm.eval, staged, stage_rules != 0,
-                                        rule_rows);
+                    constexpr bool kRO = kPhase == kPhaseEvaluate;
+                    if (stage_rules)
+                        evaluate_item<S, D, true, kRO>(a, gi, it.first, it.count, it.chunk, zig, sm.eval, staged,
+                                                       rule_rows);
+                    else
+                        evaluate_item<S, D, false, kRO>(a, gi, it.first, it.count, it.chunk, zig, sm.eval, staged,
+                                                        rule_rows);
                 }
             }
-            // The item that completes the group's evaluation writes the group's summaries.
+            // The item that completes the group's evaluation writes the group's summaries (in the
+            // phase executor a summary kernel follows the evaluation kernel instead).
+            if constexpr (kPhase == kPhaseEvaluate) continue;
             const uint32_t chunks = kGreeks ? g.problems : (g.problems + S - 1) / S;
             const unsigned units = blocks_of(g.plan.eval_paths) * chunks;
             const unsigned before = signal_done(&q.eval_done[gi], it.count);
@@ -897,17 +1040,26 @@ __global__ void __launch_bounds__(kPersistentThreads, 3)
     }
 }
 
+// The phase executor's last kernel: every problem's summary, one warp per problem, once every
+// evaluation partial is written (the evaluation kernel has finished).
+__global__ void __launch_bounds__(kPersistentThreads) batch_summarize_kernel(BatchArgs a, BatchQueue, uint32_t, int) {
+    const uint32_t warps = kPersistentThreads / 32;
+    const uint32_t i = blockIdx.x * warps + (threadIdx.x >> 5);
+    if (i < a.n_problems) summarize_problem(a, i, int(threadIdx.x & 31));
+}
+
 // ---- launcher ---------------------------------------------------------------------------------------
 
 size_t persistent_rule_bytes(int strikes, bool greeks, uint32_t rule_rows) {
     return greeks ? (sizeof(PolicyRule) + sizeof(unsigned)) * rule_rows : sizeof(PolicyRule) * size_t(strikes) * rule_rows;
 }
 
-template <int S, bool kGreeks, int D>
-static cudaError_t launch_persistent_d(const BatchArgs& a, const BatchQueue& q, uint32_t rule_rows, bool stage,
-                                       int ctas_per_sm, cudaStream_t stream, int* grid_out) {
-    auto kernel = batch_persistent_kernel<S, kGreeks, D>;
-    const size_t smem = stage ? persistent_rule_bytes(S, kGreeks, rule_rows) : 0;
+template <int kPhase, int S, bool kGreeks, int D>
+static cudaError_t prepare_persistent_d(const BatchQueue& q, uint32_t rule_rows, bool stage, int ctas_per_sm,
+                                        PersistentLaunch* out) {
+    auto kernel = batch_persistent_kernel<kPhase, S, kGreeks, D>;
+    const bool rules = stage && (kPhase == kPhaseAll || kPhase == kPhaseEvaluate);
+    const size_t smem = rules ? persistent_rule_bytes(S, kGreeks, rule_rows) : 0;
     cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
     if (e != cudaSuccess) return e;
     int per_sm = 0;
@@ -915,37 +1067,76 @@ static cudaError_t launch_persistent_d(const BatchArgs& a, const BatchQueue& q, 
     if (e != cudaSuccess) return e;
     if (per_sm < 1) return cudaErrorInvalidConfiguration;
     int device = 0, sms = 0;
-    cudaGetDevice(&device);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
-    const int resident = (ctas_per_sm > 0 && ctas_per_sm < per_sm ? ctas_per_sm : per_sm) * sms;
-    const int grid = int(q.n_items) < resident ? int(q.n_items) : resident;
-    if (grid_out) *grid_out = grid;
-    if (grid <= 0) return cudaSuccess;
-    kernel<<<grid, kPersistentThreads, smem, stream>>>(a, q, rule_rows, stage ? 1 : 0);
-    return cudaGetLastError();
+    e = cudaGetDevice(&device);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+    if (e != cudaSuccess) return e;
+    const int cap = kPhase == kPhaseAll && ctas_per_sm > 0 && ctas_per_sm < per_sm ? ctas_per_sm : per_sm;
+    const int resident = cap * sms;
+    out->kernel = reinterpret_cast<const void*>(kernel);
+    out->grid = int(q.n_items) < resident ? int(q.n_items) : resident;
+    out->smem = smem;
+    return cudaSuccess;
 }
 
-template <int S, bool kGreeks>
-static cudaError_t launch_persistent_s(const BatchArgs& a, const BatchQueue& q, uint32_t rule_rows, bool stage,
-                                       int ctas_per_sm, cudaStream_t stream, int* grid_out) {
-    switch (a.degree) {  // validated to 0..4 on the host
-        case 0: return launch_persistent_d<S, kGreeks, 0>(a, q, rule_rows, stage, ctas_per_sm, stream, grid_out);
-        case 1: return launch_persistent_d<S, kGreeks, 1>(a, q, rule_rows, stage, ctas_per_sm, stream, grid_out);
-        case 2: return launch_persistent_d<S, kGreeks, 2>(a, q, rule_rows, stage, ctas_per_sm, stream, grid_out);
-        case 3: return launch_persistent_d<S, kGreeks, 3>(a, q, rule_rows, stage, ctas_per_sm, stream, grid_out);
-        default: return launch_persistent_d<S, kGreeks, 4>(a, q, rule_rows, stage, ctas_per_sm, stream, grid_out);
+template <int kPhase, int S, bool kGreeks>
+static cudaError_t prepare_persistent_s(int degree, const BatchQueue& q, uint32_t rule_rows, bool stage,
+                                        int ctas_per_sm, PersistentLaunch* out) {
+    switch (degree) {  // validated to 0..4 on the host
+        case 0: return prepare_persistent_d<kPhase, S, kGreeks, 0>(q, rule_rows, stage, ctas_per_sm, out);
+        case 1: return prepare_persistent_d<kPhase, S, kGreeks, 1>(q, rule_rows, stage, ctas_per_sm, out);
+        case 2: return prepare_persistent_d<kPhase, S, kGreeks, 2>(q, rule_rows, stage, ctas_per_sm, out);
+        case 3: return prepare_persistent_d<kPhase, S, kGreeks, 3>(q, rule_rows, stage, ctas_per_sm, out);
+        default: return prepare_persistent_d<kPhase, S, kGreeks, 4>(q, rule_rows, stage, ctas_per_sm, out);
     }
 }
 
-cudaError_t launch_batch_persistent(const BatchArgs& a, const BatchQueue& q, int strikes, uint32_t rule_rows,
-                                    bool stage, int ctas_per_sm, cudaStream_t stream, int* grid_out) {
-    if (a.greek_partials) return launch_persistent_s<1, true>(a, q, rule_rows, stage, ctas_per_sm, stream, grid_out);
-    switch (strikes) {
-        case 1: return launch_persistent_s<1, false>(a, q, rule_rows, stage, ctas_per_sm, stream, grid_out);
-        case 2: return launch_persistent_s<2, false>(a, q, rule_rows, stage, ctas_per_sm, stream, grid_out);
-        case 4: return launch_persistent_s<4, false>(a, q, rule_rows, stage, ctas_per_sm, stream, grid_out);
-        default: return launch_persistent_s<kEvalStrikes, false>(a, q, rule_rows, stage, ctas_per_sm, stream, grid_out);
+template <int kPhase>
+static cudaError_t prepare_phase(const BatchArgs& a, const BatchQueue& q, int strikes, uint32_t rule_rows, bool stage,
+                                 int ctas_per_sm, PersistentLaunch* out) {
+    *out = PersistentLaunch{};
+    if (a.greek_partials)
+        return prepare_persistent_s<kPhase, 1, true>(a.degree, q, rule_rows, stage, ctas_per_sm, out);
+    if constexpr (kPhase == kPhaseSimulate || kPhase == kPhaseFit) {
+        // No evaluation code: one instance serves every evaluation width.
+        return prepare_persistent_s<kPhase, 1, false>(a.degree, q, rule_rows, stage, ctas_per_sm, out);
+    } else {
+        switch (strikes) {
+            case 1: return prepare_persistent_s<kPhase, 1, false>(a.degree, q, rule_rows, stage, ctas_per_sm, out);
+            case 2: return prepare_persistent_s<kPhase, 2, false>(a.degree, q, rule_rows, stage, ctas_per_sm, out);
+            case 4: return prepare_persistent_s<kPhase, 4, false>(a.degree, q, rule_rows, stage, ctas_per_sm, out);
+            default:
+                return prepare_persistent_s<kPhase, kEvalStrikes, false>(a.degree, q, rule_rows, stage, ctas_per_sm,
+                                                                         out);
+        }
     }
+}
+
+cudaError_t prepare_batch_persistent(const BatchArgs& a, const BatchQueue& q, int strikes, uint32_t rule_rows,
+                                     bool stage, int ctas_per_sm, PersistentLaunch* out) {
+    return prepare_phase<kPhaseAll>(a, q, strikes, rule_rows, stage, ctas_per_sm, out);
+}
+
+cudaError_t prepare_batch_phases(const BatchArgs& a, const BatchQueue (&q)[3], int strikes, uint32_t rule_rows,
+                                 bool stage, PersistentLaunch (&out)[4]) {
+    cudaError_t e = prepare_phase<kPhaseSimulate>(a, q[0], strikes, rule_rows, stage, 0, &out[0]);
+    if (e == cudaSuccess) e = prepare_phase<kPhaseFit>(a, q[1], strikes, rule_rows, stage, 0, &out[1]);
+    if (e == cudaSuccess) e = prepare_phase<kPhaseEvaluate>(a, q[2], strikes, rule_rows, stage, 0, &out[2]);
+    const uint32_t warps = kPersistentThreads / 32;
+    out[3] = PersistentLaunch{reinterpret_cast<const void*>(batch_summarize_kernel), 0,
+                              int((a.n_problems + warps - 1) / warps), 0};
+    return e;
+}
+
+cudaError_t enqueue_batch_persistent(const PersistentLaunch& launch, const BatchArgs& a, const BatchQueue& q,
+                                     uint32_t rule_rows, bool stage, cudaStream_t stream) {
+    if (launch.grid <= 0) return cudaSuccess;
+    BatchArgs args = a;
+    BatchQueue queue = q;
+    uint32_t rows = rule_rows;
+    int stage_rules = stage ? 1 : 0;
+    void* params[4] = {&args, &queue, &rows, &stage_rules};
+    return cudaLaunchKernel(launch.kernel, dim3(unsigned(launch.grid)), dim3(kPersistentThreads), params, launch.smem,
+                            stream);
 }
 
 }  // namespace fo

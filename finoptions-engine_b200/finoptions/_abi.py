@@ -232,12 +232,13 @@ class FoGbmSeededRequest(ctypes.Structure):
 
 class FoBatchTuning(ctypes.Structure):
     _fields_ = [("sim_blocks", ctypes.c_int32), ("eval_blocks", ctypes.c_int32), ("strikes", ctypes.c_int32),
-                ("ctas_per_sm", ctypes.c_int32)]
+                ("ctas_per_sm", ctypes.c_int32), ("phases", ctypes.c_int32)]
 
 
 class FoBatchLaunchInfo(ctypes.Structure):
     _fields_ = [("tuning", FoBatchTuning), ("source", ctypes.c_int32), ("grid", ctypes.c_int32),
-                ("items", ctypes.c_uint64), ("tuning_launches", ctypes.c_uint64)]
+                ("items", ctypes.c_uint64), ("tuning_launches", ctypes.c_uint64), ("graph_replays", ctypes.c_uint64),
+                ("graph_captures", ctypes.c_uint64)]
 
 
 PACKAGE_ROOT: Final = Path(__file__).resolve().parent

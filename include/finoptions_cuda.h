@@ -491,10 +491,12 @@ int fo_price_lsm_ragged_f64(fo_executor* executor, const fo_lsm_ragged_request* 
                             fo_batch_result_columns* out, fo_ragged_greeks_columns* greeks, fo_error* err);
 
 /* Device time of the executor's last grouped / row / ragged batch call (no counterpart in the
- * reference; a measurement hook). A batch runs as one persistent launch per wave (a wave: the groups
- * that fit the device memory budget together): kernel_ms[0] receives the milliseconds of those
- * launches summed over the call's waves and kernel_ms[1..] zero; *launches receives the number of
- * launches. Timed with CUDA events on the executor's stream. */
+ * reference; a measurement hook). A batch runs as one captured graph per wave (a wave: the groups
+ * that fit the device memory budget together) holding either one persistent launch or the three
+ * phase kernels (fo_batch_tuning.phases): kernel_ms[0] receives the milliseconds of the wave's
+ * launches summed over the call's waves; with the phase kernels kernel_ms[1..3] receive the
+ * simulation, fit and evaluation kernels' shares (zero otherwise); *launches receives the number
+ * of waves. Timed with CUDA events recorded by the graph on the executor's stream. */
 #define FO_BATCH_KERNELS 5
 int fo_executor_batch_kernel_ms(fo_executor* executor, double* kernel_ms, uint64_t capacity, uint64_t* launches);
 /* Host->device and device->host bytes the executor's last batch call copied. */
@@ -509,6 +511,8 @@ typedef struct fo_batch_tuning {
     int32_t eval_blocks;  /* evaluation blocks (256 paths each) per work item, 1..64              */
     int32_t strikes;      /* strikes an evaluation item applies together: 1, 2, 4 or 8            */
     int32_t ctas_per_sm;  /* resident CTAs per SM, 0..8 (0: as many as the registers allow)       */
+    int32_t phases;       /* 0: one persistent launch drains every item; 1: three kernels, one per */
+                          /* item kind (simulation, fits, evaluation), each with its own occupancy */
 } fo_batch_tuning;
 
 /* autotune != 0 (the default): the executor picks the shape per class of wave (path counts, rows,
@@ -523,6 +527,8 @@ typedef struct fo_batch_launch_info {
     int32_t grid;              /* CTAs launched                                            */
     uint64_t items;            /* work items of the last launch                            */
     uint64_t tuning_launches;  /* launches the tuner timed (source 2)                      */
+    uint64_t graph_replays;    /* waves of the last call replayed from the captured graph  */
+    uint64_t graph_captures;   /* waves of the last call captured (a new launch key)       */
 } fo_batch_launch_info;
 int fo_executor_batch_launch(fo_executor* executor, fo_batch_launch_info* out);
 

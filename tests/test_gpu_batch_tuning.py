@@ -21,7 +21,10 @@ from test_gpu_batch import assert_columns, gpu_batch
 
 pytestmark = pytest.mark.gpu
 
-SHAPES = [(2, 1, 8, 0), (1, 1, 8, 0), (8, 4, 8, 0), (2, 2, 4, 0), (2, 1, 2, 2), (1, 4, 1, 1)]
+# (simulation blocks per item, evaluation blocks per item, strikes per evaluation item, CTAs per SM,
+# phases): one persistent launch (phases 0) or three phase kernels (phases 1).
+SHAPES = [(2, 1, 8, 0, 0), (1, 1, 8, 0, 0), (8, 4, 8, 0, 0), (2, 2, 4, 0, 0), (2, 1, 2, 2, 0), (1, 4, 1, 1, 0),
+          (2, 1, 8, 0, 1), (4, 2, 4, 0, 1)]
 
 
 def set_shape(native_executor, shape) -> None:
@@ -77,7 +80,7 @@ def test_every_launch_shape_prices_a_grouped_batch_identically(native_executor, 
         assert status == 0, err.message
         info = launch_info(native_executor)
         assert info.source == 0 and info.tuning.sim_blocks == shape[0] and info.tuning.eval_blocks == shape[1]
-        assert info.tuning.strikes == shape[2] and info.grid > 0 and info.items > 0
+        assert info.tuning.strikes == shape[2] and info.tuning.phases == shape[4] and info.grid > 0 and info.items > 0
         results.append(out)
     for out in results[1:]:
         for got, want in zip(out, results[0], strict=True):
@@ -86,7 +89,8 @@ def test_every_launch_shape_prices_a_grouped_batch_identically(native_executor, 
 
 
 def test_every_launch_shape_gives_the_same_ragged_greeks(native_executor, fixed_shapes) -> None:
-    c = ragged_columns(9, seed=73, min_paths=1500, max_paths=9000, min_exercise=4, max_exercise=24)
+    # Up to 120,000 paths: the larger rows are fitted by teams of up to four CTAs.
+    c = ragged_columns(9, seed=73, min_paths=1500, max_paths=120_000, min_exercise=4, max_exercise=24)
     results = []
     for shape in SHAPES:
         set_shape(native_executor, shape)
@@ -118,9 +122,31 @@ def test_the_autotuner_tunes_a_class_once_and_reuses_its_shape(native_executor) 
 
 
 def test_launch_shapes_outside_their_range_are_rejected(native_executor, fixed_shapes) -> None:
-    for shape in ((0, 1, 8, 0), (2, 65, 8, 0), (2, 1, 3, 0), (2, 1, 8, 9)):
+    for shape in ((0, 1, 8, 0, 0), (2, 65, 8, 0, 0), (2, 1, 3, 0, 0), (2, 1, 8, 9, 0), (2, 1, 8, 0, 2)):
         tuning = _abi.FoBatchTuning(*shape)
         err = _abi.FoError()
         assert _abi.load().fo_executor_set_batch_tuning(native_executor.raw, 0, ctypes.byref(tuning),
                                                         ctypes.byref(err)) == _abi.FO_ERR_EXECUTION
         assert "outside its range" in err.message.decode()
+
+
+def test_a_repeated_wave_replays_its_captured_graph(native_executor, fixed_shapes) -> None:
+    """A wave is captured as a CUDA graph once per launch key; the same request again replays it, and
+    a different request captures anew. Replays give the same columns."""
+    set_shape(native_executor, (2, 1, 8, 0, 1))
+    c = grouped_columns(7, 8, seed=83, min_exercise=5, max_exercise=11)
+    req = grouped_request(c, 3000)
+    outs = []
+    for expected in ((0, 1), (1, 0), (1, 0)):
+        status, err, out = gpu_batch(native_executor, req)
+        assert status == 0, err.message
+        info = launch_info(native_executor)
+        assert (info.graph_replays, info.graph_captures) == expected
+        outs.append(out)
+    for out in outs[1:]:
+        for got, want in zip(out, outs[0], strict=True):
+            np.testing.assert_array_equal(got, want)
+    status, err, _ = gpu_batch(native_executor, grouped_request(c, 3001))
+    assert status == 0, err.message
+    assert (launch_info(native_executor).graph_replays, launch_info(native_executor).graph_captures) == (0, 1)
+    assert_columns(outs[0], _oracle.price_lsm_grouped(req, 16))
