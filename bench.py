@@ -487,6 +487,7 @@ def run_ragged(args: argparse.Namespace, executor) -> dict:
                      "kernels_ms": batch_kernel_ms(kernel_ms, calls),
                      "gpu_launches_per_call": int(launches.value), "launch_shape": batch_launch(lib, executor)}
     out["greeks_overhead"] = out["price_and_greeks"]["device_ms_per_call"] / out["plain"]["device_ms_per_call"]
+    out["executors_ms_per_call"] = {"price_and_greeks": executor_times(lib, executor, call)}  # the last call() defined
     # The north-star comparison: the same contracts (same populations, so the same price and SE)
     # priced one by one on the plain per-contract path, against the batched price + Greeks call.
     import finoptions as fo
@@ -622,6 +623,36 @@ def batch_kernel_ms(kernel_ms: list, calls: int) -> dict:
     return out
 
 
+def executor_times(lib, executor, call, repeats: int = 2) -> dict:
+    """Device milliseconds per call of the batch under each executor, with the autotuner's other
+    choices kept (the persistent launch at as many CTAs per SM as fit); the autotuner is restored
+    afterwards. The results are the same bit for bit under both."""
+    from finoptions import _abi
+
+    info = _abi.FoBatchLaunchInfo()
+    lib.fo_executor_batch_launch(executor.raw, ctypes.byref(info))
+    chosen = info.tuning
+    ms = (ctypes.c_double * 5)()
+    n = ctypes.c_uint64()
+    err = _abi.FoError()
+    out = {}
+    try:
+        for phases, name in ((0, "one_persistent_launch"), (1, "phase_kernels")):
+            shape = _abi.FoBatchTuning(chosen.sim_blocks, chosen.eval_blocks, chosen.strikes, 0, phases)
+            if lib.fo_executor_set_batch_tuning(executor.raw, 0, ctypes.byref(shape), ctypes.byref(err)):
+                raise RuntimeError(err.message.decode())
+            call()  # captures the graph of this shape
+            total = 0.0
+            for _ in range(repeats):
+                call()
+                lib.fo_executor_batch_kernel_ms(executor.raw, ms, 5, ctypes.byref(n))
+                total += ms[0]
+            out[name] = round(total / repeats, 2)
+    finally:
+        lib.fo_executor_set_batch_tuning(executor.raw, 1, None, ctypes.byref(err))
+    return out
+
+
 def batch_launch(lib, executor) -> dict:
     """The launch shape the executor used for its last batch call (autotuned per shape class)."""
     from finoptions import _abi
@@ -685,6 +716,8 @@ def run_grouped(args: argparse.Namespace, executor) -> dict:
     kernels = {"batch_persistent_kernel": {"ms_per_call": round(device_ms, 4), "share": 1.0,
                                            "algorithmic_bytes": launch_bytes,
                                            "achieved_gbs": round(launch_bytes / (device_ms / 1e3) / 1e9, 1)}}
+    shape = batch_launch(lib, executor)
+    executors = executor_times(lib, executor, call)
     dominant = "batch_persistent_kernel"
     achieved = launch_bytes / (device_ms / 1e3) / 1e9
     bound = "hbm (fits) + issue (simulation, evaluation)"
@@ -735,7 +768,8 @@ def run_grouped(args: argparse.Namespace, executor) -> dict:
                 "ms_per_call": wall / steps * 1e3, "h2d_bytes_per_step": int(h2d.value),
                 "d2h_bytes_per_step": int(d2h.value), "api": "fo_price_lsm_grouped_f64 (host columns in and out)"},
         "gpu_launches": launches,
-        "launch_shape": batch_launch(lib, executor),
+        "launch_shape": shape,
+        "executors_ms_per_call": executors,
         "kernels": kernels,
         "roofline": {"kernel": dominant, "bound": bound,
                      "achieved": round(achieved, 1), "peak": hbm_peak, "peak_source": peak_kind, "unit": "GB/s",

@@ -18,7 +18,7 @@ struct BatchTuning {
     int eval_blocks = 1;  // evaluation blocks of 256 paths per work item
     int strikes = 8;      // strikes an evaluation item applies together (1, 2, 4 or 8)
     int ctas_per_sm = 0;  // resident CTAs per SM of the persistent launch (0: as many as fit)
-    int phases = 0;       // 1: run the items as three kernels of one kind each instead of one launch
+    int phases = 0;       // 1: one kernel per item kind and a summary kernel instead of one launch
 };
 
 // Shared memory of the staged fitted rules: `strikes` x rule_rows PolicyRules, or with the Greeks

@@ -1139,7 +1139,7 @@ std::string tuning_key(const Work& work, const WaveT& w, bool greeks, int degree
 }
 
 // The autotuner: a coordinate search from the default launch shape over the executor (one persistent
-// launch or three phase kernels), the evaluation blocks per item, the simulation blocks per item,
+// launch or the phase kernels), the evaluation blocks per item, the simulation blocks per item,
 // the strikes per evaluation item and the CTAs per SM, each candidate timed by one launch of the
 // wave; a change is kept when it is at least 1% faster.
 template <typename Run>
@@ -1161,7 +1161,7 @@ Error autotune_wave(Run& run, bool greeks, int max_strikes, BatchTuning* best, u
         return Error{};
     };
     {
-        BatchTuning c = cur;  // the three phase kernels instead of one persistent launch
+        BatchTuning c = cur;  // the phase kernels instead of one persistent launch
         c.phases = 1;
         if (!(e = attempt(c)).ok()) return e;
     }

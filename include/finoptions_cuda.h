@@ -492,10 +492,10 @@ int fo_price_lsm_ragged_f64(fo_executor* executor, const fo_lsm_ragged_request* 
 
 /* Device time of the executor's last grouped / row / ragged batch call (no counterpart in the
  * reference; a measurement hook). A batch runs as one captured graph per wave (a wave: the groups
- * that fit the device memory budget together) holding either one persistent launch or the three
- * phase kernels (fo_batch_tuning.phases): kernel_ms[0] receives the milliseconds of the wave's
- * launches summed over the call's waves; with the phase kernels kernel_ms[1..3] receive the
- * simulation, fit and evaluation kernels' shares (zero otherwise); *launches receives the number
+ * that fit the device memory budget together) holding either one persistent launch or the phase
+ * kernels (fo_batch_tuning.phases): kernel_ms[0] receives the milliseconds of the wave's launches
+ * summed over the call's waves; with the phase kernels kernel_ms[1..3] receive the simulation, fit
+ * and evaluation (with the summary) kernels' shares (zero otherwise); *launches receives the number
  * of waves. Timed with CUDA events recorded by the graph on the executor's stream. */
 #define FO_BATCH_KERNELS 5
 int fo_executor_batch_kernel_ms(fo_executor* executor, double* kernel_ms, uint64_t capacity, uint64_t* launches);
@@ -511,8 +511,9 @@ typedef struct fo_batch_tuning {
     int32_t eval_blocks;  /* evaluation blocks (256 paths each) per work item, 1..64              */
     int32_t strikes;      /* strikes an evaluation item applies together: 1, 2, 4 or 8            */
     int32_t ctas_per_sm;  /* resident CTAs per SM, 0..8 (0: as many as the registers allow)       */
-    int32_t phases;       /* 0: one persistent launch drains every item; 1: three kernels, one per */
-                          /* item kind (simulation, fits, evaluation), each with its own occupancy */
+    int32_t phases;       /* 0: one persistent launch drains every item; 1: one kernel per item    */
+                          /* kind (simulation, fits, evaluation) and a summary kernel, each with  */
+                          /* its own occupancy                                                    */
 } fo_batch_tuning;
 
 /* autotune != 0 (the default): the executor picks the shape per class of wave (path counts, rows,

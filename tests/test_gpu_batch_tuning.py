@@ -22,7 +22,7 @@ from test_gpu_batch import assert_columns, gpu_batch
 pytestmark = pytest.mark.gpu
 
 # (simulation blocks per item, evaluation blocks per item, strikes per evaluation item, CTAs per SM,
-# phases): one persistent launch (phases 0) or three phase kernels (phases 1).
+# phases): one persistent launch (phases 0) or the phase kernels (phases 1).
 SHAPES = [(2, 1, 8, 0, 0), (1, 1, 8, 0, 0), (8, 4, 8, 0, 0), (2, 2, 4, 0, 0), (2, 1, 2, 2, 0), (1, 4, 1, 1, 0),
           (2, 1, 8, 0, 1), (4, 2, 4, 0, 1)]
 
