@@ -613,6 +613,19 @@ def grouped_algorithmic_bytes(c, paths: int) -> dict:
     }
 
 
+def fit_traffic(kernel: str, algorithmic: dict) -> int | None:
+    """DRAM bytes of the batch fit kernel per call: the committed ncu capture's DRAM bytes per
+    algorithmic byte (profiles/traffic.json, taken at 128 states) times this call's algorithmic
+    bytes, since both grow with the states priced."""
+    path = ROOT / "profiles" / "traffic.json"
+    if kernel != "batch_fit_kernel" or not path.is_file():
+        return None
+    entry = json.loads(path.read_text()).get("batch_fit_kernel")
+    if entry is None:
+        return None
+    return int(float(entry["dram_bytes_per_algorithmic_byte"]) * algorithmic["batch_backward_kernel"])
+
+
 def batch_kernel_ms(kernel_ms: list, calls: int) -> dict:
     """Per-call device milliseconds of a batch call's graph, split into the phase kernels when the
     executor ran them (fo_executor_batch_kernel_ms slots 1..3)."""
@@ -773,7 +786,7 @@ def run_grouped(args: argparse.Namespace, executor) -> dict:
         "kernels": kernels,
         "roofline": {"kernel": dominant, "bound": bound,
                      "achieved": round(achieved, 1), "peak": hbm_peak, "peak_source": peak_kind, "unit": "GB/s",
-                     "frac": round(achieved / hbm_peak, 4), "traffic": None},
+                     "frac": round(achieved / hbm_peak, 4), "traffic": fit_traffic(dominant, algorithmic)},
         "clocks": clocks.report(),
         "plain_per_contract": plain,
         "batched_vs_plain_same_contracts": {
