@@ -419,6 +419,10 @@ def run_ours(args: argparse.Namespace) -> dict | None:
     }
     if world == 1:
         out["cpu_baseline"] = cpu_baseline(paths)
+    else:
+        # The batch, Greeks and ragged sections are single-GPU measurements, reported at N = 1;
+        # the other ranks have left, so the multi-GPU line carries the replicated contract only.
+        args.skip_batched = args.skip_greeks = args.skip_ragged = True
     if not args.skip_batched:
         out["batched"] = run_grouped(args, executor)
     if not args.skip_greeks:
