@@ -845,6 +845,31 @@ FO_HD bool predict_continuation_d(const Model& m, double predictor, double* out)
     return true;
 }
 
+#ifdef __CUDACC__
+// predict_continuation_d for a model in shared memory that the pass reads at every path: the same
+// operations in the same order, with the fields read through a volatile reference so the compiler
+// loads them per path (broadcast shared-memory loads) instead of holding the 14 of them in
+// registers across the pass; the registers go to resident CTAs instead.
+template <int D>
+__device__ __forceinline__ bool predict_continuation_shared(const FitModel* model, double predictor, double* out) {
+    const volatile FitModel& m = *model;
+    if (!fo_isfinite(predictor)) return false;
+    const double z = D == 0 ? 0.0 : divide(predictor - m.mean, Divisor{m.scale, m.inv_scale});
+    double prediction = m.coef[0];
+    double previous = 0.0, current = 1.0;
+#pragma unroll
+    for (int j = 0; j < D; ++j) {
+        const double next = fo_fma(z - m.alpha[j], current, -m.beta[j] * previous);
+        prediction = fo_fma(m.coef[j + 1], next, prediction);
+        previous = current;
+        current = next;
+    }
+    if (!fo_isfinite(prediction)) return false;
+    *out = prediction;
+    return true;
+}
+#endif
+
 // ----------------------------------------------------------------------------------------------
 // Rank and two-norm condition diagnostic: one-sided Jacobi SVD of the <= 5x5 upper-triangular
 // transform from monomials to the orthonormal basis (regression.rs:540-577, 711-850).

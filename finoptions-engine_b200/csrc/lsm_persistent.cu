@@ -34,6 +34,10 @@ namespace {
 
 constexpr int kPersistentThreads = 256;
 constexpr int kPersistentLoads = 2;  // paths a backward thread loads together
+// The fit kernel of the phase executor runs four CTAs per SM (64 registers a thread): a thread loads
+// one path at a time and reads the row's model from shared memory per path. Resident warps hide the
+// latency better there than paths in flight per thread (measured on the grouped batch).
+constexpr int kFitKernelLoads = 1;
 // A dependency wait gives up after this long: one problem's fit on one CTA can take seconds for
 // populations of millions of paths, so the limit is well above any fit's duration.
 constexpr unsigned long long kDependencyTimeoutNs = 20000000000ull;
@@ -191,7 +195,9 @@ struct BackwardItemSmem {
 // is split over a team of CTAs (this one is member `member` of `members`), each owning a contiguous
 // range of paths, whose CTA sums are exchanged in member order before every decision, so that every
 // member fits the same model; member 0 writes the records. Thread t owns paths lo + t + m * 256
-// (m = 0, 1, ...), loading kPersistentLoads of them together. False when a team exchange gave up.
+// (m = 0, 1, ...), loading kPersistentLoads of them together (kFitKernelLoads in the fit kernel).
+// The order of a thread's paths, and so every sum, does not depend on that count. False when a team
+// exchange gave up.
 // A stored training state. The persistent launch reads rows that other CTAs of the same launch wrote,
 // so through L2 (the SM's L1 is not coherent with other SMs' writes); the fit kernel of the phase
 // executor runs after the simulation kernel has finished, so its reads may use the read-only path.
@@ -204,7 +210,7 @@ __device__ __forceinline__ double load_slab(const double* p) {
 template <int D, bool kReadOnlySlab, bool kTeam>
 __device__ bool backward_item(const BatchArgs& a, uint32_t pi, uint32_t member, uint32_t members, unsigned* timeout,
                               int* flag, BackwardItemSmem& sm) {
-    constexpr int kL = kPersistentLoads;
+    constexpr int kL = kReadOnlySlab ? kFitKernelLoads : kPersistentLoads;
     const BatchProblem pr = a.problems[pi];
     if (pr.skip_fit) return true;
     if (status_failed(&a.group_status[pr.group].train_sim_fail)) return true;
@@ -412,7 +418,7 @@ __device__ bool backward_item(const BatchArgs& a, uint32_t pi, uint32_t member, 
                 if (regression && sc[u] > K) {
                     const double intrinsic = sc[u] - K;
                     double continuation;
-                    if (!predict_continuation_d<D>(sm.model, divide(sc[u], Kd), &continuation)) {
+                    if (!predict_continuation_shared<D>(&sm.model, divide(sc[u], Kd), &continuation)) {
                         atomicMin(&st->fit_predict_fail, ((unsigned long long)order << 32) | p);
                     } else if (exercise_rule(a.tie_rule, intrinsic, continuation)) {
                         v[u] = intrinsic;
@@ -947,9 +953,10 @@ struct PhaseSmem<3, S, true> {
 template <int kPhase, int S, bool kGreeks>
 struct PhaseOccupancy {
     // Resident CTAs per SM the register budget is cut for.
-    static constexpr int value = kPhase == kPhaseSimulate ? 6
-                                 : kPhase == kPhaseEvaluate && (S == 1 || kGreeks) ? 4
-                                                                                   : 3;
+    static constexpr int value = kPhase == kPhaseSimulate                              ? 6
+                                 : kPhase == kPhaseFit                                   ? 4
+                                 : kPhase == kPhaseEvaluate && (S == 1 || kGreeks)       ? 4
+                                                                                         : 3;
 };
 
 // S: strikes an evaluation item applies together (kGreeks: one, with the adjoint). The dynamic
