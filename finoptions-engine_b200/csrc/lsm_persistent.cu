@@ -595,7 +595,9 @@ __device__ void evaluate_item(const BatchArgs& a, uint32_t gi, uint32_t first, u
                 active = 0u;
                 return;
             }
-#pragma unroll 2
+            // Four strikes per unrolled step (measured on the grouped batch: 185 ms for the
+            // evaluation phase against 194 unrolled by two, 209 by one and 204 fully).
+#pragma unroll 4
             for (int k = 0; k < S; ++k) {
                 if (!((active >> k) & 1u)) continue;
                 const double K = sm.strikes[k];
