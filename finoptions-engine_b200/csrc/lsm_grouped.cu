@@ -1415,8 +1415,14 @@ Error price_groups(fo_executor* ex, const BatchMethod& m, const std::vector<Grou
                                   "adjoint Greeks of a batch hold at most " +
                                       u(kPersistentRuleSmemBytes / (sizeof(PolicyRule) + 4)) +
                                       " observation rows per contract; observed " + u(max_rows));
-            std::vector<BatchItem> items;
-            items.reserve(w.item_bound);
+            // The items are written straight into their region of the pinned staging buffer, which
+            // the wave layout sizes for the finest cut (w.item_bound): no per-call allocation or copy.
+            BatchItem* const staged_items = reinterpret_cast<BatchItem*>(host + (L.items - in_bytes));
+            uint64_t n_items = 0;
+            auto push_item = [&](const BatchItem& it) {
+                if (n_items < w.item_bound) staged_items[n_items] = it;
+                ++n_items;
+            };
             uint32_t phase_items[3] = {0, 0, 0};  // simulation, fit, evaluation items (phase order only)
             {
                 const uint32_t sim_step = uint32_t(std::max(1, tune.sim_blocks));
@@ -1454,7 +1460,7 @@ Error price_groups(fo_executor* ex, const BatchMethod& m, const std::vector<Grou
                 uint64_t queued_fits = 0;
                 auto queue_fit = [&](uint32_t i) {
                     for (uint32_t m = 0; m < hpb[i].members; ++m)
-                        items.push_back(BatchItem{kItemBackward, i, m, hpb[i].members, 0, {0, 0, 0}});
+                        push_item(BatchItem{kItemBackward, i, m, hpb[i].members, 0, {0, 0, 0}});
                     last_fit[hpb[i].group] = queued_fits++;
                 };
                 // The phase kernels take the items kind by kind: every simulation, then every fit
@@ -1462,17 +1468,17 @@ Error price_groups(fo_executor* ex, const BatchMethod& m, const std::vector<Grou
                 for (const uint32_t gl : gorder) {
                     const uint32_t blocks = eval_blocks_for(work[w.g0 + gl].hp.train_paths);
                     for (uint32_t b = 0; b < blocks; b += sim_step)
-                        items.push_back(BatchItem{kItemSimulate, gl, b, std::min(sim_step, blocks - b), 0, {0, 0, 0}});
+                        push_item(BatchItem{kItemSimulate, gl, b, std::min(sim_step, blocks - b), 0, {0, 0, 0}});
                     if (!tune.phases)
                         for (const uint32_t i : early[gl]) queue_fit(i);
                 }
-                phase_items[0] = uint32_t(items.size());
+                phase_items[0] = uint32_t(n_items);
                 if (tune.phases) {
                     for (const auto& f : fits) queue_fit(f.second);
                 } else {
                     for (const uint32_t i : late) queue_fit(i);
                 }
-                phase_items[1] = uint32_t(items.size()) - phase_items[0];
+                phase_items[1] = uint32_t(n_items) - phase_items[0];
                 std::vector<uint32_t> eorder(G);
                 std::iota(eorder.begin(), eorder.end(), 0u);
                 std::stable_sort(eorder.begin(), eorder.end(),
@@ -1482,14 +1488,16 @@ Error price_groups(fo_executor* ex, const BatchMethod& m, const std::vector<Grou
                     const uint32_t chunks = greeks ? hg[gl].problems : (hg[gl].problems + eval_strikes - 1) / eval_strikes;
                     for (uint32_t z = 0; z < chunks; ++z)
                         for (uint32_t b = 0; b < blocks; b += eval_step)
-                            items.push_back(BatchItem{kItemEvaluate, gl, b, std::min(eval_step, blocks - b), z, {0, 0, 0}});
+                            push_item(BatchItem{kItemEvaluate, gl, b, std::min(eval_step, blocks - b), z, {0, 0, 0}});
                 }
-                phase_items[2] = uint32_t(items.size()) - phase_items[0] - phase_items[1];
-                std::memcpy(host + (L.items - in_bytes), items.data(), sizeof(BatchItem) * items.size());
+                phase_items[2] = uint32_t(n_items) - phase_items[0] - phase_items[1];
             }
+            if (n_items > w.item_bound)
+                return make_error(FO_ERR_EXECUTION, FO_CODE_INVALID_ARGUMENT,
+                                  "batch work queue of " + u(n_items) + " items exceeds its bound of " + u(w.item_bound));
             // The group and problem tables and the queue's items (the item region is sized for the
             // finest cut; only the items of this launch shape travel).
-            const size_t table_bytes = (L.items - L.groups) + sizeof(BatchItem) * items.size();
+            const size_t table_bytes = (L.items - L.groups) + sizeof(BatchItem) * n_items;
             BatchArgs a{};
             a.groups = reinterpret_cast<const BatchGroup*>(dev + L.groups);
             a.problems = reinterpret_cast<const BatchProblem*>(dev + L.problems);
@@ -1519,7 +1527,7 @@ Error price_groups(fo_executor* ex, const BatchMethod& m, const std::vector<Grou
             unsigned* counters = reinterpret_cast<unsigned*>(dev + L.counters);
             BatchQueue q{};
             q.items = reinterpret_cast<const BatchItem*>(dev + L.items);
-            q.n_items = uint32_t(items.size());
+            q.n_items = uint32_t(n_items);
             q.next = counters;
             q.timeout = counters + 1;
             q.sim_done = counters + 5;
@@ -1611,7 +1619,7 @@ Error price_groups(fo_executor* ex, const BatchMethod& m, const std::vector<Grou
             ex->batch_launches += 1;
             ex->batch_grid = grid;
             ex->batch_strikes = eval_strikes;
-            ex->batch_items = items.size();
+            ex->batch_items = n_items;
             ex->batch_d2h += L.out_bytes + sizeof(unsigned);
             FO_CUDA_TRY(cudaStreamSynchronize(s), "batch pricing");
             FO_CUDA_TRY(cudaEventElapsedTime(launch_ms, mark[0], mark[n_launches]), "event");
