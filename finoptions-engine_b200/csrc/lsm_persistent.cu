@@ -401,16 +401,32 @@ __device__ bool backward_item(const BatchArgs& a, uint32_t pi, uint32_t member, 
         const double* nxt = stage_next ? row_ptr(uint32_t(row - 1)) : cur;
 #pragma unroll
         for (int k = 0; k < kSlots; ++k) sums.acc[k] = 0.0;
+        // The fit kernel fetches the next step's value and spots before the current step's
+        // arithmetic, so their latency overlaps it (one path per thread and step); the persistent
+        // launch, at two paths per step and the heaviest kind's register budget, fetches in place.
+        constexpr bool kAhead = kReadOnlySlab;
+        double fv[kL], fsc[kL], fsn[kL];
+        auto fetch = [&](uint64_t at) {
+#pragma unroll
+            for (int u = 0; u < kL; ++u) {
+                const uint64_t p = at + uint64_t(u) * T;
+                const bool in = p < hi;
+                fv[u] = in ? values[p] : 0.0;
+                fsc[u] = in && regression ? load_slab<kReadOnlySlab>(&cur[p]) : 0.0;
+                fsn[u] = in && stage_next ? load_slab<kReadOnlySlab>(&nxt[p]) : 0.0;
+            }
+        };
+        if constexpr (kAhead) fetch(first);
         for (uint64_t base = first; base < hi; base += step) {
+            if constexpr (!kAhead) fetch(base);
             double v[kL], sc[kL], sn[kL];
 #pragma unroll
             for (int u = 0; u < kL; ++u) {
-                const uint64_t p = base + uint64_t(u) * T;
-                const bool in = p < hi;
-                v[u] = in ? values[p] : 0.0;
-                sc[u] = in && regression ? load_slab<kReadOnlySlab>(&cur[p]) : 0.0;
-                sn[u] = in && stage_next ? load_slab<kReadOnlySlab>(&nxt[p]) : 0.0;
+                v[u] = fv[u];
+                sc[u] = fsc[u];
+                sn[u] = fsn[u];
             }
+            if constexpr (kAhead) fetch(base + step);
 #pragma unroll
             for (int u = 0; u < kL; ++u) {
                 const uint64_t p = base + uint64_t(u) * T;
